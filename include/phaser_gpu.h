@@ -1,0 +1,188 @@
+/*
+ * phaser_gpu.h -- C ABI of the B200 (sm_100a) implementation of PHASER's
+ * correspondence-free registration hot path.
+ *
+ * Every entry point returns PHGPU_OK (0) or a negative status; no exception or
+ * abort crosses the ABI.  A context owns one CUDA stream pair and all device
+ * buffers for one (bandwidth, voxel grid) configuration; a context is not
+ * thread-safe, distinct contexts may be used concurrently.  Array arguments
+ * are host pointers unless the phgpu_cloud says otherwise.
+ *
+ * Each function names the reference interface it replaces (paths relative to
+ * the ethz-asl/phaser tree).
+ */
+#ifndef PHASER_GPU_H_
+#define PHASER_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHGPU_OK 0
+#define PHGPU_ERR_INVALID (-1)   /* bad argument or unsupported configuration */
+#define PHGPU_ERR_CUDA (-2)      /* CUDA runtime error (message in phgpu_last_error) */
+#define PHGPU_ERR_MEMORY (-3)    /* device allocation failed */
+#define PHGPU_ERR_STATE (-4)     /* call out of order (e.g. result before correlate) */
+
+/* fusion modes */
+#define PHGPU_FUSION_LAPLACE 0   /* SphericalCorrelationLaplace / SpatialCorrelationLaplace */
+#define PHGPU_FUSION_NONE 1      /* SphericalCorrelation / SpatialCorrelation (channel 0) */
+
+/* flags */
+#define PHGPU_FLAG_KEEP_VOLUMES 1u /* also keep the full correlation volumes */
+
+/* Configuration; names and defaults follow the reference's gflags
+ * (phaser_common/src/common/core-gflags.cc:6-40,
+ *  phaser_common/src/model/point-cloud.cc:19-20). */
+typedef struct {
+  uint32_t spherical_bandwidth;      /* phaser_core_spherical_bandwidth (75) */
+  uint32_t spherical_zero_padding;   /* phaser_core_spherical_zero_padding (0) */
+  uint32_t spatial_n_voxels;         /* phaser_core_spatial_n_voxels (100) */
+  int32_t spatial_discretize_lower;  /* phaser_core_spatial_discretize_lower (-50) */
+  int32_t spatial_discretize_upper;  /* phaser_core_spatial_discretize_upper (50) */
+  uint32_t spatial_zero_padding;     /* phaser_core_spatial_zero_padding (0; only 0 supported) */
+  float spatial_low_pass_lower;      /* phaser_core_spatial_low_pass_lower_bound (0) */
+  float spatial_low_pass_upper;      /* phaser_core_spatial_low_pass_upper_bound (100000) */
+  uint32_t n_channels;               /* channel count of the fusion (4) */
+  uint32_t fusion_levels;            /* LaplacePyramid levels (5) */
+  uint32_t spherical_fusion;         /* PHGPU_FUSION_* */
+  uint32_t spatial_fusion;           /* PHGPU_FUSION_* */
+  uint32_t max_points;               /* capacity per cloud (grows on demand) */
+  uint32_t flags;                    /* PHGPU_FLAG_* */
+  int32_t device;                    /* CUDA device ordinal */
+} phgpu_params;
+
+/* A point cloud: x, y, z, intensity as float4 plus optional per-point
+ * reflectivity and ambient values (phaser_common/include/phaser/model/
+ * point-cloud.h:18-88).  on_device = 1 when the pointers are device memory. */
+typedef struct {
+  const float* xyzi;          /* 4 * n_points floats */
+  const float* reflectivity;  /* n_points floats or NULL */
+  const float* ambient;       /* n_points floats or NULL */
+  uint32_t n_points;
+  int32_t on_device;
+} phgpu_cloud;
+
+/* Registration result (phaser_core/src/backend/registration/
+ * sph-opt-registration.cc:49-95). */
+typedef struct {
+  uint32_t rot_bin;     /* argmax of the SO(3) correlation, [beta][alpha][gamma] */
+  float rot_peak;       /* |z|^2 at the bin */
+  double zyz[3];        /* alpha, beta, gamma of the bin (rotation-utils.cc:197-208) */
+  double quat[4];       /* w, x, y, z */
+  double xyz[3];        /* Euler XYZ angles applied to the source (rotation-utils.cc:86-107) */
+  uint32_t voxel;       /* argmax of the spatial correlation, [z][x][y] */
+  float trans_peak;     /* correlation value at the voxel */
+  double trans[3];      /* translation (translation-utils.cc:40-52) */
+} phgpu_pose;
+
+typedef struct phgpu_ctx phgpu_ctx;
+
+/* Defaults of the reference's flags. */
+int phgpu_params_default(phgpu_params* params);
+
+/* Replaces the constructors SphericalCorrelation(bw, zero_padding)
+ * (phaser_core/include/phaser/backend/correlation/spherical-correlation.h:19-21),
+ * SpatialCorrelation(n_voxels, zero_padding) (spatial-correlation.h:15-17) and
+ * PhaseAligner() (phase-aligner.cc:19-45): all tables, plans and buffers are
+ * built once here and reused by every call. */
+int phgpu_ctx_create(const phgpu_params* params, phgpu_ctx** out);
+/* Replaces SphericalCorrelation::shutdown() (spherical-correlation.cc:31-52)
+ * and the spatial destructors. */
+int phgpu_ctx_destroy(phgpu_ctx* ctx);
+/* Message of the last failing call on ctx (or of the last failing
+ * phgpu_ctx_create when ctx is NULL). */
+const char* phgpu_last_error(const phgpu_ctx* ctx);
+/* The context's main CUDA stream (cudaStream_t). */
+void* phgpu_stream(phgpu_ctx* ctx);
+
+/* S^2 sampling of one cloud on the 2B x 2B grid: replaces
+ * SphericalSampler::sampleUniformly (phaser_common/src/common/
+ * spherical-sampler.cc:20-27).  side 0 = target (f), 1 = source (h). */
+int phgpu_sample_s2(phgpu_ctx* ctx, const phgpu_cloud* cloud, int side);
+/* Copies the sampled grids of a side to the host: n_channels x 4B^2 doubles
+ * in the channel order {range, intensity, reflectivity, ambient}, and the
+ * nearest-point index per grid direction (-1 when dropped).  Either may be NULL. */
+int phgpu_get_samples(phgpu_ctx* ctx, int side, double* values, int32_t* nn_index);
+
+/* SphericalCorrelationLaplace::correlateSampledSignals
+ * (spherical-correlation-laplace.cc:14-40) / SphericalCorrelation::
+ * correlateSampledSignals (spherical-correlation.cc:69-80): f[c], g[c] are
+ * 4B^2 host doubles in [theta][phi] order. */
+int phgpu_sph_correlate(phgpu_ctx* ctx, const double* const* f, const double* const* g,
+                        uint32_t n_channels);
+/* The same on the grids of the last phgpu_sample_s2 calls (no host copies). */
+int phgpu_sph_correlate_sampled(phgpu_ctx* ctx);
+/* Result of the last spherical correlation: the bin, its |z|^2 and, when
+ * corr_out is not NULL (needs PHGPU_FLAG_KEEP_VOLUMES), the volume of
+ * 8 bw_out^3 doubles: SphericalCorrelation::getCorrelation
+ * (spherical-correlation.cc:114-116). */
+int phgpu_sph_result(phgpu_ctx* ctx, uint32_t* bin, float* peak, double* corr_out);
+/* SphericalCorrelation::getBandwidth (spherical-correlation.cc:118-120). */
+uint32_t phgpu_sph_bandwidth(const phgpu_ctx* ctx);
+
+/* PhaseAligner::discretizePointcloud (phase-aligner.cc:71-125) of one cloud,
+ * optionally after the float 3x4 transform T (row-major) that
+ * RotationUtils::RotateAroundXYZ applies (rotation-utils.cc:17-24). */
+int phgpu_voxelize(phgpu_ctx* ctx, const phgpu_cloud* cloud, int side, const float* T12);
+/* Per-point linear voxel index of the last voxelize of a side
+ * (0xffffffff when skipped by the reference's guard). */
+int phgpu_get_voxel_index(phgpu_ctx* ctx, int side, uint32_t* lin, uint32_t n_points);
+/* SpatialCorrelationLaplace::correlateSignals / SpatialCorrelation::
+ * correlateSignals (spatial-correlation-laplace.cc:17-51,
+ * spatial-correlation.cc:128-175): f[c], g[c] are N^3 host doubles. */
+int phgpu_spatial_correlate(phgpu_ctx* ctx, const double* const* f, const double* const* g,
+                            uint32_t n_channels);
+/* The same on the grids of the last phgpu_voxelize calls. */
+int phgpu_spatial_correlate_voxelized(phgpu_ctx* ctx);
+/* Result of the last spatial correlation: voxel, value and optionally the
+ * N^3 correlation (PhaseAligner::getCorrelation, phase-aligner.cc:133-135). */
+int phgpu_spatial_result(phgpu_ctx* ctx, uint32_t* voxel, float* peak, double* corr_out);
+
+/* SphOptRegistration::registerPointCloud (sph-opt-registration.cc:34-47):
+ * rotation, then translation of the rotated source. */
+int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_cloud* source,
+                        phgpu_pose* out);
+
+/* Host pose arithmetic of the reference (rotation-utils.cc:86-143, 197-208;
+ * translation-utils.cc:40-52). */
+int phgpu_pose_from_bin(uint32_t bin, uint32_t bw_out, double* zyz, double* quat, double* xyz,
+                        float* T12);
+double phgpu_translation_from_index(double index, uint32_t n_voxels, int32_t lower,
+                                    int32_t upper);
+
+/* ------------------------------------------------------------------ serving
+ * Continuous-batching request server (no reference counterpart: the
+ * reference registers one pair at a time, sph-opt-registration.cc:34-47).
+ * Requests of different (bandwidth, voxel grid) shapes are admitted against an
+ * HBM budget, grouped by shape into waves and run on device-resident state. */
+typedef struct phgpu_server phgpu_server;
+
+typedef struct {
+  uint64_t hbm_budget_bytes;   /* admission budget */
+  uint32_t max_wave;           /* pairs per wave and shape */
+  uint32_t max_points;         /* capacity per cloud */
+  int32_t device;
+  uint32_t flags;
+} phgpu_server_params;
+
+int phgpu_server_create(const phgpu_server_params* params, phgpu_server** out);
+int phgpu_server_destroy(phgpu_server* srv);
+/* Submits one pair; params gives the shape (bandwidth, voxels, bounds).  The
+ * clouds are copied before the call returns.  *ticket identifies the request. */
+int phgpu_server_submit(phgpu_server* srv, const phgpu_params* params, const phgpu_cloud* target,
+                        const phgpu_cloud* source, uint64_t* ticket);
+/* Non-blocking: 1 and the pose when the ticket finished, 0 otherwise. */
+int phgpu_server_poll(phgpu_server* srv, uint64_t ticket, phgpu_pose* out, double* latency_ms);
+/* Blocks until every submitted request finished. */
+int phgpu_server_drain(phgpu_server* srv);
+const char* phgpu_server_last_error(const phgpu_server* srv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHASER_GPU_H_ */

@@ -1,0 +1,736 @@
+// Host side of the C ABI (include/phaser_gpu.h): per-configuration context,
+// FFT plans, fusion band tables, the reference's host pose arithmetic and the
+// plain one-pair-at-a-time pipeline.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/phaser_gpu.h"
+#include "ctx.h"
+#include "kernels.h"
+
+using namespace phgpu;
+
+static thread_local std::string g_create_error;
+
+#define CK(expr)                                                                   \
+  do {                                                                             \
+    cudaError_t _e = (expr);                                                       \
+    if (_e != cudaSuccess) {                                                       \
+      ctx->err = std::string(#expr) + ": " + cudaGetErrorString(_e);               \
+      return PHGPU_ERR_CUDA;                                                       \
+    }                                                                              \
+  } while (0)
+
+#define CKV(expr)                                                                  \
+  do {                                                                             \
+    int _r = (expr);                                                               \
+    if (_r != PHGPU_OK) return _r;                                                 \
+  } while (0)
+
+// ------------------------------------------------------------------ helpers
+
+namespace phgpu {
+
+bool make_fft_plan(int n, FftPlan* p, float2** d_tw, std::string* err) {
+  memset(p, 0, sizeof(*p));
+  p->n = n;
+  int m = n, ns = 0;
+  const int order[] = {8, 4, 2, 5, 3, 7, 11, 13};
+  for (int r : order) {
+    while (m % r == 0 && ns < kMaxFftStages) {
+      p->radix[ns++] = r;
+      m /= r;
+    }
+  }
+  if (m != 1 || n < 1) {
+    *err = "FFT length " + std::to_string(n) + " has a prime factor above 13 (unsupported)";
+    return false;
+  }
+  p->nstage = ns;
+  int L = n;
+  for (int s = 0; s < ns; ++s) {
+    p->L[s] = L;
+    L /= p->radix[s];
+  }
+  std::vector<float2> tw(n);
+  for (int t = 0; t < n; ++t) {
+    const double a = -2.0 * M_PI * (double)t / (double)n;
+    tw[t] = make_float2((float)cos(a), (float)sin(a));
+  }
+  if (cudaMalloc(d_tw, sizeof(float2) * n) != cudaSuccess) {
+    *err = "cudaMalloc twiddles failed";
+    return false;
+  }
+  cudaMemcpy(*d_tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice);
+  p->tw = *d_tw;
+  return true;
+}
+
+// PyramidStruct (pyramid-struct.cc:17-29) and LaplacePyramid::expand
+// (laplace-pyramid.cc:40-58) bounds with the reference's float arithmetic.
+FusionBands make_bands(uint32_t n, int levels, float div) {
+  FusionBands b;
+  memset(&b, 0, sizeof(b));
+  b.levels = levels;
+  b.n = n;
+  uint32_t cur = n;
+  for (int l = 0; l < levels; ++l) {
+    const float lower = (float)cur / div;
+    const uint32_t upper = (uint32_t)roundf((float)cur - lower);
+    const uint32_t lb = (uint32_t)roundf(lower);
+    const uint32_t elb = (uint32_t)roundf((float)cur / div);
+    b.lb[l] = lb;
+    b.sub[l] = upper;
+    b.eub[l] = cur - elb;
+    cur = upper - lb;
+  }
+  return b;
+}
+
+}  // namespace phgpu
+
+// RotationUtils::convertSO3toZYZ (rotation-utils.cc:197-208).
+static void bin_to_zyz(uint32_t loc, uint32_t bw, double* zyz) {
+  const int32_t ii = (int32_t)floor(loc / (4. * bw * bw));
+  const int32_t tmp = (int32_t)(loc - (ii * 4. * bw * bw));
+  const int32_t jj = (int32_t)floor(tmp / (2. * bw));
+  const int32_t kk = (int32_t)loc - (ii * 4 * (int32_t)bw * (int32_t)bw) - jj * (2 * (int32_t)bw);
+  const double b = (double)bw;
+  zyz[0] = M_PI * jj / b;
+  zyz[1] = M_PI * (2 * ii + 1) / (4. * bw);
+  zyz[2] = M_PI * kk / b;
+}
+
+// Hamilton product in the term order of Eigen's generic quat_product.
+static void quat_product(const double* a, const double* b, double* r) {
+  r[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+  r[1] = a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2];
+  r[2] = a[0] * b[2] + a[2] * b[0] + a[3] * b[1] - a[1] * b[3];
+  r[3] = a[0] * b[3] + a[3] * b[0] + a[1] * b[2] - a[2] * b[1];
+}
+
+int phgpu_pose_from_bin(uint32_t bin, uint32_t bw_out, double* zyz, double* quat, double* xyz, float* T12) {
+  double z[3], q[4], e[3];
+  bin_to_zyz(bin, bw_out, z);
+  // ConvertZYZtoQuaternion: AngleAxis(a, Z) * AngleAxis(b, Y) * AngleAxis(c, Z)
+  const double qa[4] = {cos(0.5 * z[0]), 0.0, 0.0, sin(0.5 * z[0])};
+  const double qb[4] = {cos(0.5 * z[1]), 0.0, sin(0.5 * z[1]), 0.0};
+  const double qc[4] = {cos(0.5 * z[2]), 0.0, 0.0, sin(0.5 * z[2])};
+  double t[4];
+  quat_product(qa, qb, t);
+  quat_product(t, qc, q);
+  // ConvertQuaternionToXYZ / fromRotation (rotation-utils.cc:86-93, 190-196)
+  const double qw = q[0], qx = q[1], qy = q[2], qz = q[3];
+  const double r11 = -2 * (qy * qz - qw * qx);
+  const double r12 = qw * qw - qx * qx - qy * qy + qz * qz;
+  const double r21 = 2 * (qx * qz + qw * qy);
+  const double r31 = -2 * (qx * qy - qw * qz);
+  const double r32 = qw * qw + qx * qx - qy * qy - qz * qz;
+  e[2] = -atan2(r31, r32);
+  e[1] = asin(r21);
+  e[0] = atan2(r11, r12);
+  if (zyz) memcpy(zyz, z, sizeof(z));
+  if (quat) memcpy(quat, q, sizeof(q));
+  if (xyz) memcpy(xyz, e, sizeof(e));
+  if (T12) {
+    // RotateAroundXYZ: Rx(a) * Ry(b) * Rz(c) in float (rotation-utils.cc:17-24,109-143)
+    const float a = (float)e[0], bb = (float)e[1], c = (float)e[2];
+    const float ca = cosf(a), sa = sinf(a), cb = cosf(bb), sb = sinf(bb), cc = cosf(c), sc = sinf(c);
+    const float X[3][3] = {{1, 0, 0}, {0, ca, -sa}, {0, sa, ca}};
+    const float Y[3][3] = {{cb, 0, sb}, {0, 1, 0}, {-sb, 0, cb}};
+    const float Z[3][3] = {{cc, sc, 0}, {-sc, cc, 0}, {0, 0, 1}};
+    float XY[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        float s = 0.0f;
+        for (int k = 0; k < 3; ++k) s += X[i][k] * Y[k][j];
+        XY[i][j] = s;
+      }
+    for (int i = 0; i < 3; ++i) {
+      for (int j = 0; j < 3; ++j) {
+        float s = 0.0f;
+        for (int k = 0; k < 3; ++k) s += XY[i][k] * Z[k][j];
+        T12[4 * i + j] = s;
+      }
+      T12[4 * i + 3] = 0.0f;
+    }
+  }
+  return PHGPU_OK;
+}
+
+double phgpu_translation_from_index(double index, uint32_t n_voxels, int32_t lower, int32_t upper) {
+  if (index == 0) return 0.0;
+  const double half = n_voxels / 2.0;
+  const double width = (double)(abs(lower) + abs(upper) + 1);
+  if (index <= half) return index * width / n_voxels;
+  return (index - n_voxels) * width / n_voxels;
+}
+
+// ------------------------------------------------------------------ context
+
+int phgpu_params_default(phgpu_params* p) {
+  if (!p) return PHGPU_ERR_INVALID;
+  memset(p, 0, sizeof(*p));
+  p->spherical_bandwidth = 75;
+  p->spherical_zero_padding = 0;
+  p->spatial_n_voxels = 100;
+  p->spatial_discretize_lower = -50;
+  p->spatial_discretize_upper = 50;
+  p->spatial_zero_padding = 0;
+  p->spatial_low_pass_lower = 0.0f;
+  p->spatial_low_pass_upper = 100000.0f;
+  p->n_channels = 4;
+  p->fusion_levels = 5;
+  p->spherical_fusion = PHGPU_FUSION_LAPLACE;
+  p->spatial_fusion = PHGPU_FUSION_LAPLACE;
+  p->max_points = 1u << 18;
+  p->flags = 0;
+  p->device = 0;
+  return PHGPU_OK;
+}
+
+const char* phgpu_last_error(const phgpu_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+void* phgpu_stream(phgpu_ctx* ctx) { return ctx ? (void*)ctx->s0 : nullptr; }
+
+uint32_t phgpu_sph_bandwidth(const phgpu_ctx* ctx) { return ctx ? (uint32_t)ctx->bw_out : 0u; }
+
+template <typename T>
+static int dalloc(phgpu_ctx* ctx, T** p, size_t bytes) {
+  if (bytes == 0) bytes = 256;
+  cudaError_t e = cudaMalloc((void**)p, bytes);
+  if (e != cudaSuccess) {
+    ctx->err = "cudaMalloc(" + std::to_string(bytes) + ") failed: " + cudaGetErrorString(e);
+    *p = nullptr;
+    return PHGPU_ERR_MEMORY;
+  }
+  ctx->allocs.push_back((void*)*p);
+  ctx->device_bytes += bytes;
+  return PHGPU_OK;
+}
+
+static void dfree(phgpu_ctx* ctx, void* p) {
+  if (!p) return;
+  auto it = std::find(ctx->allocs.begin(), ctx->allocs.end(), p);
+  if (it != ctx->allocs.end()) ctx->allocs.erase(it);
+  cudaFree(p);
+}
+
+static int ensure_cloud_capacity(phgpu_ctx* ctx, uint32_t n) {
+  if (n <= ctx->cap_points) return PHGPU_OK;
+  uint32_t cap = std::max<uint32_t>(n, ctx->cap_points * 2);
+  for (int s = 0; s < 2; ++s) {
+    dfree(ctx, ctx->d_xyzi[s]);
+    dfree(ctx, ctx->d_refl[s]);
+    dfree(ctx, ctx->d_amb[s]);
+    dfree(ctx, ctx->d_sample_scratch[s]);
+    dfree(ctx, ctx->d_lin[s]);
+    CKV(dalloc(ctx, &ctx->d_xyzi[s], sizeof(float4) * cap));
+    CKV(dalloc(ctx, &ctx->d_refl[s], sizeof(float) * cap));
+    CKV(dalloc(ctx, &ctx->d_amb[s], sizeof(float) * cap));
+    CKV(dalloc(ctx, &ctx->d_sample_scratch[s], sampler_scratch_bytes((int)cap)));
+    CKV(dalloc(ctx, &ctx->d_lin[s], sizeof(uint32_t) * cap));
+  }
+  ctx->cap_points = cap;
+  return PHGPU_OK;
+}
+
+int phgpu_ctx_create(const phgpu_params* prm, phgpu_ctx** out) {
+  if (!prm || !out) {
+    g_create_error = "null argument";
+    return PHGPU_ERR_INVALID;
+  }
+  *out = nullptr;
+  const int bw = (int)prm->spherical_bandwidth;
+  const int bw_out = bw + (int)prm->spherical_zero_padding;
+  const int N = (int)prm->spatial_n_voxels;
+  if (bw < 2 || bw > 512 || N < 1 || N > 1024 || prm->spatial_zero_padding != 0 ||
+      prm->n_channels < 1 || prm->n_channels > 4 || prm->fusion_levels < 1 ||
+      prm->fusion_levels > (uint32_t)kMaxLevels) {
+    g_create_error =
+        "unsupported configuration (2 <= bandwidth <= 512, 1 <= n_voxels <= 1024, spatial zero "
+        "padding 0, 1..4 channels, 1..8 fusion levels)";
+    return PHGPU_ERR_INVALID;
+  }
+  phgpu_ctx* ctx = new phgpu_ctx();
+  ctx->prm = *prm;
+  ctx->bw = bw;
+  ctx->bw_out = bw_out;
+  ctx->N = N;
+  if (cudaSetDevice(prm->device) != cudaSuccess) {
+    g_create_error = "cudaSetDevice failed";
+    delete ctx;
+    return PHGPU_ERR_CUDA;
+  }
+  int rc = phgpu_ctx_init(ctx);
+  if (rc != PHGPU_OK) {
+    g_create_error = ctx->err;
+    phgpu_ctx_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return PHGPU_OK;
+}
+
+int phgpu_ctx_init(phgpu_ctx* ctx) {
+  const phgpu_params* prm = &ctx->prm;
+  const int bw = ctx->bw, bw_out = ctx->bw_out, N = ctx->N;
+  CK(cudaStreamCreateWithFlags(&ctx->s0, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&ctx->s1, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&ctx->ev_a, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&ctx->ev_b, cudaEventDisableTiming));
+  CK(spatial_init_attributes());
+  CK(so3_init_attributes());
+  std::string perr;
+  if (!make_fft_plan(2 * bw, &ctx->plan_s2, &ctx->d_tw[0], &perr) ||
+      !make_fft_plan(2 * bw_out, &ctx->plan_so3, &ctx->d_tw[1], &perr) ||
+      !make_fft_plan(N, &ctx->plan_sp, &ctx->d_tw[2], &perr)) {
+    ctx->err = perr;
+    return PHGPU_ERR_INVALID;
+  }
+  ctx->bands_s2 = make_bands((uint32_t)(bw * bw), (int)prm->fusion_levels, 4.0f);
+  ctx->bands_sp = make_bands((uint32_t)N * (uint32_t)N * (uint32_t)N, (int)prm->fusion_levels, 4.0f);
+  // DH grid directions (spherical-sampler.cc:29-64), float sin/cos of float angles
+  const int n = 2 * bw;
+  std::vector<float4> grid((size_t)n * n);
+  for (int i = 0; i < n; ++i) {
+    const float th = (float)((M_PI * (double)(2 * i + 1)) / (double)(4 * bw));
+    for (int j = 0; j < n; ++j) {
+      const float ph = (float)((2.0 * M_PI * (double)j) / (double)(2 * bw));
+      const float dist = 1.0f;
+      grid[(size_t)i * n + j] = make_float4(dist * sinf(th) * cosf(ph), dist * sinf(th) * sinf(ph),
+                                            dist * cosf(th), 0.0f);
+    }
+  }
+  CKV(dalloc(ctx, &ctx->d_grid, sizeof(float4) * grid.size()));
+  CK(cudaMemcpy(ctx->d_grid, grid.data(), sizeof(float4) * grid.size(), cudaMemcpyHostToDevice));
+  // Driscoll-Healy weights (lib/SOFT/makeweights.c:68-91 behaviour)
+  std::vector<double> w(n);
+  for (int k = 0; k < n; ++k) {
+    const double th = M_PI * (2.0 * k + 1.0) / (4.0 * bw);
+    double s = 0.0;
+    for (int i = 0; i < bw; ++i) s += sin((2.0 * i + 1.0) * th) / (2.0 * i + 1.0);
+    w[k] = (2.0 / (double)bw) * sin(th) * s;
+  }
+  CKV(dalloc(ctx, &ctx->d_weights, sizeof(double) * n));
+  CK(cudaMemcpy(ctx->d_weights, w.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  CKV(dalloc(ctx, &ctx->d_legendre, sizeof(float) * legendre_table_entries(bw)));
+  CK(launch_legendre_table(bw, ctx->d_weights, ctx->d_legendre, ctx->s0));
+  // histc edges (phase-aligner.cc:27-30): float LinSpaced
+  std::vector<float> e(N);
+  const float flo = (float)prm->spatial_discretize_lower, fhi = (float)prm->spatial_discretize_upper;
+  const float step = (N == 1) ? 0.0f : (fhi - flo) / (float)(N - 1);
+  for (int i = 0; i < N; ++i) e[i] = (i == N - 1) ? fhi : (flo + (float)i * step);
+  CKV(dalloc(ctx, &ctx->d_edges, sizeof(float) * N));
+  CK(cudaMemcpy(ctx->d_edges, e.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+  // squared voxel size of the sampler rejection (point-cloud.cc:66-72)
+  const float vs = (fabsf(prm->spatial_low_pass_lower) + fabsf(prm->spatial_low_pass_upper)) /
+                   (float)prm->spatial_n_voxels;
+  ctx->max_sq = vs * vs;
+  // buffers
+  const size_t nq = (size_t)4 * bw * bw;
+  CKV(dalloc(ctx, &ctx->d_samples, sizeof(float) * 2 * 4 * nq));
+  CK(cudaMemset(ctx->d_samples, 0, sizeof(float) * 2 * 4 * nq));
+  for (int s = 0; s < 2; ++s) CKV(dalloc(ctx, &ctx->d_nn[s], sizeof(int32_t) * nq));
+  CKV(dalloc(ctx, &ctx->d_fm, sizeof(float2) * 8 * bw * n));
+  CKV(dalloc(ctx, &ctx->d_coef, sizeof(float2) * 8 * bw * bw));
+  CKV(dalloc(ctx, &ctx->d_fused, sizeof(float2) * 2 * bw * (2 * bw - 1)));
+  CK(cudaMemset(ctx->d_fused, 0, sizeof(float2) * 2 * bw * (2 * bw - 1)));
+  const size_t no = (size_t)2 * bw_out;
+  CKV(dalloc(ctx, &ctx->d_S, sizeof(float2) * no * no * bw_out));
+  CK(cudaMemset(ctx->d_S, 0, sizeof(float2) * no * no * bw_out));
+  const size_t nv = (size_t)N * N * N;
+  const size_t H = (size_t)N * N * (N / 2 + 1);
+  for (int s = 0; s < 2; ++s) CKV(dalloc(ctx, &ctx->d_grids[s], sizeof(float) * 5 * nv));
+  CKV(dalloc(ctx, &ctx->d_spec, sizeof(float2) * 8 * H));
+  CKV(dalloc(ctx, &ctx->d_cspec, sizeof(float2) * H));
+  if (prm->flags & PHGPU_FLAG_KEEP_VOLUMES) {
+    CKV(dalloc(ctx, &ctx->d_rotvol, sizeof(float) * no * no * no));
+    CKV(dalloc(ctx, &ctx->d_transvol, sizeof(float) * nv));
+  }
+  CKV(dalloc(ctx, &ctx->d_argmax, sizeof(unsigned long long) * 2));
+  CK(cudaMallocHost((void**)&ctx->h_argmax, sizeof(unsigned long long) * 2));
+  ctx->h_argmax[0] = ctx->h_argmax[1] = 0ull;
+  CKV(ensure_cloud_capacity(ctx, prm->max_points ? prm->max_points : (1u << 18)));
+  CK(cudaStreamSynchronize(ctx->s0));
+  return PHGPU_OK;
+}
+
+int phgpu_ctx_destroy(phgpu_ctx* ctx) {
+  if (!ctx) return PHGPU_OK;
+  cudaSetDevice(ctx->prm.device);
+  if (ctx->s0) cudaStreamSynchronize(ctx->s0);
+  if (ctx->s1) cudaStreamSynchronize(ctx->s1);
+  for (void* p : ctx->allocs) cudaFree(p);
+  ctx->allocs.clear();
+  for (int i = 0; i < 3; ++i)
+    if (ctx->d_tw[i]) cudaFree(ctx->d_tw[i]);
+  if (ctx->h_argmax) cudaFreeHost(ctx->h_argmax);
+  if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
+  if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
+  if (ctx->s0) cudaStreamDestroy(ctx->s0);
+  if (ctx->s1) cudaStreamDestroy(ctx->s1);
+  delete ctx;
+  return PHGPU_OK;
+}
+
+// ------------------------------------------------------------------ stages
+
+// S^2 channel count with data: {range, intensity} always, + reflectivity, + ambient.
+static int s2_channels(const phgpu_cloud* c) {
+  return c->ambient ? 4 : (c->reflectivity ? 3 : 2);
+}
+
+int phgpu_upload_cloud(phgpu_ctx* ctx, const phgpu_cloud* c, int side, cudaStream_t st) {
+  CKV(ensure_cloud_capacity(ctx, c->n_points));
+  const cudaMemcpyKind kind = c->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (c->n_points) {
+    CK(cudaMemcpyAsync(ctx->d_xyzi[side], c->xyzi, sizeof(float4) * c->n_points, kind, st));
+    if (c->reflectivity)
+      CK(cudaMemcpyAsync(ctx->d_refl[side], c->reflectivity, sizeof(float) * c->n_points, kind, st));
+    if (c->ambient)
+      CK(cudaMemcpyAsync(ctx->d_amb[side], c->ambient, sizeof(float) * c->n_points, kind, st));
+  }
+  ctx->np[side] = c->n_points;
+  ctx->has_refl[side] = c->reflectivity != nullptr;
+  ctx->has_amb[side] = c->ambient != nullptr;
+  return PHGPU_OK;
+}
+
+static int run_sample(phgpu_ctx* ctx, int side, cudaStream_t st) {
+  SampleArgs a;
+  a.xyzi = ctx->d_xyzi[side];
+  a.refl = ctx->has_refl[side] ? ctx->d_refl[side] : nullptr;
+  a.amb = ctx->has_amb[side] ? ctx->d_amb[side] : nullptr;
+  a.n_points = (int)ctx->np[side];
+  a.max_points = (int)ctx->cap_points;
+  a.grid = ctx->d_grid;
+  a.n_queries = 4 * ctx->bw * ctx->bw;
+  a.max_sq = ctx->max_sq;
+  a.n_out_ch = 4;
+  a.out = ctx->d_samples + (size_t)side * 4 * a.n_queries;
+  a.nn_idx = ctx->d_nn[side];
+  a.scratch = ctx->d_sample_scratch[side];
+  CK(launch_sample(a, st));
+  ctx->sampled[side] = true;
+  return PHGPU_OK;
+}
+
+int phgpu_sample_s2(phgpu_ctx* ctx, const phgpu_cloud* cloud, int side) {
+  if (!ctx || !cloud || side < 0 || side > 1) return PHGPU_ERR_INVALID;
+  cudaSetDevice(ctx->prm.device);
+  CKV(phgpu_upload_cloud(ctx, cloud, side, ctx->s0));
+  CKV(run_sample(ctx, side, ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s0));
+  return PHGPU_OK;
+}
+
+int phgpu_get_samples(phgpu_ctx* ctx, int side, double* values, int32_t* nn_index) {
+  if (!ctx || side < 0 || side > 1) return PHGPU_ERR_INVALID;
+  if (!ctx->sampled[side]) {
+    ctx->err = "no samples for this side";
+    return PHGPU_ERR_STATE;
+  }
+  cudaSetDevice(ctx->prm.device);
+  const size_t nq = (size_t)4 * ctx->bw * ctx->bw;
+  if (values) {
+    std::vector<float> tmp(4 * nq);
+    CK(cudaMemcpy(tmp.data(), ctx->d_samples + (size_t)side * 4 * nq, sizeof(float) * 4 * nq,
+                  cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < 4 * nq; ++i) values[i] = tmp[i];
+  }
+  if (nn_index) CK(cudaMemcpy(nn_index, ctx->d_nn[side], sizeof(int32_t) * nq, cudaMemcpyDeviceToHost));
+  return PHGPU_OK;
+}
+
+// Spherical correlation of the sample grids currently in d_samples.
+int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st) {
+  const int bw = ctx->bw;
+  const size_t nq = (size_t)4 * bw * bw;
+  for (int side = 0; side < 2; ++side) {
+    ShtArgs s;
+    s.bw = bw;
+    s.n_sig = n_data;
+    s.signal = ctx->d_samples + (size_t)side * 4 * nq;
+    s.tw = ctx->plan_s2.tw;
+    s.table = ctx->d_legendre;
+    s.fm = ctx->d_fm + (size_t)side * 4 * bw * 2 * bw;
+    s.coef = ctx->d_coef + (size_t)side * n_data * bw * bw;
+    CK(launch_sht(s, st));
+  }
+  FuseS2Args f;
+  f.bw = bw;
+  f.n_data_ch = n_data;
+  f.n_total_ch = n_total;
+  f.laplace = laplace;
+  f.bands = ctx->bands_s2;
+  f.coef = ctx->d_coef;
+  f.fused = ctx->d_fused;
+  CK(launch_fuse_s2(f, st));
+  CK(cudaMemsetAsync(ctx->d_argmax, 0, sizeof(unsigned long long), st));
+  So3Args o;
+  o.bw_in = bw;
+  o.bw_out = ctx->bw_out;
+  o.fused = ctx->d_fused;
+  o.S = ctx->d_S;
+  o.plan = &ctx->plan_so3;
+  o.argmax = ctx->d_argmax;
+  o.volume = ctx->d_rotvol;
+  CK(launch_so3(o, st));
+  CK(cudaMemcpyAsync(ctx->h_argmax, ctx->d_argmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  ctx->have_rot = true;
+  return PHGPU_OK;
+}
+
+int phgpu_sph_correlate(phgpu_ctx* ctx, const double* const* f, const double* const* g, uint32_t C) {
+  if (!ctx || !f || !g || C < 1 || C > 4) {
+    if (ctx) ctx->err = "phgpu_sph_correlate: 1..4 channels required";
+    return PHGPU_ERR_INVALID;
+  }
+  cudaSetDevice(ctx->prm.device);
+  const size_t nq = (size_t)4 * ctx->bw * ctx->bw;
+  std::vector<float> tmp(2 * 4 * nq, 0.0f);
+  for (uint32_t c = 0; c < C; ++c)
+    for (size_t i = 0; i < nq; ++i) {
+      tmp[c * nq + i] = (float)f[c][i];
+      tmp[4 * nq + c * nq + i] = (float)g[c][i];
+    }
+  CK(cudaMemcpyAsync(ctx->d_samples, tmp.data(), sizeof(float) * tmp.size(), cudaMemcpyHostToDevice, ctx->s0));
+  const int laplace = (C >= 2 && ctx->prm.spherical_fusion == PHGPU_FUSION_LAPLACE) ? 1 : 0;
+  CKV(phgpu_run_sph(ctx, (int)C, (int)C, laplace, ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s0));
+  return PHGPU_OK;
+}
+
+int phgpu_sph_correlate_sampled(phgpu_ctx* ctx) {
+  if (!ctx) return PHGPU_ERR_INVALID;
+  if (!ctx->sampled[0] || !ctx->sampled[1]) {
+    ctx->err = "both sides must be sampled first";
+    return PHGPU_ERR_STATE;
+  }
+  cudaSetDevice(ctx->prm.device);
+  const int nd = std::max(ctx->has_amb[0] || ctx->has_amb[1] ? 4 : 0,
+                          ctx->has_refl[0] || ctx->has_refl[1] ? 3 : 2);
+  const int laplace = ctx->prm.spherical_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
+  CKV(phgpu_run_sph(ctx, laplace ? nd : 1, (int)ctx->prm.n_channels, laplace, ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s0));
+  return PHGPU_OK;
+}
+
+int phgpu_sph_result(phgpu_ctx* ctx, uint32_t* bin, float* peak, double* corr_out) {
+  if (!ctx) return PHGPU_ERR_INVALID;
+  if (!ctx->have_rot) {
+    ctx->err = "no spherical correlation computed";
+    return PHGPU_ERR_STATE;
+  }
+  cudaSetDevice(ctx->prm.device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  const unsigned long long k = ctx->h_argmax[0];
+  if (bin) *bin = unpack_index(k);
+  if (peak) *peak = float_from_order_bits((uint32_t)(k >> 32));
+  if (corr_out) {
+    if (!ctx->d_rotvol) {
+      ctx->err = "volumes not kept (PHGPU_FLAG_KEEP_VOLUMES)";
+      return PHGPU_ERR_STATE;
+    }
+    const size_t n = (size_t)8 * ctx->bw_out * ctx->bw_out * ctx->bw_out;
+    std::vector<float> tmp(n);
+    CK(cudaMemcpy(tmp.data(), ctx->d_rotvol, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) corr_out[i] = tmp[i];
+  }
+  return PHGPU_OK;
+}
+
+// Spatial channel count with data: {intensity, range} always, + reflectivity, + ambient.
+static int sp_channels(int has_refl, int has_amb) { return has_amb ? 4 : (has_refl ? 3 : 2); }
+
+int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, cudaStream_t st) {
+  const size_t nv = (size_t)ctx->N * ctx->N * ctx->N;
+  CK(cudaMemsetAsync(ctx->d_grids[side], 0, sizeof(float) * (n_data + 1) * nv, st));
+  VoxelArgs v;
+  v.xyzi = ctx->d_xyzi[side];
+  v.refl = ctx->has_refl[side] ? ctx->d_refl[side] : nullptr;
+  v.amb = ctx->has_amb[side] ? ctx->d_amb[side] : nullptr;
+  v.n_points = (int)ctx->np[side];
+  v.N = ctx->N;
+  v.edges = ctx->d_edges;
+  v.has_T = T12 ? 1 : 0;
+  for (int i = 0; i < 12; ++i) v.T[i] = T12 ? T12[i] : 0.0f;
+  v.n_data_ch = n_data;
+  v.grids = ctx->d_grids[side];
+  v.lin_out = ctx->d_lin[side];
+  CK(launch_voxelize(v, st));
+  ctx->vox_ch[side] = n_data;
+  ctx->voxelized[side] = true;
+  return PHGPU_OK;
+}
+
+int phgpu_voxelize(phgpu_ctx* ctx, const phgpu_cloud* cloud, int side, const float* T12) {
+  if (!ctx || !cloud || side < 0 || side > 1) return PHGPU_ERR_INVALID;
+  cudaSetDevice(ctx->prm.device);
+  CKV(phgpu_upload_cloud(ctx, cloud, side, ctx->s0));
+  CKV(phgpu_run_voxelize(ctx, side, T12, 4, ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s0));
+  return PHGPU_OK;
+}
+
+int phgpu_get_voxel_index(phgpu_ctx* ctx, int side, uint32_t* lin, uint32_t n_points) {
+  if (!ctx || side < 0 || side > 1 || !lin) return PHGPU_ERR_INVALID;
+  if (!ctx->voxelized[side] || n_points > ctx->np[side]) {
+    ctx->err = "no voxelisation for this side / too many points requested";
+    return PHGPU_ERR_STATE;
+  }
+  cudaSetDevice(ctx->prm.device);
+  CK(cudaMemcpy(lin, ctx->d_lin[side], sizeof(uint32_t) * n_points, cudaMemcpyDeviceToHost));
+  return PHGPU_OK;
+}
+
+static SpatialArgs spatial_args(phgpu_ctx* ctx, int n_data, int n_total, int laplace, int means) {
+  SpatialArgs a;
+  a.N = ctx->N;
+  a.n_data_ch = n_data;
+  a.n_total_ch = n_total;
+  a.laplace = laplace;
+  a.bands = ctx->bands_sp;
+  a.grids_f = ctx->d_grids[0];
+  a.grids_g = ctx->d_grids[1];
+  a.grids_are_means = means;
+  a.spec = ctx->d_spec;
+  a.cspec = ctx->d_cspec;
+  a.plan = &ctx->plan_sp;
+  a.argmax = ctx->d_argmax + 1;
+  a.volume = ctx->d_transvol;
+  return a;
+}
+
+int phgpu_run_spatial(phgpu_ctx* ctx, int n_data, int n_total, int laplace, int means, cudaStream_t st) {
+  SpatialArgs a = spatial_args(ctx, n_data, n_total, laplace, means);
+  CK(launch_spatial_forward(a, 0, st));
+  CK(launch_spatial_forward(a, 1, st));
+  CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), st));
+  CK(launch_spatial_combine(a, st));
+  CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost, st));
+  ctx->have_trans = true;
+  return PHGPU_OK;
+}
+
+int phgpu_spatial_correlate(phgpu_ctx* ctx, const double* const* f, const double* const* g, uint32_t C) {
+  if (!ctx || !f || !g || C < 1 || C > 4) {
+    if (ctx) ctx->err = "phgpu_spatial_correlate: 1..4 channels required";
+    return PHGPU_ERR_INVALID;
+  }
+  cudaSetDevice(ctx->prm.device);
+  const size_t nv = (size_t)ctx->N * ctx->N * ctx->N;
+  const int laplace = ctx->prm.spatial_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
+  std::vector<float> tmp(nv);
+  for (int side = 0; side < 2; ++side) {
+    const double* const* src = side == 0 ? f : g;
+    for (uint32_t c = 0; c < C; ++c) {
+      for (size_t i = 0; i < nv; ++i) tmp[i] = (float)src[c][i];
+      CK(cudaMemcpy(ctx->d_grids[side] + c * nv, tmp.data(), sizeof(float) * nv, cudaMemcpyHostToDevice));
+    }
+  }
+  CKV(phgpu_run_spatial(ctx, (int)C, (int)C, laplace, 1, ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s0));
+  return PHGPU_OK;
+}
+
+int phgpu_spatial_correlate_voxelized(phgpu_ctx* ctx) {
+  if (!ctx) return PHGPU_ERR_INVALID;
+  if (!ctx->voxelized[0] || !ctx->voxelized[1] || ctx->vox_ch[0] != ctx->vox_ch[1]) {
+    ctx->err = "both sides must be voxelised with the same channel count first";
+    return PHGPU_ERR_STATE;
+  }
+  cudaSetDevice(ctx->prm.device);
+  const int laplace = ctx->prm.spatial_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
+  CKV(phgpu_run_spatial(ctx, ctx->vox_ch[0], (int)ctx->prm.n_channels, laplace, 0, ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s0));
+  return PHGPU_OK;
+}
+
+int phgpu_spatial_result(phgpu_ctx* ctx, uint32_t* voxel, float* peak, double* corr_out) {
+  if (!ctx) return PHGPU_ERR_INVALID;
+  if (!ctx->have_trans) {
+    ctx->err = "no spatial correlation computed";
+    return PHGPU_ERR_STATE;
+  }
+  cudaSetDevice(ctx->prm.device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  const unsigned long long k = ctx->h_argmax[1];
+  if (voxel) *voxel = unpack_index(k);
+  if (peak) *peak = float_from_order_bits((uint32_t)(k >> 32));
+  if (corr_out) {
+    if (!ctx->d_transvol) {
+      ctx->err = "volumes not kept (PHGPU_FLAG_KEEP_VOLUMES)";
+      return PHGPU_ERR_STATE;
+    }
+    const size_t n = (size_t)ctx->N * ctx->N * ctx->N;
+    std::vector<float> tmp(n);
+    CK(cudaMemcpy(tmp.data(), ctx->d_transvol, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) corr_out[i] = tmp[i];
+  }
+  return PHGPU_OK;
+}
+
+// ------------------------------------------------------------------ pipeline
+
+int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_cloud* source,
+                        phgpu_pose* out) {
+  if (!ctx || !target || !source || !out) return PHGPU_ERR_INVALID;
+  cudaSetDevice(ctx->prm.device);
+  cudaStream_t s0 = ctx->s0, s1 = ctx->s1;
+  CKV(phgpu_upload_cloud(ctx, target, 0, s0));
+  CKV(phgpu_upload_cloud(ctx, source, 1, s0));
+  const int laplace_s2 = ctx->prm.spherical_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
+  const int laplace_sp = ctx->prm.spatial_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
+  const int nd_s2 = std::max(s2_channels(target), s2_channels(source));
+  const int nd_sp = sp_channels(target->reflectivity || source->reflectivity,
+                                target->ambient || source->ambient);
+  // target translation side overlaps the rotation stage
+  CK(cudaEventRecord(ctx->ev_a, s0));
+  CK(cudaStreamWaitEvent(s1, ctx->ev_a, 0));
+  CKV(phgpu_run_voxelize(ctx, 0, nullptr, nd_sp, s1));
+  SpatialArgs sa = spatial_args(ctx, nd_sp, (int)ctx->prm.n_channels, laplace_sp, 0);
+  CK(launch_spatial_forward(sa, 0, s1));
+  CK(cudaEventRecord(ctx->ev_b, s1));
+  // rotation
+  CKV(run_sample(ctx, 0, s0));
+  CKV(run_sample(ctx, 1, s0));
+  CKV(phgpu_run_sph(ctx, laplace_s2 ? nd_s2 : 1, (int)ctx->prm.n_channels, laplace_s2, s0));
+  CK(cudaStreamSynchronize(s0));
+  const unsigned long long rk = ctx->h_argmax[0];
+  out->rot_bin = unpack_index(rk);
+  out->rot_peak = float_from_order_bits((uint32_t)(rk >> 32));
+  float T[12];
+  phgpu_pose_from_bin(out->rot_bin, (uint32_t)ctx->bw_out, out->zyz, out->quat, out->xyz, T);
+  // translation of the rotated source
+  CKV(phgpu_run_voxelize(ctx, 1, T, nd_sp, s0));
+  CK(launch_spatial_forward(sa, 1, s0));
+  CK(cudaStreamWaitEvent(s0, ctx->ev_b, 0));
+  CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), s0));
+  CK(launch_spatial_combine(sa, s0));
+  CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost, s0));
+  ctx->have_trans = true;
+  CK(cudaStreamSynchronize(s0));
+  const unsigned long long tk = ctx->h_argmax[1];
+  out->voxel = unpack_index(tk);
+  out->trans_peak = float_from_order_bits((uint32_t)(tk >> 32));
+  const uint32_t N = (uint32_t)ctx->N;
+  const uint32_t xyz[3] = {(out->voxel / N) % N, out->voxel % N, out->voxel / (N * N)};
+  for (int a = 0; a < 3; ++a)
+    out->trans[a] = phgpu_translation_from_index((double)xyz[a], N, ctx->prm.spatial_discretize_lower,
+                                                 ctx->prm.spatial_discretize_upper);
+  return PHGPU_OK;
+}

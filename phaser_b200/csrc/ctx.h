@@ -1,0 +1,71 @@
+// Context state shared by the C ABI (capi.cu) and the request server
+// (server.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/phaser_gpu.h"
+#include "kernels.h"
+
+struct phgpu_ctx {
+  phgpu_params prm;
+  int bw = 0, bw_out = 0, N = 0;
+  float max_sq = 0.0f;
+  std::string err;
+  cudaStream_t s0 = nullptr, s1 = nullptr;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+  // plans and tables
+  phgpu::FftPlan plan_s2, plan_so3, plan_sp;
+  float2* d_tw[3] = {nullptr, nullptr, nullptr};
+  phgpu::FusionBands bands_s2, bands_sp;
+  float4* d_grid = nullptr;
+  double* d_weights = nullptr;
+  float* d_legendre = nullptr;
+  float* d_edges = nullptr;
+  // clouds
+  uint32_t cap_points = 0;
+  float4* d_xyzi[2] = {nullptr, nullptr};
+  float* d_refl[2] = {nullptr, nullptr};
+  float* d_amb[2] = {nullptr, nullptr};
+  void* d_sample_scratch[2] = {nullptr, nullptr};
+  uint32_t* d_lin[2] = {nullptr, nullptr};
+  uint32_t np[2] = {0, 0};
+  int has_refl[2] = {0, 0}, has_amb[2] = {0, 0};
+  // rotation
+  float* d_samples = nullptr;  // [2][4][4B^2]
+  int32_t* d_nn[2] = {nullptr, nullptr};
+  float2* d_fm = nullptr;
+  float2* d_coef = nullptr;
+  float2* d_fused = nullptr;
+  float2* d_S = nullptr;
+  float* d_rotvol = nullptr;
+  // translation
+  float* d_grids[2] = {nullptr, nullptr};  // [(C+1)][N^3]
+  float2* d_spec = nullptr;
+  float2* d_cspec = nullptr;
+  float* d_transvol = nullptr;
+  int vox_ch[2] = {0, 0};
+  // results
+  unsigned long long* d_argmax = nullptr;  // [rot, trans]
+  unsigned long long* h_argmax = nullptr;  // pinned
+  bool sampled[2] = {false, false};
+  bool voxelized[2] = {false, false};
+  bool have_rot = false, have_trans = false;
+  // bookkeeping
+  std::vector<void*> allocs;
+  size_t device_bytes = 0;
+};
+
+int phgpu_ctx_init(phgpu_ctx* ctx);
+int phgpu_upload_cloud(phgpu_ctx* ctx, const phgpu_cloud* c, int side, cudaStream_t st);
+int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st);
+int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, cudaStream_t st);
+int phgpu_run_spatial(phgpu_ctx* ctx, int n_data, int n_total, int laplace, int means, cudaStream_t st);
+
+namespace phgpu {
+bool make_fft_plan(int n, FftPlan* p, float2** d_tw, std::string* err);
+FusionBands make_bands(uint32_t n, int levels, float div);
+}  // namespace phgpu

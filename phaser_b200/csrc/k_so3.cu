@@ -1,0 +1,203 @@
+// Inverse SO(3) transform of the correlation coefficients, |z|^2 and argmax.
+//
+// Reference behaviour (phaser_core/lib/SOFT/so3_correlate_fftw.c:102-161 and
+// soft_fftw.c:1036-1914 with flag = 1, called from
+// phaser_core/src/backend/correlation/spherical-correlation.cc:248-279):
+//   c(l, m1, m2) = 2 pi sqrt(2/(2l+1)) fhat(l, -m1) (-1)^(m1+m2) conj(hhat(l, -m2))
+//   S_{m1 m2}(beta_k) = sum_l c(l, m1, m2) dtilde^l_{m1 m2}(beta_k)
+//   z(beta, alpha, gamma) = (B / pi) (1 / 2B) sum S_{m1 m2}(beta) e^{-i(m1 alpha + m2 gamma)}
+// where only one member of each pair (m1, m2) / (-m1, -m2) is synthesised
+// (the half H = {m1 > 0, m2 != -m1} + {(-m, m)} + {(0, m2 >= 0)}) and the
+// other is its conjugate, so z is real.  Output layout [beta][alpha][gamma].
+//
+// Design: one block per order class (p, q), 0 <= p <= q < B.  Thread k runs
+// the FP64 three-term recurrence of dtilde^l_{p q}(beta_k) in l (the Wigner
+// table is never stored) and accumulates in FP32 the four outputs the class
+// feeds through the d-symmetries
+//   d_{q p} = (-1)^(q-p) d_{p q},  d_{p,-q}(b) = d_{q,-p}(b) = (-1)^(l+p) d_{p q}(pi - b)
+// at beta_k and at the mirrored beta_{2B-1-k}.  Only b = m2 >= 0 is kept
+// (half spectrum); the gamma transform is a Hermitian complex-to-real one.
+#include "kernels.h"
+
+namespace phgpu {
+
+__device__ __forceinline__ float2 fused_at(const float2* __restrict__ fz, int bw, int side, int l, int m) {
+  return fz[((size_t)side * bw + l) * (2 * bw - 1) + (m + bw - 1)];
+}
+
+// conj(b) * a * s
+__device__ __forceinline__ float2 prod_conj(float2 a, float2 b, float s) {
+  return make_float2(s * (a.x * b.x + a.y * b.y), s * (a.y * b.x - a.x * b.y));
+}
+
+__global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz, float2* __restrict__ S) {
+  extern __shared__ double sm[];
+  double* fa = sm;
+  double* fb = fa + bw_in;
+  double* sh = fb + bw_in;
+  float2* cv = (float2*)(sh + bw_in);  // [4][bw_in]
+  const int cidx = blockIdx.x;
+  int q = (int)floor((sqrt(8.0 * cidx + 1.0) - 1.0) * 0.5);
+  while ((q + 1) * (q + 2) / 2 <= cidx) ++q;
+  while (q * (q + 1) / 2 > cidx) --q;
+  const int p = cidx - q * (q + 1) / 2;
+  const int nl = bw_in - q;
+  const double dp = p, dq = q;
+  for (int i = threadIdx.x; i < nl; i += blockDim.x) {
+    const int l = q + i;
+    const double dl = l;
+    const double tnext = sqrt(((dl + 1) * (dl + 1) - dp * dp) * ((dl + 1) * (dl + 1) - dq * dq));
+    fb[i] = sqrt((2 * dl + 3) / (2 * dl + 1)) * (dl + 1) * (2 * dl + 1) / tnext;
+    sh[i] = (l == 0) ? 0.0 : -dp * dq / (dl * (dl + 1));
+    double a = 0.0;
+    if (l > 0) {
+      const double tcur = sqrt((dl * dl - dp * dp) * (dl * dl - dq * dq));
+      a = -sqrt((2 * dl + 3) / (2 * dl - 1)) * (dl + 1) / dl * tcur / tnext;
+    }
+    fa[i] = a;
+    const float wn = (float)(2.0 * M_PI * sqrt(2.0 / (2.0 * dl + 1.0)));
+    const float spq = ((p + q) & 1) ? -wn : wn;
+    const float slp = ((l + p) & 1) ? -1.0f : 1.0f;
+    // v0: (p, q)
+    cv[0 * bw_in + i] = prod_conj(fused_at(fz, bw_in, 0, l, -p), fused_at(fz, bw_in, 1, l, -q), spq);
+    // v1: (q, p) with d_{qp} = (-1)^(q-p) d_{pq}: sign (-1)^(p+q) (-1)^(q-p) = +1
+    cv[1 * bw_in + i] = prod_conj(fused_at(fz, bw_in, 0, l, -q), fused_at(fz, bw_in, 1, l, -p), wn);
+    if (p == q) {
+      // (-p, p) in the synthesised half: c(l,-p,p) = w F(l,p) conj(H(l,-p)), d factor (-1)^(l+p)
+      cv[2 * bw_in + i] = prod_conj(fused_at(fz, bw_in, 0, l, p), fused_at(fz, bw_in, 1, l, -p), wn * slp);
+      cv[3 * bw_in + i] = make_float2(0.f, 0.f);
+    } else {
+      // (p, -q) and (q, -p), conjugated into (-p, q) and (-q, p)
+      cv[2 * bw_in + i] = prod_conj(fused_at(fz, bw_in, 0, l, -p), fused_at(fz, bw_in, 1, l, q), spq * slp);
+      cv[3 * bw_in + i] = prod_conj(fused_at(fz, bw_in, 0, l, -q), fused_at(fz, bw_in, 1, l, p), spq * slp);
+    }
+  }
+  __syncthreads();
+  const int n = 2 * bw_out;
+  const int Bo = bw_out;
+  // seed normalisation: 0.5 [log((2q+1)/2) + lgamma(2q+1) - lgamma(q-p+1) - lgamma(q+p+1)]
+  const double lnorm = 0.5 * (log((2.0 * q + 1.0) / 2.0) + lgamma(2.0 * q + 1.0) - lgamma(dq - dp + 1.0) -
+                              lgamma(dq + dp + 1.0));
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const double beta = M_PI * (2.0 * k + 1.0) / (4.0 * bw_out);
+    const double cb = cos(beta);
+    double sh2, ch2;
+    sincos(0.5 * beta, &sh2, &ch2);
+    const double lg = lnorm + (dq + dp) * log(ch2) + (q > p ? (dq - dp) * log(sh2) : 0.0);
+    double dcur = exp(lg), dprev = 0.0;
+    float2 a0 = make_float2(0.f, 0.f), a1 = a0, a2 = a0, a3 = a0;
+    for (int i = 0; i < nl; ++i) {
+      const float d = (float)dcur;
+      const float2 c0 = cv[i], c1 = cv[bw_in + i], c2 = cv[2 * bw_in + i], c3 = cv[3 * bw_in + i];
+      a0.x = fmaf(c0.x, d, a0.x);
+      a0.y = fmaf(c0.y, d, a0.y);
+      a1.x = fmaf(c1.x, d, a1.x);
+      a1.y = fmaf(c1.y, d, a1.y);
+      a2.x = fmaf(c2.x, d, a2.x);
+      a2.y = fmaf(c2.y, d, a2.y);
+      a3.x = fmaf(c3.x, d, a3.x);
+      a3.y = fmaf(c3.y, d, a3.y);
+      const double dn = fa[i] * dprev + fb[i] * (cb + sh[i]) * dcur;
+      dprev = dcur;
+      dcur = dn;
+    }
+    const int km = n - 1 - k;
+    float2* Sk = S + (size_t)k * n * Bo;
+    float2* Sm = S + (size_t)km * n * Bo;
+    Sk[(size_t)p * Bo + q] = a0;  // (a = p, b = q)
+    if (p == q) {
+      if (p > 0) Sm[(size_t)(n - p) * Bo + p] = a2;  // (-p, p) at mirrored beta
+    } else if (p == 0) {
+      Sk[(size_t)q * Bo + 0] = a1;                     // (q, 0)
+      Sk[(size_t)(n - q) * Bo + 0] = cconj(a1);        // (-q, 0) = conj((q, 0))
+    } else {
+      Sk[(size_t)q * Bo + p] = a1;                     // (q, p)
+      Sm[(size_t)(n - p) * Bo + q] = cconj(a2);        // (-p, q) = conj((p, -q))
+      Sm[(size_t)(n - q) * Bo + p] = cconj(a3);        // (-q, p) = conj((q, -p))
+    }
+  }
+}
+
+// Forward DFT over a (alpha) for a tile of b columns at one beta.
+__global__ void k_so3_fft_a(int bw_in, int bw_out, float2* __restrict__ S, FftPlan plan) {
+  extern __shared__ float2 tile[];
+  constexpr int Wt = 16;
+  const int n = 2 * bw_out, Bo = bw_out;
+  const int k = blockIdx.y;
+  const int b0 = blockIdx.x * Wt;
+  const int wt = min(Wt, bw_in - b0);
+  float2* Sk = S + (size_t)k * n * Bo;
+  for (int e = threadIdx.x; e < n * Wt; e += blockDim.x) {
+    const int a = e / Wt, bt = e % Wt;
+    // rows with |m1| >= bw_in are not synthesised: read them as zero
+    const bool row_ok = (a < bw_in) || (a > n - bw_in);
+    tile[e] = (bt < wt && row_ok) ? Sk[(size_t)a * Bo + b0 + bt] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  fft_smem<false>(tile, Wt, 1, Wt, plan);
+  for (int e = threadIdx.x; e < n * Wt; e += blockDim.x) {
+    const int a = e / Wt, bt = e % Wt;
+    if (bt < wt) Sk[(size_t)a * Bo + b0 + bt] = tile[e];
+  }
+}
+
+// Hermitian complex-to-real transform over gamma, |z|^2 and argmax.
+__global__ void k_so3_c2r(int bw_in, int bw_out, const float2* __restrict__ S, FftPlan plan,
+                          unsigned long long* __restrict__ argmax, float* __restrict__ volume) {
+  extern __shared__ float2 rows[];
+  constexpr int R = 8;
+  const int n = 2 * bw_out, Bo = bw_out;
+  const int k = blockIdx.y;
+  const int r0 = blockIdx.x * R;
+  const int nr = min(R, n - r0);
+  for (int e = threadIdx.x; e < R * n; e += blockDim.x) rows[e] = make_float2(0.f, 0.f);
+  __syncthreads();
+  for (int e = threadIdx.x; e < nr * Bo; e += blockDim.x) {
+    const int r = e / Bo, b = e % Bo;
+    float2* row = rows + r * n;
+    const float2 u = b < bw_in ? S[((size_t)k * n + r0 + r) * Bo + b] : make_float2(0.f, 0.f);
+    row[fft_freq2pos(b, plan)] = cconj(u);
+    if (b > 0) row[fft_freq2pos(n - b, plan)] = u;
+  }
+  __syncthreads();
+  fft_smem<true>(rows, R, n, 1, plan);
+  const float K = (float)((1.0 / (double)n) * ((double)bw_out / M_PI));
+  unsigned long long best = 0ull;
+  for (int e = threadIdx.x; e < R * n; e += blockDim.x) {
+    const int r = e / n, g = e % n;
+    if (r < nr) {
+      const float v = rows[e].x * K;
+      const float v2 = v * v;
+      const int alpha = fft_pos2freq(r0 + r, plan);
+      const uint32_t idx = ((uint32_t)k * n + (uint32_t)alpha) * n + g;
+      const unsigned long long key = pack_argmax(v2, idx);
+      best = key > best ? key : best;
+      if (volume) volume[idx] = v2;
+    }
+  }
+  warp_argmax_commit(best, argmax);
+}
+
+cudaError_t so3_init_attributes() {
+  const int m = 227 * 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_so3_fft_a, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_so3_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+  return e;
+}
+
+cudaError_t launch_so3(const So3Args& a, cudaStream_t st) {
+  const int ncls = a.bw_in * (a.bw_in + 1) / 2;
+  const int n = 2 * a.bw_out;
+  int thr = ((n + 31) / 32) * 32;
+  if (thr > 512) thr = 512;
+  const size_t sm1 = (size_t)a.bw_in * 3 * sizeof(double) + (size_t)a.bw_in * 4 * sizeof(float2);
+  k_so3_synth<<<ncls, thr, sm1, st>>>(a.bw_in, a.bw_out, a.fused, a.S);
+  dim3 g2((a.bw_in + 15) / 16, n);
+  k_so3_fft_a<<<g2, 256, (size_t)n * 16 * sizeof(float2), st>>>(a.bw_in, a.bw_out, a.S, *a.plan);
+  dim3 g3((n + 7) / 8, n);
+  k_so3_c2r<<<g3, 256, (size_t)8 * n * sizeof(float2), st>>>(a.bw_in, a.bw_out, a.S, *a.plan, a.argmax,
+                                                             a.volume);
+  return cudaGetLastError();
+}
+
+}  // namespace phgpu

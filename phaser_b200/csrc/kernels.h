@@ -1,0 +1,107 @@
+// Internal launch interface of the PHASER registration kernels.  Host code in
+// capi.cu owns every buffer; kernels only see raw device pointers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace phgpu {
+
+// ------------------------------------------------------------ S^2 sampling
+struct SampleArgs {
+  const float4* xyzi;   // [n_points] x, y, z, intensity
+  const float* refl;    // [n_points] or null
+  const float* amb;     // [n_points] or null
+  int n_points;
+  int max_points;       // scratch sizing
+  const float4* grid;   // [n_queries] DH grid directions (host-computed)
+  int n_queries;
+  float max_sq;         // squared voxel size (rejection threshold)
+  int n_out_ch;         // channels written (1..4)
+  float* out;           // [n_out_ch][n_queries]
+  int32_t* nn_idx;      // [n_queries] or null
+  void* scratch;        // sampler_scratch_bytes(max_points)
+};
+size_t sampler_scratch_bytes(int max_points);
+cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st);
+
+// ------------------------------------------------------------ forward SHT
+// Legendre table: for m in [0,B), l in [m,B), k in [0,2B):
+//   T[off(m) + (l-m)*2B + k] = w_k * Pbar_l^m(cos theta_k)
+size_t legendre_table_entries(int bw);
+cudaError_t launch_legendre_table(int bw, const double* weights_dev, float* table, cudaStream_t st);
+
+struct ShtArgs {
+  int bw;
+  int n_sig;              // signals (sides x channels)
+  const float* signal;    // [n_sig][2B][2B]
+  const float2* tw;       // exp(-2 pi i t / 2B), t in [0, 2B)
+  const float* table;     // Legendre table
+  float2* fm;             // scratch [n_sig][B][2B]
+  float2* coef;           // [n_sig][B (l)][B (m>=0)]
+};
+cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st);
+
+struct FuseS2Args {
+  int bw;
+  int n_data_ch;          // channels with data per side
+  int n_total_ch;         // divisor of the channel mean (reference channel count)
+  int laplace;            // 0: take channel 0 (plain SphericalCorrelation)
+  FusionBands bands;      // for n = B^2
+  const float2* coef;     // [2][n_data_ch][B][B]   (side-major)
+  float2* fused;          // [2][B (l)][2B-1 (m + B - 1)]
+};
+cudaError_t launch_fuse_s2(const FuseS2Args& a, cudaStream_t st);
+
+// ------------------------------------------------------------ SO(3)
+struct So3Args {
+  int bw_in;              // degree limit
+  int bw_out;             // output grid 2*bw_out
+  const float2* fused;    // [2][bw_in][2 bw_in - 1]
+  float2* S;              // [2 bw_out (beta)][2 bw_out (a)][bw_out (b)]
+  const FftPlan* plan;    // length 2 bw_out
+  unsigned long long* argmax;  // packed (value^2, index)
+  float* volume;          // optional (2 bw_out)^3 |z|^2, [beta][alpha][gamma]
+};
+cudaError_t launch_so3(const So3Args& a, cudaStream_t st);
+cudaError_t so3_init_attributes();  // once per device
+
+// ------------------------------------------------------------ spatial
+struct VoxelArgs {
+  const float4* xyzi;
+  const float* refl;
+  const float* amb;
+  int n_points;
+  int N;
+  const float* edges;     // [N]
+  int has_T;
+  float T[12];            // 3x4 row-major, applied in PCL order
+  int n_data_ch;          // channels accumulated (1..4) in order {int, range, refl, amb}
+  float* grids;           // [n_data_ch + 1][N^3] sums, last = count
+  uint32_t* lin_out;      // optional per-point linear index (or 0xffffffff)
+};
+cudaError_t launch_voxelize(const VoxelArgs& a, cudaStream_t st);
+
+struct SpatialArgs {
+  int N;
+  int n_data_ch;          // channels per side with data
+  int n_total_ch;         // mean divisor
+  int laplace;            // 0: plain SpatialCorrelation on channel 0
+  FusionBands bands;      // for n = N^3
+  const float* grids_f;   // [n_data_ch + 1][N^3] target sums + count (normalised here)
+  const float* grids_g;   // source
+  int grids_are_means;    // 1: grids already hold values (no count plane)
+  float2* spec;           // [2 n_data_ch][N][N][N/2+1]
+  float2* cspec;          // [N][N][N/2+1]
+  const FftPlan* plan;    // length N
+  unsigned long long* argmax;
+  float* volume;          // optional N^3 correlation, [z][x][y]
+};
+cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t st);
+cudaError_t launch_spatial_combine(const SpatialArgs& a, cudaStream_t st);
+cudaError_t spatial_init_attributes();  // once per device
+
+}  // namespace phgpu

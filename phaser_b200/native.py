@@ -1,0 +1,311 @@
+"""ctypes binding of the C ABI in include/phaser_gpu.h.
+
+Loads phaser_b200/_lib/libphaser_gpu.so (built by ``python -m phaser_b200.build``).
+There is no CPU fallback: if the library or a CUDA device is missing, every
+entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "_lib", "libphaser_gpu.so")
+
+PHGPU_OK = 0
+PHGPU_FUSION_LAPLACE = 0
+PHGPU_FUSION_NONE = 1
+PHGPU_FLAG_KEEP_VOLUMES = 1
+
+
+class PhgpuError(RuntimeError):
+    pass
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("spherical_bandwidth", C.c_uint32),
+        ("spherical_zero_padding", C.c_uint32),
+        ("spatial_n_voxels", C.c_uint32),
+        ("spatial_discretize_lower", C.c_int32),
+        ("spatial_discretize_upper", C.c_int32),
+        ("spatial_zero_padding", C.c_uint32),
+        ("spatial_low_pass_lower", C.c_float),
+        ("spatial_low_pass_upper", C.c_float),
+        ("n_channels", C.c_uint32),
+        ("fusion_levels", C.c_uint32),
+        ("spherical_fusion", C.c_uint32),
+        ("spatial_fusion", C.c_uint32),
+        ("max_points", C.c_uint32),
+        ("flags", C.c_uint32),
+        ("device", C.c_int32),
+    ]
+
+
+class Cloud(C.Structure):
+    _fields_ = [
+        ("xyzi", C.c_void_p),
+        ("reflectivity", C.c_void_p),
+        ("ambient", C.c_void_p),
+        ("n_points", C.c_uint32),
+        ("on_device", C.c_int32),
+    ]
+
+
+class Pose(C.Structure):
+    _fields_ = [
+        ("rot_bin", C.c_uint32),
+        ("rot_peak", C.c_float),
+        ("zyz", C.c_double * 3),
+        ("quat", C.c_double * 4),
+        ("xyz", C.c_double * 3),
+        ("voxel", C.c_uint32),
+        ("trans_peak", C.c_float),
+        ("trans", C.c_double * 3),
+    ]
+
+    def as_dict(self):
+        return dict(rot_bin=self.rot_bin, rot_peak=self.rot_peak, zyz=list(self.zyz),
+                    quat=list(self.quat), xyz=list(self.xyz), voxel=self.voxel,
+                    trans_peak=self.trans_peak, trans=list(self.trans))
+
+
+class ServerParams(C.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_uint64),
+        ("max_wave", C.c_uint32),
+        ("max_points", C.c_uint32),
+        ("device", C.c_int32),
+        ("flags", C.c_uint32),
+    ]
+
+
+# every symbol the header declares (checked by the CPU tests)
+EXPORTED = [
+    "phgpu_params_default", "phgpu_ctx_create", "phgpu_ctx_destroy", "phgpu_last_error",
+    "phgpu_stream", "phgpu_sample_s2", "phgpu_get_samples", "phgpu_sph_correlate",
+    "phgpu_sph_correlate_sampled", "phgpu_sph_result", "phgpu_sph_bandwidth", "phgpu_voxelize",
+    "phgpu_get_voxel_index", "phgpu_spatial_correlate", "phgpu_spatial_correlate_voxelized",
+    "phgpu_spatial_result", "phgpu_register_pair", "phgpu_pose_from_bin",
+    "phgpu_translation_from_index", "phgpu_server_create", "phgpu_server_destroy",
+    "phgpu_server_submit", "phgpu_server_poll", "phgpu_server_drain", "phgpu_server_last_error",
+]
+
+_LIB = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (no GPU needed just to load it)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise PhgpuError(f"CUDA library not built: {path} (run python -m phaser_b200.build)")
+    lib = C.CDLL(path)
+    vp = C.c_void_p
+    lib.phgpu_params_default.argtypes = [C.POINTER(Params)]
+    lib.phgpu_ctx_create.argtypes = [C.POINTER(Params), C.POINTER(vp)]
+    lib.phgpu_ctx_destroy.argtypes = [vp]
+    lib.phgpu_last_error.restype = C.c_char_p
+    lib.phgpu_last_error.argtypes = [vp]
+    lib.phgpu_stream.restype = vp
+    lib.phgpu_stream.argtypes = [vp]
+    lib.phgpu_sample_s2.argtypes = [vp, C.POINTER(Cloud), C.c_int]
+    lib.phgpu_get_samples.argtypes = [vp, C.c_int, vp, vp]
+    lib.phgpu_sph_correlate.argtypes = [vp, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_uint32]
+    lib.phgpu_sph_correlate_sampled.argtypes = [vp]
+    lib.phgpu_sph_result.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_float), vp]
+    lib.phgpu_sph_bandwidth.restype = C.c_uint32
+    lib.phgpu_sph_bandwidth.argtypes = [vp]
+    lib.phgpu_voxelize.argtypes = [vp, C.POINTER(Cloud), C.c_int, vp]
+    lib.phgpu_get_voxel_index.argtypes = [vp, C.c_int, vp, C.c_uint32]
+    lib.phgpu_spatial_correlate.argtypes = [vp, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_uint32]
+    lib.phgpu_spatial_correlate_voxelized.argtypes = [vp]
+    lib.phgpu_spatial_result.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_float), vp]
+    lib.phgpu_register_pair.argtypes = [vp, C.POINTER(Cloud), C.POINTER(Cloud), C.POINTER(Pose)]
+    lib.phgpu_pose_from_bin.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp, vp]
+    lib.phgpu_translation_from_index.restype = C.c_double
+    lib.phgpu_translation_from_index.argtypes = [C.c_double, C.c_uint32, C.c_int32, C.c_int32]
+    lib.phgpu_server_create.argtypes = [C.POINTER(ServerParams), C.POINTER(vp)]
+    lib.phgpu_server_destroy.argtypes = [vp]
+    lib.phgpu_server_submit.argtypes = [vp, C.POINTER(Params), C.POINTER(Cloud), C.POINTER(Cloud),
+                                        C.POINTER(C.c_uint64)]
+    lib.phgpu_server_poll.argtypes = [vp, C.c_uint64, C.POINTER(Pose), C.POINTER(C.c_double)]
+    lib.phgpu_server_drain.argtypes = [vp]
+    lib.phgpu_server_last_error.restype = C.c_char_p
+    lib.phgpu_server_last_error.argtypes = [vp]
+    _LIB = lib
+    return lib
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    load().phgpu_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _addr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    # torch tensor
+    return a.data_ptr()
+
+
+def make_cloud(xyzi, reflectivity=None, ambient=None) -> tuple[Cloud, list]:
+    """Build a phgpu_cloud from numpy arrays (host) or torch CUDA tensors."""
+    keep = []
+    on_dev = 0
+    try:
+        import torch
+        if isinstance(xyzi, torch.Tensor) and xyzi.is_cuda:
+            on_dev = 1
+    except Exception:  # pragma: no cover - torch is always present here
+        pass
+    if not on_dev:
+        xyzi = np.ascontiguousarray(xyzi, np.float32)
+        reflectivity = None if reflectivity is None else np.ascontiguousarray(reflectivity, np.float32)
+        ambient = None if ambient is None else np.ascontiguousarray(ambient, np.float32)
+    keep += [xyzi, reflectivity, ambient]
+    n = int(xyzi.shape[0])
+    c = Cloud(_addr(xyzi), _addr(reflectivity), _addr(ambient), n, on_dev)
+    return c, keep
+
+
+def translation_from_index(index, n_voxels, lower, upper) -> float:
+    return load().phgpu_translation_from_index(float(index), int(n_voxels), int(lower), int(upper))
+
+
+def pose_from_bin(bin_, bw_out):
+    zyz = np.zeros(3)
+    q = np.zeros(4)
+    xyz = np.zeros(3)
+    T = np.zeros(12, np.float32)
+    load().phgpu_pose_from_bin(int(bin_), int(bw_out), zyz.ctypes.data, q.ctypes.data, xyz.ctypes.data,
+                               T.ctypes.data)
+    return zyz, q, xyz, T.reshape(3, 4)
+
+
+class Context:
+    """One configuration's device state (C ABI phgpu_ctx)."""
+
+    def __init__(self, params: Params | None = None, **kw):
+        lib = load()
+        self.params = params if params is not None else default_params(**kw)
+        if params is not None:
+            for k, v in kw.items():
+                setattr(self.params, k, v)
+        h = C.c_void_p()
+        rc = lib.phgpu_ctx_create(C.byref(self.params), C.byref(h))
+        if rc != PHGPU_OK:
+            raise PhgpuError(f"phgpu_ctx_create failed ({rc}): {lib.phgpu_last_error(None).decode()}")
+        self.h = h
+        self.lib = lib
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.phgpu_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc):
+        if rc != PHGPU_OK:
+            raise PhgpuError(f"phaser_gpu error {rc}: {self.lib.phgpu_last_error(self.h).decode()}")
+
+    @property
+    def bw(self):
+        return self.params.spherical_bandwidth
+
+    @property
+    def bw_out(self):
+        return self.params.spherical_bandwidth + self.params.spherical_zero_padding
+
+    @property
+    def n_voxels(self):
+        return self.params.spatial_n_voxels
+
+    @property
+    def stream(self):
+        return self.lib.phgpu_stream(self.h)
+
+    # ---- sampling
+    def sample_s2(self, xyzi, reflectivity=None, ambient=None, side=0):
+        c, keep = make_cloud(xyzi, reflectivity, ambient)
+        self.check(self.lib.phgpu_sample_s2(self.h, C.byref(c), side))
+
+    def samples(self, side):
+        nq = 4 * self.bw * self.bw
+        v = np.zeros(4 * nq)
+        idx = np.zeros(nq, np.int32)
+        self.check(self.lib.phgpu_get_samples(self.h, side, v.ctypes.data, idx.ctypes.data))
+        return v.reshape(4, nq), idx
+
+    # ---- rotation
+    def sph_correlate(self, f, g):
+        f = [np.ascontiguousarray(x, np.float64) for x in f]
+        g = [np.ascontiguousarray(x, np.float64) for x in g]
+        fp = (C.c_void_p * len(f))(*[x.ctypes.data for x in f])
+        gp = (C.c_void_p * len(g))(*[x.ctypes.data for x in g])
+        self.check(self.lib.phgpu_sph_correlate(self.h, fp, gp, len(f)))
+
+    def sph_correlate_sampled(self):
+        self.check(self.lib.phgpu_sph_correlate_sampled(self.h))
+
+    def sph_result(self, volume=False):
+        b = C.c_uint32()
+        pk = C.c_float()
+        vol = np.zeros((2 * self.bw_out) ** 3) if volume else None
+        self.check(self.lib.phgpu_sph_result(self.h, C.byref(b), C.byref(pk),
+                                             None if vol is None else vol.ctypes.data))
+        return (b.value, pk.value, vol) if volume else (b.value, pk.value)
+
+    # ---- translation
+    def voxelize(self, xyzi, reflectivity=None, ambient=None, side=0, T=None):
+        c, keep = make_cloud(xyzi, reflectivity, ambient)
+        Tp = None
+        if T is not None:
+            T = np.ascontiguousarray(T, np.float32).reshape(12)
+            Tp = T.ctypes.data
+        self.check(self.lib.phgpu_voxelize(self.h, C.byref(c), side, Tp))
+
+    def voxel_index(self, side, n_points):
+        out = np.zeros(n_points, np.uint32)
+        self.check(self.lib.phgpu_get_voxel_index(self.h, side, out.ctypes.data, n_points))
+        return out
+
+    def spatial_correlate(self, f, g):
+        f = [np.ascontiguousarray(x, np.float64) for x in f]
+        g = [np.ascontiguousarray(x, np.float64) for x in g]
+        fp = (C.c_void_p * len(f))(*[x.ctypes.data for x in f])
+        gp = (C.c_void_p * len(g))(*[x.ctypes.data for x in g])
+        self.check(self.lib.phgpu_spatial_correlate(self.h, fp, gp, len(f)))
+
+    def spatial_correlate_voxelized(self):
+        self.check(self.lib.phgpu_spatial_correlate_voxelized(self.h))
+
+    def spatial_result(self, volume=False):
+        v = C.c_uint32()
+        pk = C.c_float()
+        vol = np.zeros(self.n_voxels ** 3) if volume else None
+        self.check(self.lib.phgpu_spatial_result(self.h, C.byref(v), C.byref(pk),
+                                                 None if vol is None else vol.ctypes.data))
+        return (v.value, pk.value, vol) if volume else (v.value, pk.value)
+
+    # ---- full pipeline
+    def register_pair(self, target, source) -> Pose:
+        """target/source: (xyzi, reflectivity) tuples of numpy arrays or torch CUDA tensors."""
+        ct, k1 = make_cloud(*target)
+        cs, k2 = make_cloud(*source)
+        pose = Pose()
+        self.check(self.lib.phgpu_register_pair(self.h, C.byref(ct), C.byref(cs), C.byref(pose)))
+        return pose
