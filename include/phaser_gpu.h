@@ -154,6 +154,19 @@ int phgpu_pose_from_bin(uint32_t bin, uint32_t bw_out, double* zyz, double* quat
 double phgpu_translation_from_index(double index, uint32_t n_voxels, int32_t lower,
                                     int32_t upper);
 
+/* ------------------------------------------------------------------ tracing
+ * Per-stage device time measured with CUDA events on each stage's launching
+ * stream (the reference times stages on the host clock,
+ * phaser_common/include/phaser/common/statistic-utils.h:10-18). */
+int phgpu_profile_enable(phgpu_ctx* ctx, int enable);
+/* Accumulated milliseconds and call counts per stage since the last read
+ * (synchronises the context's streams; resets the accumulators). */
+int phgpu_profile_read(phgpu_ctx* ctx, double* ms, unsigned long long* calls, int n);
+int phgpu_profile_stage_count(void);
+const char* phgpu_profile_stage_name(int stage);
+/* Kernels launched by this library since it was loaded (all contexts). */
+unsigned long long phgpu_launch_count(void);
+
 /* ------------------------------------------------------------------ serving
  * Continuous-batching request server (no reference counterpart: the
  * reference registers one pair at a time, sph-opt-registration.cc:34-47).
@@ -171,8 +184,10 @@ typedef struct {
 
 int phgpu_server_create(const phgpu_server_params* params, phgpu_server** out);
 int phgpu_server_destroy(phgpu_server* srv);
-/* Submits one pair; params gives the shape (bandwidth, voxels, bounds).  The
- * clouds are copied before the call returns.  *ticket identifies the request. */
+/* Submits one pair; params gives the shape (bandwidth, voxels, bounds).  Host
+ * clouds are copied before the call returns; device clouds (on_device = 1 for
+ * both) are read in place and must stay valid until the ticket completes.
+ * *ticket identifies the request. */
 int phgpu_server_submit(phgpu_server* srv, const phgpu_params* params, const phgpu_cloud* target,
                         const phgpu_cloud* source, uint64_t* ticket);
 /* Non-blocking: 1 and the pose when the ticket finished, 0 otherwise. */

@@ -50,8 +50,15 @@ bool make_fft_plan(int n, FftPlan* p, float2** d_tw, std::string* err) {
       m /= r;
     }
   }
+  for (int r = 17; m > 1 && r <= kMaxGenericRadix && ns < kMaxFftStages; r += 2) {
+    while (m % r == 0 && ns < kMaxFftStages) {
+      p->radix[ns++] = r;
+      m /= r;
+    }
+  }
   if (m != 1 || n < 1) {
-    *err = "FFT length " + std::to_string(n) + " has a prime factor above 13 (unsupported)";
+    *err = "FFT length " + std::to_string(n) + " has a prime factor above " +
+           std::to_string(kMaxGenericRadix) + " (unsupported)";
     return false;
   }
   p->nstage = ns;
@@ -173,6 +180,74 @@ double phgpu_translation_from_index(double index, uint32_t n_voxels, int32_t low
   if (index <= half) return index * width / n_voxels;
   return (index - n_voxels) * width / n_voxels;
 }
+
+// ------------------------------------------------------------------ profiler
+
+static cudaEvent_t pool_event(phgpu_ctx* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+ProfScope::ProfScope(phgpu_ctx* ctx, cudaStream_t st, int stg) : c(ctx), s(st), stage(stg) {
+  if (c->prof_on) {
+    a = pool_event(c);
+    cudaEventRecord(a, s);
+  }
+}
+
+ProfScope::~ProfScope() {
+  if (!a) return;
+  cudaEvent_t b = pool_event(c);
+  cudaEventRecord(b, s);
+  c->prof_recs.push_back(ProfRec{stage, a, b});
+}
+
+static const char* kStageNames[PS_COUNT] = {"upload", "s2_sample", "sht", "fuse_s2", "so3_synth",
+                                            "so3_fft", "voxelize", "spatial_fwd", "fuse_z", "spatial_inv"};
+
+int phgpu_profile_enable(phgpu_ctx* ctx, int enable) {
+  if (!ctx) return PHGPU_ERR_INVALID;
+  ctx->prof_on = enable != 0;
+  return PHGPU_OK;
+}
+
+int phgpu_profile_read(phgpu_ctx* ctx, double* ms, unsigned long long* calls, int n) {
+  if (!ctx) return PHGPU_ERR_INVALID;
+  cudaSetDevice(ctx->prm.device);
+  CK(cudaStreamSynchronize(ctx->s0));
+  CK(cudaStreamSynchronize(ctx->s1));
+  for (const ProfRec& r : ctx->prof_recs) {
+    float t = 0.0f;
+    if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+      ctx->prof_ms[r.stage] += t;
+      ctx->prof_n[r.stage] += 1;
+    }
+    ctx->ev_pool.push_back(r.a);
+    ctx->ev_pool.push_back(r.b);
+  }
+  ctx->prof_recs.clear();
+  for (int i = 0; i < n && i < PS_COUNT; ++i) {
+    if (ms) ms[i] = ctx->prof_ms[i];
+    if (calls) calls[i] = ctx->prof_n[i];
+    ctx->prof_ms[i] = 0.0;
+    ctx->prof_n[i] = 0;
+  }
+  return PHGPU_OK;
+}
+
+const char* phgpu_profile_stage_name(int stage) {
+  return (stage >= 0 && stage < PS_COUNT) ? kStageNames[stage] : "";
+}
+
+int phgpu_profile_stage_count(void) { return PS_COUNT; }
+
+unsigned long long phgpu_launch_count(void) { return g_launch_count.load(); }
 
 // ------------------------------------------------------------------ context
 
@@ -298,6 +373,13 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
     ctx->err = perr;
     return PHGPU_ERR_INVALID;
   }
+  if (spatial_slab_path(N)) {
+    if (!make_fft_plan(N / 2, &ctx->plan_sp_half, &ctx->d_tw[3], &perr)) {
+      ctx->err = perr;
+      return PHGPU_ERR_INVALID;
+    }
+    ctx->has_sp_half = true;
+  }
   ctx->bands_s2 = make_bands((uint32_t)(bw * bw), (int)prm->fusion_levels, 4.0f);
   ctx->bands_sp = make_bands((uint32_t)N * (uint32_t)N * (uint32_t)N, (int)prm->fusion_levels, 4.0f);
   // DH grid directions (spherical-sampler.cc:29-64), float sin/cos of float angles
@@ -350,7 +432,7 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   CKV(dalloc(ctx, &ctx->d_S, sizeof(float2) * no * no * bw_out));
   CK(cudaMemset(ctx->d_S, 0, sizeof(float2) * no * no * bw_out));
   const size_t nv = (size_t)N * N * N;
-  const size_t H = (size_t)N * N * (N / 2 + 1);
+  const size_t H = (size_t)N * N * spatial_h2p(N);
   for (int s = 0; s < 2; ++s) CKV(dalloc(ctx, &ctx->d_grids[s], sizeof(float) * 5 * nv));
   CKV(dalloc(ctx, &ctx->d_spec, sizeof(float2) * 8 * H));
   CKV(dalloc(ctx, &ctx->d_cspec, sizeof(float2) * H));
@@ -373,9 +455,14 @@ int phgpu_ctx_destroy(phgpu_ctx* ctx) {
   if (ctx->s1) cudaStreamSynchronize(ctx->s1);
   for (void* p : ctx->allocs) cudaFree(p);
   ctx->allocs.clear();
-  for (int i = 0; i < 3; ++i)
+  for (int i = 0; i < 4; ++i)
     if (ctx->d_tw[i]) cudaFree(ctx->d_tw[i]);
   if (ctx->h_argmax) cudaFreeHost(ctx->h_argmax);
+  for (const ProfRec& r : ctx->prof_recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
   if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
   if (ctx->s0) cudaStreamDestroy(ctx->s0);
@@ -421,7 +508,10 @@ static int run_sample(phgpu_ctx* ctx, int side, cudaStream_t st) {
   a.out = ctx->d_samples + (size_t)side * 4 * a.n_queries;
   a.nn_idx = ctx->d_nn[side];
   a.scratch = ctx->d_sample_scratch[side];
-  CK(launch_sample(a, st));
+  {
+    ProfScope ps(ctx, st, PS_SAMPLE);
+    CK(launch_sample(a, st));
+  }
   ctx->sampled[side] = true;
   return PHGPU_OK;
 }
@@ -466,6 +556,7 @@ int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStre
     s.table = ctx->d_legendre;
     s.fm = ctx->d_fm + (size_t)side * 4 * bw * 2 * bw;
     s.coef = ctx->d_coef + (size_t)side * n_data * bw * bw;
+    ProfScope ps(ctx, st, PS_SHT);
     CK(launch_sht(s, st));
   }
   FuseS2Args f;
@@ -476,7 +567,10 @@ int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStre
   f.bands = ctx->bands_s2;
   f.coef = ctx->d_coef;
   f.fused = ctx->d_fused;
-  CK(launch_fuse_s2(f, st));
+  {
+    ProfScope ps(ctx, st, PS_FUSE_S2);
+    CK(launch_fuse_s2(f, st));
+  }
   CK(cudaMemsetAsync(ctx->d_argmax, 0, sizeof(unsigned long long), st));
   So3Args o;
   o.bw_in = bw;
@@ -486,7 +580,14 @@ int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStre
   o.plan = &ctx->plan_so3;
   o.argmax = ctx->d_argmax;
   o.volume = ctx->d_rotvol;
-  CK(launch_so3(o, st));
+  {
+    ProfScope ps(ctx, st, PS_SO3_SYNTH);
+    CK(launch_so3_synth(o, st));
+  }
+  {
+    ProfScope ps(ctx, st, PS_SO3_FFT);
+    CK(launch_so3_fft(o, st));
+  }
   CK(cudaMemcpyAsync(ctx->h_argmax, ctx->d_argmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   ctx->have_rot = true;
   return PHGPU_OK;
@@ -569,7 +670,10 @@ int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, c
   v.n_data_ch = n_data;
   v.grids = ctx->d_grids[side];
   v.lin_out = ctx->d_lin[side];
-  CK(launch_voxelize(v, st));
+  {
+    ProfScope ps(ctx, st, PS_VOXELIZE);
+    CK(launch_voxelize(v, st));
+  }
   ctx->vox_ch[side] = n_data;
   ctx->voxelized[side] = true;
   return PHGPU_OK;
@@ -608,6 +712,7 @@ static SpatialArgs spatial_args(phgpu_ctx* ctx, int n_data, int n_total, int lap
   a.spec = ctx->d_spec;
   a.cspec = ctx->d_cspec;
   a.plan = &ctx->plan_sp;
+  a.plan_half = ctx->has_sp_half ? &ctx->plan_sp_half : nullptr;
   a.argmax = ctx->d_argmax + 1;
   a.volume = ctx->d_transvol;
   return a;
@@ -615,10 +720,20 @@ static SpatialArgs spatial_args(phgpu_ctx* ctx, int n_data, int n_total, int lap
 
 int phgpu_run_spatial(phgpu_ctx* ctx, int n_data, int n_total, int laplace, int means, cudaStream_t st) {
   SpatialArgs a = spatial_args(ctx, n_data, n_total, laplace, means);
-  CK(launch_spatial_forward(a, 0, st));
-  CK(launch_spatial_forward(a, 1, st));
+  {
+    ProfScope ps(ctx, st, PS_SPATIAL_FWD);
+    CK(launch_spatial_forward(a, 0, st));
+    CK(launch_spatial_forward(a, 1, st));
+  }
   CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), st));
-  CK(launch_spatial_combine(a, st));
+  {
+    ProfScope ps(ctx, st, PS_FUSE_Z);
+    CK(launch_spatial_fuse_z(a, st));
+  }
+  {
+    ProfScope ps(ctx, st, PS_SPATIAL_INV);
+    CK(launch_spatial_inverse(a, st));
+  }
   CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, sizeof(unsigned long long),
                      cudaMemcpyDeviceToHost, st));
   ctx->have_trans = true;
@@ -690,8 +805,11 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
   if (!ctx || !target || !source || !out) return PHGPU_ERR_INVALID;
   cudaSetDevice(ctx->prm.device);
   cudaStream_t s0 = ctx->s0, s1 = ctx->s1;
-  CKV(phgpu_upload_cloud(ctx, target, 0, s0));
-  CKV(phgpu_upload_cloud(ctx, source, 1, s0));
+  {
+    ProfScope ps(ctx, s0, PS_UPLOAD);
+    CKV(phgpu_upload_cloud(ctx, target, 0, s0));
+    CKV(phgpu_upload_cloud(ctx, source, 1, s0));
+  }
   const int laplace_s2 = ctx->prm.spherical_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
   const int laplace_sp = ctx->prm.spatial_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
   const int nd_s2 = std::max(s2_channels(target), s2_channels(source));
@@ -702,7 +820,10 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
   CK(cudaStreamWaitEvent(s1, ctx->ev_a, 0));
   CKV(phgpu_run_voxelize(ctx, 0, nullptr, nd_sp, s1));
   SpatialArgs sa = spatial_args(ctx, nd_sp, (int)ctx->prm.n_channels, laplace_sp, 0);
-  CK(launch_spatial_forward(sa, 0, s1));
+  {
+    ProfScope ps(ctx, s1, PS_SPATIAL_FWD);
+    CK(launch_spatial_forward(sa, 0, s1));
+  }
   CK(cudaEventRecord(ctx->ev_b, s1));
   // rotation
   CKV(run_sample(ctx, 0, s0));
@@ -716,10 +837,20 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
   phgpu_pose_from_bin(out->rot_bin, (uint32_t)ctx->bw_out, out->zyz, out->quat, out->xyz, T);
   // translation of the rotated source
   CKV(phgpu_run_voxelize(ctx, 1, T, nd_sp, s0));
-  CK(launch_spatial_forward(sa, 1, s0));
+  {
+    ProfScope ps(ctx, s0, PS_SPATIAL_FWD);
+    CK(launch_spatial_forward(sa, 1, s0));
+  }
   CK(cudaStreamWaitEvent(s0, ctx->ev_b, 0));
   CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), s0));
-  CK(launch_spatial_combine(sa, s0));
+  {
+    ProfScope ps(ctx, s0, PS_FUSE_Z);
+    CK(launch_spatial_fuse_z(sa, s0));
+  }
+  {
+    ProfScope ps(ctx, s0, PS_SPATIAL_INV);
+    CK(launch_spatial_inverse(sa, s0));
+  }
   CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, sizeof(unsigned long long),
                      cudaMemcpyDeviceToHost, s0));
   ctx->have_trans = true;

@@ -10,6 +10,26 @@
 #include "../../include/phaser_gpu.h"
 #include "kernels.h"
 
+// Stages timed by the optional per-stage profiler (phgpu_profile_*).
+enum ProfStage {
+  PS_UPLOAD = 0,
+  PS_SAMPLE,
+  PS_SHT,
+  PS_FUSE_S2,
+  PS_SO3_SYNTH,
+  PS_SO3_FFT,
+  PS_VOXELIZE,
+  PS_SPATIAL_FWD,
+  PS_FUSE_Z,
+  PS_SPATIAL_INV,
+  PS_COUNT
+};
+
+struct ProfRec {
+  int stage;
+  cudaEvent_t a, b;
+};
+
 struct phgpu_ctx {
   phgpu_params prm;
   int bw = 0, bw_out = 0, N = 0;
@@ -18,8 +38,9 @@ struct phgpu_ctx {
   cudaStream_t s0 = nullptr, s1 = nullptr;
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
   // plans and tables
-  phgpu::FftPlan plan_s2, plan_so3, plan_sp;
-  float2* d_tw[3] = {nullptr, nullptr, nullptr};
+  phgpu::FftPlan plan_s2, plan_so3, plan_sp, plan_sp_half;
+  bool has_sp_half = false;
+  float2* d_tw[4] = {nullptr, nullptr, nullptr, nullptr};
   phgpu::FusionBands bands_s2, bands_sp;
   float4* d_grid = nullptr;
   double* d_weights = nullptr;
@@ -54,9 +75,25 @@ struct phgpu_ctx {
   bool sampled[2] = {false, false};
   bool voxelized[2] = {false, false};
   bool have_rot = false, have_trans = false;
+  // profiler
+  bool prof_on = false;
+  std::vector<ProfRec> prof_recs;
+  std::vector<cudaEvent_t> ev_pool;
+  double prof_ms[PS_COUNT] = {0};
+  unsigned long long prof_n[PS_COUNT] = {0};
   // bookkeeping
   std::vector<void*> allocs;
   size_t device_bytes = 0;
+};
+
+// Records start/end events of one stage on its stream when profiling is on.
+struct ProfScope {
+  phgpu_ctx* c;
+  cudaStream_t s;
+  int stage;
+  cudaEvent_t a = nullptr;
+  ProfScope(phgpu_ctx* ctx, cudaStream_t st, int stg);
+  ~ProfScope();
 };
 
 int phgpu_ctx_init(phgpu_ctx* ctx);

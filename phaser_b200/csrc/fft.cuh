@@ -181,6 +181,49 @@ __device__ __forceinline__ void fft_stage(float2* buf, int ntrans, int tstride, 
   }
 }
 
+// Radix-R stage for any R <= kMaxGenericRadix (rare lengths with a large prime
+// factor): O(R^2) butterfly through a local buffer, twiddles from the table.
+constexpr int kMaxGenericRadix = 128;
+
+template <bool INV>
+__device__ __noinline__ void fft_stage_generic(float2* buf, int R, int ntrans, int tstride, int estride, int n,
+                                               int L, const float2* __restrict__ tw, int tid, int nthr) {
+  const int m = L / R;
+  const int nb = n / R;
+  const int total = ntrans * nb;
+  const int twstep = n / L;
+  const int es = m * estride;
+  const int rstep = n / R;
+  float2 x[kMaxGenericRadix];
+  for (int it = tid; it < total; it += nthr) {
+    int t, bf;
+    if (estride == 1) {
+      t = it / nb;
+      bf = it - t * nb;
+    } else {
+      bf = it / ntrans;
+      t = it - bf * ntrans;
+    }
+    const int blk = bf / m;
+    const int j2 = bf - blk * m;
+    float2* base = buf + t * tstride + (blk * L + j2) * estride;
+    for (int j = 0; j < R; ++j) {
+      x[j] = base[j * es];
+      if (INV && j > 0) x[j] = cmul(x[j], cconj(__ldg(&tw[twstep * j2 * j])));
+    }
+    for (int k = 0; k < R; ++k) {
+      float2 acc = x[0];
+      for (int j = 1; j < R; ++j) {
+        float2 w = __ldg(&tw[rstep * ((j * k) % R)]);
+        if (INV) w = cconj(w);
+        acc = cadd(acc, cmul(x[j], w));
+      }
+      if (!INV && k > 0) acc = cmul(acc, __ldg(&tw[twstep * j2 * k]));
+      base[k * es] = acc;
+    }
+  }
+}
+
 // Batched in-place transform.  Caller synchronises before; the function ends
 // with __syncthreads().  All threads of the block must call it.
 template <bool INV>
@@ -199,10 +242,220 @@ __device__ void fft_smem(float2* buf, int ntrans, int tstride, int estride, cons
       case 8: fft_stage<8, INV>(buf, ntrans, tstride, estride, p.n, L, p.tw, tid, nthr); break;
       case 11: fft_stage<11, INV>(buf, ntrans, tstride, estride, p.n, L, p.tw, tid, nthr); break;
       case 13: fft_stage<13, INV>(buf, ntrans, tstride, estride, p.n, L, p.tw, tid, nthr); break;
-      default: break;
+      default:
+        fft_stage_generic<INV>(buf, p.radix[s], ntrans, tstride, estride, p.n, L, p.tw, tid, nthr);
+        break;
     }
     __syncthreads();
   }
 }
+
+// ------------------------------------------------------------------------
+// Compile-time plans for the lengths the workloads use.  The factorisation
+// matches the host planner (radix 8 first, then 4, 2, 5, 3) so positions and
+// frequencies agree with the runtime plan of the same length.
+template <int N>
+struct FixedFft {
+  static constexpr int count = 0;
+};
+template <>
+struct FixedFft<16> {
+  static constexpr int count = 2;
+  static constexpr int r[2] = {8, 2};
+};
+template <>
+struct FixedFft<32> {
+  static constexpr int count = 2;
+  static constexpr int r[2] = {8, 4};
+};
+template <>
+struct FixedFft<100> {
+  static constexpr int count = 3;
+  static constexpr int r[3] = {4, 5, 5};
+};
+template <>
+struct FixedFft<64> {
+  static constexpr int count = 2;
+  static constexpr int r[2] = {8, 8};
+};
+template <>
+struct FixedFft<128> {
+  static constexpr int count = 3;
+  static constexpr int r[3] = {8, 8, 2};
+};
+template <>
+struct FixedFft<200> {
+  static constexpr int count = 3;
+  static constexpr int r[3] = {8, 5, 5};
+};
+template <>
+struct FixedFft<256> {
+  static constexpr int count = 3;
+  static constexpr int r[3] = {8, 8, 4};
+};
+template <>
+struct FixedFft<512> {
+  static constexpr int count = 3;
+  static constexpr int r[3] = {8, 8, 8};
+};
+
+template <int N>
+constexpr bool fixed_fft_supported() {
+  return FixedFft<N>::count > 0;
+}
+
+template <int N, int S>
+__host__ __device__ constexpr int fixed_L() {
+  if constexpr (S == 0) {
+    return N;
+  } else {
+    return fixed_L<N, S - 1>() / FixedFft<N>::r[S - 1];
+  }
+}
+
+template <int N, int S = 0>
+__host__ __device__ __forceinline__ int fixed_freq2pos(int k) {
+  if constexpr (S >= FixedFft<N>::count) {
+    return 0;
+  } else {
+    constexpr int r = FixedFft<N>::r[S];
+    constexpr int m = fixed_L<N, S>() / r;
+    return (k % r) * m + fixed_freq2pos<N, S + 1>(k / r);
+  }
+}
+
+template <int N, int S = 0>
+__host__ __device__ __forceinline__ int fixed_pos2freq(int pos) {
+  if constexpr (S >= FixedFft<N>::count) {
+    return 0;
+  } else {
+    constexpr int r = FixedFft<N>::r[S];
+    constexpr int m = fixed_L<N, S>() / r;
+    return (pos / m) + r * fixed_pos2freq<N, S + 1>(pos % m);
+  }
+}
+
+// One stage with compile-time length, radix and block length.  LOG2T >= 0:
+// column mode with 2^LOG2T transforms and the transform index fastest;
+// LOG2T < 0: row mode (estride 1), butterfly index fastest.
+template <int N, int R, int L, bool INV, int LOG2T>
+__device__ __forceinline__ void fixed_stage(float2* buf, int ntrans, int tstride, int estride,
+                                            const float2* __restrict__ tw, int tid, int nthr) {
+  constexpr int m = L / R;
+  constexpr int nb = N / R;
+  constexpr int twstep = N / L;
+  const int total = ntrans * nb;
+  const int es = m * estride;
+  for (int it = tid; it < total; it += nthr) {
+    int t, bf;
+    if constexpr (LOG2T >= 0) {
+      bf = it >> LOG2T;
+      t = it & ((1 << LOG2T) - 1);
+    } else if constexpr (LOG2T == -2) {
+      bf = it / ntrans;
+      t = it - bf * ntrans;
+    } else {
+      t = it / nb;
+      bf = it - t * nb;
+    }
+    const int blk = bf / m;
+    const int j2 = bf - blk * m;
+    float2* base = buf + t * tstride + (blk * L + j2) * estride;
+    float2 x[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) x[j] = base[j * es];
+    if constexpr (INV) {
+#pragma unroll
+      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], cconj(__ldg(&tw[twstep * j2 * k])));
+      dft_small<R, true>(x);
+    } else {
+      dft_small<R, false>(x);
+#pragma unroll
+      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], __ldg(&tw[twstep * j2 * k]));
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) base[j * es] = x[j];
+  }
+}
+
+template <int N, bool INV, int LOG2T, int SI = 0>
+__device__ __forceinline__ void fixed_stages(float2* buf, int ntrans, int tstride, int estride,
+                                             const float2* __restrict__ tw, int tid, int nthr) {
+  if constexpr (SI < FixedFft<N>::count) {
+    constexpr int S = INV ? (FixedFft<N>::count - 1 - SI) : SI;
+    fixed_stage<N, FixedFft<N>::r[S], fixed_L<N, S>(), INV, LOG2T>(buf, ntrans, tstride, estride, tw, tid, nthr);
+    __syncthreads();
+    fixed_stages<N, INV, LOG2T, SI + 1>(buf, ntrans, tstride, estride, tw, tid, nthr);
+  }
+}
+
+// Batched in-place transform with a compile-time plan (same contract as
+// fft_smem).  LOG2T >= 0: columns, ntrans == 2^LOG2T; LOG2T == -2: columns,
+// any ntrans; LOG2T == -1: rows (estride 1).
+template <int N, bool INV, int LOG2T = -1>
+__device__ __forceinline__ void fft_fixed(float2* buf, int ntrans, int tstride, int estride,
+                                          const float2* __restrict__ tw) {
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nthr = blockDim.x * blockDim.y * blockDim.z;
+  fixed_stages<N, INV, LOG2T>(buf, ntrans, tstride, estride, tw, tid, nthr);
+}
+
+// Dispatch helpers: NF > 0 uses the compile-time plan of length NF, NF == 0
+// the runtime plan.
+template <int NF, bool INV, int LOG2T = -1>
+__device__ __forceinline__ void fft_any(float2* buf, int ntrans, int tstride, int estride, const FftPlan& p) {
+  if constexpr (NF > 0) {
+    fft_fixed<NF, INV, LOG2T>(buf, ntrans, tstride, estride, p.tw);
+  } else {
+    fft_smem<INV>(buf, ntrans, tstride, estride, p);
+  }
+}
+
+template <int NF>
+__device__ __forceinline__ int freq2pos(int k, const FftPlan& p) {
+  if constexpr (NF > 0) {
+    return fixed_freq2pos<NF>(k);
+  } else {
+    return fft_freq2pos(k, p);
+  }
+}
+
+template <int NF>
+__device__ __forceinline__ int pos2freq(int pos, const FftPlan& p) {
+  if constexpr (NF > 0) {
+    return fixed_pos2freq<NF>(pos);
+  } else {
+    return fft_pos2freq(pos, p);
+  }
+}
+
+// Host dispatch of a kernel template on the transform length.
+#define PHGPU_DISPATCH_N(n, ...)            \
+  switch (n) {                              \
+    case 64: {                              \
+      constexpr int NF = 64;                \
+      __VA_ARGS__;                          \
+    } break;                                \
+    case 128: {                             \
+      constexpr int NF = 128;               \
+      __VA_ARGS__;                          \
+    } break;                                \
+    case 200: {                             \
+      constexpr int NF = 200;               \
+      __VA_ARGS__;                          \
+    } break;                                \
+    case 256: {                             \
+      constexpr int NF = 256;               \
+      __VA_ARGS__;                          \
+    } break;                                \
+    case 512: {                             \
+      constexpr int NF = 512;               \
+      __VA_ARGS__;                          \
+    } break;                                \
+    default: {                              \
+      constexpr int NF = 0;                 \
+      __VA_ARGS__;                          \
+    } break;                                \
+  }
 
 }  // namespace phgpu

@@ -64,38 +64,82 @@ __global__ void k_project(const float4* __restrict__ xyzi, int P, float4* __rest
   const float oy = (float)__dmul_rn(st, sp);
   proj[i] = make_float4(ox, oy, oz, 0.0f);
   range[i] = dist;
+  // points at the origin or with non-finite coordinates have no direction:
+  // they are left out of the search structure
+  if (!(isfinite(ox) && isfinite(oy) && isfinite(oz))) {
+    key[i] = 0xffffffffu;
+    return;
+  }
   const uint32_t k = cell_key(ox, oy, oz);
   key[i] = k;
   atomicAdd(&cell_count[k], 1u);
 }
 
-// Exclusive scan of the 32768 fine-cell counts (one block of 1024 threads).
-__global__ void k_cell_scan(const uint32_t* __restrict__ count, uint32_t* __restrict__ start) {
-  __shared__ uint32_t part[1024];
-  const int t = threadIdx.x;
+// Exclusive scan of the 32768 fine-cell counts (one block of 1024 threads,
+// 32 consecutive cells per thread) and the compact list of non-empty coarse
+// cells {start, count, coarse id}.
+__global__ void __launch_bounds__(1024) k_cell_scan(const uint32_t* __restrict__ count, uint32_t* __restrict__ start,
+                                                    uint4* __restrict__ clist, uint32_t* __restrict__ n_coarse) {
+  __shared__ uint32_t wsum[32];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   constexpr int per = kFineCells / 1024;
   uint32_t local[per];
+  const uint4* src = reinterpret_cast<const uint4*>(count + t * per);
   uint32_t s = 0;
 #pragma unroll
-  for (int j = 0; j < per; ++j) {
-    local[j] = count[t * per + j];
-    s += local[j];
+  for (int j = 0; j < per / 4; ++j) {
+    const uint4 v = src[j];
+    local[4 * j] = v.x;
+    local[4 * j + 1] = v.y;
+    local[4 * j + 2] = v.z;
+    local[4 * j + 3] = v.w;
+    s += v.x + v.y + v.z + v.w;
   }
-  part[t] = s;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    const uint32_t v = t >= off ? part[t - off] : 0u;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
-  }
-  uint32_t run = part[t] - s;
+  uint32_t incl = s;
 #pragma unroll
-  for (int j = 0; j < per; ++j) {
-    start[t * per + j] = run;
-    run += local[j];
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
   }
-  if (t == 1023) start[kFineCells] = part[1023];
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += v;
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  uint32_t run = (warp > 0 ? wsum[warp - 1] : 0u) + incl - s;
+  uint4* dst = reinterpret_cast<uint4*>(start + t * per);
+#pragma unroll
+  for (int j = 0; j < per / 4; ++j) {
+    uint4 o;
+    o.x = run;
+    run += local[4 * j];
+    o.y = run;
+    run += local[4 * j + 1];
+    o.z = run;
+    run += local[4 * j + 2];
+    o.w = run;
+    run += local[4 * j + 3];
+    dst[j] = o;
+  }
+  if (t == 1023) start[kFineCells] = run;
+  // a coarse cell is 64 consecutive fine cells = 2 threads
+  __syncthreads();
+  if ((t & 1) == 0) {
+    const int c = t >> 1;
+    const uint32_t cs = __ldcg(&start[c * 64]);
+    const uint32_t ce = __ldcg(&start[c * 64 + 64]);  // start[kFineCells] = total for the last cell
+    if (ce > cs) {
+      const uint32_t slot = atomicAdd(n_coarse, 1u);
+      clist[slot] = make_uint4(cs, ce - cs, (uint32_t)c, 0u);
+    }
+  }
 }
 
 __global__ void k_scatter(int P, const float4* __restrict__ proj, const uint32_t* __restrict__ key,
@@ -104,60 +148,53 @@ __global__ void k_scatter(int P, const float4* __restrict__ proj, const uint32_t
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
   const uint32_t k = key[i];
+  if (k == 0xffffffffu) return;
   const uint32_t slot = start[k] + atomicAdd(&cursor[k], 1u);
   const float4 p = proj[i];
   sorted[slot] = make_float4(p.x, p.y, p.z, __int_as_float(i));
 }
 
-__global__ void k_fine_bounds(const float4* __restrict__ sorted, const uint32_t* __restrict__ start,
-                              float* __restrict__ fbox) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= kFineCells) return;
-  const uint32_t s = start[c], e = start[c + 1];
-  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (uint32_t j = s; j < e; ++j) {
-    const float4 p = sorted[j];
-    lo[0] = fminf(lo[0], p.x);
-    lo[1] = fminf(lo[1], p.y);
-    lo[2] = fminf(lo[2], p.z);
-    hi[0] = fmaxf(hi[0], p.x);
-    hi[1] = fmaxf(hi[1], p.y);
-    hi[2] = fmaxf(hi[2], p.z);
-  }
-  float* b = fbox + 6 * c;
-  b[0] = lo[0];
-  b[1] = lo[1];
-  b[2] = lo[2];
-  b[3] = hi[0];
-  b[4] = hi[1];
-  b[5] = hi[2];
-}
+__device__ __forceinline__ uint32_t ord(float v) { return float_order_bits(v); }
 
-// Coarse cells: merged boxes and the compact list of non-empty cells.
-// clist entries: {start, count, coarse id, pad} + box (6 floats).
-__global__ void k_coarse_bounds(const uint32_t* __restrict__ start, const float* __restrict__ fbox,
-                                uint4* __restrict__ clist, float* __restrict__ cbox,
-                                uint32_t* __restrict__ n_coarse) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= kCoarseCells) return;
-  const uint32_t s = start[c * 64], e = start[c * 64 + 64];
-  if (e == s) return;
-  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (int f = 0; f < 64; ++f) {
-    const int fc = c * 64 + f;
-    if (start[fc + 1] == start[fc]) continue;
-    const float* b = fbox + 6 * fc;
+// Tight boxes of fine and coarse cells: thread per sorted point, warp-segmented
+// min/max over lanes of the same cell, one atomic per segment.  Boxes hold
+// order-preserving bits: lo[c*3+a] (init 0xffffffff), hi[c*3+a] (init 0).
+__global__ void k_cell_bounds(const uint32_t* __restrict__ n_sorted, const float4* __restrict__ sorted,
+                              uint32_t* __restrict__ flo, uint32_t* __restrict__ fhi, uint32_t* __restrict__ clo,
+                              uint32_t* __restrict__ chi) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < (int)*n_sorted;
+  float4 p = valid ? sorted[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t fk = valid ? cell_key(p.x, p.y, p.z) : 0xffffffffu;
+  const uint32_t v[3] = {ord(p.x), ord(p.y), ord(p.z)};
+  // fine cell segments
+  {
+    const unsigned peers = __match_any_sync(0xffffffffu, fk);
+    const int leader = __ffs(peers) - 1;
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
-      lo[a] = fminf(lo[a], b[a]);
-      hi[a] = fmaxf(hi[a], b[3 + a]);
+      const uint32_t mn = __reduce_min_sync(peers, v[a]);
+      const uint32_t mx = __reduce_max_sync(peers, v[a]);
+      if (valid && (int)(threadIdx.x & 31) == leader) {
+        atomicMin(&flo[fk * 3 + a], mn);
+        atomicMax(&fhi[fk * 3 + a], mx);
+      }
     }
   }
-  const uint32_t slot = atomicAdd(n_coarse, 1u);
-  clist[slot] = make_uint4(s, e - s, (uint32_t)c, 0u);
-  float* o = cbox + 6 * slot;
-  for (int a = 0; a < 3; ++a) {
-    o[a] = lo[a];
-    o[3 + a] = hi[a];
+  // coarse cell segments
+  {
+    const uint32_t ck = valid ? fk >> 6 : 0xffffffffu;
+    const unsigned peers = __match_any_sync(0xffffffffu, ck);
+    const int leader = __ffs(peers) - 1;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const uint32_t mn = __reduce_min_sync(peers, v[a]);
+      const uint32_t mx = __reduce_max_sync(peers, v[a]);
+      if (valid && (int)(threadIdx.x & 31) == leader) {
+        atomicMin(&clo[ck * 3 + a], mn);
+        atomicMax(&chi[ck * 3 + a], mx);
+      }
+    }
   }
 }
 
@@ -166,6 +203,17 @@ __device__ __forceinline__ float box_lb2(float qx, float qy, float qz, const flo
   const float dy = fmaxf(fmaxf(b[1] - qy, qy - b[4]), 0.0f);
   const float dz = fmaxf(fmaxf(b[2] - qz, qz - b[5]), 0.0f);
   return dx * dx + dy * dy + dz * dz;
+}
+
+__device__ __forceinline__ float box_lb2_ord(float qx, float qy, float qz, const uint32_t* lo,
+                                             const uint32_t* hi) {
+  float b[6];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    b[a] = float_from_order_bits(__ldg(&lo[a]));
+    b[3 + a] = float_from_order_bits(__ldg(&hi[a]));
+  }
+  return box_lb2(qx, qy, qz, b);
 }
 
 __device__ __forceinline__ float ref_dist2(float qx, float qy, float qz, float4 p) {
@@ -185,78 +233,165 @@ __device__ __forceinline__ void nn_update(float d, int idx, float& best, int& bi
   }
 }
 
-constexpr int kQueryThreads = 256;
+__device__ __forceinline__ void warp_nn_min(float& best, int& bidx) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+    nn_update(ob, oi, best, bidx);
+  }
+}
 
-// One thread per grid direction.  Writes the sampled channels
-// {range, intensity, reflectivity, ambient} (float) into out[ch][query] for
-// ch < n_out_ch and the nearest index (or -1) into nn_idx.
+constexpr int kQueryThreads = 256;
+constexpr float kPruneMargin = 0.99999f;  // lower bound * margin must exceed the best to prune
+
+// Best-first scan of one coarse cell: its non-empty fine cells are visited in
+// ascending order of their box lower bound until the bound exceeds the best
+// distance.  best / bidx are warp-uniform on entry and on exit.
+__device__ __forceinline__ void scan_coarse(int cid, float qx, float qy, float qz,
+                                            const float4* __restrict__ sorted,
+                                            const uint32_t* __restrict__ fstart,
+                                            const uint32_t* __restrict__ flo,
+                                            const uint32_t* __restrict__ fhi, float& best, int& bidx) {
+  const int lane = threadIdx.x & 31;
+  float lb[2];
+  uint32_t fs[2], fe[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int fc = cid * 64 + h * 32 + lane;
+    fs[h] = __ldg(&fstart[fc]);
+    fe[h] = __ldg(&fstart[fc + 1]);
+    lb[h] = fe[h] > fs[h] ? box_lb2_ord(qx, qy, qz, flo + 3 * fc, fhi + 3 * fc) : INFINITY;
+  }
+  // at most 64 picks: every pick retires one fine cell
+  for (int pick = 0; pick < 64; ++pick) {
+    // warp argmin of the remaining lower bounds
+    const int hsel = lb[1] < lb[0] ? 1 : 0;
+    float m = lb[hsel];
+    int who = lane * 2 + hsel;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float om = __shfl_xor_sync(0xffffffffu, m, o);
+      const int ow = __shfl_xor_sync(0xffffffffu, who, o);
+      if (om < m || (om == m && ow < who)) {
+        m = om;
+        who = ow;
+      }
+    }
+    if (!(m < INFINITY) || !(m * kPruneMargin <= best)) break;  // done, or nothing within the bound
+    const int src = who >> 1, h = who & 1;
+    const uint32_t s = __shfl_sync(0xffffffffu, h ? fs[1] : fs[0], src);
+    const uint32_t e = __shfl_sync(0xffffffffu, h ? fe[1] : fe[0], src);
+    if (lane == src) lb[h] = INFINITY;
+    for (uint32_t j = s + lane; j < e; j += 32) {
+      const float4 p = sorted[j];
+      nn_update(ref_dist2(qx, qy, qz, p), __float_as_int(p.w), best, bidx);
+    }
+    warp_nn_min(best, bidx);
+  }
+}
+
+// One warp per grid direction (grid-stride).  The bound starts from one
+// representative point per non-empty coarse cell; the coarse cell of the
+// nearest representative is searched first, then every other coarse cell whose
+// box lies within the bound.  Writes the sampled channels {range, intensity,
+// reflectivity, ambient} (float) into out[ch][query] for ch < n_out_ch and the
+// nearest index (or -1) into nn_idx.
 __global__ void __launch_bounds__(kQueryThreads)
 k_nn_query(int nq, const float4* __restrict__ grid, const float4* __restrict__ sorted,
-           const uint32_t* __restrict__ fstart, const float* __restrict__ fbox,
-           const uint4* __restrict__ clist, const float* __restrict__ cbox,
+           const uint32_t* __restrict__ fstart, const uint32_t* __restrict__ flo,
+           const uint32_t* __restrict__ fhi, const uint4* __restrict__ clist,
+           const uint32_t* __restrict__ clo, const uint32_t* __restrict__ chi,
            const uint32_t* __restrict__ n_coarse_p, float max_sq, const float4* __restrict__ xyzi,
            const double* __restrict__ range, const float* __restrict__ refl,
            const float* __restrict__ amb, int n_out_ch, float* __restrict__ out,
            int32_t* __restrict__ nn_idx) {
-  __shared__ uint4 s_list[kCoarseCells];
+  __shared__ uint32_t s_cid[kCoarseCells];
   __shared__ float s_box[kCoarseCells * 6];
   __shared__ float4 s_rep[kCoarseCells];
   const int nc = (int)*n_coarse_p;
   for (int i = threadIdx.x; i < nc; i += blockDim.x) {
     const uint4 e = clist[i];
-    s_list[i] = e;
+    s_cid[i] = e.z;
     s_rep[i] = sorted[e.x];
-  }
-  for (int i = threadIdx.x; i < nc * 6; i += blockDim.x) s_box[i] = cbox[i];
-  __syncthreads();
-  const int qi = blockIdx.x * blockDim.x + threadIdx.x;
-  if (qi >= nq) return;
-  const float4 q = grid[qi];
-  float best = INFINITY;
-  int bidx = 0x7fffffff;
-  for (int c = 0; c < nc; ++c) {
-    const float4 r = s_rep[c];
-    nn_update(ref_dist2(q.x, q.y, q.z, r), __float_as_int(r.w), best, bidx);
-  }
-  for (int c = 0; c < nc; ++c) {
-    if (box_lb2(q.x, q.y, q.z, s_box + 6 * c) * 0.99999f > best) continue;
-    const uint32_t cid = s_list[c].z;
-    for (int f = 0; f < 64; ++f) {
-      const int fc = (int)cid * 64 + f;
-      const uint32_t s = __ldg(&fstart[fc]), e = __ldg(&fstart[fc + 1]);
-      if (s == e) continue;
-      if (box_lb2(q.x, q.y, q.z, fbox + 6 * fc) * 0.99999f > best) continue;
-      for (uint32_t j = s; j < e; ++j) {
-        const float4 p = sorted[j];
-        nn_update(ref_dist2(q.x, q.y, q.z, p), __float_as_int(p.w), best, bidx);
-      }
+    for (int a = 0; a < 3; ++a) {
+      s_box[6 * i + a] = float_from_order_bits(clo[e.z * 3 + a]);
+      s_box[6 * i + 3 + a] = float_from_order_bits(chi[e.z * 3 + a]);
     }
   }
-  const bool ok = (bidx != 0x7fffffff) && !(best > max_sq);
-  float v[4] = {0.f, 0.f, 0.f, 0.f};
-  if (ok) {
-    v[0] = (float)range[bidx];
-    v[1] = xyzi[bidx].w;
-    v[2] = refl ? refl[bidx] : 0.0f;
-    v[3] = amb ? amb[bidx] : 0.0f;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int qi = blockIdx.x * wpb + (threadIdx.x >> 5); qi < nq; qi += gridDim.x * wpb) {
+    const float4 q = grid[qi];
+    float best = INFINITY;
+    int bidx = 0x7fffffff;
+    // representatives: remember which coarse cell gave each lane's best
+    int bcell = -1;
+    for (int c = lane; c < nc; c += 32) {
+      const float4 r = s_rep[c];
+      const float d = ref_dist2(q.x, q.y, q.z, r);
+      const int id = __float_as_int(r.w);
+      if (d < best || (d == best && id < bidx)) {
+        best = d;
+        bidx = id;
+        bcell = c;
+      }
+    }
+    int first = bcell;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+      const int oc = __shfl_xor_sync(0xffffffffu, first, o);
+      if (ob < best || (ob == best && oi < bidx)) {
+        best = ob;
+        bidx = oi;
+        first = oc;
+      }
+    }
+    if (first >= 0) scan_coarse((int)s_cid[first], q.x, q.y, q.z, sorted, fstart, flo, fhi, best, bidx);
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+      const int c = c0 + lane;
+      const bool cand = c < nc && c != first && box_lb2(q.x, q.y, q.z, s_box + 6 * c) * kPruneMargin <= best;
+      unsigned cmask = __ballot_sync(0xffffffffu, cand);
+      while (cmask) {
+        const int cc = c0 + __ffs(cmask) - 1;
+        cmask &= cmask - 1;
+        if (box_lb2(q.x, q.y, q.z, s_box + 6 * cc) * kPruneMargin > best) continue;  // warp-uniform
+        scan_coarse((int)s_cid[cc], q.x, q.y, q.z, sorted, fstart, flo, fhi, best, bidx);
+      }
+    }
+    if (lane == 0) {
+      const bool ok = (bidx != 0x7fffffff) && !(best > max_sq);
+      float v[4] = {0.f, 0.f, 0.f, 0.f};
+      if (ok) {
+        v[0] = (float)range[bidx];
+        v[1] = xyzi[bidx].w;
+        v[2] = refl ? refl[bidx] : 0.0f;
+        v[3] = amb ? amb[bidx] : 0.0f;
+      }
+      for (int c = 0; c < n_out_ch; ++c) out[(size_t)c * nq + qi] = v[c];
+      if (nn_idx) nn_idx[qi] = ok ? bidx : -1;
+    }
   }
-  for (int ch = 0; ch < n_out_ch; ++ch) out[(size_t)ch * nq + qi] = v[ch];
-  if (nn_idx) nn_idx[qi] = ok ? bidx : -1;
 }
 
 // ---------------------------------------------------------------- launcher
 
+std::atomic<unsigned long long> g_launch_count{0};
+
 size_t sampler_scratch_bytes(int max_points) {
   size_t b = 0;
-  b += (size_t)max_points * sizeof(float4);   // proj
-  b += (size_t)max_points * sizeof(double);   // range
-  b += (size_t)max_points * sizeof(uint32_t); // key
-  b += (size_t)max_points * sizeof(float4);   // sorted
-  b += (size_t)kFineCells * sizeof(uint32_t) * 2;  // count, cursor
-  b += (size_t)(kFineCells + 1) * sizeof(uint32_t);
-  b += (size_t)kFineCells * 6 * sizeof(float);
+  b += (size_t)max_points * sizeof(float4);    // proj
+  b += (size_t)max_points * sizeof(double);    // range
+  b += (size_t)max_points * sizeof(uint32_t);  // key
+  b += (size_t)max_points * sizeof(float4);    // sorted
+  b += (size_t)kFineCells * sizeof(uint32_t) * 2;   // count, cursor
+  b += (size_t)(kFineCells + 4) * sizeof(uint32_t);  // start
+  b += (size_t)kFineCells * 6 * sizeof(uint32_t);    // fine boxes
   b += (size_t)kCoarseCells * sizeof(uint4);
-  b += (size_t)kCoarseCells * 6 * sizeof(float);
+  b += (size_t)kCoarseCells * 6 * sizeof(uint32_t);
   b += 256;
   return b + 16 * 256;
 }
@@ -275,28 +410,42 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   float4* sorted = (float4*)carve(p, (size_t)a.max_points * sizeof(float4));
   uint32_t* count = (uint32_t*)carve(p, (size_t)kFineCells * sizeof(uint32_t));
   uint32_t* cursor = (uint32_t*)carve(p, (size_t)kFineCells * sizeof(uint32_t));
-  uint32_t* start = (uint32_t*)carve(p, (size_t)(kFineCells + 1) * sizeof(uint32_t));
-  float* fbox = (float*)carve(p, (size_t)kFineCells * 6 * sizeof(float));
+  uint32_t* start = (uint32_t*)carve(p, (size_t)(kFineCells + 4) * sizeof(uint32_t));
+  uint32_t* flo = (uint32_t*)carve(p, (size_t)kFineCells * 3 * sizeof(uint32_t));
+  uint32_t* fhi = (uint32_t*)carve(p, (size_t)kFineCells * 3 * sizeof(uint32_t));
   uint4* clist = (uint4*)carve(p, (size_t)kCoarseCells * sizeof(uint4));
-  float* cbox = (float*)carve(p, (size_t)kCoarseCells * 6 * sizeof(float));
+  uint32_t* clo = (uint32_t*)carve(p, (size_t)kCoarseCells * 3 * sizeof(uint32_t));
+  uint32_t* chi = (uint32_t*)carve(p, (size_t)kCoarseCells * 3 * sizeof(uint32_t));
   uint32_t* ncoarse = (uint32_t*)carve(p, 256);
 
-  cudaMemsetAsync(count, 0, (size_t)kFineCells * sizeof(uint32_t), st);
-  cudaMemsetAsync(cursor, 0, (size_t)kFineCells * sizeof(uint32_t), st);
+  // count and cursor are adjacent: one memset
+  cudaMemsetAsync(count, 0, (size_t)2 * kFineCells * sizeof(uint32_t), st);
+  cudaMemsetAsync(flo, 0xff, (size_t)kFineCells * 3 * sizeof(uint32_t), st);
+  cudaMemsetAsync(fhi, 0, (size_t)kFineCells * 3 * sizeof(uint32_t), st);
+  cudaMemsetAsync(clo, 0xff, (size_t)kCoarseCells * 3 * sizeof(uint32_t), st);
+  cudaMemsetAsync(chi, 0, (size_t)kCoarseCells * 3 * sizeof(uint32_t), st);
   cudaMemsetAsync(ncoarse, 0, sizeof(uint32_t), st);
   const int P = a.n_points;
+  int launched = 0;
   if (P > 0) {
     k_project<<<(P + 255) / 256, 256, 0, st>>>(a.xyzi, P, proj, range, key, count);
+    ++launched;
   }
-  k_cell_scan<<<1, 1024, 0, st>>>(count, start);
+  k_cell_scan<<<1, 1024, 0, st>>>(count, start, clist, ncoarse);
+  ++launched;
   if (P > 0) {
     k_scatter<<<(P + 255) / 256, 256, 0, st>>>(P, proj, key, start, cursor, sorted);
+    k_cell_bounds<<<(P + 255) / 256, 256, 0, st>>>(start + kFineCells, sorted, flo, fhi, clo, chi);
+    launched += 2;
   }
-  k_fine_bounds<<<kFineCells / 256, 256, 0, st>>>(sorted, start, fbox);
-  k_coarse_bounds<<<kCoarseCells / 128, 128, 0, st>>>(start, fbox, clist, cbox, ncoarse);
-  k_nn_query<<<(a.n_queries + kQueryThreads - 1) / kQueryThreads, kQueryThreads, 0, st>>>(
-      a.n_queries, a.grid, sorted, start, fbox, clist, cbox, ncoarse, a.max_sq, a.xyzi, range,
-      a.refl, a.amb, a.n_out_ch, a.out, a.nn_idx);
+  const int wpb = kQueryThreads / 32;
+  int blocks = (a.n_queries + wpb - 1) / wpb;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_nn_query<<<blocks, kQueryThreads, 0, st>>>(a.n_queries, a.grid, sorted, start, flo, fhi, clist, clo, chi,
+                                               ncoarse, a.max_sq, a.xyzi, range, a.refl, a.amb, a.n_out_ch,
+                                               a.out, a.nn_idx);
+  ++launched;
+  count_launches(launched);
   return cudaGetLastError();
 }
 

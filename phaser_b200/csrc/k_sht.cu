@@ -67,6 +67,7 @@ __global__ void k_legendre_table(int bw, const double* __restrict__ w, float* __
 cudaError_t launch_legendre_table(int bw, const double* weights_dev, float* table, cudaStream_t st) {
   const int tot = bw * 2 * bw;
   k_legendre_table<<<(tot + 127) / 128, 128, 0, st>>>(bw, weights_dev, table);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -128,6 +129,7 @@ cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st) {
   k_sht_phi<<<g1, 128, n * sizeof(float), st>>>(a.bw, a.signal, a.tw, a.fm);
   dim3 g2(a.bw, a.n_sig);
   k_sht_legendre<<<g2, 256, n * sizeof(float2), st>>>(a.bw, a.table, a.fm, a.coef);
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -190,6 +192,7 @@ __global__ void k_fuse_s2(FuseS2Args a) {
 cudaError_t launch_fuse_s2(const FuseS2Args& a, cudaStream_t st) {
   const int tot = a.bw * (2 * a.bw - 1);
   k_fuse_s2<<<(tot + 255) / 256, 256, 0, st>>>(a);
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -119,10 +119,12 @@ __global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz
 }
 
 // Forward DFT over a (alpha) for a tile of b columns at one beta.
+template <int NF>
 __global__ void k_so3_fft_a(int bw_in, int bw_out, float2* __restrict__ S, FftPlan plan) {
   extern __shared__ float2 tile[];
   constexpr int Wt = 16;
-  const int n = 2 * bw_out, Bo = bw_out;
+  const int n = NF > 0 ? NF : 2 * bw_out;
+  const int Bo = n / 2;
   const int k = blockIdx.y;
   const int b0 = blockIdx.x * Wt;
   const int wt = min(Wt, bw_in - b0);
@@ -134,7 +136,7 @@ __global__ void k_so3_fft_a(int bw_in, int bw_out, float2* __restrict__ S, FftPl
     tile[e] = (bt < wt && row_ok) ? Sk[(size_t)a * Bo + b0 + bt] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  fft_smem<false>(tile, Wt, 1, Wt, plan);
+  fft_any<NF, false, 4>(tile, Wt, 1, Wt, plan);
   for (int e = threadIdx.x; e < n * Wt; e += blockDim.x) {
     const int a = e / Wt, bt = e % Wt;
     if (bt < wt) Sk[(size_t)a * Bo + b0 + bt] = tile[e];
@@ -142,33 +144,35 @@ __global__ void k_so3_fft_a(int bw_in, int bw_out, float2* __restrict__ S, FftPl
 }
 
 // Hermitian complex-to-real transform over gamma, |z|^2 and argmax.
+template <int NF>
 __global__ void k_so3_c2r(int bw_in, int bw_out, const float2* __restrict__ S, FftPlan plan,
                           unsigned long long* __restrict__ argmax, float* __restrict__ volume) {
   extern __shared__ float2 rows[];
-  constexpr int R = 8;
-  const int n = 2 * bw_out, Bo = bw_out;
+  constexpr int R = 16;
+  const int n = NF > 0 ? NF : 2 * bw_out;
+  const int Bo = n / 2;
   const int k = blockIdx.y;
   const int r0 = blockIdx.x * R;
   const int nr = min(R, n - r0);
   for (int e = threadIdx.x; e < R * n; e += blockDim.x) rows[e] = make_float2(0.f, 0.f);
   __syncthreads();
   for (int e = threadIdx.x; e < nr * Bo; e += blockDim.x) {
-    const int r = e / Bo, b = e % Bo;
+    const int r = e / Bo, b = e - r * Bo;
     float2* row = rows + r * n;
     const float2 u = b < bw_in ? S[((size_t)k * n + r0 + r) * Bo + b] : make_float2(0.f, 0.f);
-    row[fft_freq2pos(b, plan)] = cconj(u);
-    if (b > 0) row[fft_freq2pos(n - b, plan)] = u;
+    row[freq2pos<NF>(b, plan)] = cconj(u);
+    if (b > 0) row[freq2pos<NF>(n - b, plan)] = u;
   }
   __syncthreads();
-  fft_smem<true>(rows, R, n, 1, plan);
-  const float K = (float)((1.0 / (double)n) * ((double)bw_out / M_PI));
+  fft_any<NF, true>(rows, R, n, 1, plan);
+  const float K = (float)((1.0 / (double)n) * ((double)Bo / M_PI));
   unsigned long long best = 0ull;
   for (int e = threadIdx.x; e < R * n; e += blockDim.x) {
-    const int r = e / n, g = e % n;
+    const int r = e / n, g = e - r * n;
     if (r < nr) {
       const float v = rows[e].x * K;
       const float v2 = v * v;
-      const int alpha = fft_pos2freq(r0 + r, plan);
+      const int alpha = pos2freq<NF>(r0 + r, plan);
       const uint32_t idx = ((uint32_t)k * n + (uint32_t)alpha) * n + g;
       const unsigned long long key = pack_argmax(v2, idx);
       best = key > best ? key : best;
@@ -178,25 +182,44 @@ __global__ void k_so3_c2r(int bw_in, int bw_out, const float2* __restrict__ S, F
   warp_argmax_commit(best, argmax);
 }
 
-cudaError_t so3_init_attributes() {
+template <int NF>
+static cudaError_t so3_attrs() {
   const int m = 227 * 1024;
-  cudaError_t e = cudaFuncSetAttribute(k_so3_fft_a, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_so3_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+  cudaError_t e = cudaFuncSetAttribute(k_so3_fft_a<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_so3_c2r<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
   return e;
 }
 
-cudaError_t launch_so3(const So3Args& a, cudaStream_t st) {
+cudaError_t so3_init_attributes() {
+  cudaError_t e = cudaSuccess;
+  for (int n : {64, 128, 200, 256, 512, 0}) {
+    cudaError_t r = cudaSuccess;
+    PHGPU_DISPATCH_N(n, r = so3_attrs<NF>());
+    if (r != cudaSuccess) e = r;
+  }
+  return e;
+}
+
+cudaError_t launch_so3_synth(const So3Args& a, cudaStream_t st) {
   const int ncls = a.bw_in * (a.bw_in + 1) / 2;
   const int n = 2 * a.bw_out;
   int thr = ((n + 31) / 32) * 32;
   if (thr > 512) thr = 512;
   const size_t sm1 = (size_t)a.bw_in * 3 * sizeof(double) + (size_t)a.bw_in * 4 * sizeof(float2);
   k_so3_synth<<<ncls, thr, sm1, st>>>(a.bw_in, a.bw_out, a.fused, a.S);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_so3_fft(const So3Args& a, cudaStream_t st) {
+  const int n = 2 * a.bw_out;
   dim3 g2((a.bw_in + 15) / 16, n);
-  k_so3_fft_a<<<g2, 256, (size_t)n * 16 * sizeof(float2), st>>>(a.bw_in, a.bw_out, a.S, *a.plan);
-  dim3 g3((n + 7) / 8, n);
-  k_so3_c2r<<<g3, 256, (size_t)8 * n * sizeof(float2), st>>>(a.bw_in, a.bw_out, a.S, *a.plan, a.argmax,
-                                                             a.volume);
+  dim3 g3((n + 15) / 16, n);
+  PHGPU_DISPATCH_N(n,
+      k_so3_fft_a<NF><<<g2, 256, (size_t)n * 16 * sizeof(float2), st>>>(a.bw_in, a.bw_out, a.S, *a.plan);
+      k_so3_c2r<NF><<<g3, 256, (size_t)16 * n * sizeof(float2), st>>>(a.bw_in, a.bw_out, a.S, *a.plan,
+                                                                       a.argmax, a.volume));
+  count_launches(2);
   return cudaGetLastError();
 }
 

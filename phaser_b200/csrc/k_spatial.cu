@@ -74,96 +74,115 @@ __global__ void k_voxelize(VoxelArgs a) {
 }
 
 cudaError_t launch_voxelize(const VoxelArgs& a, cudaStream_t st) {
-  if (a.n_points > 0) k_voxelize<<<(a.n_points + 255) / 256, 256, 0, st>>>(a);
+  if (a.n_points > 0) {
+    k_voxelize<<<(a.n_points + 255) / 256, 256, 0, st>>>(a);
+    count_launches(1);
+  }
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- A1
+constexpr int kRowsR2C = 16;
+
 // rows r = z*N + x of one channel; out spec[ch][r][ky], ky in [0, N/2].
+template <int NF>
 __global__ void k_r2c_y(int N, const float* __restrict__ grid, const float* __restrict__ count,
                         float2* __restrict__ spec, FftPlan plan) {
   extern __shared__ float2 rows[];
-  constexpr int R = 8;
-  const int H2 = N / 2 + 1;
-  const size_t nrows = (size_t)N * N;
+  constexpr int R = kRowsR2C;
+  const int n = NF > 0 ? NF : N;
+  const int H2 = n / 2 + 1;
+  const int H2p = spatial_h2p(n);
+  const size_t nrows = (size_t)n * n;
   const size_t r0 = (size_t)blockIdx.x * R;
-  for (int e = threadIdx.x; e < R * N; e += blockDim.x) {
-    const int rr = e / N, y = e % N;
+  for (int e = threadIdx.x; e < R * n; e += blockDim.x) {
+    const int rr = e / n, y = e - rr * n;
     const size_t r = r0 + rr;
     float v = 0.0f;
     if (r < nrows) {
-      v = grid[r * N + y];
+      v = grid[r * n + y];
       if (count) {
-        const float q = v / count[r * N + y];
+        const float q = v / count[r * n + y];
         v = isfinite(q) ? q : 0.0f;
       }
     }
     rows[e] = make_float2(v, 0.0f);
   }
   __syncthreads();
-  fft_smem<false>(rows, R, N, 1, plan);
+  fft_any<NF, false>(rows, R, n, 1, plan);
   for (int e = threadIdx.x; e < R * H2; e += blockDim.x) {
-    const int rr = e / H2, ky = e % H2;
+    const int rr = e / H2, ky = e - rr * H2;
     const size_t r = r0 + rr;
-    if (r < nrows) spec[r * H2 + ky] = rows[rr * N + fft_freq2pos(ky, plan)];
+    if (r < nrows) spec[r * H2p + ky] = rows[rr * n + freq2pos<NF>(ky, plan)];
   }
 }
 
 // ---------------------------------------------------------------- A2 / C1
 // In-place transform along x for a tile of ky at one z: spec[z][x][ky].
-template <bool INV>
+template <int NF, bool INV>
 __global__ void k_fft_x(int N, float2* __restrict__ spec, FftPlan plan) {
   extern __shared__ float2 tile[];
   constexpr int Wt = 16;
-  const int H2 = N / 2 + 1;
+  const int n = NF > 0 ? NF : N;
+  const int H2 = n / 2 + 1;
+  const int H2p = spatial_h2p(n);
   const int ky0 = blockIdx.x * Wt;
   const int wt = min(Wt, H2 - ky0);
-  float2* base = spec + (size_t)blockIdx.z * N * N * H2 + (size_t)blockIdx.y * N * H2;
-  for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
+  float2* base = spec + (size_t)blockIdx.y * n * H2p;
+  for (int e = threadIdx.x; e < n * Wt; e += blockDim.x) {
     const int x = e / Wt, t = e % Wt;
-    tile[e] = t < wt ? base[(size_t)x * H2 + ky0 + t] : make_float2(0.f, 0.f);
+    tile[e] = t < wt ? base[(size_t)x * H2p + ky0 + t] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  fft_smem<INV>(tile, Wt, 1, Wt, plan);
-  for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
+  fft_any<NF, INV, 4>(tile, Wt, 1, Wt, plan);
+  for (int e = threadIdx.x; e < n * Wt; e += blockDim.x) {
     const int x = e / Wt, t = e % Wt;
-    if (t < wt) base[(size_t)x * H2 + ky0 + t] = tile[e];
+    if (t < wt) base[(size_t)x * H2p + ky0 + t] = tile[e];
   }
 }
 
 // ---------------------------------------------------------------- B
 // For one x position (digit-reversed) and a tile of ky: forward z FFT of all
 // 2C arrays, fusion + cross power, inverse z FFT of the product.
-__global__ void k_fuse_z(SpatialArgs a, FftPlan plan, int Wt) {
+template <int NF>
+__global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int Wt, int x_natural) {
   extern __shared__ float2 tile[];  // [z][arr][t]
-  const int N = a.N, H2 = N / 2 + 1;
+  const int N = NF > 0 ? NF : a.N;
+  const int H2 = N / 2 + 1;
+  const int H2p = spatial_h2p(N);
   const int C = a.n_data_ch;
   const int A = a.laplace ? 2 * C : 2;
   const int ky0 = blockIdx.x * Wt;
   const int wt = min(Wt, H2 - ky0);
   const int xp = blockIdx.y;
-  const size_t plane = (size_t)N * N * H2;
+  const size_t plane = (size_t)N * N * H2p;
   const int rowlen = A * Wt;
-  for (int e = threadIdx.x; e < N * rowlen; e += blockDim.x) {
-    const int z = e / rowlen, rem = e % rowlen, ar = rem / Wt, t = rem % Wt;
+  // tiles start at ky0 (multiple of Wt) in rows padded to 8 complex: load two
+  // complex per 16-byte access
+  const int half = Wt >> 1;
+  for (int e = threadIdx.x; e < N * A * half; e += blockDim.x) {
+    const int z = e / (A * half), rem = e - z * (A * half), ar = rem / half, t2 = rem - ar * half;
     // arrays: f channels 0..C-1 then g channels; plain mode uses channel 0 of each side
     const int src = a.laplace ? ar : (ar == 0 ? 0 : C);
-    tile[e] = t < wt ? a.spec[(size_t)src * plane + ((size_t)z * N + xp) * H2 + ky0 + t]
-                     : make_float2(0.f, 0.f);
+    const float4 v = *reinterpret_cast<const float4*>(
+        a.spec + (size_t)src * plane + ((size_t)z * N + xp) * H2p + ky0 + 2 * t2);
+    float2* d = tile + (size_t)z * rowlen + ar * Wt + 2 * t2;
+    d[0] = make_float2(v.x, v.y);
+    d[1] = make_float2(v.z, v.w);
   }
   __syncthreads();
-  fft_smem<false>(tile, rowlen, 1, rowlen, plan);
-  const int kx = fft_pos2freq(xp, plan);
+  fft_any<NF, false, -2>(tile, rowlen, 1, rowlen, plan);
+  const int kx = x_natural ? xp : pos2freq<NF>(xp, plan);
   const uint32_t nv = (uint32_t)N * (uint32_t)N * (uint32_t)N;
   for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
-    const int zp = e / Wt, t = e % Wt;
+    const int zp = e / Wt, t = e - zp * Wt;
     float2* row = tile + (size_t)zp * rowlen;
     float2 F, G;
     if (!a.laplace) {
       F = row[t];
       G = row[Wt + t];
     } else {
-      const int kz = fft_pos2freq(zp, plan);
+      const int kz = pos2freq<NF>(zp, plan);
       const uint32_t klin = ((uint32_t)kz * N + (uint32_t)kx) * (uint32_t)H2 + (uint32_t)(ky0 + t);
       const uint32_t p = (uint32_t)(((uint64_t)klin + (nv >> 1)) % nv);
       const int op = fusion_op(p, a.bands);
@@ -200,50 +219,164 @@ __global__ void k_fuse_z(SpatialArgs a, FftPlan plan, int Wt) {
         }
       }
     }
-    // complexMulSeq: C = F * conj(G)
-    const float2 prod = make_float2(F.x * G.x - F.y * (-G.y), F.x * (-G.y) + F.y * G.x);
-    row[t] = prod;  // only this thread reads or writes position (zp, t)
+    // complexMulSeq: C = F * conj(G); only this thread touches position (zp, t)
+    row[t] = make_float2(F.x * G.x - F.y * (-G.y), F.x * (-G.y) + F.y * G.x);
   }
   __syncthreads();
-  fft_smem<true>(tile, Wt, 1, rowlen, plan);
+  fft_any<NF, true, -2>(tile, Wt, 1, rowlen, plan);
   for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
-    const int z = e / Wt, t = e % Wt;
-    if (t < wt) a.cspec[((size_t)z * N + xp) * H2 + ky0 + t] = tile[(size_t)z * rowlen + t];
+    const int z = e / Wt, t = e - z * Wt;
+    if (t < wt) a.cspec[((size_t)z * N + xp) * H2p + ky0 + t] = tile[(size_t)z * rowlen + t];
   }
 }
 
 // ---------------------------------------------------------------- C2
+template <int NF>
 __global__ void k_c2r_y(int N, const float2* __restrict__ cspec, FftPlan plan,
                         unsigned long long* __restrict__ argmax, float* __restrict__ volume) {
   extern __shared__ float2 rows[];
-  constexpr int R = 8;
-  const int H2 = N / 2 + 1;
-  const size_t nrows = (size_t)N * N;
+  constexpr int R = kRowsR2C;
+  const int n = NF > 0 ? NF : N;
+  const int H2 = n / 2 + 1;
+  const int H2p = spatial_h2p(n);
+  const size_t nrows = (size_t)n * n;
   const size_t r0 = (size_t)blockIdx.x * R;
-  for (int e = threadIdx.x; e < R * N; e += blockDim.x) rows[e] = make_float2(0.f, 0.f);
+  for (int e = threadIdx.x; e < R * n; e += blockDim.x) rows[e] = make_float2(0.f, 0.f);
   __syncthreads();
-  const int hmax = (N - 1) / 2;  // last ky with a mirrored partner
+  const int hmax = (n - 1) / 2;  // last ky with a mirrored partner
   for (int e = threadIdx.x; e < R * H2; e += blockDim.x) {
-    const int rr = e / H2, ky = e % H2;
+    const int rr = e / H2, ky = e - rr * H2;
     const size_t r = r0 + rr;
     if (r >= nrows) continue;
-    const float2 v = cspec[r * H2 + ky];
-    float2* row = rows + rr * N;
-    row[fft_freq2pos(ky, plan)] = v;
-    if (ky >= 1 && ky <= hmax) row[fft_freq2pos(N - ky, plan)] = cconj(v);
+    const float2 v = cspec[r * H2p + ky];
+    float2* row = rows + rr * n;
+    row[freq2pos<NF>(ky, plan)] = v;
+    if (ky >= 1 && ky <= hmax) row[freq2pos<NF>(n - ky, plan)] = cconj(v);
   }
   __syncthreads();
-  fft_smem<true>(rows, R, N, 1, plan);
+  fft_any<NF, true>(rows, R, n, 1, plan);
   unsigned long long best = 0ull;
-  for (int e = threadIdx.x; e < R * N; e += blockDim.x) {
-    const int rr = e / N, y = e % N;
+  for (int e = threadIdx.x; e < R * n; e += blockDim.x) {
+    const int rr = e / n, y = e - rr * n;
     const size_t r = r0 + rr;
     if (r < nrows) {
       const float v = rows[e].x;
-      const uint32_t idx = (uint32_t)(r * N + y);
+      const uint32_t idx = (uint32_t)(r * n + y);
       const unsigned long long key = pack_argmax(v, idx);
       best = key > best ? key : best;
       if (volume) volume[idx] = v;
+    }
+  }
+  warp_argmax_commit(best, argmax);
+}
+
+// ---------------------------------------------------------------- z-slab
+// Fused forward r2c over (x, y) of one z-slab of one channel (NF even, the
+// slab of NF/2 x NF complex fits in shared memory).  Rows x = 2r and 2r+1 are
+// packed as real and imaginary parts of one complex row; FFT over y (NF
+// points), FFT over r (NF/2 points), then the two real spectra are separated
+// in the 2-D frequency domain,
+//   A = (W[ky][k] + conj W[-ky][-k]) / 2,  B = (W[ky][k] - conj W[-ky][-k]) / 2i,
+// and combined over the even/odd x split,
+//   X[k][ky] = A + w_N^k B,  X[k + N/2][ky] = A - w_N^k B.
+// Output rows are in natural kx order.
+template <int NF>
+__global__ void __launch_bounds__(1024) k_slab_fwd(const float* __restrict__ grids, size_t grid_cstride,
+                                                   const float* __restrict__ count, float2* __restrict__ spec,
+                                                   size_t spec_cstride, FftPlan pN, FftPlan pH) {
+  constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1, Q = NF / 4;
+  const int H2p = spatial_h2p(N);
+  extern __shared__ float2 W[];  // [NH][N]
+  const int z = blockIdx.x, c = blockIdx.y;
+  const float* g = grids + (size_t)c * grid_cstride + (size_t)z * N * N;
+  const float* cnt = count ? count + (size_t)z * N * N : nullptr;
+  for (int e = threadIdx.x; e < NH * Q; e += blockDim.x) {
+    const int r = e / Q, y4 = (e - r * Q) * 4;
+    float4 a = *reinterpret_cast<const float4*>(g + (size_t)(2 * r) * N + y4);
+    float4 b = *reinterpret_cast<const float4*>(g + (size_t)(2 * r + 1) * N + y4);
+    if (cnt) {
+      const float4 ca = *reinterpret_cast<const float4*>(cnt + (size_t)(2 * r) * N + y4);
+      const float4 cb = *reinterpret_cast<const float4*>(cnt + (size_t)(2 * r + 1) * N + y4);
+      float q;
+      q = a.x / ca.x; a.x = isfinite(q) ? q : 0.f;
+      q = a.y / ca.y; a.y = isfinite(q) ? q : 0.f;
+      q = a.z / ca.z; a.z = isfinite(q) ? q : 0.f;
+      q = a.w / ca.w; a.w = isfinite(q) ? q : 0.f;
+      q = b.x / cb.x; b.x = isfinite(q) ? q : 0.f;
+      q = b.y / cb.y; b.y = isfinite(q) ? q : 0.f;
+      q = b.z / cb.z; b.z = isfinite(q) ? q : 0.f;
+      q = b.w / cb.w; b.w = isfinite(q) ? q : 0.f;
+    }
+    float2* d = W + r * N + y4;
+    d[0] = make_float2(a.x, b.x);
+    d[1] = make_float2(a.y, b.y);
+    d[2] = make_float2(a.z, b.z);
+    d[3] = make_float2(a.w, b.w);
+  }
+  __syncthreads();
+  fft_fixed<N, false, -1>(W, NH, N, 1, pN.tw);   // over y, rows
+  fft_fixed<NH, false, -2>(W, N, 1, N, pH.tw);   // over r, columns
+  float2* out = spec + (size_t)c * spec_cstride + (size_t)z * N * H2p;
+  for (int e = threadIdx.x; e < NH * H2; e += blockDim.x) {
+    const int k = e / H2, ky = e - k * H2;
+    const float2 w1 = W[fixed_freq2pos<NH>(k) * N + fixed_freq2pos<N>(ky)];
+    const float2 w2 = W[fixed_freq2pos<NH>(k == 0 ? 0 : NH - k) * N + fixed_freq2pos<N>(ky == 0 ? 0 : N - ky)];
+    const float2 A = make_float2(0.5f * (w1.x + w2.x), 0.5f * (w1.y - w2.y));
+    const float2 B = make_float2(0.5f * (w1.y + w2.y), -0.5f * (w1.x - w2.x));  // (w1 - conj w2) / 2i
+    const float2 tB = cmul(__ldg(&pN.tw[k]), B);
+    out[(size_t)k * H2p + ky] = cadd(A, tB);
+    out[(size_t)(k + NH) * H2p + ky] = csub(A, tB);
+  }
+}
+
+// Fused inverse of one z-slab: inverse over x and the real inverse over y of
+// the product spectrum (natural kx), first-occurrence argmax of the signed
+// output.  The ky = 0 and ky = N/2 columns are first projected onto their
+// x-Hermitian parts, which is what a half-complex inverse reads (only the real
+// parts of its DC and Nyquist terms after the inverse over x).
+template <int NF>
+__global__ void __launch_bounds__(1024) k_slab_inv(const float2* __restrict__ cspec, FftPlan pN, FftPlan pH,
+                                                   unsigned long long* __restrict__ argmax,
+                                                   float* __restrict__ volume) {
+  constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1;
+  const int H2p = spatial_h2p(N);
+  extern __shared__ float2 W[];  // [NH][N]
+  const int z = blockIdx.x;
+  const float2* X = cspec + (size_t)z * N * H2p;
+  for (int e = threadIdx.x; e < NH * H2; e += blockDim.x) {
+    const int k = e / H2, ky = e - k * H2;
+    float2 x0 = X[(size_t)k * H2p + ky];
+    float2 x1 = X[(size_t)(k + NH) * H2p + ky];
+    if (ky == 0 || ky == NH) {
+      const float2 m0 = X[(size_t)(k == 0 ? 0 : N - k) * H2p + ky];  // kx = -k
+      const float2 m1 = X[(size_t)(NH - k) * H2p + ky];               // kx = -(k + N/2)
+      x0 = make_float2(0.5f * (x0.x + m0.x), 0.5f * (x0.y - m0.y));
+      x1 = make_float2(0.5f * (x1.x + m1.x), 0.5f * (x1.y - m1.y));
+    }
+    const float2 A = make_float2(0.5f * (x0.x + x1.x), 0.5f * (x0.y + x1.y));
+    const float2 B = cmul(make_float2(0.5f * (x0.x - x1.x), 0.5f * (x0.y - x1.y)), cconj(__ldg(&pN.tw[k])));
+    // W = A + i B at (k, ky); its mirror (-k, -ky) holds conj(A) + i conj(B)
+    W[fixed_freq2pos<NH>(k) * N + fixed_freq2pos<N>(ky)] = make_float2(A.x - B.y, A.y + B.x);
+    if (ky >= 1 && ky < NH)
+      W[fixed_freq2pos<NH>(k == 0 ? 0 : NH - k) * N + fixed_freq2pos<N>(N - ky)] =
+          make_float2(A.x + B.y, -A.y + B.x);
+  }
+  __syncthreads();
+  fft_fixed<NH, true, -2>(W, N, 1, N, pH.tw);   // over r, columns
+  fft_fixed<N, true, -1>(W, NH, N, 1, pN.tw);   // over y, rows
+  unsigned long long best = 0ull;
+  for (int e = threadIdx.x; e < NH * N; e += blockDim.x) {
+    const int r = e / N, y = e - r * N;
+    const float2 v = W[e];
+    const float a0 = 2.0f * v.x, a1 = 2.0f * v.y;
+    const uint32_t i0 = (uint32_t)(((size_t)z * N + 2 * r) * N + y);
+    const uint32_t i1 = i0 + N;
+    unsigned long long k0 = pack_argmax(a0, i0), k1 = pack_argmax(a1, i1);
+    k0 = k1 > k0 ? k1 : k0;
+    best = k0 > best ? k0 : best;
+    if (volume) {
+      volume[i0] = a0;
+      volume[i1] = a1;
     }
   }
   warp_argmax_commit(best, argmax);
@@ -253,52 +386,118 @@ __global__ void k_c2r_y(int N, const float2* __restrict__ cspec, FftPlan plan,
 
 constexpr int kMaxSmem = 227 * 1024;
 
-cudaError_t spatial_init_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(k_fuse_z, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_r2c_y, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fft_x<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fft_x<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_c2r_y, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+template <int NF>
+static cudaError_t set_attrs() {
+  cudaError_t e = cudaFuncSetAttribute(k_fuse_z<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_r2c_y<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fft_x<NF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fft_x<NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_c2r_y<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
   return e;
 }
 
+cudaError_t spatial_init_attributes() {
+  cudaError_t e = cudaSuccess;
+  for (int n : {64, 128, 200, 256, 512, 0}) {
+    cudaError_t r = cudaSuccess;
+    PHGPU_DISPATCH_N(n, r = set_attrs<NF>());
+    if (r != cudaSuccess) e = r;
+  }
+  for (auto fn : {(const void*)k_slab_fwd<64>, (const void*)k_slab_fwd<128>, (const void*)k_slab_fwd<200>,
+                  (const void*)k_slab_inv<64>, (const void*)k_slab_inv<128>, (const void*)k_slab_inv<200>}) {
+    cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+    if (r != cudaSuccess) e = r;
+  }
+  return e;
+}
+
+bool spatial_slab_path(int N) { return N == 64 || N == 128 || N == 200; }
+
+#define PHGPU_DISPATCH_SLAB(n, ...) \
+  switch (n) {                      \
+    case 64: {                      \
+      constexpr int NF = 64;        \
+      __VA_ARGS__;                  \
+    } break;                        \
+    case 128: {                     \
+      constexpr int NF = 128;       \
+      __VA_ARGS__;                  \
+    } break;                        \
+    default: {                      \
+      constexpr int NF = 200;       \
+      __VA_ARGS__;                  \
+    } break;                        \
+  }
+
 // Tile width of the z pass: as many ky columns as fit (<= 8) in shared memory.
 static int fuse_z_tile(int N, int A) {
-  int wt = 8;
-  while (wt > 1 && (size_t)N * A * wt * sizeof(float2) > (size_t)kMaxSmem) wt >>= 1;
+  int wt = 8;  // >= 2: the loader moves two complex per 16-byte access
+  while (wt > 2 && (size_t)N * A * wt * sizeof(float2) > (size_t)kMaxSmem) wt >>= 1;
   return wt;
 }
 
 cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t st) {
   const int N = a.N, H2 = N / 2 + 1;
   const size_t nv = (size_t)N * N * N;
-  const size_t plane = (size_t)N * N * H2;
+  const size_t plane = (size_t)N * N * spatial_h2p(N);
   const float* grids = side == 0 ? a.grids_f : a.grids_g;
   const int nch = a.laplace ? a.n_data_ch : 1;
   const float* count = a.grids_are_means ? nullptr : grids + (size_t)a.n_data_ch * nv;
-  const int nrowblk = (int)((nv / N + 7) / 8);
+  if (spatial_slab_path(N) && a.plan_half) {
+    float2* spec = a.spec + (size_t)(side * a.n_data_ch) * plane;
+    dim3 g(N, nch);
+    const size_t sm = (size_t)(N / 2) * N * sizeof(float2);
+    PHGPU_DISPATCH_SLAB(N, k_slab_fwd<NF><<<g, 1024, sm, st>>>(grids, nv, count, spec, plane, *a.plan, *a.plan_half));
+    count_launches(1);
+    return cudaGetLastError();
+  }
+  const int nrowblk = (int)((nv / N + kRowsR2C - 1) / kRowsR2C);
   for (int c = 0; c < nch; ++c) {
     float2* spec = a.spec + (size_t)(side * a.n_data_ch + c) * plane;
-    k_r2c_y<<<nrowblk, 256, (size_t)8 * N * sizeof(float2), st>>>(N, grids + (size_t)c * nv, count, spec, *a.plan);
-    dim3 g((H2 + 15) / 16, N, 1);
-    k_fft_x<false><<<g, 256, (size_t)N * 16 * sizeof(float2), st>>>(N, spec, *a.plan);
+    const float* g = grids + (size_t)c * nv;
+    dim3 gx((H2 + 15) / 16, N, 1);
+    PHGPU_DISPATCH_N(N,
+        k_r2c_y<NF><<<nrowblk, 256, (size_t)kRowsR2C * N * sizeof(float2), st>>>(N, g, count, spec, *a.plan);
+        k_fft_x<NF, false><<<gx, 256, (size_t)N * 16 * sizeof(float2), st>>>(N, spec, *a.plan));
+    count_launches(2);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_spatial_combine(const SpatialArgs& a, cudaStream_t st) {
+cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st) {
   const int N = a.N, H2 = N / 2 + 1;
   const int A = a.laplace ? 2 * a.n_data_ch : 2;
   const int wt = fuse_z_tile(N, A);
   const size_t smB = (size_t)N * A * wt * sizeof(float2);
   if (smB > (size_t)kMaxSmem) return cudaErrorInvalidConfiguration;
   dim3 gB((H2 + wt - 1) / wt, N);
-  k_fuse_z<<<gB, 256, smB, st>>>(a, *a.plan, wt);
-  dim3 gC((H2 + 15) / 16, N, 1);
-  k_fft_x<true><<<gC, 256, (size_t)N * 16 * sizeof(float2), st>>>(N, a.cspec, *a.plan);
-  const int nrowblk = (int)(((size_t)N * N + 7) / 8);
-  k_c2r_y<<<nrowblk, 256, (size_t)8 * N * sizeof(float2), st>>>(N, a.cspec, *a.plan, a.argmax, a.volume);
+  const int xnat = (spatial_slab_path(N) && a.plan_half) ? 1 : 0;
+  PHGPU_DISPATCH_N(N, k_fuse_z<NF><<<gB, 512, smB, st>>>(a, *a.plan, wt, xnat));
+  count_launches(1);
   return cudaGetLastError();
+}
+
+cudaError_t launch_spatial_inverse(const SpatialArgs& a, cudaStream_t st) {
+  const int N = a.N, H2 = N / 2 + 1;
+  if (spatial_slab_path(N) && a.plan_half) {
+    const size_t sm = (size_t)(N / 2) * N * sizeof(float2);
+    PHGPU_DISPATCH_SLAB(N, k_slab_inv<NF><<<N, 1024, sm, st>>>(a.cspec, *a.plan, *a.plan_half, a.argmax, a.volume));
+    count_launches(1);
+    return cudaGetLastError();
+  }
+  dim3 gC((H2 + 15) / 16, N, 1);
+  const int nrowblk = (int)(((size_t)N * N + kRowsR2C - 1) / kRowsR2C);
+  PHGPU_DISPATCH_N(N,
+      k_fft_x<NF, true><<<gC, 256, (size_t)N * 16 * sizeof(float2), st>>>(N, a.cspec, *a.plan);
+      k_c2r_y<NF><<<nrowblk, 256, (size_t)kRowsR2C * N * sizeof(float2), st>>>(N, a.cspec, *a.plan, a.argmax, a.volume));
+  count_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spatial_combine(const SpatialArgs& a, cudaStream_t st) {
+  cudaError_t e = launch_spatial_fuse_z(a, st);
+  if (e == cudaSuccess) e = launch_spatial_inverse(a, st);
+  return e;
 }
 
 }  // namespace phgpu

@@ -5,10 +5,16 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "common.cuh"
 #include "fft.cuh"
 
 namespace phgpu {
+
+// Number of kernels this library has launched (all contexts).
+extern std::atomic<unsigned long long> g_launch_count;
+inline void count_launches(int n) { g_launch_count.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 
 // ------------------------------------------------------------ S^2 sampling
 struct SampleArgs {
@@ -66,7 +72,8 @@ struct So3Args {
   unsigned long long* argmax;  // packed (value^2, index)
   float* volume;          // optional (2 bw_out)^3 |z|^2, [beta][alpha][gamma]
 };
-cudaError_t launch_so3(const So3Args& a, cudaStream_t st);
+cudaError_t launch_so3_synth(const So3Args& a, cudaStream_t st);  // coefficient product + Wigner synthesis
+cudaError_t launch_so3_fft(const So3Args& a, cudaStream_t st);    // alpha FFT + gamma C2R + argmax
 cudaError_t so3_init_attributes();  // once per device
 
 // ------------------------------------------------------------ spatial
@@ -94,14 +101,21 @@ struct SpatialArgs {
   const float* grids_f;   // [n_data_ch + 1][N^3] target sums + count (normalised here)
   const float* grids_g;   // source
   int grids_are_means;    // 1: grids already hold values (no count plane)
-  float2* spec;           // [2 n_data_ch][N][N][N/2+1]
-  float2* cspec;          // [N][N][N/2+1]
+  float2* spec;           // [2 n_data_ch][N (z)][N (x)][H2p (ky)]
+  float2* cspec;          // [N][N][H2p]
   const FftPlan* plan;    // length N
+  const FftPlan* plan_half;  // length N/2 (z-slab kernels), may be null
   unsigned long long* argmax;
   float* volume;          // optional N^3 correlation, [z][x][y]
 };
 cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t st);
 cudaError_t launch_spatial_combine(const SpatialArgs& a, cudaStream_t st);
+cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st);   // z FFTs + fusion + cross power
+cudaError_t launch_spatial_inverse(const SpatialArgs& a, cudaStream_t st);  // inverse x + C2R y + argmax
 cudaError_t spatial_init_attributes();  // once per device
+// Row length of the half spectra: N/2 + 1 rounded up to 8 complex (64 B).
+__host__ __device__ inline int spatial_h2p(int N) { return ((N / 2 + 1) + 7) / 8 * 8; }
+// True when the fused z-slab kernels handle this N (the slab fits in shared memory).
+bool spatial_slab_path(int N);
 
 }  // namespace phgpu

@@ -30,6 +30,10 @@ using Clock = std::chrono::steady_clock;
 struct Request {
   uint64_t ticket = 0;
   phgpu_params prm;
+  // device-resident inputs are used in place (the caller keeps them alive
+  // until the ticket completes); host inputs are copied at submit
+  phgpu_cloud tdev{}, sdev{};
+  bool on_device = false;
   std::vector<float> txyzi, trefl, tamb, sxyzi, srefl, samb;
   uint32_t tn = 0, sn = 0;
   bool t_refl = false, t_amb = false, s_refl = false, s_amb = false;
@@ -53,7 +57,7 @@ ShapeKey key_of(const phgpu_params& p) {
 // Device bytes of one context (upper estimate used for admission).
 uint64_t estimate_bytes(const phgpu_params& p, uint32_t max_points) {
   const uint64_t bw = p.spherical_bandwidth, bo = bw + p.spherical_zero_padding, N = p.spatial_n_voxels;
-  const uint64_t nv = N * N * N, H = N * N * (N / 2 + 1);
+  const uint64_t nv = N * N * N, H = N * N * ((N / 2 + 1 + 7) / 8 * 8);
   uint64_t b = 0;
   b += 4 * 4 * bw * bw * 2;                 // samples
   b += 8 * bw * 2 * bw * 8 + 8 * bw * bw * 8;  // fm, coef
@@ -144,6 +148,10 @@ struct phgpu_server {
                     r->t_amb ? r->tamb.data() : nullptr, r->tn, 0};
       phgpu_cloud s{r->sxyzi.data(), r->s_refl ? r->srefl.data() : nullptr,
                     r->s_amb ? r->samb.data() : nullptr, r->sn, 0};
+      if (r->on_device) {
+        t = r->tdev;
+        s = r->sdev;
+      }
       const int rc = phgpu_register_pair(ctx, &t, &s, &r->pose);
       std::lock_guard<std::mutex> lk(mu);
       r->status = rc;
@@ -221,8 +229,14 @@ int phgpu_server_submit(phgpu_server* s, const phgpu_params* params, const phgpu
   r->prm = *params;
   r->tn = target->n_points;
   r->sn = source->n_points;
-  copy_cloud(target, r->txyzi, r->trefl, r->tamb, r->t_refl, r->t_amb);
-  copy_cloud(source, r->sxyzi, r->srefl, r->samb, r->s_refl, r->s_amb);
+  if (target->on_device && source->on_device) {
+    r->on_device = true;
+    r->tdev = *target;
+    r->sdev = *source;
+  } else {
+    copy_cloud(target, r->txyzi, r->trefl, r->tamb, r->t_refl, r->t_amb);
+    copy_cloud(source, r->sxyzi, r->srefl, r->samb, r->s_refl, r->s_amb);
+  }
   r->t_submit = Clock::now();
   {
     std::lock_guard<std::mutex> lk(s->mu);

@@ -91,6 +91,8 @@ EXPORTED = [
     "phgpu_spatial_result", "phgpu_register_pair", "phgpu_pose_from_bin",
     "phgpu_translation_from_index", "phgpu_server_create", "phgpu_server_destroy",
     "phgpu_server_submit", "phgpu_server_poll", "phgpu_server_drain", "phgpu_server_last_error",
+    "phgpu_profile_enable", "phgpu_profile_read", "phgpu_profile_stage_count",
+    "phgpu_profile_stage_name", "phgpu_launch_count",
 ]
 
 _LIB = None
@@ -136,6 +138,12 @@ def load(path: str = LIB_PATH):
     lib.phgpu_server_drain.argtypes = [vp]
     lib.phgpu_server_last_error.restype = C.c_char_p
     lib.phgpu_server_last_error.argtypes = [vp]
+    lib.phgpu_profile_enable.argtypes = [vp, C.c_int]
+    lib.phgpu_profile_read.argtypes = [vp, vp, vp, C.c_int]
+    lib.phgpu_profile_stage_count.restype = C.c_int
+    lib.phgpu_profile_stage_name.restype = C.c_char_p
+    lib.phgpu_profile_stage_name.argtypes = [C.c_int]
+    lib.phgpu_launch_count.restype = C.c_ulonglong
     _LIB = lib
     return lib
 
@@ -175,6 +183,10 @@ def make_cloud(xyzi, reflectivity=None, ambient=None) -> tuple[Cloud, list]:
     n = int(xyzi.shape[0])
     c = Cloud(_addr(xyzi), _addr(reflectivity), _addr(ambient), n, on_dev)
     return c, keep
+
+
+def launch_count() -> int:
+    return int(load().phgpu_launch_count())
 
 
 def translation_from_index(index, n_voxels, lower, upper) -> float:
@@ -237,6 +249,18 @@ class Context:
     @property
     def stream(self):
         return self.lib.phgpu_stream(self.h)
+
+    # ---- tracing
+    def profile(self, enable=True):
+        self.check(self.lib.phgpu_profile_enable(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        n = self.lib.phgpu_profile_stage_count()
+        ms = np.zeros(n)
+        calls = np.zeros(n, np.uint64)
+        self.check(self.lib.phgpu_profile_read(self.h, ms.ctypes.data, calls.ctypes.data, n))
+        names = [self.lib.phgpu_profile_stage_name(i).decode() for i in range(n)]
+        return {nm: (float(ms[i]), int(calls[i])) for i, nm in enumerate(names)}
 
     # ---- sampling
     def sample_s2(self, xyzi, reflectivity=None, ambient=None, side=0):
@@ -309,3 +333,57 @@ class Context:
         pose = Pose()
         self.check(self.lib.phgpu_register_pair(self.h, C.byref(ct), C.byref(cs), C.byref(pose)))
         return pose
+
+
+class Server:
+    """Continuous-batching request server (C ABI phgpu_server_*)."""
+
+    def __init__(self, workers=4, hbm_budget_bytes=150 << 30, max_points=1 << 18, device=0, flags=0):
+        lib = load()
+        self.lib = lib
+        sp = ServerParams(int(hbm_budget_bytes), int(workers), int(max_points), int(device), int(flags))
+        h = C.c_void_p()
+        rc = lib.phgpu_server_create(C.byref(sp), C.byref(h))
+        if rc != PHGPU_OK:
+            raise PhgpuError(f"phgpu_server_create failed ({rc})")
+        self.h = h
+        self._keep = {}
+
+    def submit(self, params: Params, target, source) -> int:
+        ct, k1 = make_cloud(*target)
+        cs, k2 = make_cloud(*source)
+        t = C.c_uint64()
+        rc = self.lib.phgpu_server_submit(self.h, C.byref(params), C.byref(ct), C.byref(cs), C.byref(t))
+        if rc != PHGPU_OK:
+            raise PhgpuError(f"submit failed ({rc}): {self.lib.phgpu_server_last_error(self.h).decode()}")
+        if ct.on_device:
+            self._keep[t.value] = (k1, k2)  # device inputs are read in place
+        return t.value
+
+    def poll(self, ticket):
+        pose = Pose()
+        lat = C.c_double()
+        rc = self.lib.phgpu_server_poll(self.h, C.c_uint64(ticket), C.byref(pose), C.byref(lat))
+        if rc < 0:
+            raise PhgpuError(f"request {ticket} failed ({rc}): {self.lib.phgpu_server_last_error(self.h).decode()}")
+        if rc == 0:
+            return None
+        self._keep.pop(ticket, None)
+        return pose, lat.value
+
+    def drain(self):
+        rc = self.lib.phgpu_server_drain(self.h)
+        if rc != PHGPU_OK:
+            raise PhgpuError(f"drain failed ({rc})")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.phgpu_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

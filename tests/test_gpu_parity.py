@@ -1,0 +1,254 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerances: integer / index results (rotation bin, translation voxel, sample
+nearest-neighbour indices, voxel indices) must be identical; FP32 correlation
+volumes must be within a relative L2 error of 1e-5 of the FP64 oracle.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+REL_L2 = 1e-5
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "soft_reference_small.npz")
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def nat():
+    from phaser_b200 import native
+    native.load()
+    return native
+
+
+def ctx(nat, **kw):
+    kw.setdefault("spherical_bandwidth", 4)
+    kw.setdefault("spatial_n_voxels", 4)
+    return nat.Context(**kw)
+
+
+def test_spatial_delta_known_answer(nat):
+    # phaser_core/test/translation-alignment/spatial-correlation-test.cc:59-79
+    f = np.zeros(27)
+    g = np.zeros(27)
+    f[0] = 1
+    g[1] = 1
+    c = ctx(nat, spatial_n_voxels=3, spatial_fusion=nat.PHGPU_FUSION_NONE)
+    c.spatial_correlate([f], [g])
+    vox, _ = c.spatial_result()
+    assert list(O.ind2sub(vox, 3, 3)) == [0, 2, 0]
+
+
+@pytest.mark.parametrize("N,C", [(3, 4), (4, 4), (5, 3), (8, 4), (9, 2), (16, 4), (30, 3), (64, 4),
+                                 (128, 3), (40, 2)])
+def test_spatial_laplace_vs_oracle(nat, N, C):
+    rng = np.random.default_rng(N * 7 + C)
+    f = rng.standard_normal((C, N ** 3))
+    g = rng.standard_normal((C, N ** 3))
+    c = ctx(nat, spatial_n_voxels=N, flags=nat.PHGPU_FLAG_KEEP_VOLUMES)
+    c.spatial_correlate(list(f), list(g))
+    vox, peak, vol = c.spatial_result(volume=True)
+    ref = O.spatial_correlation(f, g, N, laplace=True)
+    assert rel_l2(vol, ref) <= REL_L2
+    assert vox == O.argmax(ref)
+
+
+@pytest.mark.parametrize("N", [3, 6, 10, 32, 64])
+def test_spatial_plain_vs_oracle(nat, N):
+    rng = np.random.default_rng(N)
+    f = rng.random((1, N ** 3))
+    g = rng.random((1, N ** 3))
+    c = ctx(nat, spatial_n_voxels=N, spatial_fusion=nat.PHGPU_FUSION_NONE,
+            flags=nat.PHGPU_FLAG_KEEP_VOLUMES)
+    c.spatial_correlate(list(f), list(g))
+    vox, peak, vol = c.spatial_result(volume=True)
+    ref = O.spatial_correlation(f, g, N, laplace=False)
+    assert rel_l2(vol, ref) <= REL_L2
+    assert vox == O.argmax(ref)
+
+
+def test_spatial_shift_property_full_size(nat):
+    # size-independent property at N = 200: every channel of the source is the
+    # target circularly shifted by d voxels -> C(k) = w(k) e^{i k d} with w >= 0
+    # for all three fusion rules, so the correlation peaks exactly at the shift.
+    N = 200
+    rng = np.random.default_rng(5)
+    f = rng.random((3, N, N, N), dtype=np.float32).astype(np.float64)
+    d = (17, 181, 3)  # (z, x, y)
+    g = np.roll(f, shift=(-d[0], -d[1], -d[2]), axis=(1, 2, 3))
+    c = ctx(nat, spatial_n_voxels=N)
+    c.spatial_correlate([x.reshape(-1) for x in f], [x.reshape(-1) for x in g])
+    vox, _ = c.spatial_result()
+    assert vox == (d[0] * N + d[1]) * N + d[2]
+
+
+@pytest.mark.parametrize("bw,pad,C", [(4, 0, 1), (8, 0, 4), (8, 2, 4), (12, 0, 3), (16, 0, 2),
+                                      (16, 3, 4), (32, 0, 4), (25, 0, 3)])
+def test_spherical_vs_oracle(nat, bw, pad, C):
+    rng = np.random.default_rng(bw * 100 + pad * 10 + C)
+    f = rng.standard_normal((C, 4 * bw * bw))
+    g = rng.standard_normal((C, 4 * bw * bw))
+    c = ctx(nat, spherical_bandwidth=bw, spherical_zero_padding=pad, flags=nat.PHGPU_FLAG_KEEP_VOLUMES)
+    c.sph_correlate(list(f), list(g))
+    b, peak, vol = c.sph_result(volume=True)
+    ref = O.spherical_correlation(f, g, bw, bw + pad)
+    assert rel_l2(vol, ref) <= REL_L2
+    assert b == O.argmax(ref)
+    assert c.lib.phgpu_sph_bandwidth(c.h) == bw + pad
+
+
+def test_spherical_vs_soft_golden(nat):
+    # fixtures produced by the reference's own SOFT sources (tests/golden)
+    d = np.load(GOLD)
+    c = ctx(nat, spherical_bandwidth=8, flags=nat.PHGPU_FLAG_KEEP_VOLUMES)
+    c.sph_correlate(list(d["sph_b8_f"]), list(d["sph_b8_g"]))
+    b, _, vol = c.sph_result(volume=True)
+    assert b == int(d["sph_b8_argmax"])
+    assert rel_l2(vol, d["sph_b8_corr"]) <= REL_L2
+    c1 = ctx(nat, spherical_bandwidth=6, spherical_zero_padding=2, flags=nat.PHGPU_FLAG_KEEP_VOLUMES)
+    c1.sph_correlate(list(d["sph1_b6p2_f"]), list(d["sph1_b6p2_g"]))
+    b1, _, vol1 = c1.sph_result(volume=True)
+    assert b1 == int(np.argmax(d["sph1_b6p2_corr"]))
+    assert rel_l2(vol1, d["sph1_b6p2_corr"]) <= REL_L2
+
+
+def test_spatial_vs_golden(nat):
+    d = np.load(GOLD)
+    c = ctx(nat, spatial_n_voxels=6, flags=nat.PHGPU_FLAG_KEEP_VOLUMES)
+    c.spatial_correlate(list(d["spat_n6_f"]), list(d["spat_n6_g"]))
+    v, _, vol = c.spatial_result(volume=True)
+    assert v == int(np.argmax(d["spat_n6_c"]))
+    assert rel_l2(vol, d["spat_n6_c"]) <= REL_L2
+
+
+@pytest.fixture(scope="module")
+def pair0():
+    from phaser_b200 import scene
+    return scene.workload_pair(0, 0)
+
+
+def test_sampling_vs_oracle(nat, pair0):
+    bw = 32
+    c = ctx(nat, spherical_bandwidth=bw)
+    for side, cl in enumerate([pair0.target, pair0.source]):
+        c.sample_s2(cl.xyzi, cl.reflectivity, side=side)
+        vals, idx = c.samples(side)
+        ov, oidx = O.sample_cloud(cl.xyzi, cl.reflectivity, None, bw)
+        # nearest-neighbour assignment is exact on these inputs (see DESIGN: the
+        # projection rounds acos/atan2 once, glibc's float versions may differ
+        # by one ulp, which did not change any nearest neighbour here)
+        assert np.array_equal(idx, oidx)
+        np.testing.assert_allclose(vals[0], ov[0], rtol=1e-7)   # range (float of double)
+        np.testing.assert_array_equal(vals[1], ov[1].astype(np.float32))  # intensity
+
+
+def test_sampling_rejection_and_empty(nat):
+    # max squared distance from the low-pass bounds / n_voxels (point-cloud.cc:66-72)
+    bw = 8
+    c = ctx(nat, spherical_bandwidth=bw, spatial_low_pass_lower=0, spatial_low_pass_upper=1,
+            spatial_n_voxels=2)  # (1/2)^2 = 0.25 squared distance
+    pts = np.array([[3.0, 0.0, 0.0, 0.5], [0.0, 0.0, -2.0, 0.25]], np.float32)
+    c.sample_s2(pts, side=0)
+    vals, idx = c.samples(0)
+    ov, oidx = O.sample_cloud(pts, None, None, bw, max_sq=0.25)
+    assert np.array_equal(idx, oidx)
+    assert (idx == -1).any() and (idx >= 0).any()
+    np.testing.assert_allclose(vals, ov.astype(np.float32), rtol=1e-7)
+    # points without a direction (origin, NaN) are never sampled
+    pts2 = np.array([[0.0, 0.0, 0.0, 0.9], [np.nan, 1.0, 0.0, 0.8], [0.0, 2.0, 0.0, 0.3],
+                     [1.0, 1.0, 1.0, 0.7]], np.float32)
+    c2 = ctx(nat, spherical_bandwidth=bw)
+    c2.sample_s2(pts2, side=0)
+    vals2, idx2 = c2.samples(0)
+    ov2, oidx2 = O.sample_cloud(pts2, None, None, bw)
+    assert np.array_equal(idx2, oidx2)
+    assert set(np.unique(idx2)) <= {2, 3}
+    # empty cloud: every sample dropped
+    c.sample_s2(np.zeros((0, 4), np.float32), side=1)
+    vals, idx = c.samples(1)
+    assert (idx == -1).all() and (vals == 0).all()
+
+
+def test_voxel_index_exact_with_edge_cases(nat, pair0):
+    N, lo, hi = 64, -10, 10
+    c = ctx(nat, spatial_n_voxels=N, spatial_discretize_lower=lo, spatial_discretize_upper=hi)
+    edge = np.array([[10.0, 10.0, 10.0, 1], [-10.0, -10.0, -10.0, 1], [-11.0, 0.0, 0.0, 1],
+                     [0.0, -11.0, 0.0, 1], [0.0, 0.0, -11.0, 1], [11.0, 11.0, 11.0, 1],
+                     [np.nan, 0.0, 0.0, 1], [0.0, 0.0, 9.9999, 1]], np.float32)
+    pts = np.concatenate([pair0.target.xyzi, edge])
+    c.voxelize(pts, None, side=0)
+    lin = c.voxel_index(0, pts.shape[0])
+    assert np.array_equal(lin, O.voxel_index(pts, N, lo, hi))
+    T = O.rotation_xyz(0.7, -0.3, 2.9)
+    c.voxelize(pair0.source.xyzi, None, side=1, T=T)
+    lin = c.voxel_index(1, pair0.source.xyzi.shape[0])
+    assert np.array_equal(lin, O.voxel_index(O.transform(pair0.source.xyzi, T), N, lo, hi))
+
+
+def _register_and_compare(nat, w, pair, want_volumes):
+    c = ctx(nat, spherical_bandwidth=w["bw"], spatial_n_voxels=w["n_voxels"],
+            spatial_discretize_lower=w["lo"], spatial_discretize_upper=w["hi"],
+            flags=nat.PHGPU_FLAG_KEEP_VOLUMES if want_volumes else 0)
+    pose = c.register_pair((pair.target.xyzi, pair.target.reflectivity),
+                           (pair.source.xyzi, pair.source.reflectivity))
+    res = O.register_pair(pair.target.xyzi, pair.target.reflectivity, pair.source.xyzi,
+                          pair.source.reflectivity, w["bw"], w["n_voxels"], w["lo"], w["hi"],
+                          want_volumes=want_volumes)
+    opose = res[0] if want_volumes else res
+    assert pose.rot_bin == opose.rot_bin
+    assert pose.voxel == opose.voxel
+    assert list(pose.xyz) == list(opose.xyz)
+    assert list(pose.trans) == list(opose.trans)
+    if want_volumes:
+        _, _, rvol = c.sph_result(volume=True)
+        _, _, tvol = c.spatial_result(volume=True)
+        assert rel_l2(rvol, res[1]) <= REL_L2
+        assert rel_l2(tvol, res[2]) <= REL_L2
+    return c, pose
+
+
+def test_register_pair_workload0(nat, pair0):
+    from phaser_b200 import scene
+    _register_and_compare(nat, scene.WORKLOADS[0], pair0, want_volumes=True)
+
+
+@pytest.mark.parametrize("k", [0, 1])
+def test_register_pair_workload1_full_size(nat, k):
+    # B = 100, N = 200, ~130k points, 3 channels: the benchmark workload
+    from phaser_b200 import scene
+    pair = scene.workload_pair(1, k)
+    c, pose = _register_and_compare(nat, scene.WORKLOADS[1], pair, want_volumes=(k == 0))
+    # same result when called again on the same context (state fully reset)
+    pose2 = c.register_pair((pair.target.xyzi, pair.target.reflectivity),
+                            (pair.source.xyzi, pair.source.reflectivity))
+    assert (pose2.rot_bin, pose2.voxel) == (pose.rot_bin, pose.voxel)
+
+
+def test_device_resident_inputs(nat, pair0):
+    import torch
+    from phaser_b200 import scene
+    w = scene.WORKLOADS[0]
+    c = ctx(nat, spherical_bandwidth=w["bw"], spatial_n_voxels=w["n_voxels"],
+            spatial_discretize_lower=w["lo"], spatial_discretize_upper=w["hi"])
+    t = torch.from_numpy(pair0.target.xyzi).cuda()
+    s = torch.from_numpy(pair0.source.xyzi).cuda()
+    p_dev = c.register_pair((t, None), (s, None))
+    p_host = c.register_pair((pair0.target.xyzi, None), (pair0.source.xyzi, None))
+    assert (p_dev.rot_bin, p_dev.voxel) == (p_host.rot_bin, p_host.voxel)
+
+
+def test_invalid_configuration_reports_error(nat):
+    with pytest.raises(nat.PhgpuError):
+        nat.Context(spherical_bandwidth=4, spatial_n_voxels=4, spatial_zero_padding=2)
+    with pytest.raises(nat.PhgpuError):
+        nat.Context(spherical_bandwidth=4, spatial_n_voxels=131)  # prime factor above 128
+    c = ctx(nat)
+    with pytest.raises(nat.PhgpuError):
+        c.sph_result()  # nothing computed yet
