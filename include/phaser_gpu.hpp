@@ -1,0 +1,260 @@
+// phaser_gpu.hpp -- header-only C++ drop-ins for phaser_core's correlation and
+// aligner classes, backed by the C ABI of phaser_gpu.h (B200, sm_100a).
+//
+// The class names, constructor arguments and member functions follow
+//   SphericalCorrelation          phaser_core/include/phaser/backend/correlation/spherical-correlation.h:19-33
+//   SphericalCorrelationLaplace   .../spherical-correlation-laplace.h
+//   SpatialCorrelation            .../spatial-correlation.h:15-23
+//   SpatialCorrelationLaplace     .../spatial-correlation-laplace.h
+//   PhaseAligner                  phaser_core/include/phaser/backend/alignment/phase-aligner.h:17-26
+//   SphOptRegistration            phaser_core/include/phaser/backend/registration/sph-opt-registration.h
+// so a caller swaps the include and the namespace (phaser_gpu instead of
+// phaser_core).  Errors throw std::runtime_error (the reference aborts through
+// glog CHECKs instead).  Eigen::VectorXd arguments are accepted when Eigen is
+// included before this header (PHASER_GPU_WITH_EIGEN), raw double pointers
+// otherwise.
+#ifndef PHASER_GPU_HPP_
+#define PHASER_GPU_HPP_
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "phaser_gpu.h"
+
+#if defined(EIGEN_WORLD_VERSION) && !defined(PHASER_GPU_WITH_EIGEN)
+#define PHASER_GPU_WITH_EIGEN 1
+#endif
+
+namespace phaser_gpu {
+
+using SampledSignal = std::vector<double>;
+
+// Flag-backed parameters with the reference's defaults
+// (phaser_common/src/common/core-gflags.cc:6-40).
+inline phgpu_params default_params() {
+  phgpu_params p;
+  phgpu_params_default(&p);
+  return p;
+}
+
+namespace detail {
+inline void check(int rc, const phgpu_ctx* ctx, const char* what) {
+  if (rc != PHGPU_OK)
+    throw std::runtime_error(std::string(what) + ": " + phgpu_last_error(ctx));
+}
+
+// Owns one device context.
+class Context {
+ public:
+  explicit Context(const phgpu_params& p) {
+    check(phgpu_ctx_create(&p, &ctx_), nullptr, "phgpu_ctx_create");
+  }
+  ~Context() { phgpu_ctx_destroy(ctx_); }
+  Context(const Context&) = delete;
+  Context& operator=(const Context&) = delete;
+  phgpu_ctx* get() const { return ctx_; }
+
+ private:
+  phgpu_ctx* ctx_ = nullptr;
+};
+}  // namespace detail
+
+// SphericalCorrelation(bw, zero_padding): single-signal correlation
+// (correlateSampledSignals uses the first channel, spherical-correlation.cc:69-80).
+class SphericalCorrelation {
+ public:
+  explicit SphericalCorrelation(const uint32_t bw = 100, const uint32_t zero_padding = 0,
+                                const phgpu_params& base = default_params())
+      : SphericalCorrelation(bw, zero_padding, PHGPU_FUSION_NONE, base) {}
+  virtual ~SphericalCorrelation() { delete ctx_; }
+
+  // f[c], g[c]: 4 bw^2 samples in [theta][phi] order.
+  virtual void correlateSampledSignals(const std::vector<SampledSignal>& f,
+                                       const std::vector<SampledSignal>& g) {
+    if (f.size() != g.size() || f.empty())
+      throw std::invalid_argument("correlateSampledSignals: channel counts differ or are zero");
+    const size_t nc = fusion_ == PHGPU_FUSION_LAPLACE ? f.size() : 1;
+    std::vector<const double*> fp(nc), gp(nc);
+    for (size_t c = 0; c < nc; ++c) {
+      if (f[c].size() != 4ull * bw_ * bw_ || g[c].size() != 4ull * bw_ * bw_)
+        throw std::invalid_argument("correlateSampledSignals: expected 4 bw^2 samples per channel");
+      fp[c] = f[c].data();
+      gp[c] = g[c].data();
+    }
+    detail::check(phgpu_sph_correlate(ctx_->get(), fp.data(), gp.data(), (uint32_t)nc), ctx_->get(),
+                  "phgpu_sph_correlate");
+    have_ = true;
+  }
+
+  // |z|^2 over the (2 bw_out)^3 grid, [beta][alpha][gamma].
+  std::vector<double> getCorrelation() const {
+    std::vector<double> out((size_t)8 * bw_out_ * bw_out_ * bw_out_);
+    if (have_)
+      detail::check(phgpu_sph_result(ctx_->get(), nullptr, nullptr, out.data()), ctx_->get(),
+                    "phgpu_sph_result");
+    return out;
+  }
+  // argmax bin of the last correlation (what PhaseCorrelationEval extracts)
+  uint32_t getPeakBin() const {
+    uint32_t b = 0;
+    detail::check(phgpu_sph_result(ctx_->get(), &b, nullptr, nullptr), ctx_->get(), "phgpu_sph_result");
+    return b;
+  }
+  uint32_t getBandwidth() const noexcept { return bw_out_; }
+  void shutdown() {}
+
+ protected:
+  SphericalCorrelation(const uint32_t bw, const uint32_t zero_padding, const uint32_t fusion,
+                       const phgpu_params& base)
+      : bw_(bw), bw_out_(bw + zero_padding), fusion_(fusion) {
+    phgpu_params p = base;
+    p.spherical_bandwidth = bw;
+    p.spherical_zero_padding = zero_padding;
+    p.spherical_fusion = fusion;
+    p.flags |= PHGPU_FLAG_KEEP_VOLUMES;
+    if (p.spatial_n_voxels == 0) p.spatial_n_voxels = 4;
+    ctx_ = new detail::Context(p);
+  }
+  uint32_t bw_, bw_out_, fusion_;
+  detail::Context* ctx_ = nullptr;
+  bool have_ = false;
+};
+
+// SphericalCorrelationLaplace: channel fusion, >= 2 channels
+// (spherical-correlation-laplace.cc:14-17).
+class SphericalCorrelationLaplace : public SphericalCorrelation {
+ public:
+  explicit SphericalCorrelationLaplace(const uint32_t bw = 100, const uint32_t zero_padding = 0,
+                                       const phgpu_params& base = default_params())
+      : SphericalCorrelation(bw, zero_padding, PHGPU_FUSION_LAPLACE, base) {}
+  void correlateSampledSignals(const std::vector<SampledSignal>& f,
+                               const std::vector<SampledSignal>& g) override {
+    if (f.size() < 2) throw std::invalid_argument("SphericalCorrelationLaplace needs at least 2 channels");
+    SphericalCorrelation::correlateSampledSignals(f, g);
+  }
+};
+
+// SpatialCorrelation(n_voxels, zero_padding) / SpatialCorrelationLaplace.
+// correlateSignals returns a pointer owned by the object, valid until the next
+// call (spatial-correlation.cc:128-175).
+class SpatialCorrelation {
+ public:
+  explicit SpatialCorrelation(const uint32_t n_voxels, const uint32_t zero_padding = 0,
+                              const phgpu_params& base = default_params())
+      : n_(n_voxels) {
+    if (zero_padding != 0) throw std::invalid_argument("spatial zero padding is not supported");
+    make(base, PHGPU_FUSION_NONE);
+  }
+  virtual ~SpatialCorrelation() { delete ctx_; }
+
+  double* correlateSignals(const std::vector<const double*>& f, const std::vector<const double*>& g) {
+    if (f.size() != g.size() || f.empty())
+      throw std::invalid_argument("correlateSignals: channel counts differ or are zero");
+    detail::check(phgpu_spatial_correlate(ctx_->get(), f.data(), g.data(), (uint32_t)f.size()),
+                  ctx_->get(), "phgpu_spatial_correlate");
+    c_.resize((size_t)n_ * n_ * n_);
+    detail::check(phgpu_spatial_result(ctx_->get(), &peak_voxel_, nullptr, c_.data()), ctx_->get(),
+                  "phgpu_spatial_result");
+    return c_.data();
+  }
+#ifdef PHASER_GPU_WITH_EIGEN
+  double* correlateSignals(const std::vector<Eigen::VectorXd*>& f, const std::vector<Eigen::VectorXd*>& g) {
+    std::vector<const double*> fp, gp;
+    for (auto* v : f) fp.push_back(v->data());
+    for (auto* v : g) gp.push_back(v->data());
+    return correlateSignals(fp, gp);
+  }
+#endif
+  uint32_t getZeroPadding() const { return 0; }
+  uint32_t getCorrelationSize() const { return n_ * n_ * n_; }
+  uint32_t getPeakVoxel() const { return peak_voxel_; }
+
+ protected:
+  SpatialCorrelation(const uint32_t n_voxels, int fusion, const phgpu_params& base) : n_(n_voxels) {
+    make(base, fusion);
+  }
+  void make(const phgpu_params& base, int fusion) {
+    phgpu_params p = base;
+    p.spatial_n_voxels = n_;
+    p.spatial_fusion = (uint32_t)fusion;
+    p.flags |= PHGPU_FLAG_KEEP_VOLUMES;
+    if (p.spherical_bandwidth < 2) p.spherical_bandwidth = 2;
+    ctx_ = new detail::Context(p);
+  }
+  uint32_t n_;
+  detail::Context* ctx_ = nullptr;
+  std::vector<double> c_;
+  uint32_t peak_voxel_ = 0;
+};
+
+class SpatialCorrelationLaplace : public SpatialCorrelation {
+ public:
+  explicit SpatialCorrelationLaplace(const uint32_t n_voxels, const uint32_t zero_padding = 0,
+                                     const phgpu_params& base = default_params())
+      : SpatialCorrelation(n_voxels, PHGPU_FUSION_LAPLACE, base) {
+    if (zero_padding != 0) throw std::invalid_argument("spatial zero padding is not supported");
+  }
+};
+
+// A cloud as the aligner and registration see it: x, y, z, intensity per
+// point and optional reflectivity / ambient (phaser_common's model::PointCloud).
+struct CloudView {
+  const float* xyzi = nullptr;
+  const float* reflectivity = nullptr;
+  const float* ambient = nullptr;
+  uint32_t n_points = 0;
+  bool on_device = false;
+  phgpu_cloud c() const { return phgpu_cloud{xyzi, reflectivity, ambient, n_points, on_device ? 1 : 0}; }
+};
+
+// PhaseAligner: voxelise both clouds and correlate (phase-aligner.cc:47-69).
+class PhaseAligner {
+ public:
+  explicit PhaseAligner(const phgpu_params& base = default_params()) : prm_(base) {
+    phgpu_params p = base;
+    p.flags |= PHGPU_FLAG_KEEP_VOLUMES;
+    ctx_ = new detail::Context(p);
+  }
+  ~PhaseAligner() { delete ctx_; }
+  void alignRegistered(const CloudView& prev, const CloudView& reg) {
+    phgpu_cloud a = prev.c(), b = reg.c();
+    detail::check(phgpu_voxelize(ctx_->get(), &a, 0, nullptr), ctx_->get(), "phgpu_voxelize");
+    detail::check(phgpu_voxelize(ctx_->get(), &b, 1, nullptr), ctx_->get(), "phgpu_voxelize");
+    detail::check(phgpu_spatial_correlate_voxelized(ctx_->get()), ctx_->get(), "phgpu_spatial_correlate");
+  }
+  std::vector<double> getCorrelation() const {
+    std::vector<double> out((size_t)prm_.spatial_n_voxels * prm_.spatial_n_voxels * prm_.spatial_n_voxels);
+    detail::check(phgpu_spatial_result(ctx_->get(), nullptr, nullptr, out.data()), ctx_->get(),
+                  "phgpu_spatial_result");
+    return out;
+  }
+  uint32_t getNumberOfVoxels() const noexcept { return prm_.spatial_n_voxels; }
+  // the reference returns the int bounds through uint32 (phase-aligner.cc:141-147)
+  uint32_t getLowerBound() const noexcept { return (uint32_t)prm_.spatial_discretize_lower; }
+  uint32_t getUpperBound() const noexcept { return (uint32_t)prm_.spatial_discretize_upper; }
+
+ private:
+  phgpu_params prm_;
+  detail::Context* ctx_ = nullptr;
+};
+
+// SphOptRegistration::registerPointCloud(prev = target, cur = source).
+class SphOptRegistration {
+ public:
+  explicit SphOptRegistration(const phgpu_params& base = default_params()) : ctx_(base) {}
+  phgpu_pose registerPointCloud(const CloudView& cloud_prev, const CloudView& cloud_cur) {
+    phgpu_cloud t = cloud_prev.c(), s = cloud_cur.c();
+    phgpu_pose pose;
+    detail::check(phgpu_register_pair(ctx_.get(), &t, &s, &pose), ctx_.get(), "phgpu_register_pair");
+    return pose;
+  }
+
+ private:
+  detail::Context ctx_;
+};
+
+}  // namespace phaser_gpu
+
+#endif  // PHASER_GPU_HPP_

@@ -1,0 +1,150 @@
+"""Python mirror of phaser_core's correlation, aligner and registration classes
+on top of the C ABI (phaser_b200.native).  Names, arguments and return values
+follow the reference:
+
+  SphericalSampler            phaser_common/include/phaser/common/spherical-sampler.h:13-18
+  SphericalCorrelation        phaser_core/include/phaser/backend/correlation/spherical-correlation.h:19-33
+  SphericalCorrelationLaplace .../spherical-correlation-laplace.h
+  SpatialCorrelation          .../spatial-correlation.h:15-23
+  SpatialCorrelationLaplace   .../spatial-correlation-laplace.h
+  PhaseAligner                phaser_core/include/phaser/backend/alignment/phase-aligner.h:17-26
+  SphOptRegistration          phaser_core/include/phaser/backend/registration/sph-opt-registration.h
+
+Everything runs on the GPU through libphaser_gpu.so; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import native
+from .native import Context, default_params
+
+
+class SphericalSampler:
+    """SphericalSampler(bw).sampleUniformly(cloud) -> [4, 4 bw^2] channels
+    {range, intensity, reflectivity, ambient} in [theta][phi] order."""
+
+    def __init__(self, bandwidth: int, **params):
+        self._bw = int(bandwidth)
+        self._ctx = Context(spherical_bandwidth=self._bw, spatial_n_voxels=params.pop("spatial_n_voxels", 4),
+                            **params)
+
+    def sampleUniformly(self, xyzi, reflectivity=None, ambient=None):
+        self._ctx.sample_s2(xyzi, reflectivity, ambient, side=0)
+        vals, _ = self._ctx.samples(0)
+        return vals
+
+    def getInitializedBandwith(self) -> int:
+        return self._bw
+
+
+class SphericalCorrelation:
+    """SphericalCorrelation(bw, zero_padding); correlateSampledSignals uses the
+    first channel (spherical-correlation.cc:69-80)."""
+
+    _fusion = native.PHGPU_FUSION_NONE
+
+    def __init__(self, bw: int = 100, zero_padding: int = 0):
+        self._bw = int(bw)
+        self._bw_out = int(bw) + int(zero_padding)
+        self._ctx = Context(spherical_bandwidth=self._bw, spherical_zero_padding=int(zero_padding),
+                            spatial_n_voxels=4, spherical_fusion=self._fusion,
+                            flags=native.PHGPU_FLAG_KEEP_VOLUMES)
+        self._have = False
+
+    def correlateSampledSignals(self, f, g):
+        if len(f) != len(g) or len(f) == 0:
+            raise ValueError("channel counts differ or are zero")
+        n = len(f) if self._fusion == native.PHGPU_FUSION_LAPLACE else 1
+        self._ctx.sph_correlate(list(f)[:n], list(g)[:n])
+        self._have = True
+
+    def getCorrelation(self) -> np.ndarray:
+        if not self._have:
+            return np.zeros(8 * self._bw_out ** 3)
+        return self._ctx.sph_result(volume=True)[2]
+
+    def getPeak(self):
+        return self._ctx.sph_result()
+
+    def getBandwidth(self) -> int:
+        return self._bw_out
+
+    def shutdown(self):
+        self._ctx.close()
+
+
+class SphericalCorrelationLaplace(SphericalCorrelation):
+    _fusion = native.PHGPU_FUSION_LAPLACE
+
+    def correlateSampledSignals(self, f, g):
+        if len(f) < 2:
+            raise ValueError("SphericalCorrelationLaplace needs at least 2 channels")
+        super().correlateSampledSignals(f, g)
+
+
+class SpatialCorrelation:
+    """SpatialCorrelation(n_voxels, zero_padding).correlateSignals(f, g) -> N^3
+    correlation (spatial-correlation.cc:128-175)."""
+
+    _fusion = native.PHGPU_FUSION_NONE
+
+    def __init__(self, n_voxels: int, zero_padding: int = 0):
+        if zero_padding:
+            raise ValueError("spatial zero padding is not supported")
+        self._n = int(n_voxels)
+        self._ctx = Context(spherical_bandwidth=2, spatial_n_voxels=self._n, spatial_fusion=self._fusion,
+                            flags=native.PHGPU_FLAG_KEEP_VOLUMES)
+
+    def correlateSignals(self, f, g) -> np.ndarray:
+        self._ctx.spatial_correlate(list(f), list(g))
+        return self._ctx.spatial_result(volume=True)[2]
+
+    def getZeroPadding(self) -> int:
+        return 0
+
+    def getCorrelationSize(self) -> int:
+        return self._n ** 3
+
+
+class SpatialCorrelationLaplace(SpatialCorrelation):
+    _fusion = native.PHGPU_FUSION_LAPLACE
+
+
+class PhaseAligner:
+    """PhaseAligner: voxelise both clouds and correlate (phase-aligner.cc:47-69)."""
+
+    def __init__(self, n_voxels=100, lower=-50, upper=50):
+        self._n, self._lo, self._hi = int(n_voxels), int(lower), int(upper)
+        self._ctx = Context(spherical_bandwidth=2, spatial_n_voxels=self._n, spatial_discretize_lower=self._lo,
+                            spatial_discretize_upper=self._hi, flags=native.PHGPU_FLAG_KEEP_VOLUMES)
+
+    def alignRegistered(self, cloud_prev, cloud_reg):
+        """cloud_* = (xyzi, reflectivity) or (xyzi, reflectivity, ambient)."""
+        self._ctx.voxelize(*cloud_prev, side=0)
+        self._ctx.voxelize(*cloud_reg, side=1)
+        self._ctx.spatial_correlate_voxelized()
+
+    def getCorrelation(self) -> np.ndarray:
+        return self._ctx.spatial_result(volume=True)[2]
+
+    def getNumberOfVoxels(self) -> int:
+        return self._n
+
+    def getLowerBound(self) -> int:
+        return self._lo
+
+    def getUpperBound(self) -> int:
+        return self._hi
+
+
+class SphOptRegistration:
+    """registerPointCloud(prev = target, cur = source) -> pose dict
+    (sph-opt-registration.cc:34-95)."""
+
+    def __init__(self, bandwidth=75, n_voxels=100, lower=-50, upper=50, **params):
+        self._ctx = Context(spherical_bandwidth=int(bandwidth), spatial_n_voxels=int(n_voxels),
+                            spatial_discretize_lower=int(lower), spatial_discretize_upper=int(upper), **params)
+
+    def registerPointCloud(self, cloud_prev, cloud_cur) -> dict:
+        return self._ctx.register_pair(cloud_prev, cloud_cur).as_dict()

@@ -1,0 +1,57 @@
+// Drives the C++ drop-ins of include/phaser_gpu.hpp the way phaser_core's
+// registration calls the reference classes; prints one line per check.
+// Built and run by tests/test_cpp_dropin.py.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "phaser_gpu.hpp"
+
+int main() {
+  using namespace phaser_gpu;
+  // spatial delta known answer (phaser_core/test/translation-alignment/
+  // spatial-correlation-test.cc:59-79): f[0] = 1, g[1] = 1 -> Ind2Sub (0, 2, 0)
+  {
+    std::vector<double> f(27, 0.0), g(27, 0.0);
+    f[0] = 1.0;
+    g[1] = 1.0;
+    SpatialCorrelation corr(3u);
+    double* c = corr.correlateSignals({f.data()}, {g.data()});
+    size_t best = 0;
+    for (size_t i = 1; i < 27; ++i)
+      if (c[i] > c[best]) best = i;
+    const unsigned x = (best / 3) % 3, y = best % 3, z = best / 9;
+    std::printf("spatial_delta %u %u %u\n", x, y, z);
+    if (!(x == 0 && y == 2 && z == 0)) return 1;
+  }
+  // Laplace spherical correlation of 4 channels through the drop-in
+  {
+    const uint32_t bw = 8;
+    std::vector<SampledSignal> f(4, SampledSignal(4 * bw * bw)), g(4, SampledSignal(4 * bw * bw));
+    unsigned s = 12345;
+    for (auto* side : {&f, &g})
+      for (auto& ch : *side)
+        for (auto& v : ch) {
+          s = s * 1103515245u + 12345u;
+          v = ((s >> 8) & 0xffff) / 65535.0 - 0.5;
+        }
+    SphericalCorrelationLaplace corr(bw);
+    corr.correlateSampledSignals(f, g);
+    const std::vector<double> vol = corr.getCorrelation();
+    size_t best = 0;
+    for (size_t i = 1; i < vol.size(); ++i)
+      if (vol[i] > vol[best]) best = i;
+    std::printf("sph_laplace_bin %zu %u bw_out %u\n", best, corr.getPeakBin(), corr.getBandwidth());
+    if (best != corr.getPeakBin() || vol.size() != 8u * bw * bw * bw) return 2;
+  }
+  // invalid configuration is reported as an exception, not an abort
+  try {
+    SpatialCorrelation bad(4u, 2u);
+    return 3;
+  } catch (const std::invalid_argument&) {
+    std::printf("zero_padding_rejected\n");
+  }
+  std::printf("ok\n");
+  return 0;
+}
