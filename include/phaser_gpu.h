@@ -167,6 +167,14 @@ const char* phgpu_profile_stage_name(int stage);
 /* Kernels launched by this library since it was loaded (all contexts). */
 unsigned long long phgpu_launch_count(void);
 
+/* Self-test of the shared-memory FFT engines (no reference counterpart):
+ * transforms ntrans sequences of length n (complex interleaved, natural order,
+ * sequence-major, in place in `data`) laid out as shared-memory rows or
+ * columns; engine 0 = runtime plan, 1 = compile-time plan, 2 = register-tail
+ * plan (1 and 2 for n in {32, 64, 100, 128, 200, 256, 512}).  Forward =
+ * exp(-2 pi i jk/n), inverse = exp(+2 pi i jk/n), both unnormalised. */
+int phgpu_selftest_fft(int n, int ntrans, int inverse, int columns, int engine, float* data);
+
 /* ------------------------------------------------------------------ serving
  * Continuous-batching request server (no reference counterpart: the
  * reference registers one pair at a time, sph-opt-registration.cc:34-47).

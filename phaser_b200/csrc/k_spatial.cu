@@ -23,6 +23,7 @@
 // tile) + fusion + cross power + inverse FFT along z; C1 inverse FFT along x;
 // C2 complex-to-real along y with argmax.  Forward transforms leave x and z in
 // digit-reversed order; the inverse transforms consume that order directly.
+#include "fft2.cuh"
 #include "kernels.h"
 
 namespace phgpu {
@@ -279,14 +280,18 @@ __global__ void k_c2r_y(int N, const float2* __restrict__ cspec, FftPlan plan,
 //   A = (W[ky][k] + conj W[-ky][-k]) / 2,  B = (W[ky][k] - conj W[-ky][-k]) / 2i,
 // and combined over the even/odd x split,
 //   X[k][ky] = A + w_N^k B,  X[k + N/2][ky] = A - w_N^k B.
-// Output rows are in natural kx order.
+// Output rows are in natural kx order.  Shared rows have the odd stride N + 1.
+
+// mean of a voxel: sum / count, 0 for empty voxels (reference: non-finite -> 0)
+__device__ __forceinline__ float voxel_mean(float v, float c) { return c > 0.0f ? v * __frcp_rn(c) : 0.0f; }
+
 template <int NF>
-__global__ void __launch_bounds__(1024) k_slab_fwd(const float* __restrict__ grids, size_t grid_cstride,
+__global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __restrict__ grids, size_t grid_cstride,
                                                    const float* __restrict__ count, float2* __restrict__ spec,
                                                    size_t spec_cstride, FftPlan pN, FftPlan pH) {
-  constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1, Q = NF / 4;
+  constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1, Q = NF / 4, S = NF + 1;
   const int H2p = spatial_h2p(N);
-  extern __shared__ float2 W[];  // [NH][N]
+  extern __shared__ float2 W[];  // [NH][S]
   const int z = blockIdx.x, c = blockIdx.y;
   const float* g = grids + (size_t)c * grid_cstride + (size_t)z * N * N;
   const float* cnt = count ? count + (size_t)z * N * N : nullptr;
@@ -297,30 +302,23 @@ __global__ void __launch_bounds__(1024) k_slab_fwd(const float* __restrict__ gri
     if (cnt) {
       const float4 ca = *reinterpret_cast<const float4*>(cnt + (size_t)(2 * r) * N + y4);
       const float4 cb = *reinterpret_cast<const float4*>(cnt + (size_t)(2 * r + 1) * N + y4);
-      float q;
-      q = a.x / ca.x; a.x = isfinite(q) ? q : 0.f;
-      q = a.y / ca.y; a.y = isfinite(q) ? q : 0.f;
-      q = a.z / ca.z; a.z = isfinite(q) ? q : 0.f;
-      q = a.w / ca.w; a.w = isfinite(q) ? q : 0.f;
-      q = b.x / cb.x; b.x = isfinite(q) ? q : 0.f;
-      q = b.y / cb.y; b.y = isfinite(q) ? q : 0.f;
-      q = b.z / cb.z; b.z = isfinite(q) ? q : 0.f;
-      q = b.w / cb.w; b.w = isfinite(q) ? q : 0.f;
+      a = make_float4(voxel_mean(a.x, ca.x), voxel_mean(a.y, ca.y), voxel_mean(a.z, ca.z), voxel_mean(a.w, ca.w));
+      b = make_float4(voxel_mean(b.x, cb.x), voxel_mean(b.y, cb.y), voxel_mean(b.z, cb.z), voxel_mean(b.w, cb.w));
     }
-    float2* d = W + r * N + y4;
+    float2* d = W + r * S + y4;
     d[0] = make_float2(a.x, b.x);
     d[1] = make_float2(a.y, b.y);
     d[2] = make_float2(a.z, b.z);
     d[3] = make_float2(a.w, b.w);
   }
   __syncthreads();
-  fft_fixed<N, false, -1>(W, NH, N, 1, pN.tw);   // over y, rows
-  fft_fixed<NH, false, -2>(W, N, 1, N, pH.tw);   // over r, columns
+  fft_tail<N, false, false>(W, NH, S, pN.tw);  // over y, rows
+  fft_tail<NH, false, true>(W, N, S, pH.tw);   // over r, columns
   float2* out = spec + (size_t)c * spec_cstride + (size_t)z * N * H2p;
   for (int e = threadIdx.x; e < NH * H2; e += blockDim.x) {
     const int k = e / H2, ky = e - k * H2;
-    const float2 w1 = W[fixed_freq2pos<NH>(k) * N + fixed_freq2pos<N>(ky)];
-    const float2 w2 = W[fixed_freq2pos<NH>(k == 0 ? 0 : NH - k) * N + fixed_freq2pos<N>(ky == 0 ? 0 : N - ky)];
+    const float2 w1 = W[fixed_freq2pos<NH>(k) * S + fixed_freq2pos<N>(ky)];
+    const float2 w2 = W[fixed_freq2pos<NH>(k == 0 ? 0 : NH - k) * S + fixed_freq2pos<N>(ky == 0 ? 0 : N - ky)];
     const float2 A = make_float2(0.5f * (w1.x + w2.x), 0.5f * (w1.y - w2.y));
     const float2 B = make_float2(0.5f * (w1.y + w2.y), -0.5f * (w1.x - w2.x));  // (w1 - conj w2) / 2i
     const float2 tB = cmul(__ldg(&pN.tw[k]), B);
@@ -335,12 +333,12 @@ __global__ void __launch_bounds__(1024) k_slab_fwd(const float* __restrict__ gri
 // x-Hermitian parts, which is what a half-complex inverse reads (only the real
 // parts of its DC and Nyquist terms after the inverse over x).
 template <int NF>
-__global__ void __launch_bounds__(1024) k_slab_inv(const float2* __restrict__ cspec, FftPlan pN, FftPlan pH,
-                                                   unsigned long long* __restrict__ argmax,
+__global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* __restrict__ cspec, FftPlan pN,
+                                                   FftPlan pH, unsigned long long* __restrict__ argmax,
                                                    float* __restrict__ volume) {
-  constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1;
+  constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1, S = NF + 1;
   const int H2p = spatial_h2p(N);
-  extern __shared__ float2 W[];  // [NH][N]
+  extern __shared__ float2 W[];  // [NH][S]
   const int z = blockIdx.x;
   const float2* X = cspec + (size_t)z * N * H2p;
   for (int e = threadIdx.x; e < NH * H2; e += blockDim.x) {
@@ -356,18 +354,18 @@ __global__ void __launch_bounds__(1024) k_slab_inv(const float2* __restrict__ cs
     const float2 A = make_float2(0.5f * (x0.x + x1.x), 0.5f * (x0.y + x1.y));
     const float2 B = cmul(make_float2(0.5f * (x0.x - x1.x), 0.5f * (x0.y - x1.y)), cconj(__ldg(&pN.tw[k])));
     // W = A + i B at (k, ky); its mirror (-k, -ky) holds conj(A) + i conj(B)
-    W[fixed_freq2pos<NH>(k) * N + fixed_freq2pos<N>(ky)] = make_float2(A.x - B.y, A.y + B.x);
+    W[fixed_freq2pos<NH>(k) * S + fixed_freq2pos<N>(ky)] = make_float2(A.x - B.y, A.y + B.x);
     if (ky >= 1 && ky < NH)
-      W[fixed_freq2pos<NH>(k == 0 ? 0 : NH - k) * N + fixed_freq2pos<N>(N - ky)] =
+      W[fixed_freq2pos<NH>(k == 0 ? 0 : NH - k) * S + fixed_freq2pos<N>(N - ky)] =
           make_float2(A.x + B.y, -A.y + B.x);
   }
   __syncthreads();
-  fft_fixed<NH, true, -2>(W, N, 1, N, pH.tw);   // over r, columns
-  fft_fixed<N, true, -1>(W, NH, N, 1, pN.tw);   // over y, rows
+  fft_tail<NH, true, true>(W, N, S, pH.tw);    // over r, columns
+  fft_tail<N, true, false>(W, NH, S, pN.tw);   // over y, rows
   unsigned long long best = 0ull;
   for (int e = threadIdx.x; e < NH * N; e += blockDim.x) {
     const int r = e / N, y = e - r * N;
-    const float2 v = W[e];
+    const float2 v = W[r * S + y];
     const float a0 = 2.0f * v.x, a1 = 2.0f * v.y;
     const uint32_t i0 = (uint32_t)(((size_t)z * N + 2 * r) * N + y);
     const uint32_t i1 = i0 + N;
@@ -446,8 +444,9 @@ cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t 
   if (spatial_slab_path(N) && a.plan_half) {
     float2* spec = a.spec + (size_t)(side * a.n_data_ch) * plane;
     dim3 g(N, nch);
-    const size_t sm = (size_t)(N / 2) * N * sizeof(float2);
-    PHGPU_DISPATCH_SLAB(N, k_slab_fwd<NF><<<g, 1024, sm, st>>>(grids, nv, count, spec, plane, *a.plan, *a.plan_half));
+    const size_t sm = (size_t)(N / 2) * (N + 1) * sizeof(float2);
+    PHGPU_DISPATCH_SLAB(N, k_slab_fwd<NF><<<g, tail_threads<NF>(), sm, st>>>(grids, nv, count, spec, plane, *a.plan,
+                                                                             *a.plan_half));
     count_launches(1);
     return cudaGetLastError();
   }
@@ -480,8 +479,9 @@ cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st) {
 cudaError_t launch_spatial_inverse(const SpatialArgs& a, cudaStream_t st) {
   const int N = a.N, H2 = N / 2 + 1;
   if (spatial_slab_path(N) && a.plan_half) {
-    const size_t sm = (size_t)(N / 2) * N * sizeof(float2);
-    PHGPU_DISPATCH_SLAB(N, k_slab_inv<NF><<<N, 1024, sm, st>>>(a.cspec, *a.plan, *a.plan_half, a.argmax, a.volume));
+    const size_t sm = (size_t)(N / 2) * (N + 1) * sizeof(float2);
+    PHGPU_DISPATCH_SLAB(N, k_slab_inv<NF><<<N, tail_threads<NF>(), sm, st>>>(a.cspec, *a.plan, *a.plan_half, a.argmax,
+                                                                             a.volume));
     count_launches(1);
     return cudaGetLastError();
   }

@@ -92,7 +92,7 @@ EXPORTED = [
     "phgpu_translation_from_index", "phgpu_server_create", "phgpu_server_destroy",
     "phgpu_server_submit", "phgpu_server_poll", "phgpu_server_drain", "phgpu_server_last_error",
     "phgpu_profile_enable", "phgpu_profile_read", "phgpu_profile_stage_count",
-    "phgpu_profile_stage_name", "phgpu_launch_count",
+    "phgpu_profile_stage_name", "phgpu_launch_count", "phgpu_selftest_fft",
 ]
 
 _LIB = None
@@ -144,6 +144,7 @@ def load(path: str = LIB_PATH):
     lib.phgpu_profile_stage_name.restype = C.c_char_p
     lib.phgpu_profile_stage_name.argtypes = [C.c_int]
     lib.phgpu_launch_count.restype = C.c_ulonglong
+    lib.phgpu_selftest_fft.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
     _LIB = lib
     return lib
 
@@ -183,6 +184,16 @@ def make_cloud(xyzi, reflectivity=None, ambient=None) -> tuple[Cloud, list]:
     n = int(xyzi.shape[0])
     c = Cloud(_addr(xyzi), _addr(reflectivity), _addr(ambient), n, on_dev)
     return c, keep
+
+
+def selftest_fft(x: np.ndarray, inverse=False, columns=False, engine=2) -> np.ndarray:
+    """Run one of the shared-memory FFT engines on x (complex, [ntrans, n])."""
+    a = np.ascontiguousarray(x, np.complex64).copy()
+    ntrans, n = a.shape
+    rc = load().phgpu_selftest_fft(n, ntrans, 1 if inverse else 0, 1 if columns else 0, engine, a.ctypes.data)
+    if rc != PHGPU_OK:
+        raise PhgpuError(f"phgpu_selftest_fft failed ({rc})")
+    return a
 
 
 def launch_count() -> int:

@@ -1,0 +1,34 @@
+"""The three shared-memory FFT engines against numpy, rows and columns,
+forward and inverse (tolerance: FP32 transform error)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [32, 64, 100, 128, 200, 256, 512]
+
+
+@pytest.mark.parametrize("engine", [0, 1, 2])
+@pytest.mark.parametrize("n", SIZES)
+@pytest.mark.parametrize("columns", [False, True])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_fft_engine(engine, n, columns, inverse):
+    from phaser_b200 import native
+    rng = np.random.default_rng(n + 7 * engine)
+    ntrans = max(1, min(24, (200 * 1024) // ((n + 1) * 8)))
+    x = (rng.standard_normal((ntrans, n)) + 1j * rng.standard_normal((ntrans, n))).astype(np.complex64)
+    y = native.selftest_fft(x, inverse=inverse, columns=columns, engine=engine)
+    ref = np.fft.ifft(x.astype(np.complex128), axis=1) * n if inverse else np.fft.fft(x.astype(np.complex128), axis=1)
+    err = np.abs(y - ref).max() / np.abs(ref).max()
+    assert err < 5e-6, err
+
+
+@pytest.mark.parametrize("n", [3, 12, 38, 134, 201])
+def test_fft_runtime_engine_odd_lengths(n):
+    from phaser_b200 import native
+    rng = np.random.default_rng(n)
+    x = (rng.standard_normal((4, n)) + 1j * rng.standard_normal((4, n))).astype(np.complex64)
+    for inverse in (False, True):
+        y = native.selftest_fft(x, inverse=inverse, columns=False, engine=0)
+        ref = np.fft.ifft(x.astype(np.complex128), axis=1) * n if inverse else np.fft.fft(x.astype(np.complex128), axis=1)
+        assert np.abs(y - ref).max() / np.abs(ref).max() < 5e-6

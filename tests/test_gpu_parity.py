@@ -3,6 +3,13 @@
 Tolerances: integer / index results (rotation bin, translation voxel, sample
 nearest-neighbour indices, voxel indices) must be identical; FP32 correlation
 volumes must be within a relative L2 error of 1e-5 of the FP64 oracle.
+
+Laplace fusion keeps, per frequency, the channel of largest energy.  Where two
+channels' FP64 energies differ by less than 1e-4 (relative), FP32 rounding may
+pick the other one; such a flip changes one whole coefficient (about 1/sqrt(n)
+of the volume's norm).  The spatial Laplace tests therefore remove those
+ambiguous frequencies from the difference before applying the 1e-5 bound, and
+bound their number.
 """
 import os
 
@@ -34,6 +41,37 @@ def ctx(nat, **kw):
     return nat.Context(**kw)
 
 
+def ambiguous_max_frequencies(f, g, N, gap=1e-4):
+    """Half-spectrum linear indices (kz, kx, ky) of MAX-rule positions whose top
+    two channel energies (f or g side) differ by less than `gap` relatively."""
+    if len(f) < 2:
+        return np.zeros(0, np.int64)
+    out = []
+    for X in (f, g):
+        S = np.fft.rfftn(np.asarray(X).reshape(-1, N, N, N), axes=(1, 2, 3)).reshape(len(X), -1)
+        e = np.sort(np.abs(S) ** 2, axis=0)
+        out.append(np.nonzero(e[-1] - e[-2] < gap * e[-1])[0])
+    cand = np.unique(np.concatenate(out))
+    nv = N ** 3
+    return np.array([k for k in cand if O.fusion_rule(int((k + (nv >> 1)) % nv), nv) == 0], dtype=np.int64)
+
+
+def tie_masked_rel_l2(vol, ref, f, g, N):
+    """Relative L2 of vol - ref after zeroing the ambiguous MAX frequencies
+    (and their Hermitian mirrors in the ky = 0 and ky = N/2 planes)."""
+    H = N // 2 + 1
+    amb = ambiguous_max_frequencies(f, g, N)
+    D = np.fft.rfftn((np.asarray(vol) - np.asarray(ref)).reshape(N, N, N))
+    for k in amb:
+        kz, rem = divmod(int(k), N * H)
+        kx, ky = divmod(rem, H)
+        D[kz, kx, ky] = 0
+        if ky == 0 or (N % 2 == 0 and ky == N // 2):
+            D[(-kz) % N, (-kx) % N, ky] = 0
+    r = np.fft.irfftn(D, s=(N, N, N), axes=(0, 1, 2))
+    return float(np.linalg.norm(r) / np.linalg.norm(ref)), len(amb)
+
+
 def test_spatial_delta_known_answer(nat):
     # phaser_core/test/translation-alignment/spatial-correlation-test.cc:59-79
     f = np.zeros(27)
@@ -56,11 +94,13 @@ def test_spatial_laplace_vs_oracle(nat, N, C):
     c.spatial_correlate(list(f), list(g))
     vox, peak, vol = c.spatial_result(volume=True)
     ref = O.spatial_correlation(f, g, N, laplace=True)
-    assert rel_l2(vol, ref) <= REL_L2
+    err, n_amb = tie_masked_rel_l2(vol, ref, f, g, N)
+    assert err <= REL_L2
+    assert n_amb <= 4 + 1e-3 * N * N * (N // 2 + 1)
     assert vox == O.argmax(ref)
 
 
-@pytest.mark.parametrize("N", [3, 6, 10, 32, 64])
+@pytest.mark.parametrize("N", [3, 6, 10, 32, 64, 256])
 def test_spatial_plain_vs_oracle(nat, N):
     rng = np.random.default_rng(N)
     f = rng.random((1, N ** 3))
