@@ -26,6 +26,7 @@ extern "C" {
 #define PHGPU_ERR_CUDA (-2)      /* CUDA runtime error (message in phgpu_last_error) */
 #define PHGPU_ERR_MEMORY (-3)    /* device allocation failed */
 #define PHGPU_ERR_STATE (-4)     /* call out of order (e.g. result before correlate) */
+#define PHGPU_ERR_LIMIT (-5)     /* size beyond a fixed limit (phgpu_sample_s2_noalloc) */
 
 /* fusion modes */
 #define PHGPU_FUSION_LAPLACE 0   /* SphericalCorrelationLaplace / SpatialCorrelationLaplace */
@@ -107,6 +108,25 @@ int phgpu_sample_s2(phgpu_ctx* ctx, const phgpu_cloud* cloud, int side);
  * in the channel order {range, intensity, reflectivity, ambient}, and the
  * nearest-point index per grid direction (-1 when dropped).  Either may be NULL. */
 int phgpu_get_samples(phgpu_ctx* ctx, int side, double* values, int32_t* nn_index);
+
+/* S^2 sampling that allocates no device memory (no counterpart in the
+ * reference; same kernels and results as phgpu_sample_s2 + phgpu_get_samples).
+ * For callers that cannot allocate once running.  bw = params->spherical_
+ * bandwidth, rejection radius from params->spatial_low_pass_* and
+ * spatial_n_voxels as in a context.  The cloud must be on the device
+ * (on_device = 1); values_dev receives 4 x 4bw^2 floats (channels {range,
+ * intensity, reflectivity, ambient}, [theta][phi]) and nn_index_dev (or NULL)
+ * 4bw^2 indices.  Runs asynchronously on `stream` (cudaStream_t, NULL = the
+ * legacy default stream) on the current device.  Scratch is one fixed
+ * device array per device: bw > PHGPU_NOALLOC_MAX_BANDWIDTH or n_points >
+ * PHGPU_NOALLOC_MAX_POINTS returns PHGPU_ERR_LIMIT; calls that overlap on
+ * one device race on the array.  The first call on each device looks the
+ * array up (and may load the module there): make it before any stream
+ * capture. */
+#define PHGPU_NOALLOC_MAX_POINTS (1 << 18)
+#define PHGPU_NOALLOC_MAX_BANDWIDTH 128
+int phgpu_sample_s2_noalloc(const phgpu_params* params, const phgpu_cloud* cloud, float* values_dev,
+                            int32_t* nn_index_dev, void* stream);
 
 /* SphericalCorrelationLaplace::correlateSampledSignals
  * (spherical-correlation-laplace.cc:14-40) / SphericalCorrelation::

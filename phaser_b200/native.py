@@ -15,6 +15,10 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "_lib", "libphaser_gpu.so")
 
 PHGPU_OK = 0
+PHGPU_ERR_INVALID = -1
+PHGPU_ERR_LIMIT = -5
+NOALLOC_MAX_POINTS = 1 << 18
+NOALLOC_MAX_BANDWIDTH = 128
 PHGPU_FUSION_LAPLACE = 0
 PHGPU_FUSION_NONE = 1
 PHGPU_FLAG_KEEP_VOLUMES = 1
@@ -93,6 +97,7 @@ EXPORTED = [
     "phgpu_server_submit", "phgpu_server_poll", "phgpu_server_drain", "phgpu_server_last_error",
     "phgpu_profile_enable", "phgpu_profile_read", "phgpu_profile_stage_count",
     "phgpu_profile_stage_name", "phgpu_launch_count", "phgpu_selftest_fft",
+    "phgpu_sample_s2_noalloc",
 ]
 
 _LIB = None
@@ -145,6 +150,8 @@ def load(path: str = LIB_PATH):
     lib.phgpu_profile_stage_name.argtypes = [C.c_int]
     lib.phgpu_launch_count.restype = C.c_ulonglong
     lib.phgpu_selftest_fft.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    lib.phgpu_sample_s2_noalloc.argtypes = [C.POINTER(Params), C.POINTER(Cloud), C.c_void_p, C.c_void_p,
+                                            C.c_void_p]
     _LIB = lib
     return lib
 
@@ -184,6 +191,16 @@ def make_cloud(xyzi, reflectivity=None, ambient=None) -> tuple[Cloud, list]:
     n = int(xyzi.shape[0])
     c = Cloud(_addr(xyzi), _addr(reflectivity), _addr(ambient), n, on_dev)
     return c, keep
+
+
+def sample_s2_noalloc(params: Params, xyzi, reflectivity, ambient, values_dev, nn_index_dev=None,
+                      stream=None) -> int:
+    """phgpu_sample_s2_noalloc on device tensors; returns the status code.
+    values_dev: float32 CUDA tensor of 4 * 4bw^2, nn_index_dev: int32 of 4bw^2
+    or None; stream: a torch.cuda.Stream (None = legacy default stream)."""
+    c, keep = make_cloud(xyzi, reflectivity, ambient)
+    return load().phgpu_sample_s2_noalloc(C.byref(params), C.byref(c), _addr(values_dev), _addr(nn_index_dev),
+                                          None if stream is None else stream.cuda_stream)
 
 
 def selftest_fft(x: np.ndarray, inverse=False, columns=False, engine=2) -> np.ndarray:
