@@ -313,7 +313,7 @@ static int ensure_cloud_capacity(phgpu_ctx* ctx, uint32_t n) {
     CKV(dalloc(ctx, &ctx->d_xyzi[s], sizeof(float4) * cap));
     CKV(dalloc(ctx, &ctx->d_refl[s], sizeof(float) * cap));
     CKV(dalloc(ctx, &ctx->d_amb[s], sizeof(float) * cap));
-    CKV(dalloc(ctx, &ctx->d_sample_scratch[s], sampler_scratch_bytes((int)cap)));
+    CKV(dalloc(ctx, &ctx->d_sample_scratch[s], sampler_scratch_bytes((int)cap, 4 * ctx->bw * ctx->bw)));
     CKV(dalloc(ctx, &ctx->d_lin[s], sizeof(uint32_t) * cap));
   }
   ctx->cap_points = cap;
@@ -503,6 +503,7 @@ static int run_sample(phgpu_ctx* ctx, int side, cudaStream_t st) {
   a.max_points = (int)ctx->cap_points;
   a.grid = ctx->d_grid;
   a.n_queries = 4 * ctx->bw * ctx->bw;
+  a.n2b = 2 * ctx->bw;
   a.max_sq = ctx->max_sq;
   a.n_out_ch = 4;
   a.out = ctx->d_samples + (size_t)side * 4 * a.n_queries;

@@ -11,10 +11,19 @@
 //
 // Acceleration structure: points are bucketed on a 32^3 grid over
 // [-1.0625, 1.0625]^3 ordered coarse-cell-major (8^3 coarse cells of 4^3 fine
-// cells), with exact per-cell bounding boxes.  A query first takes an upper
-// bound from one representative point per non-empty coarse cell, then scans
-// only cells whose box lies within that bound (with a 1e-5 relative margin so
-// float rounding can never prune the true nearest point).
+// cells), with exact per-cell bounding boxes.  Cells are only pruned when
+// their box lies beyond the current best distance (with a 1e-5 relative
+// margin so float rounding can never prune the true nearest point), so the
+// search is exact whatever bound it starts from.
+//
+// On the 2B x 2B Driscoll-Healy grid (k_nn_grid) the bound starts close to
+// the answer: projection also drops every point into the grid's (theta, phi)
+// bin and marks the bin in a per-phi-column row bitmask.  A direction takes
+// the nearest occupied bins above and below it in its own and the two
+// neighbouring columns on each side, plus every point of its own fine cell;
+// far from the scanned band (most directions of a LiDAR scan) this lands
+// within about one bin of the final distance.  Other direction sets
+// (k_nn_query) start from one representative point per coarse cell.
 #include "kernels.h"
 
 namespace phgpu {
@@ -44,9 +53,16 @@ __device__ __forceinline__ uint32_t cell_key(float x, float y, float z) {
 __device__ __forceinline__ float acos_f(float x) { return (float)acos((double)x); }
 __device__ __forceinline__ float atan2_f(float y, float x) { return (float)atan2((double)y, (double)x); }
 
+// Bins of the 2B x 2B direction grid: row i covers theta in [i, i + 1) * pi / 2B,
+// column j covers phi within pi / 2B of 2 pi j / 2B.  binmap[i * n2b + j] =
+// lowest point index in the bin (init 0xffffffff), colmask[j * W + i / 32]
+// bit i % 32 set when the bin is occupied (W = (n2b + 31) / 32).
+__host__ __device__ __forceinline__ int bin_words(int n2b) { return (n2b + 31) >> 5; }
+
 __global__ void k_project(const float4* __restrict__ xyzi, int P, float4* __restrict__ proj,
                           double* __restrict__ range, uint32_t* __restrict__ key,
-                          uint32_t* __restrict__ cell_count) {
+                          uint32_t* __restrict__ cell_count, int n2b, uint32_t* __restrict__ binmap,
+                          uint32_t* __restrict__ colmask) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
   const float4 p = xyzi[i];
@@ -73,6 +89,14 @@ __global__ void k_project(const float4* __restrict__ xyzi, int P, float4* __rest
   const uint32_t k = cell_key(ox, oy, oz);
   key[i] = k;
   atomicAdd(&cell_count[k], 1u);
+  if (n2b > 0) {
+    const double w = M_PI / (double)n2b;  // bin height in theta, half bin width in phi
+    const int bi = min(max((int)(tx / w), 0), n2b - 1);
+    int bj = (int)floor(ty / (2.0 * w) + 0.5);
+    bj = bj >= n2b ? bj - n2b : max(bj, 0);
+    atomicMin(&binmap[bi * n2b + bj], (uint32_t)i);
+    atomicOr(&colmask[bj * bin_words(n2b) + (bi >> 5)], 1u << (bi & 31));
+  }
 }
 
 // Exclusive scan of the 32768 fine-cell counts (one block of 1024 threads,
@@ -291,6 +315,25 @@ __device__ __forceinline__ void scan_coarse(int cid, float qx, float qy, float q
   }
 }
 
+// Writes the sampled channels {range, intensity, reflectivity, ambient}
+// (float) of the nearest point into out[ch][qi] for ch < n_out_ch and its
+// index (or -1) into nn_idx; a match farther than max_sq is dropped.
+__device__ __forceinline__ void emit_sample(int qi, int nq, float best, int bidx, float max_sq,
+                                            const float4* __restrict__ xyzi, const double* __restrict__ range,
+                                            const float* __restrict__ refl, const float* __restrict__ amb,
+                                            int n_out_ch, float* __restrict__ out, int32_t* __restrict__ nn_idx) {
+  const bool ok = (bidx != 0x7fffffff) && !(best > max_sq);
+  float v[4] = {0.f, 0.f, 0.f, 0.f};
+  if (ok) {
+    v[0] = (float)range[bidx];
+    v[1] = xyzi[bidx].w;
+    v[2] = refl ? refl[bidx] : 0.0f;
+    v[3] = amb ? amb[bidx] : 0.0f;
+  }
+  for (int c = 0; c < n_out_ch; ++c) out[(size_t)c * nq + qi] = v[c];
+  if (nn_idx) nn_idx[qi] = ok ? bidx : -1;
+}
+
 // One warp per grid direction (grid-stride).  The bound starts from one
 // representative point per non-empty coarse cell; the coarse cell of the
 // nearest representative is searched first, then every other coarse cell whose
@@ -362,18 +405,132 @@ k_nn_query(int nq, const float4* __restrict__ grid, const float4* __restrict__ s
         scan_coarse((int)s_cid[cc], q.x, q.y, q.z, sorted, fstart, flo, fhi, best, bidx);
       }
     }
-    if (lane == 0) {
-      const bool ok = (bidx != 0x7fffffff) && !(best > max_sq);
-      float v[4] = {0.f, 0.f, 0.f, 0.f};
-      if (ok) {
-        v[0] = (float)range[bidx];
-        v[1] = xyzi[bidx].w;
-        v[2] = refl ? refl[bidx] : 0.0f;
-        v[3] = amb ? amb[bidx] : 0.0f;
-      }
-      for (int c = 0; c < n_out_ch; ++c) out[(size_t)c * nq + qi] = v[c];
-      if (nn_idx) nn_idx[qi] = ok ? bidx : -1;
+    if (lane == 0) emit_sample(qi, nq, best, bidx, max_sq, xyzi, range, refl, amb, n_out_ch, out, nn_idx);
+  }
+}
+
+// Scans points [s, e) of the sorted array, four loads in flight per lane.
+__device__ __forceinline__ void scan_points(uint32_t s, uint32_t e, float qx, float qy, float qz,
+                                            const float4* __restrict__ sorted, float& best, int& bidx) {
+  const int lane = threadIdx.x & 31;
+  for (uint32_t j = s + lane; j < e; j += 128) {
+    float4 p[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (j + 32 * u < e) p[u] = sorted[j + 32 * u];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (j + 32 * u < e) nn_update(ref_dist2(qx, qy, qz, p[u]), __float_as_int(p[u].w), best, bidx);
+  }
+}
+
+// Nearest occupied row at or below (dir > 0) / above (dir < 0) row i in a
+// column bitmask of W words; -1 when there is none.
+__device__ __forceinline__ int nearest_row(const uint32_t* __restrict__ cm, int W, int i, int dir) {
+  int w = i >> 5;
+  const int b = i & 31;
+  uint32_t m = __ldg(&cm[w]);
+  if (dir > 0) {
+    m &= 0xffffffffu << b;
+    while (!m && ++w < W) m = __ldg(&cm[w]);
+    return m ? (w << 5) + __ffs(m) - 1 : -1;
+  }
+  m &= b == 31 ? 0xffffffffu : ((1u << (b + 1)) - 1u);
+  while (!m && --w >= 0) m = __ldg(&cm[w]);
+  return m ? (w << 5) + 31 - __clz(m) : -1;
+}
+
+// One warp per direction of the 2B x 2B grid (grid-stride).  Bound: the
+// points of the nearest occupied bins above and below in columns j-2..j+2
+// (lanes 0..9), then all points of the direction's own fine cell; if no
+// column near it holds any point, one representative per coarse cell.  Then
+// every coarse cell whose box lies within the bound is opened and each of its
+// fine cells within the bound is scanned; lanes keep private minima inside a
+// coarse cell and the warp minimum (the bound for the next) is refreshed after it.
+__global__ void __launch_bounds__(kQueryThreads)
+k_nn_grid(int n2b, const float4* __restrict__ grid, const float4* __restrict__ proj,
+          const uint32_t* __restrict__ binmap, const uint32_t* __restrict__ colmask,
+          const float4* __restrict__ sorted, const uint32_t* __restrict__ fstart,
+          const uint32_t* __restrict__ flo, const uint32_t* __restrict__ fhi, const uint4* __restrict__ clist,
+          const uint32_t* __restrict__ clo, const uint32_t* __restrict__ chi,
+          const uint32_t* __restrict__ n_coarse_p, float max_sq, const float4* __restrict__ xyzi,
+          const double* __restrict__ range, const float* __restrict__ refl, const float* __restrict__ amb,
+          int n_out_ch, float* __restrict__ out, int32_t* __restrict__ nn_idx) {
+  __shared__ uint32_t s_cid[kCoarseCells];
+  __shared__ float s_box[kCoarseCells * 6];
+  __shared__ float4 s_rep[kCoarseCells];
+  const int nc = (int)*n_coarse_p;
+  for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+    const uint4 e = clist[i];
+    s_cid[i] = e.z;
+    s_rep[i] = sorted[e.x];
+    for (int a = 0; a < 3; ++a) {
+      s_box[6 * i + a] = float_from_order_bits(clo[e.z * 3 + a]);
+      s_box[6 * i + 3 + a] = float_from_order_bits(chi[e.z * 3 + a]);
     }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const int nq = n2b * n2b;
+  const int W = bin_words(n2b);
+  for (int qi = blockIdx.x * wpb + (threadIdx.x >> 5); qi < nq; qi += gridDim.x * wpb) {
+    const float4 q = grid[qi];
+    float best = INFINITY;
+    int bidx = 0x7fffffff;
+    if (lane < 10) {
+      const int i = qi / n2b, j = qi - i * n2b;
+      int jj = j + (lane >> 1) - 2;
+      jj = jj < 0 ? jj + n2b : (jj >= n2b ? jj - n2b : jj);
+      const int row = nearest_row(colmask + (size_t)jj * W, W, i, (lane & 1) ? 1 : -1);
+      if (row >= 0) {
+        const uint32_t sidx = __ldg(&binmap[row * n2b + jj]);
+        nn_update(ref_dist2(q.x, q.y, q.z, __ldg(&proj[sidx])), (int)sidx, best, bidx);
+      }
+    }
+    const uint32_t own = cell_key(q.x, q.y, q.z);
+    scan_points(__ldg(&fstart[own]), __ldg(&fstart[own + 1]), q.x, q.y, q.z, sorted, best, bidx);
+    warp_nn_min(best, bidx);
+    if (!(best < INFINITY)) {
+      for (int c = lane; c < nc; c += 32) {
+        const float4 r = s_rep[c];
+        nn_update(ref_dist2(q.x, q.y, q.z, r), __float_as_int(r.w), best, bidx);
+      }
+      warp_nn_min(best, bidx);
+    }
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+      const int c = c0 + lane;
+      const bool cand = c < nc && box_lb2(q.x, q.y, q.z, s_box + 6 * c) * kPruneMargin <= best;
+      unsigned cmask = __ballot_sync(0xffffffffu, cand);
+      while (cmask) {
+        const int cc = c0 + __ffs(cmask) - 1;
+        cmask &= cmask - 1;
+        const int cid = (int)s_cid[cc];
+        uint32_t fs[2], fe[2];
+        bool in[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t fc = (uint32_t)(cid * 64 + h * 32 + lane);
+          fs[h] = __ldg(&fstart[fc]);
+          fe[h] = __ldg(&fstart[fc + 1]);
+          in[h] = fe[h] > fs[h] && fc != own &&
+                  box_lb2_ord(q.x, q.y, q.z, flo + 3 * fc, fhi + 3 * fc) * kPruneMargin <= best;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          unsigned fmask = __ballot_sync(0xffffffffu, in[h]);
+          while (fmask) {
+            const int src = __ffs(fmask) - 1;
+            fmask &= fmask - 1;
+            const uint32_t s1 = __shfl_sync(0xffffffffu, fs[h], src);
+            const uint32_t e1 = __shfl_sync(0xffffffffu, fe[h], src);
+            scan_points(s1, e1, q.x, q.y, q.z, sorted, best, bidx);
+          }
+        }
+        warp_nn_min(best, bidx);
+      }
+    }
+    if (lane == 0) emit_sample(qi, nq, best, bidx, max_sq, xyzi, range, refl, amb, n_out_ch, out, nn_idx);
   }
 }
 
@@ -381,8 +538,8 @@ k_nn_query(int nq, const float4* __restrict__ grid, const float4* __restrict__ s
 
 std::atomic<unsigned long long> g_launch_count{0};
 
-size_t sampler_scratch_bytes(int max_points) {
-  size_t b = 0;
+size_t sampler_scratch_bytes(int max_points, int max_queries) {
+  size_t b = (size_t)max_queries * sizeof(uint32_t) * 2;  // bin map + column masks (<= one word per bin)
   b += (size_t)max_points * sizeof(float4);    // proj
   b += (size_t)max_points * sizeof(double);    // range
   b += (size_t)max_points * sizeof(uint32_t);  // key
@@ -417,6 +574,10 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   uint32_t* clo = (uint32_t*)carve(p, (size_t)kCoarseCells * 3 * sizeof(uint32_t));
   uint32_t* chi = (uint32_t*)carve(p, (size_t)kCoarseCells * 3 * sizeof(uint32_t));
   uint32_t* ncoarse = (uint32_t*)carve(p, 256);
+  const int n2b = a.n2b;
+  const size_t nbins = (size_t)n2b * n2b, nmask = (size_t)n2b * bin_words(n2b);
+  uint32_t* binmap = (uint32_t*)carve(p, nbins * sizeof(uint32_t));
+  uint32_t* colmask = (uint32_t*)carve(p, nmask * sizeof(uint32_t));
 
   // count and cursor are adjacent: one memset
   cudaMemsetAsync(count, 0, (size_t)2 * kFineCells * sizeof(uint32_t), st);
@@ -425,10 +586,14 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   cudaMemsetAsync(clo, 0xff, (size_t)kCoarseCells * 3 * sizeof(uint32_t), st);
   cudaMemsetAsync(chi, 0, (size_t)kCoarseCells * 3 * sizeof(uint32_t), st);
   cudaMemsetAsync(ncoarse, 0, sizeof(uint32_t), st);
+  if (n2b > 0) {
+    cudaMemsetAsync(binmap, 0xff, nbins * sizeof(uint32_t), st);
+    cudaMemsetAsync(colmask, 0, nmask * sizeof(uint32_t), st);
+  }
   const int P = a.n_points;
   int launched = 0;
   if (P > 0) {
-    k_project<<<(P + 255) / 256, 256, 0, st>>>(a.xyzi, P, proj, range, key, count);
+    k_project<<<(P + 255) / 256, 256, 0, st>>>(a.xyzi, P, proj, range, key, count, n2b, binmap, colmask);
     ++launched;
   }
   k_cell_scan<<<1, 1024, 0, st>>>(count, start, clist, ncoarse);
@@ -441,9 +606,15 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   const int wpb = kQueryThreads / 32;
   int blocks = (a.n_queries + wpb - 1) / wpb;
   if (blocks > 148 * 8) blocks = 148 * 8;
-  k_nn_query<<<blocks, kQueryThreads, 0, st>>>(a.n_queries, a.grid, sorted, start, flo, fhi, clist, clo, chi,
-                                               ncoarse, a.max_sq, a.xyzi, range, a.refl, a.amb, a.n_out_ch,
-                                               a.out, a.nn_idx);
+  if (n2b > 0) {
+    k_nn_grid<<<blocks, kQueryThreads, 0, st>>>(n2b, a.grid, proj, binmap, colmask, sorted, start, flo, fhi, clist,
+                                                clo, chi, ncoarse, a.max_sq, a.xyzi, range, a.refl, a.amb,
+                                                a.n_out_ch, a.out, a.nn_idx);
+  } else {
+    k_nn_query<<<blocks, kQueryThreads, 0, st>>>(a.n_queries, a.grid, sorted, start, flo, fhi, clist, clo, chi,
+                                                 ncoarse, a.max_sq, a.xyzi, range, a.refl, a.amb, a.n_out_ch,
+                                                 a.out, a.nn_idx);
+  }
   ++launched;
   count_launches(launched);
   return cudaGetLastError();

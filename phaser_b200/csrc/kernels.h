@@ -25,13 +25,14 @@ struct SampleArgs {
   int max_points;       // scratch sizing
   const float4* grid;   // [n_queries] DH grid directions (host-computed)
   int n_queries;
+  int n2b = 0;          // 2B when grid is the 2B x 2B DH grid (bin-seeded search), else 0
   float max_sq;         // squared voxel size (rejection threshold)
   int n_out_ch;         // channels written (1..4)
   float* out;           // [n_out_ch][n_queries]
   int32_t* nn_idx;      // [n_queries] or null
-  void* scratch;        // sampler_scratch_bytes(max_points)
+  void* scratch;        // sampler_scratch_bytes(max_points, >= n_queries)
 };
-size_t sampler_scratch_bytes(int max_points);
+size_t sampler_scratch_bytes(int max_points, int max_queries);
 cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st);
 
 // ------------------------------------------------------------ forward SHT

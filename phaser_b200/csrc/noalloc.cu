@@ -74,7 +74,7 @@ int phgpu_sample_s2_noalloc(const phgpu_params* params, const phgpu_cloud* cloud
   const int bw = (int)params->spherical_bandwidth;
   if (bw < 1 || params->spatial_n_voxels < 1) return PHGPU_ERR_INVALID;
   if (bw > kMaxBw || cloud->n_points > (uint64_t)kMaxPoints) return PHGPU_ERR_LIMIT;
-  if (sampler_scratch_bytes(kMaxPoints) + kGridBytes > kScratchBytes) return PHGPU_ERR_LIMIT;
+  if (sampler_scratch_bytes(kMaxPoints, 4 * kMaxBw * kMaxBw) + kGridBytes > kScratchBytes) return PHGPU_ERR_LIMIT;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PHGPU_ERR_CUDA;
   cudaStream_t st = (cudaStream_t)stream;
@@ -107,6 +107,7 @@ int phgpu_sample_s2_noalloc(const phgpu_params* params, const phgpu_cloud* cloud
   a.max_points = kMaxPoints;
   a.grid = reinterpret_cast<const float4*>(scratch);
   a.n_queries = 4 * bw * bw;
+  a.n2b = 2 * bw;
   // squared voxel size of the rejection, as the context computes it
   const float vs = (fabsf(params->spatial_low_pass_lower) + fabsf(params->spatial_low_pass_upper)) /
                    (float)params->spatial_n_voxels;
