@@ -433,7 +433,10 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   CK(cudaMemset(ctx->d_S, 0, sizeof(float2) * no * no * bw_out));
   const size_t nv = (size_t)N * N * N;
   const size_t H = (size_t)N * N * spatial_h2p(N);
-  for (int s = 0; s < 2; ++s) CKV(dalloc(ctx, &ctx->d_grids[s], sizeof(float) * 5 * nv));
+  for (int s = 0; s < 2; ++s) {
+    CKV(dalloc(ctx, &ctx->d_grids[s], sizeof(float) * 5 * nv));
+    CKV(dalloc(ctx, &ctx->d_rowlive[s], (size_t)N * N));
+  }
   CKV(dalloc(ctx, &ctx->d_spec, sizeof(float2) * 8 * H));
   CKV(dalloc(ctx, &ctx->d_cspec, sizeof(float2) * H));
   if (prm->flags & PHGPU_FLAG_KEEP_VOLUMES) {
@@ -658,7 +661,11 @@ static int sp_channels(int has_refl, int has_amb) { return has_amb ? 4 : (has_re
 
 int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, cudaStream_t st) {
   const size_t nv = (size_t)ctx->N * ctx->N * ctx->N;
-  CK(cudaMemsetAsync(ctx->d_grids[side], 0, sizeof(float) * (n_data + 1) * nv, st));
+  if (ctx->clean_planes[side] < n_data + 1) {
+    CK(cudaMemsetAsync(ctx->d_grids[side], 0, sizeof(float) * (n_data + 1) * nv, st));
+    CK(cudaMemsetAsync(ctx->d_rowlive[side], 0, (size_t)ctx->N * ctx->N, st));
+  }
+  ctx->clean_planes[side] = 0;
   VoxelArgs v;
   v.xyzi = ctx->d_xyzi[side];
   v.refl = ctx->has_refl[side] ? ctx->d_refl[side] : nullptr;
@@ -671,12 +678,27 @@ int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, c
   v.n_data_ch = n_data;
   v.grids = ctx->d_grids[side];
   v.lin_out = ctx->d_lin[side];
+  v.rowlive = ctx->d_rowlive[side];
   {
     ProfScope ps(ctx, st, PS_VOXELIZE);
     CK(launch_voxelize(v, st));
   }
   ctx->vox_ch[side] = n_data;
   ctx->voxelized[side] = true;
+  ctx->grids_live[side] = true;
+  return PHGPU_OK;
+}
+
+// After the forward transform of a voxelised side inside register_pair (the
+// grids are internal there): zero what the voxelisation wrote, so the next
+// voxelisation of this side needs no full-grid memset.
+static int clear_voxelized(phgpu_ctx* ctx, int side, cudaStream_t st) {
+  const int planes = ctx->vox_ch[side] + 1;
+  const size_t nv = (size_t)ctx->N * ctx->N * ctx->N;
+  CK(launch_clear_voxels(ctx->d_lin[side], (int)ctx->np[side], ctx->d_grids[side], nv, planes,
+                         ctx->d_rowlive[side], ctx->N, st));
+  ctx->clean_planes[side] = planes;
+  ctx->grids_live[side] = false;
   return PHGPU_OK;
 }
 
@@ -710,6 +732,9 @@ static SpatialArgs spatial_args(phgpu_ctx* ctx, int n_data, int n_total, int lap
   a.grids_f = ctx->d_grids[0];
   a.grids_g = ctx->d_grids[1];
   a.grids_are_means = means;
+  // row flags describe voxelised grids only (host-written grids are dense)
+  a.rowlive_f = means ? nullptr : ctx->d_rowlive[0];
+  a.rowlive_g = means ? nullptr : ctx->d_rowlive[1];
   a.spec = ctx->d_spec;
   a.cspec = ctx->d_cspec;
   a.plan = &ctx->plan_sp;
@@ -751,6 +776,8 @@ int phgpu_spatial_correlate(phgpu_ctx* ctx, const double* const* f, const double
   const int laplace = ctx->prm.spatial_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
   std::vector<float> tmp(nv);
   for (int side = 0; side < 2; ++side) {
+    ctx->clean_planes[side] = 0;
+    ctx->grids_live[side] = false;
     const double* const* src = side == 0 ? f : g;
     for (uint32_t c = 0; c < C; ++c) {
       for (size_t i = 0; i < nv; ++i) tmp[i] = (float)src[c][i];
@@ -764,8 +791,8 @@ int phgpu_spatial_correlate(phgpu_ctx* ctx, const double* const* f, const double
 
 int phgpu_spatial_correlate_voxelized(phgpu_ctx* ctx) {
   if (!ctx) return PHGPU_ERR_INVALID;
-  if (!ctx->voxelized[0] || !ctx->voxelized[1] || ctx->vox_ch[0] != ctx->vox_ch[1]) {
-    ctx->err = "both sides must be voxelised with the same channel count first";
+  if (!ctx->grids_live[0] || !ctx->grids_live[1] || ctx->vox_ch[0] != ctx->vox_ch[1]) {
+    ctx->err = "both sides must be voxelised (phgpu_voxelize) with the same channel count first";
     return PHGPU_ERR_STATE;
   }
   cudaSetDevice(ctx->prm.device);
@@ -825,6 +852,7 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
     ProfScope ps(ctx, s1, PS_SPATIAL_FWD);
     CK(launch_spatial_forward(sa, 0, s1));
   }
+  CKV(clear_voxelized(ctx, 0, s1));
   CK(cudaEventRecord(ctx->ev_b, s1));
   // rotation
   CKV(run_sample(ctx, 0, s0));
@@ -842,6 +870,7 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
     ProfScope ps(ctx, s0, PS_SPATIAL_FWD);
     CK(launch_spatial_forward(sa, 1, s0));
   }
+  CKV(clear_voxelized(ctx, 1, s0));
   CK(cudaStreamWaitEvent(s0, ctx->ev_b, 0));
   CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), s0));
   {

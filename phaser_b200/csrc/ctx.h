@@ -65,6 +65,11 @@ struct phgpu_ctx {
   float* d_rotvol = nullptr;
   // translation
   float* d_grids[2] = {nullptr, nullptr};  // [(C+1)][N^3]
+  uint8_t* d_rowlive[2] = {nullptr, nullptr};  // [N][N] rows holding a point of the last voxelisation
+  // leading grid planes (and row flags) known to be zero: a voxelisation whose
+  // grids were cleared afterwards leaves them zero, so the next one needs no memset
+  int clean_planes[2] = {0, 0};
+  bool grids_live[2] = {false, false};  // grids hold the last voxelisation (not yet cleared)
   float2* d_spec = nullptr;
   float2* d_cspec = nullptr;
   float* d_transvol = nullptr;

@@ -141,7 +141,7 @@ constexpr int tail_threads() {
 // butterflies of the same row.
 template <int N, int R, int L, bool INV, bool COL>
 __device__ __forceinline__ void tail_smem_stage(float2* buf, int ntrans, int stride, const float2* __restrict__ tw,
-                                                int tid, int T) {
+                                                int tid, int T, const int* rowmap = nullptr) {
   constexpr int m = L / R;
   constexpr int nb = N / R;  // butterflies per transform
   constexpr int twstep = N / L;
@@ -165,7 +165,8 @@ __device__ __forceinline__ void tail_smem_stage(float2* buf, int ntrans, int str
   const int off = blk * L + j2;
   const int es = COL ? m * stride : m;
   for (int t = t0; t < ntrans; t += lanes) {
-    float2* base = COL ? buf + t + (size_t)off * stride : buf + (size_t)t * stride + off;
+    const int tt = (!COL && rowmap) ? rowmap[t] : t;
+    float2* base = COL ? buf + tt + (size_t)off * stride : buf + (size_t)tt * stride + off;
     float2 x[R];
 #pragma unroll
     for (int j = 0; j < R; ++j) x[j] = base[j * es];
@@ -186,7 +187,8 @@ __device__ __forceinline__ void tail_smem_stage(float2* buf, int ntrans, int str
 // Register blocks: neighbouring threads take neighbouring transforms (rows
 // need an odd-ish row stride, e.g. N + 1, to stay conflict-free).
 template <int N, bool INV, bool COL>
-__device__ __forceinline__ void tail_reg_stage(float2* buf, int ntrans, int stride, int tid, int T) {
+__device__ __forceinline__ void tail_reg_stage(float2* buf, int ntrans, int stride, int tid, int T,
+                                               const int* rowmap = nullptr) {
   using P = Tail<N>;
   constexpr int M = P::TA * P::TB;
   constexpr int nbk = N / M;  // register blocks per transform
@@ -194,7 +196,8 @@ __device__ __forceinline__ void tail_reg_stage(float2* buf, int ntrans, int stri
   const int bk = tid / lanes;
   if (bk >= nbk) return;
   for (int t = tid - bk * lanes; t < ntrans; t += lanes) {
-    float2* base = COL ? buf + t + (size_t)(bk * M) * stride : buf + (size_t)t * stride + bk * M;
+    const int tt = (!COL && rowmap) ? rowmap[t] : t;
+    float2* base = COL ? buf + tt + (size_t)(bk * M) * stride : buf + (size_t)tt * stride + bk * M;
     const int es = COL ? stride : 1;
     float2 x[M];
 #pragma unroll
@@ -208,28 +211,31 @@ __device__ __forceinline__ void tail_reg_stage(float2* buf, int ntrans, int stri
 // Batched in-place transform.  Same position convention as fft_fixed<N>.
 // Caller synchronises before; ends with __syncthreads().  T = blockDim.x must
 // be a multiple of every stage's butterfly count (tail_threads<N>() is).
+// Rows only: with rowmap, transform t is row rowmap[t] (t < ntrans), which
+// lets a caller transform just the rows that are not all zero.
 template <int N, bool INV, bool COL>
-__device__ __forceinline__ void fft_tail(float2* buf, int ntrans, int stride, const float2* __restrict__ tw) {
+__device__ __forceinline__ void fft_tail(float2* buf, int ntrans, int stride, const float2* __restrict__ tw,
+                                         const int* rowmap = nullptr) {
   using P = Tail<N>;
   static_assert(P::ok, "no register-tail plan for this length");
   const int tid = threadIdx.x, T = blockDim.x;
   if constexpr (!INV) {
-    tail_smem_stage<N, P::S0, N, false, COL>(buf, ntrans, stride, tw, tid, T);
+    tail_smem_stage<N, P::S0, N, false, COL>(buf, ntrans, stride, tw, tid, T, rowmap);
     __syncthreads();
     if constexpr (P::S1 > 1) {
-      tail_smem_stage<N, P::S1, N / P::S0, false, COL>(buf, ntrans, stride, tw, tid, T);
+      tail_smem_stage<N, P::S1, N / P::S0, false, COL>(buf, ntrans, stride, tw, tid, T, rowmap);
       __syncthreads();
     }
-    tail_reg_stage<N, false, COL>(buf, ntrans, stride, tid, T);
+    tail_reg_stage<N, false, COL>(buf, ntrans, stride, tid, T, rowmap);
     __syncthreads();
   } else {
-    tail_reg_stage<N, true, COL>(buf, ntrans, stride, tid, T);
+    tail_reg_stage<N, true, COL>(buf, ntrans, stride, tid, T, rowmap);
     __syncthreads();
     if constexpr (P::S1 > 1) {
-      tail_smem_stage<N, P::S1, N / P::S0, true, COL>(buf, ntrans, stride, tw, tid, T);
+      tail_smem_stage<N, P::S1, N / P::S0, true, COL>(buf, ntrans, stride, tw, tid, T, rowmap);
       __syncthreads();
     }
-    tail_smem_stage<N, P::S0, N, true, COL>(buf, ntrans, stride, tw, tid, T);
+    tail_smem_stage<N, P::S0, N, true, COL>(buf, ntrans, stride, tw, tid, T, rowmap);
     __syncthreads();
   }
 }

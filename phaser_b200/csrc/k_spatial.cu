@@ -65,6 +65,8 @@ __global__ void k_voxelize(VoxelArgs a) {
   const bool ok = lin < nv;
   if (a.lin_out) a.lin_out[i] = ok ? lin : 0xffffffffu;
   if (!ok) return;
+  // the row of lin, not (bz, bx): an out-of-range bin (-1) wraps into another row
+  if (a.rowlive) a.rowlive[lin / N] = 1;
   float* g = a.grids;
   atomicAdd(&g[lin], p.w);
   const float r = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
@@ -77,6 +79,25 @@ __global__ void k_voxelize(VoxelArgs a) {
 cudaError_t launch_voxelize(const VoxelArgs& a, cudaStream_t st) {
   if (a.n_points > 0) {
     k_voxelize<<<(a.n_points + 255) / 256, 256, 0, st>>>(a);
+    count_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+__global__ void k_clear_voxels(const uint32_t* __restrict__ lin, int n_points, float* __restrict__ grids, size_t nv,
+                               int n_planes, uint8_t* __restrict__ rowlive, int N) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_points) return;
+  const uint32_t l = lin[i];
+  if (l == 0xffffffffu) return;
+  for (int p = 0; p < n_planes; ++p) grids[(size_t)p * nv + l] = 0.0f;
+  if (rowlive) rowlive[l / (uint32_t)N] = 0;
+}
+
+cudaError_t launch_clear_voxels(const uint32_t* lin, int n_points, float* grids, size_t nv, int n_planes,
+                                uint8_t* rowlive, int N, cudaStream_t st) {
+  if (n_points > 0) {
+    k_clear_voxels<<<(n_points + 255) / 256, 256, 0, st>>>(lin, n_points, grids, nv, n_planes, rowlive, N);
     count_launches(1);
   }
   return cudaGetLastError();
@@ -287,16 +308,31 @@ __device__ __forceinline__ float voxel_mean(float v, float c) { return c > 0.0f 
 
 template <int NF>
 __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __restrict__ grids, size_t grid_cstride,
-                                                   const float* __restrict__ count, float2* __restrict__ spec,
+                                                   const float* __restrict__ count,
+                                                   const uint8_t* __restrict__ rowlive, float2* __restrict__ spec,
                                                    size_t spec_cstride, FftPlan pN, FftPlan pH) {
   constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1, Q = NF / 4, S = NF + 1;
   const int H2p = spatial_h2p(N);
   extern __shared__ float2 W[];  // [NH][S]
+  __shared__ int s_flag[NH];      // packed row r may hold a point (row flags), else all zero
+  __shared__ int s_live[NH];      // packed row r holds a non-zero value
+  __shared__ int s_rows[NH];      // compact list of those rows
+  __shared__ int s_nrows;
   const int z = blockIdx.x, c = blockIdx.y;
   const float* g = grids + (size_t)c * grid_cstride + (size_t)z * N * N;
   const float* cnt = count ? count + (size_t)z * N * N : nullptr;
+  for (int r = threadIdx.x; r < NH; r += blockDim.x) {
+    s_live[r] = 0;
+    s_flag[r] = rowlive ? (rowlive[z * N + 2 * r] | rowlive[z * N + 2 * r + 1]) : 1;
+  }
+  __syncthreads();
   for (int e = threadIdx.x; e < NH * Q; e += blockDim.x) {
     const int r = e / Q, y4 = (e - r * Q) * 4;
+    if (!s_flag[r]) {  // no point in either row: skip the loads
+      float2* d = W + r * S + y4;
+      d[0] = d[1] = d[2] = d[3] = make_float2(0.f, 0.f);
+      continue;
+    }
     float4 a = *reinterpret_cast<const float4*>(g + (size_t)(2 * r) * N + y4);
     float4 b = *reinterpret_cast<const float4*>(g + (size_t)(2 * r + 1) * N + y4);
     if (cnt) {
@@ -310,11 +346,34 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
     d[1] = make_float2(a.y, b.y);
     d[2] = make_float2(a.z, b.z);
     d[3] = make_float2(a.w, b.w);
+    if ((a.x != 0.f) | (a.y != 0.f) | (a.z != 0.f) | (a.w != 0.f) | (b.x != 0.f) | (b.y != 0.f) | (b.z != 0.f) |
+        (b.w != 0.f))
+      s_live[r] = 1;
   }
   __syncthreads();
-  fft_tail<N, false, false>(W, NH, S, pN.tw);  // over y, rows
-  fft_tail<NH, false, true>(W, N, S, pH.tw);   // over r, columns
+  if (threadIdx.x < 32) {
+    int base = 0;
+    for (int r0 = 0; r0 < NH; r0 += 32) {
+      const bool live = r0 + (int)threadIdx.x < NH && s_live[r0 + threadIdx.x];
+      const unsigned m = __ballot_sync(0xffffffffu, live);
+      if (live) s_rows[base + __popc(m & ((1u << threadIdx.x) - 1u))] = r0 + threadIdx.x;
+      base += __popc(m);
+    }
+    if (threadIdx.x == 0) s_nrows = base;
+  }
+  __syncthreads();
+  const int nrows = s_nrows;
   float2* out = spec + (size_t)c * spec_cstride + (size_t)z * N * H2p;
+  if (nrows == 0) {  // empty slab: its 2-D spectrum is zero
+    for (int e = threadIdx.x; e < N * H2; e += blockDim.x) {
+      const int k = e / H2, ky = e - k * H2;
+      out[(size_t)k * H2p + ky] = make_float2(0.f, 0.f);
+    }
+    return;
+  }
+  // rows that are all zero stay zero under the y transform
+  fft_tail<N, false, false>(W, nrows, S, pN.tw, s_rows);  // over y, live rows
+  fft_tail<NH, false, true>(W, N, S, pH.tw);               // over r, columns
   for (int e = threadIdx.x; e < NH * H2; e += blockDim.x) {
     const int k = e / H2, ky = e - k * H2;
     const float2 w1 = W[fixed_freq2pos<NH>(k) * S + fixed_freq2pos<N>(ky)];
@@ -384,6 +443,14 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
 
 constexpr int kMaxSmem = 227 * 1024;
 
+// Opt-in dynamic shared memory: everything the static shared memory leaves.
+static cudaError_t allow_max_smem(const void* fn) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem - (int)fa.sharedSizeBytes);
+}
+
 template <int NF>
 static cudaError_t set_attrs() {
   cudaError_t e = cudaFuncSetAttribute(k_fuse_z<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
@@ -403,7 +470,7 @@ cudaError_t spatial_init_attributes() {
   }
   for (auto fn : {(const void*)k_slab_fwd<64>, (const void*)k_slab_fwd<128>, (const void*)k_slab_fwd<200>,
                   (const void*)k_slab_inv<64>, (const void*)k_slab_inv<128>, (const void*)k_slab_inv<200>}) {
-    cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+    cudaError_t r = allow_max_smem(fn);
     if (r != cudaSuccess) e = r;
   }
   return e;
@@ -445,8 +512,9 @@ cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t 
     float2* spec = a.spec + (size_t)(side * a.n_data_ch) * plane;
     dim3 g(N, nch);
     const size_t sm = (size_t)(N / 2) * (N + 1) * sizeof(float2);
-    PHGPU_DISPATCH_SLAB(N, k_slab_fwd<NF><<<g, tail_threads<NF>(), sm, st>>>(grids, nv, count, spec, plane, *a.plan,
-                                                                             *a.plan_half));
+    const uint8_t* rowlive = side == 0 ? a.rowlive_f : a.rowlive_g;
+    PHGPU_DISPATCH_SLAB(N, k_slab_fwd<NF><<<g, tail_threads<NF>(), sm, st>>>(grids, nv, count, rowlive, spec, plane,
+                                                                             *a.plan, *a.plan_half));
     count_launches(1);
     return cudaGetLastError();
   }

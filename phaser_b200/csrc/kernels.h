@@ -90,8 +90,13 @@ struct VoxelArgs {
   int n_data_ch;          // channels accumulated (1..4) in order {int, range, refl, amb}
   float* grids;           // [n_data_ch + 1][N^3] sums, last = count
   uint32_t* lin_out;      // optional per-point linear index (or 0xffffffff)
+  uint8_t* rowlive;       // optional [N (z)][N (x)]: set to 1 for every row a point lands in
 };
 cudaError_t launch_voxelize(const VoxelArgs& a, cudaStream_t st);
+// Zeroes what one voxelisation wrote: planes [0, n_planes) at every point's
+// voxel (lin[i] != 0xffffffff) and the point's row flag.
+cudaError_t launch_clear_voxels(const uint32_t* lin, int n_points, float* grids, size_t nv, int n_planes,
+                                uint8_t* rowlive, int N, cudaStream_t st);
 
 struct SpatialArgs {
   int N;
@@ -102,6 +107,8 @@ struct SpatialArgs {
   const float* grids_f;   // [n_data_ch + 1][N^3] target sums + count (normalised here)
   const float* grids_g;   // source
   int grids_are_means;    // 1: grids already hold values (no count plane)
+  const uint8_t* rowlive_f;  // optional row flags of the grids (rows never flagged are all zero)
+  const uint8_t* rowlive_g;
   float2* spec;           // [2 n_data_ch][N (z)][N (x)][H2p (ky)]
   float2* cspec;          // [N][N][H2p]
   const FftPlan* plan;    // length N

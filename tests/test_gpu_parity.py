@@ -100,6 +100,28 @@ def test_spatial_laplace_vs_oracle(nat, N, C):
     assert vox == O.argmax(ref)
 
 
+@pytest.mark.parametrize("N,C", [(64, 3), (128, 2), (200, 3)])
+def test_spatial_sparse_vs_oracle(nat, N, C):
+    """Voxel grids of LiDAR scans are sparse: whole z slabs and most x rows are
+    empty (the slab kernels skip them)."""
+    rng = np.random.default_rng(N + 100 * C)
+    f = np.zeros((C, N, N, N))
+    g = np.zeros((C, N, N, N))
+    for X, z0 in ((f, N // 4), (g, N // 3)):
+        for z in range(z0, z0 + N // 4):
+            rows = rng.choice(N, N // 6, replace=False)
+            X[:, z, rows, :] = rng.standard_normal((C, len(rows), N)) * (rng.random((C, len(rows), N)) < 0.3)
+    f = f.reshape(C, -1)
+    g = g.reshape(C, -1)
+    c = ctx(nat, spatial_n_voxels=N, flags=nat.PHGPU_FLAG_KEEP_VOLUMES)
+    c.spatial_correlate(list(f), list(g))
+    vox, peak, vol = c.spatial_result(volume=True)
+    ref = O.spatial_correlation(f, g, N, laplace=True)
+    err, n_amb = tie_masked_rel_l2(vol, ref, f, g, N)
+    assert err <= REL_L2
+    assert vox == O.argmax(ref)
+
+
 @pytest.mark.parametrize("N", [3, 6, 10, 32, 64, 256])
 def test_spatial_plain_vs_oracle(nat, N):
     rng = np.random.default_rng(N)
@@ -269,6 +291,39 @@ def test_register_pair_workload1_full_size(nat, k):
     pose2 = c.register_pair((pair.target.xyzi, pair.target.reflectivity),
                             (pair.source.xyzi, pair.source.reflectivity))
     assert (pose2.rot_bin, pose2.voxel) == (pose.rot_bin, pose.voxel)
+
+
+def test_context_reuse_leaves_no_state():
+    """Grids are cleared point by point after each registration instead of
+    being memset: a context that registered other pairs first must give the
+    volumes of a fresh one (up to the summation order of the voxel atomics,
+    hence 1e-6 rather than bit equality; a left-over voxel of the other pair
+    would change them at the 1e-2 level), and the public voxelise + correlate
+    path must still work after registrations."""
+    from phaser_b200 import native, scene
+    w = scene.WORKLOADS[1]
+    kw = dict(spherical_bandwidth=w["bw"], spatial_n_voxels=w["n_voxels"], spatial_discretize_lower=w["lo"],
+              spatial_discretize_upper=w["hi"], flags=native.PHGPU_FLAG_KEEP_VOLUMES)
+    a, b = scene.workload_pair(1, 1), scene.workload_pair(1, 0)
+    args = lambda p: ((p.target.xyzi, p.target.reflectivity), (p.source.xyzi, p.source.reflectivity))
+    used = native.Context(**kw)
+    used.register_pair(*args(a))
+    pose_used = used.register_pair(*args(b))
+    fresh = native.Context(**kw)
+    pose_fresh = fresh.register_pair(*args(b))
+    assert (pose_used.rot_bin, pose_used.voxel) == (pose_fresh.rot_bin, pose_fresh.voxel)
+    assert rel_l2(used.spatial_result(volume=True)[2], fresh.spatial_result(volume=True)[2]) <= 1e-6
+    assert rel_l2(used.sph_result(volume=True)[2], fresh.sph_result(volume=True)[2]) <= 1e-6
+    # voxelise + correlate on both contexts (the used one has cleared grids)
+    T = O.rotation_xyz(*pose_fresh.xyz)
+    for c in (used, fresh):
+        c.voxelize(b.target.xyzi, b.target.reflectivity, side=0)
+        c.voxelize(b.source.xyzi, b.source.reflectivity, side=1, T=T)
+        c.spatial_correlate_voxelized()
+    vu, fu = used.spatial_result(volume=True)[2], fresh.spatial_result(volume=True)[2]
+    assert rel_l2(vu, fu) <= 1e-6
+    used.close()
+    fresh.close()
 
 
 def test_device_resident_inputs(nat, pair0):
