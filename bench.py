@@ -305,7 +305,9 @@ def main():
     ctx.close()
 
     # ---------------- served pipeline, device-resident inputs (value)
-    srv = nat.Server(workers=a.workers, hbm_budget_bytes=150 << 30, device=local)
+    # host inputs are borrowed (pinned, copied to the device inside each request)
+    srv = nat.Server(workers=a.workers, hbm_budget_bytes=150 << 30, device=local,
+                     flags=nat.PHGPU_SERVER_BORROW_HOST)
 
     def served_round(inputs, n):
         tickets = [srv.submit(params, *inputs[i % len(inputs)]) for i in range(n)]

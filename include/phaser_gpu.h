@@ -207,15 +207,20 @@ typedef struct {
   uint32_t max_wave;           /* pairs per wave and shape */
   uint32_t max_points;         /* capacity per cloud */
   int32_t device;
-  uint32_t flags;
+  uint32_t flags;              /* PHGPU_SERVER_* */
 } phgpu_server_params;
+
+/* Host clouds are read in place by the worker (copied to the device inside the
+ * request, asynchronously when the memory is pinned) instead of being copied
+ * at submit; the caller keeps them valid until the ticket completes. */
+#define PHGPU_SERVER_BORROW_HOST 1u
 
 int phgpu_server_create(const phgpu_server_params* params, phgpu_server** out);
 int phgpu_server_destroy(phgpu_server* srv);
 /* Submits one pair; params gives the shape (bandwidth, voxels, bounds).  Host
- * clouds are copied before the call returns; device clouds (on_device = 1 for
- * both) are read in place and must stay valid until the ticket completes.
- * *ticket identifies the request. */
+ * clouds are copied before the call returns (unless PHGPU_SERVER_BORROW_HOST);
+ * device clouds (on_device = 1 for both) are read in place and must stay
+ * valid until the ticket completes.  *ticket identifies the request. */
 int phgpu_server_submit(phgpu_server* srv, const phgpu_params* params, const phgpu_cloud* target,
                         const phgpu_cloud* source, uint64_t* ticket);
 /* Non-blocking: 1 and the pose when the ticket finished, 0 otherwise. */

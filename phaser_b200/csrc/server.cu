@@ -30,10 +30,11 @@ using Clock = std::chrono::steady_clock;
 struct Request {
   uint64_t ticket = 0;
   phgpu_params prm;
-  // device-resident inputs are used in place (the caller keeps them alive
-  // until the ticket completes); host inputs are copied at submit
+  // device-resident inputs (and host inputs under PHGPU_SERVER_BORROW_HOST)
+  // are used in place: the caller keeps them alive until the ticket
+  // completes; other host inputs are copied at submit
   phgpu_cloud tdev{}, sdev{};
-  bool on_device = false;
+  bool in_place = false;
   std::vector<float> txyzi, trefl, tamb, sxyzi, srefl, samb;
   uint32_t tn = 0, sn = 0;
   bool t_refl = false, t_amb = false, s_refl = false, s_amb = false;
@@ -148,7 +149,7 @@ struct phgpu_server {
                     r->t_amb ? r->tamb.data() : nullptr, r->tn, 0};
       phgpu_cloud s{r->sxyzi.data(), r->s_refl ? r->srefl.data() : nullptr,
                     r->s_amb ? r->samb.data() : nullptr, r->sn, 0};
-      if (r->on_device) {
+      if (r->in_place) {
         t = r->tdev;
         s = r->sdev;
       }
@@ -229,8 +230,8 @@ int phgpu_server_submit(phgpu_server* s, const phgpu_params* params, const phgpu
   r->prm = *params;
   r->tn = target->n_points;
   r->sn = source->n_points;
-  if (target->on_device && source->on_device) {
-    r->on_device = true;
+  if ((target->on_device && source->on_device) || (s->prm.flags & PHGPU_SERVER_BORROW_HOST)) {
+    r->in_place = true;
     r->tdev = *target;
     r->sdev = *source;
   } else {

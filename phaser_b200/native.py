@@ -22,6 +22,7 @@ NOALLOC_MAX_BANDWIDTH = 128
 PHGPU_FUSION_LAPLACE = 0
 PHGPU_FUSION_NONE = 1
 PHGPU_FLAG_KEEP_VOLUMES = 1
+PHGPU_SERVER_BORROW_HOST = 1
 
 
 class PhgpuError(RuntimeError):
@@ -376,6 +377,7 @@ class Server:
             raise PhgpuError(f"phgpu_server_create failed ({rc})")
         self.h = h
         self._keep = {}
+        self._borrow = bool(int(flags) & PHGPU_SERVER_BORROW_HOST)
 
     def submit(self, params: Params, target, source) -> int:
         ct, k1 = make_cloud(*target)
@@ -384,8 +386,8 @@ class Server:
         rc = self.lib.phgpu_server_submit(self.h, C.byref(params), C.byref(ct), C.byref(cs), C.byref(t))
         if rc != PHGPU_OK:
             raise PhgpuError(f"submit failed ({rc}): {self.lib.phgpu_server_last_error(self.h).decode()}")
-        if ct.on_device:
-            self._keep[t.value] = (k1, k2)  # device inputs are read in place
+        if (ct.on_device and cs.on_device) or self._borrow:
+            self._keep[t.value] = (k1, k2)  # read in place until the ticket completes
         return t.value
 
     def poll(self, ticket):
