@@ -443,9 +443,11 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
     CKV(dalloc(ctx, &ctx->d_rotvol, sizeof(float) * no * no * no));
     CKV(dalloc(ctx, &ctx->d_transvol, sizeof(float) * nv));
   }
-  CKV(dalloc(ctx, &ctx->d_argmax, sizeof(unsigned long long) * 2));
-  CK(cudaMallocHost((void**)&ctx->h_argmax, sizeof(unsigned long long) * 2));
-  ctx->h_argmax[0] = ctx->h_argmax[1] = 0ull;
+  // [0] rotation argmax, [1] translation argmax, [2] kernel status bits (sticky)
+  CKV(dalloc(ctx, &ctx->d_argmax, sizeof(unsigned long long) * 3));
+  CK(cudaMemset(ctx->d_argmax, 0, sizeof(unsigned long long) * 3));
+  CK(cudaMallocHost((void**)&ctx->h_argmax, sizeof(unsigned long long) * 3));
+  ctx->h_argmax[0] = ctx->h_argmax[1] = ctx->h_argmax[2] = 0ull;
   CKV(ensure_cloud_capacity(ctx, prm->max_points ? prm->max_points : (1u << 18)));
   CK(cudaStreamSynchronize(ctx->s0));
   return PHGPU_OK;
@@ -740,6 +742,7 @@ static SpatialArgs spatial_args(phgpu_ctx* ctx, int n_data, int n_total, int lap
   a.plan = &ctx->plan_sp;
   a.plan_half = ctx->has_sp_half ? &ctx->plan_sp_half : nullptr;
   a.argmax = ctx->d_argmax + 1;
+  a.status = ctx->d_argmax + 2;
   a.volume = ctx->d_transvol;
   return a;
 }
@@ -760,7 +763,7 @@ int phgpu_run_spatial(phgpu_ctx* ctx, int n_data, int n_total, int laplace, int 
     ProfScope ps(ctx, st, PS_SPATIAL_INV);
     CK(launch_spatial_inverse(a, st));
   }
-  CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, sizeof(unsigned long long),
+  CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, 2 * sizeof(unsigned long long),
                      cudaMemcpyDeviceToHost, st));
   ctx->have_trans = true;
   return PHGPU_OK;
@@ -810,6 +813,10 @@ int phgpu_spatial_result(phgpu_ctx* ctx, uint32_t* voxel, float* peak, double* c
   }
   cudaSetDevice(ctx->prm.device);
   CK(cudaStreamSynchronize(ctx->s0));
+  if (ctx->h_argmax[2]) {
+    ctx->err = "a bulk-copy wait in the translation kernels timed out";
+    return PHGPU_ERR_CUDA;
+  }
   const unsigned long long k = ctx->h_argmax[1];
   if (voxel) *voxel = unpack_index(k);
   if (peak) *peak = float_from_order_bits((uint32_t)(k >> 32));
@@ -881,10 +888,14 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
     ProfScope ps(ctx, s0, PS_SPATIAL_INV);
     CK(launch_spatial_inverse(sa, s0));
   }
-  CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, sizeof(unsigned long long),
+  CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, 2 * sizeof(unsigned long long),
                      cudaMemcpyDeviceToHost, s0));
   ctx->have_trans = true;
   CK(cudaStreamSynchronize(s0));
+  if (ctx->h_argmax[2]) {
+    ctx->err = "a bulk-copy wait in the translation kernels timed out";
+    return PHGPU_ERR_CUDA;
+  }
   const unsigned long long tk = ctx->h_argmax[1];
   out->voxel = unpack_index(tk);
   out->trans_peak = float_from_order_bits((uint32_t)(tk >> 32));

@@ -23,6 +23,8 @@
 // tile) + fusion + cross power + inverse FFT along z; C1 inverse FFT along x;
 // C2 complex-to-real along y with argmax.  Forward transforms leave x and z in
 // digit-reversed order; the inverse transforms consume that order directly.
+#include <cuda.h>  // CUtensorMap (encoded through the runtime's driver entry point)
+
 #include "fft2.cuh"
 #include "kernels.h"
 
@@ -166,9 +168,37 @@ __global__ void k_fft_x(int N, float2* __restrict__ spec, FftPlan plan) {
 // ---------------------------------------------------------------- B
 // For one x position (digit-reversed) and a tile of ky: forward z FFT of all
 // 2C arrays, fusion + cross power, inverse z FFT of the product.
+//
+// The [z][array][ky tile] block arrives by one bulk tensor copy per z chunk
+// (TMA, when the host could encode the tensor map; each box <= 256 z rows)
+// into the same layout the element loader produces.  Dynamic shared memory:
+// tile [zrows][rowlen] float2 | mbarrier (16 B) | fusion bands.
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Waits for phase 0 of a shared-memory mbarrier; gives up after a bounded
+// number of polls (returns false).
+__device__ __forceinline__ bool mbar_wait0(uint64_t* bar) {
+  uint32_t done = 0;
+  for (int it = 0; it < (1 << 22) && !done; ++it) {
+    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+                 : "=r"(done)
+                 : "r"(smem_addr(bar))
+                 : "memory");
+  }
+  return done != 0;
+}
+
+struct FuseZTma {
+  int enabled;  // tensor map valid
+  int zbox;     // z rows per copy
+  int chunks;   // copies (zbox * chunks >= N)
+};
+
 template <int NF>
-__global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int Wt, int x_natural) {
-  extern __shared__ float2 tile[];  // [z][arr][t]
+__global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int Wt, int x_natural,
+                                                const __grid_constant__ CUtensorMap tmap, FuseZTma tma) {
+  extern __shared__ __align__(128) float2 tile[];  // [z][arr][t]
   const int N = NF > 0 ? NF : a.N;
   const int H2 = N / 2 + 1;
   const int H2p = spatial_h2p(N);
@@ -179,23 +209,58 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
   const int xp = blockIdx.y;
   const size_t plane = (size_t)N * N * H2p;
   const int rowlen = A * Wt;
-  // tiles start at ky0 (multiple of Wt) in rows padded to 8 complex: load two
-  // complex per 16-byte access
-  const int half = Wt >> 1;
-  for (int e = threadIdx.x; e < N * A * half; e += blockDim.x) {
-    const int z = e / (A * half), rem = e - z * (A * half), ar = rem / half, t2 = rem - ar * half;
-    // arrays: f channels 0..C-1 then g channels; plain mode uses channel 0 of each side
-    const int src = a.laplace ? ar : (ar == 0 ? 0 : C);
-    const float4 v = *reinterpret_cast<const float4*>(
-        a.spec + (size_t)src * plane + ((size_t)z * N + xp) * H2p + ky0 + 2 * t2);
-    float2* d = tile + (size_t)z * rowlen + ar * Wt + 2 * t2;
-    d[0] = make_float2(v.x, v.y);
-    d[1] = make_float2(v.z, v.w);
+  const int zrows = tma.enabled ? tma.zbox * tma.chunks : N;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tile + (size_t)zrows * rowlen);
+  FusionBands* s_bands = reinterpret_cast<FusionBands*>(bar + 2);
+  if (threadIdx.x == 0) *s_bands = a.bands;  // divergent band lookups are cheap in shared memory
+  // the bulk copy needs a 128-byte aligned destination (block-uniform test)
+  const bool use_tma = tma.enabled && (smem_addr(tile) & 127u) == 0;
+  if (use_tma) {
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)));
+      asm volatile("fence.mbarrier_init.release.cluster;");
+      asm volatile("fence.proxy.async.shared::cta;");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t bytes = (uint32_t)((size_t)zrows * rowlen * sizeof(float2));
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                   : "memory");
+      for (int ch = 0; ch < tma.chunks; ++ch) {
+        const int z0 = ch * tma.zbox;
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(tile + (size_t)z0 * rowlen)),
+            "l"(&tmap), "r"(ky0), "r"(0), "r"(xp), "r"(z0), "r"(smem_addr(bar))
+            : "memory");
+      }
+    }
+    if (!mbar_wait0(bar)) {
+      if (threadIdx.x == 0) atomicOr(a.status, 1ull);
+      mbar_wait0(bar);  // once more (bounded) so no copy is left in flight
+    }
+  } else {
+    // tiles start at ky0 (multiple of Wt) in rows padded to 8 complex: load two
+    // complex per 16-byte access
+    const int half = Wt >> 1;
+    for (int e = threadIdx.x; e < N * A * half; e += blockDim.x) {
+      const int z = e / (A * half), rem = e - z * (A * half), ar = rem / half, t2 = rem - ar * half;
+      // arrays: f channels 0..C-1 then g channels; plain mode uses channel 0 of each side
+      const int src = a.laplace ? ar : (ar == 0 ? 0 : C);
+      const float4 v = *reinterpret_cast<const float4*>(
+          a.spec + (size_t)src * plane + ((size_t)z * N + xp) * H2p + ky0 + 2 * t2);
+      float2* d = tile + (size_t)z * rowlen + ar * Wt + 2 * t2;
+      d[0] = make_float2(v.x, v.y);
+      d[1] = make_float2(v.z, v.w);
+    }
   }
   __syncthreads();
   fft_any<NF, false, -2>(tile, rowlen, 1, rowlen, plan);
   const int kx = x_natural ? xp : pos2freq<NF>(xp, plan);
   const uint32_t nv = (uint32_t)N * (uint32_t)N * (uint32_t)N;
+  // MEAN divides by the total channel count: a product with the reciprocal,
+  // exact for the reference's 4 channels (within one rounding otherwise)
+  const float inv_total = 1.0f / (float)a.n_total_ch;
   for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
     const int zp = e / Wt, t = e - zp * Wt;
     float2* row = tile + (size_t)zp * rowlen;
@@ -206,40 +271,30 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
     } else {
       const int kz = pos2freq<NF>(zp, plan);
       const uint32_t klin = ((uint32_t)kz * N + (uint32_t)kx) * (uint32_t)H2 + (uint32_t)(ky0 + t);
-      const uint32_t p = (uint32_t)(((uint64_t)klin + (nv >> 1)) % nv);
-      const int op = fusion_op(p, a.bands);
-      if (op == kFuseZero) {
-        F = make_float2(0.f, 0.f);
-        G = F;
-      } else if (op == kFuseMean) {
-        float fr = 0.f, fi = 0.f, gr = 0.f, gi = 0.f;
-        for (int c = 0; c < C; ++c) {
-          fr += row[c * Wt + t].x;
-          fi += row[c * Wt + t].y;
-          gr += row[(C + c) * Wt + t].x;
-          gi += row[(C + c) * Wt + t].y;
-        }
-        const float inv = (float)a.n_total_ch;
-        F = make_float2(fr / inv, fi / inv);
-        G = make_float2(gr / inv, gi / inv);
-      } else {
-        float bf = -1.f, bg = -1.f;
-        F = G = make_float2(0.f, 0.f);
-        for (int c = 0; c < C; ++c) {
-          const float2 u = row[c * Wt + t];
-          const float2 v = row[(C + c) * Wt + t];
-          const float eu = u.x * u.x + u.y * u.y;
-          const float ev = v.x * v.x + v.y * v.y;
-          if (eu > bf) {
-            bf = eu;
-            F = u;
-          }
-          if (ev > bg) {
-            bg = ev;
-            G = v;
-          }
-        }
+      // (klin + nv/2) mod nv with klin < nv
+      uint32_t p = klin + (nv >> 1);
+      if (p >= nv || p < klin) p -= nv;
+      const int op = fusion_op(p, *s_bands);
+      // one branch-free pass serves every rule (a divergent switch between
+      // the rules cost more than the arithmetic): channel sums for MEAN, the
+      // first channel of largest energy for MAX
+      float2 sf = make_float2(0.f, 0.f), sg = sf, mf = sf, mg = sf;
+      float bf = -1.f, bg = -1.f;
+      for (int c = 0; c < C; ++c) {
+        const float2 u = row[c * Wt + t];
+        const float2 v = row[(C + c) * Wt + t];
+        sf = cadd(sf, u);
+        sg = cadd(sg, v);
+        const float eu = u.x * u.x + u.y * u.y;
+        const float ev = v.x * v.x + v.y * v.y;
+        mf = eu > bf ? u : mf;
+        bf = eu > bf ? eu : bf;
+        mg = ev > bg ? v : mg;
+        bg = ev > bg ? ev : bg;
       }
+      const float inv = inv_total;
+      F = op == kFuseMax ? mf : (op == kFuseMean ? make_float2(sf.x * inv, sf.y * inv) : make_float2(0.f, 0.f));
+      G = op == kFuseMax ? mg : (op == kFuseMean ? make_float2(sg.x * inv, sg.y * inv) : make_float2(0.f, 0.f));
     }
     // complexMulSeq: C = F * conj(G); only this thread touches position (zp, t)
     row[t] = make_float2(F.x * G.x - F.y * (-G.y), F.x * (-G.y) + F.y * G.x);
@@ -496,9 +551,31 @@ bool spatial_slab_path(int N) { return N == 64 || N == 128 || N == 200; }
 
 // Tile width of the z pass: as many ky columns as fit (<= 8) in shared memory.
 static int fuse_z_tile(int N, int A) {
-  int wt = 8;  // >= 2: the loader moves two complex per 16-byte access
-  while (wt > 2 && (size_t)N * A * wt * sizeof(float2) > (size_t)kMaxSmem) wt >>= 1;
+  // >= 2: the loader moves two complex per 16-byte access, and a bulk copy's
+  // innermost extent must be a multiple of 16 bytes
+  int wt = 8;
+  const int chunks = (N + 255) / 256;                       // bulk copies of <= 256 z rows
+  const size_t rows = (size_t)chunks * ((N + chunks - 1) / chunks);
+  const size_t extra = 16 + sizeof(FusionBands);
+  while (wt > 2 && rows * A * wt * sizeof(float2) + extra > (size_t)kMaxSmem) wt >>= 1;
   return wt;
+}
+
+// cuTensorMapEncodeTiled through the runtime (no link against the driver
+// library); null when unavailable, in which case the element loader is used.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
 }
 
 cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t st) {
@@ -535,11 +612,31 @@ cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st) {
   const int N = a.N, H2 = N / 2 + 1;
   const int A = a.laplace ? 2 * a.n_data_ch : 2;
   const int wt = fuse_z_tile(N, A);
-  const size_t smB = (size_t)N * A * wt * sizeof(float2);
+  // bulk tensor copies of the [z][array][ky] tile (element = one complex)
+  CUtensorMap tmap;
+  memset(&tmap, 0, sizeof(tmap));
+  FuseZTma tma{0, N, 1};
+  if (EncodeTiledFn enc = encode_tiled()) {
+    const size_t plane = (size_t)N * N * spatial_h2p(N);
+    const int chunks = (N + 255) / 256;
+    const int zbox = (N + chunks - 1) / chunks;
+    const cuuint64_t dims[4] = {(cuuint64_t)spatial_h2p(N), (cuuint64_t)A, (cuuint64_t)N, (cuuint64_t)N};
+    const cuuint64_t strides[3] = {(cuuint64_t)(a.laplace ? plane : plane * a.n_data_ch) * sizeof(float2),
+                                   (cuuint64_t)spatial_h2p(N) * sizeof(float2),
+                                   (cuuint64_t)N * spatial_h2p(N) * sizeof(float2)};
+    const cuuint32_t box[4] = {(cuuint32_t)wt, (cuuint32_t)A, 1u, (cuuint32_t)zbox};
+    const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+    if (enc(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)a.spec, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+      tma = FuseZTma{1, zbox, chunks};
+  }
+  const size_t rows = (size_t)tma.zbox * tma.chunks;
+  const size_t smB = rows * A * wt * sizeof(float2) + 16 + sizeof(FusionBands);
   if (smB > (size_t)kMaxSmem) return cudaErrorInvalidConfiguration;
   dim3 gB((H2 + wt - 1) / wt, N);
   const int xnat = (spatial_slab_path(N) && a.plan_half) ? 1 : 0;
-  PHGPU_DISPATCH_N(N, k_fuse_z<NF><<<gB, 512, smB, st>>>(a, *a.plan, wt, xnat));
+  PHGPU_DISPATCH_N(N, k_fuse_z<NF><<<gB, 512, smB, st>>>(a, *a.plan, wt, xnat, tmap, tma));
   count_launches(1);
   return cudaGetLastError();
 }

@@ -115,6 +115,7 @@ struct SpatialArgs {
   const FftPlan* plan_half;  // length N/2 (z-slab kernels), may be null
   unsigned long long* argmax;
   float* volume;          // optional N^3 correlation, [z][x][y]
+  unsigned long long* status;  // bit 0: a bulk-copy wait gave up (result invalid)
 };
 cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t st);
 cudaError_t launch_spatial_combine(const SpatialArgs& a, cudaStream_t st);
