@@ -61,8 +61,8 @@ __host__ __device__ __forceinline__ int bin_words(int n2b) { return (n2b + 31) >
 
 __global__ void k_project(const float4* __restrict__ xyzi, int P, float4* __restrict__ proj,
                           double* __restrict__ range, uint32_t* __restrict__ key,
-                          uint32_t* __restrict__ cell_count, int n2b, uint32_t* __restrict__ binmap,
-                          uint32_t* __restrict__ colmask) {
+                          uint32_t* __restrict__ cell_count, uint32_t* __restrict__ coarse_count, int n2b,
+                          uint32_t* __restrict__ binmap, uint32_t* __restrict__ colmask) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
   const float4 p = xyzi[i];
@@ -88,7 +88,17 @@ __global__ void k_project(const float4* __restrict__ xyzi, int P, float4* __rest
   }
   const uint32_t k = cell_key(ox, oy, oz);
   key[i] = k;
-  atomicAdd(&cell_count[k], 1u);
+  // consecutive points of a scan mostly share cells: one atomic per group of
+  // lanes with the same key (a plain per-point atomic serialised on the
+  // ~1000 points of a coarse cell)
+  {
+    const unsigned act = __activemask();
+    const int lane = threadIdx.x & 31;
+    const unsigned pf = __match_any_sync(act, k);
+    if (lane == __ffs(pf) - 1) atomicAdd(&cell_count[k], (uint32_t)__popc(pf));
+    const unsigned pc = __match_any_sync(act, k >> 6);
+    if (lane == __ffs(pc) - 1) atomicAdd(&coarse_count[k >> 6], (uint32_t)__popc(pc));
+  }
   if (n2b > 0) {
     const double w = M_PI / (double)n2b;  // bin height in theta, half bin width in phi
     const int bi = min(max((int)(tx / w), 0), n2b - 1);
@@ -99,69 +109,47 @@ __global__ void k_project(const float4* __restrict__ xyzi, int P, float4* __rest
   }
 }
 
-// Exclusive scan of the 32768 fine-cell counts (one block of 1024 threads,
-// 32 consecutive cells per thread) and the compact list of non-empty coarse
-// cells {start, count, coarse id}.
-__global__ void __launch_bounds__(1024) k_cell_scan(const uint32_t* __restrict__ count, uint32_t* __restrict__ start,
-                                                    uint4* __restrict__ clist, uint32_t* __restrict__ n_coarse) {
-  __shared__ uint32_t wsum[32];
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  constexpr int per = kFineCells / 1024;
-  uint32_t local[per];
-  const uint4* src = reinterpret_cast<const uint4*>(count + t * per);
-  uint32_t s = 0;
-#pragma unroll
-  for (int j = 0; j < per / 4; ++j) {
-    const uint4 v = src[j];
-    local[4 * j] = v.x;
-    local[4 * j + 1] = v.y;
-    local[4 * j + 2] = v.z;
-    local[4 * j + 3] = v.w;
-    s += v.x + v.y + v.z + v.w;
+// Exclusive scan of the 32768 fine-cell counts and the compact list of
+// non-empty coarse cells {start, count, coarse id} in coarse-id order: one
+// 64-thread block per coarse cell (= its 64 fine cells) takes its base and
+// list slot from the 512 coarse counts that precede it, then scans its own
+// fine counts.
+__global__ void __launch_bounds__(64) k_cell_scan(const uint32_t* __restrict__ count,
+                                                  const uint32_t* __restrict__ coarse_count,
+                                                  uint32_t* __restrict__ start, uint4* __restrict__ clist,
+                                                  uint32_t* __restrict__ n_coarse) {
+  __shared__ uint32_t s_pts[2], s_ne[2], s_fine[2];
+  const int c = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  uint32_t pts = 0, ne = 0;
+  for (int i = t; i < c; i += 64) {
+    const uint32_t v = __ldg(&coarse_count[i]);
+    pts += v;
+    ne += v > 0u ? 1u : 0u;
   }
-  uint32_t incl = s;
+  const uint32_t v = __ldg(&count[c * 64 + t]);
+  uint32_t incl = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
+    pts += __shfl_xor_sync(0xffffffffu, pts, o);
+    ne += __shfl_xor_sync(0xffffffffu, ne, o);
+    const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += u;
   }
-  if (lane == 31) wsum[warp] = incl;
-  __syncthreads();
-  if (warp == 0) {
-    uint32_t w = wsum[lane];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t v = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += v;
-    }
-    wsum[lane] = w;
+  if (lane == 0) {
+    s_pts[warp] = pts;
+    s_ne[warp] = ne;
   }
+  if (lane == 31) s_fine[warp] = incl;
   __syncthreads();
-  uint32_t run = (warp > 0 ? wsum[warp - 1] : 0u) + incl - s;
-  uint4* dst = reinterpret_cast<uint4*>(start + t * per);
-#pragma unroll
-  for (int j = 0; j < per / 4; ++j) {
-    uint4 o;
-    o.x = run;
-    run += local[4 * j];
-    o.y = run;
-    run += local[4 * j + 1];
-    o.z = run;
-    run += local[4 * j + 2];
-    o.w = run;
-    run += local[4 * j + 3];
-    dst[j] = o;
-  }
-  if (t == 1023) start[kFineCells] = run;
-  // a coarse cell is 64 consecutive fine cells = 2 threads
-  __syncthreads();
-  if ((t & 1) == 0) {
-    const int c = t >> 1;
-    const uint32_t cs = __ldcg(&start[c * 64]);
-    const uint32_t ce = __ldcg(&start[c * 64 + 64]);  // start[kFineCells] = total for the last cell
-    if (ce > cs) {
-      const uint32_t slot = atomicAdd(n_coarse, 1u);
-      clist[slot] = make_uint4(cs, ce - cs, (uint32_t)c, 0u);
+  const uint32_t base = s_pts[0] + s_pts[1], slot = s_ne[0] + s_ne[1];
+  const uint32_t excl = incl - v + (warp ? s_fine[0] : 0u);
+  start[c * 64 + t] = base + excl;
+  if (t == 63) {
+    const uint32_t total = excl + v;
+    if (total > 0) clist[slot] = make_uint4(base, total, (uint32_t)c, 0u);
+    if (c == kCoarseCells - 1) {
+      start[kFineCells] = base + total;
+      *n_coarse = slot + (total > 0 ? 1u : 0u);
     }
   }
 }
@@ -545,12 +533,13 @@ size_t sampler_scratch_bytes(int max_points, int max_queries) {
   b += (size_t)max_points * sizeof(uint32_t);  // key
   b += (size_t)max_points * sizeof(float4);    // sorted
   b += (size_t)kFineCells * sizeof(uint32_t) * 2;   // count, cursor
+  b += (size_t)kCoarseCells * sizeof(uint32_t);      // coarse counts
   b += (size_t)(kFineCells + 4) * sizeof(uint32_t);  // start
   b += (size_t)kFineCells * 6 * sizeof(uint32_t);    // fine boxes
   b += (size_t)kCoarseCells * sizeof(uint4);
   b += (size_t)kCoarseCells * 6 * sizeof(uint32_t);
   b += 256;
-  return b + 16 * 256;
+  return b + 20 * 256;  // carve() rounds each of the regions up to 256 bytes
 }
 
 static inline char* carve(char*& p, size_t bytes) {
@@ -567,6 +556,7 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   float4* sorted = (float4*)carve(p, (size_t)a.max_points * sizeof(float4));
   uint32_t* count = (uint32_t*)carve(p, (size_t)kFineCells * sizeof(uint32_t));
   uint32_t* cursor = (uint32_t*)carve(p, (size_t)kFineCells * sizeof(uint32_t));
+  uint32_t* ccount = (uint32_t*)carve(p, (size_t)kCoarseCells * sizeof(uint32_t));
   uint32_t* start = (uint32_t*)carve(p, (size_t)(kFineCells + 4) * sizeof(uint32_t));
   uint32_t* flo = (uint32_t*)carve(p, (size_t)kFineCells * 3 * sizeof(uint32_t));
   uint32_t* fhi = (uint32_t*)carve(p, (size_t)kFineCells * 3 * sizeof(uint32_t));
@@ -579,13 +569,12 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   uint32_t* binmap = (uint32_t*)carve(p, nbins * sizeof(uint32_t));
   uint32_t* colmask = (uint32_t*)carve(p, nmask * sizeof(uint32_t));
 
-  // count and cursor are adjacent: one memset
-  cudaMemsetAsync(count, 0, (size_t)2 * kFineCells * sizeof(uint32_t), st);
+  // count, cursor and coarse counts are adjacent: one memset
+  cudaMemsetAsync(count, 0, (size_t)(2 * kFineCells + kCoarseCells) * sizeof(uint32_t), st);
   cudaMemsetAsync(flo, 0xff, (size_t)kFineCells * 3 * sizeof(uint32_t), st);
   cudaMemsetAsync(fhi, 0, (size_t)kFineCells * 3 * sizeof(uint32_t), st);
   cudaMemsetAsync(clo, 0xff, (size_t)kCoarseCells * 3 * sizeof(uint32_t), st);
   cudaMemsetAsync(chi, 0, (size_t)kCoarseCells * 3 * sizeof(uint32_t), st);
-  cudaMemsetAsync(ncoarse, 0, sizeof(uint32_t), st);
   if (n2b > 0) {
     cudaMemsetAsync(binmap, 0xff, nbins * sizeof(uint32_t), st);
     cudaMemsetAsync(colmask, 0, nmask * sizeof(uint32_t), st);
@@ -593,10 +582,10 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   const int P = a.n_points;
   int launched = 0;
   if (P > 0) {
-    k_project<<<(P + 255) / 256, 256, 0, st>>>(a.xyzi, P, proj, range, key, count, n2b, binmap, colmask);
+    k_project<<<(P + 255) / 256, 256, 0, st>>>(a.xyzi, P, proj, range, key, count, ccount, n2b, binmap, colmask);
     ++launched;
   }
-  k_cell_scan<<<1, 1024, 0, st>>>(count, start, clist, ncoarse);
+  k_cell_scan<<<kCoarseCells, 64, 0, st>>>(count, ccount, start, clist, ncoarse);
   ++launched;
   if (P > 0) {
     k_scatter<<<(P + 255) / 256, 256, 0, st>>>(P, proj, key, start, cursor, sorted);
