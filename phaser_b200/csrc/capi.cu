@@ -431,6 +431,12 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   const size_t no = (size_t)2 * bw_out;
   CKV(dalloc(ctx, &ctx->d_S, sizeof(float2) * no * no * bw_out));
   CK(cudaMemset(ctx->d_S, 0, sizeof(float2) * no * no * bw_out));
+  {
+    std::vector<double> bt(3 * (size_t)no);
+    so3_beta_table(bw_out, bt.data());
+    CKV(dalloc(ctx, &ctx->d_beta_tab, sizeof(double) * bt.size()));
+    CK(cudaMemcpy(ctx->d_beta_tab, bt.data(), sizeof(double) * bt.size(), cudaMemcpyHostToDevice));
+  }
   const size_t nv = (size_t)N * N * N;
   const size_t H = (size_t)N * N * spatial_h2p(N);
   for (int s = 0; s < 2; ++s) {
@@ -582,6 +588,7 @@ int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStre
   o.bw_in = bw;
   o.bw_out = ctx->bw_out;
   o.fused = ctx->d_fused;
+  o.beta_tab = ctx->d_beta_tab;
   o.S = ctx->d_S;
   o.plan = &ctx->plan_so3;
   o.argmax = ctx->d_argmax;

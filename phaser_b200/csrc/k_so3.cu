@@ -30,12 +30,18 @@ __device__ __forceinline__ float2 prod_conj(float2 a, float2 b, float s) {
   return make_float2(s * (a.x * b.x + a.y * b.y), s * (a.y * b.x - a.x * b.y));
 }
 
-__global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz, float2* __restrict__ S) {
+// KB betas per thread (k = t, t + ceil(n / KB), ...): the coefficient loads
+// from shared memory serve KB recurrences.
+constexpr int kSynthBetas = 2;
+
+__global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz, const double* __restrict__ btab,
+                            float2* __restrict__ S) {
   extern __shared__ double sm[];
   double* fa = sm;
   double* fb = fa + bw_in;
-  double* sh = fb + bw_in;
-  float2* cv = (float2*)(sh + bw_in);  // [4][bw_in]
+  double* gs = fb + bw_in;            // fb * shift
+  double* s_lnorm = gs + bw_in;       // one value (slot padded to 16 bytes)
+  float2* cv = (float2*)(s_lnorm + 2);  // [4][bw_in]
   const int cidx = blockIdx.x;
   int q = (int)floor((sqrt(8.0 * cidx + 1.0) - 1.0) * 0.5);
   while ((q + 1) * (q + 2) / 2 <= cidx) ++q;
@@ -47,8 +53,9 @@ __global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz
     const int l = q + i;
     const double dl = l;
     const double tnext = sqrt(((dl + 1) * (dl + 1) - dp * dp) * ((dl + 1) * (dl + 1) - dq * dq));
-    fb[i] = sqrt((2 * dl + 3) / (2 * dl + 1)) * (dl + 1) * (2 * dl + 1) / tnext;
-    sh[i] = (l == 0) ? 0.0 : -dp * dq / (dl * (dl + 1));
+    const double b = sqrt((2 * dl + 3) / (2 * dl + 1)) * (dl + 1) * (2 * dl + 1) / tnext;
+    fb[i] = b;
+    gs[i] = (l == 0) ? 0.0 : b * (-dp * dq / (dl * (dl + 1)));
     double a = 0.0;
     if (l > 0) {
       const double tcur = sqrt((dl * dl - dp * dp) * (dl * dl - dq * dq));
@@ -72,49 +79,79 @@ __global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz
       cv[3 * bw_in + i] = prod_conj(fused_at(fz, bw_in, 0, l, -q), fused_at(fz, bw_in, 1, l, p), spq * slp);
     }
   }
+  if (threadIdx.x == 0) {
+    // seed normalisation: 0.5 [log((2q+1)/2) + lgamma(2q+1) - lgamma(q-p+1) - lgamma(q+p+1)]
+    *s_lnorm = 0.5 * (log((2.0 * q + 1.0) / 2.0) + lgamma(2.0 * q + 1.0) - lgamma(dq - dp + 1.0) -
+                      lgamma(dq + dp + 1.0));
+  }
   __syncthreads();
   const int n = 2 * bw_out;
   const int Bo = bw_out;
-  // seed normalisation: 0.5 [log((2q+1)/2) + lgamma(2q+1) - lgamma(q-p+1) - lgamma(q+p+1)]
-  const double lnorm = 0.5 * (log((2.0 * q + 1.0) / 2.0) + lgamma(2.0 * q + 1.0) - lgamma(dq - dp + 1.0) -
-                              lgamma(dq + dp + 1.0));
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const double beta = M_PI * (2.0 * k + 1.0) / (4.0 * bw_out);
-    const double cb = cos(beta);
-    double sh2, ch2;
-    sincos(0.5 * beta, &sh2, &ch2);
-    const double lg = lnorm + (dq + dp) * log(ch2) + (q > p ? (dq - dp) * log(sh2) : 0.0);
-    double dcur = exp(lg), dprev = 0.0;
-    float2 a0 = make_float2(0.f, 0.f), a1 = a0, a2 = a0, a3 = a0;
+  const int stride = (n + kSynthBetas - 1) / kSynthBetas;
+  const double lnorm = *s_lnorm;
+  for (int k0 = threadIdx.x; k0 < stride; k0 += blockDim.x) {
+    double cb[kSynthBetas], dcur[kSynthBetas], dprev[kSynthBetas];
+    float2 acc[kSynthBetas][4];
+#pragma unroll
+    for (int u = 0; u < kSynthBetas; ++u) {
+      const int k = min(k0 + u * stride, n - 1);
+      cb[u] = __ldg(&btab[k]);
+      // d^q_{pq}(beta) = exp(lnorm) cos(beta/2)^(q+p) sin(beta/2)^(q-p)
+      const double lg = lnorm + (dq + dp) * __ldg(&btab[n + k]) + (q > p ? (dq - dp) * __ldg(&btab[2 * n + k]) : 0.0);
+      dcur[u] = exp(lg);
+      dprev[u] = 0.0;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] = make_float2(0.f, 0.f);
+    }
     for (int i = 0; i < nl; ++i) {
-      const float d = (float)dcur;
       const float2 c0 = cv[i], c1 = cv[bw_in + i], c2 = cv[2 * bw_in + i], c3 = cv[3 * bw_in + i];
-      a0.x = fmaf(c0.x, d, a0.x);
-      a0.y = fmaf(c0.y, d, a0.y);
-      a1.x = fmaf(c1.x, d, a1.x);
-      a1.y = fmaf(c1.y, d, a1.y);
-      a2.x = fmaf(c2.x, d, a2.x);
-      a2.y = fmaf(c2.y, d, a2.y);
-      a3.x = fmaf(c3.x, d, a3.x);
-      a3.y = fmaf(c3.y, d, a3.y);
-      const double dn = fa[i] * dprev + fb[i] * (cb + sh[i]) * dcur;
-      dprev = dcur;
-      dcur = dn;
+      const double a = fa[i], b = fb[i], g = gs[i];
+#pragma unroll
+      for (int u = 0; u < kSynthBetas; ++u) {
+        const float d = (float)dcur[u];
+        acc[u][0].x = fmaf(c0.x, d, acc[u][0].x);
+        acc[u][0].y = fmaf(c0.y, d, acc[u][0].y);
+        acc[u][1].x = fmaf(c1.x, d, acc[u][1].x);
+        acc[u][1].y = fmaf(c1.y, d, acc[u][1].y);
+        acc[u][2].x = fmaf(c2.x, d, acc[u][2].x);
+        acc[u][2].y = fmaf(c2.y, d, acc[u][2].y);
+        acc[u][3].x = fmaf(c3.x, d, acc[u][3].x);
+        acc[u][3].y = fmaf(c3.y, d, acc[u][3].y);
+        // d^{l+1} = a d^{l-1} + b (cos beta + shift) d^l
+        const double dn = a * dprev[u] + fma(b, cb[u], g) * dcur[u];
+        dprev[u] = dcur[u];
+        dcur[u] = dn;
+      }
     }
-    const int km = n - 1 - k;
-    float2* Sk = S + (size_t)k * n * Bo;
-    float2* Sm = S + (size_t)km * n * Bo;
-    Sk[(size_t)p * Bo + q] = a0;  // (a = p, b = q)
-    if (p == q) {
-      if (p > 0) Sm[(size_t)(n - p) * Bo + p] = a2;  // (-p, p) at mirrored beta
-    } else if (p == 0) {
-      Sk[(size_t)q * Bo + 0] = a1;                     // (q, 0)
-      Sk[(size_t)(n - q) * Bo + 0] = cconj(a1);        // (-q, 0) = conj((q, 0))
-    } else {
-      Sk[(size_t)q * Bo + p] = a1;                     // (q, p)
-      Sm[(size_t)(n - p) * Bo + q] = cconj(a2);        // (-p, q) = conj((p, -q))
-      Sm[(size_t)(n - q) * Bo + p] = cconj(a3);        // (-q, p) = conj((q, -p))
+#pragma unroll
+    for (int u = 0; u < kSynthBetas; ++u) {
+      const int k = k0 + u * stride;
+      if (k >= n) continue;
+      const int km = n - 1 - k;
+      float2* Sk = S + (size_t)k * n * Bo;
+      float2* Sm = S + (size_t)km * n * Bo;
+      Sk[(size_t)p * Bo + q] = acc[u][0];  // (a = p, b = q)
+      if (p == q) {
+        if (p > 0) Sm[(size_t)(n - p) * Bo + p] = acc[u][2];  // (-p, p) at mirrored beta
+      } else if (p == 0) {
+        Sk[(size_t)q * Bo + 0] = acc[u][1];                     // (q, 0)
+        Sk[(size_t)(n - q) * Bo + 0] = cconj(acc[u][1]);        // (-q, 0) = conj((q, 0))
+      } else {
+        Sk[(size_t)q * Bo + p] = acc[u][1];                     // (q, p)
+        Sm[(size_t)(n - p) * Bo + q] = cconj(acc[u][2]);        // (-p, q) = conj((p, -q))
+        Sm[(size_t)(n - q) * Bo + p] = cconj(acc[u][3]);        // (-q, p) = conj((q, -p))
+      }
     }
+  }
+}
+
+void so3_beta_table(int bw_out, double* tab) {
+  const int n = 2 * bw_out;
+  for (int k = 0; k < n; ++k) {
+    const double beta = M_PI * (2.0 * k + 1.0) / (4.0 * bw_out);
+    tab[k] = cos(beta);
+    tab[n + k] = log(cos(0.5 * beta));
+    tab[2 * n + k] = log(sin(0.5 * beta));
   }
 }
 
@@ -203,10 +240,10 @@ cudaError_t so3_init_attributes() {
 cudaError_t launch_so3_synth(const So3Args& a, cudaStream_t st) {
   const int ncls = a.bw_in * (a.bw_in + 1) / 2;
   const int n = 2 * a.bw_out;
-  int thr = ((n + 31) / 32) * 32;
+  int thr = (((n + kSynthBetas - 1) / kSynthBetas + 31) / 32) * 32;
   if (thr > 512) thr = 512;
-  const size_t sm1 = (size_t)a.bw_in * 3 * sizeof(double) + (size_t)a.bw_in * 4 * sizeof(float2);
-  k_so3_synth<<<ncls, thr, sm1, st>>>(a.bw_in, a.bw_out, a.fused, a.S);
+  const size_t sm1 = (size_t)a.bw_in * 3 * sizeof(double) + 2 * sizeof(double) + (size_t)a.bw_in * 4 * sizeof(float2);
+  k_so3_synth<<<ncls, thr, sm1, st>>>(a.bw_in, a.bw_out, a.fused, a.beta_tab, a.S);
   count_launches(1);
   return cudaGetLastError();
 }
