@@ -424,7 +424,6 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   CKV(dalloc(ctx, &ctx->d_samples, sizeof(float) * 2 * 4 * nq));
   CK(cudaMemset(ctx->d_samples, 0, sizeof(float) * 2 * 4 * nq));
   for (int s = 0; s < 2; ++s) CKV(dalloc(ctx, &ctx->d_nn[s], sizeof(int32_t) * nq));
-  CKV(dalloc(ctx, &ctx->d_fm, sizeof(float2) * 8 * bw * n));
   CKV(dalloc(ctx, &ctx->d_coef, sizeof(float2) * 8 * bw * bw));
   CKV(dalloc(ctx, &ctx->d_fused, sizeof(float2) * 2 * bw * (2 * bw - 1)));
   CK(cudaMemset(ctx->d_fused, 0, sizeof(float2) * 2 * bw * (2 * bw - 1)));
@@ -566,7 +565,6 @@ int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStre
     s.signal = ctx->d_samples + (size_t)side * 4 * nq;
     s.tw = ctx->plan_s2.tw;
     s.table = ctx->d_legendre;
-    s.fm = ctx->d_fm + (size_t)side * 4 * bw * 2 * bw;
     s.coef = ctx->d_coef + (size_t)side * n_data * bw * bw;
     ProfScope ps(ctx, st, PS_SHT);
     CK(launch_sht(s, st));

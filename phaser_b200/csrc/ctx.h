@@ -58,7 +58,6 @@ struct phgpu_ctx {
   // rotation
   float* d_samples = nullptr;  // [2][4][4B^2]
   int32_t* d_nn[2] = {nullptr, nullptr};
-  float2* d_fm = nullptr;
   float2* d_coef = nullptr;
   float2* d_fused = nullptr;
   float2* d_S = nullptr;

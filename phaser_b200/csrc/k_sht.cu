@@ -71,48 +71,84 @@ cudaError_t launch_legendre_table(int bw, const double* weights_dev, float* tabl
   return cudaGetLastError();
 }
 
-// phi DFT: block per (signal, theta row); thread per order m.
-__global__ void k_sht_phi(int bw, const float* __restrict__ sig, const float2* __restrict__ tw,
-                          float2* __restrict__ fm) {
-  extern __shared__ float row[];
-  const int n = 2 * bw;
-  const int s = blockIdx.y, k = blockIdx.x;
-  const float* src = sig + ((size_t)s * n + k) * n;
-  for (int j = threadIdx.x; j < n; j += blockDim.x) row[j] = src[j];
-  __syncthreads();
-  const float scale = (float)(2.5066282746310002 / (double)n);  // sqrt(2 pi) / 2B
-  for (int m = threadIdx.x; m < bw; m += blockDim.x) {
-    float ar = 0.f, ai = 0.f;
-    int t = 0;
-    for (int j = 0; j < n; ++j) {
-      const float2 w = __ldg(&tw[t]);
-      ar = fmaf(row[j], w.x, ar);
-      ai = fmaf(row[j], w.y, ai);
-      t += m;
-      if (t >= n) t -= n;
-    }
-    fm[((size_t)s * bw + m) * n + k] = make_float2(ar * scale, ai * scale);
-  }
-}
+// Fused transform: block per (order pair {m, B-1-m}, signal), so every block
+// carries B + 1 Legendre degrees.  Phase 1: warps take theta rows k, lanes
+// the phi samples j (four loads in flight), and one pass over a row gives
+// F_m(theta_k) for both orders.  Phase 2: warps take (order, degree) tasks
+// and lanes the rows k of the table.
+constexpr int kShtThreads = 1024;
 
-// Legendre contraction: block per (m, signal); warp per degree l, lanes over k.
-__global__ void k_sht_legendre(int bw, const float* __restrict__ table, const float2* __restrict__ fm,
-                               float2* __restrict__ coef) {
-  extern __shared__ float2 fk[];
+__global__ void __launch_bounds__(kShtThreads) k_sht(int bw, const float* __restrict__ sig,
+                                                     const float2* __restrict__ tw, const float* __restrict__ table,
+                                                     float2* __restrict__ coef) {
+  extern __shared__ float2 sh[];
   const int n = 2 * bw;
-  const int m = blockIdx.x, s = blockIdx.y;
-  const float2* src = fm + ((size_t)s * bw + m) * n;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) fk[k] = src[k];
+  const int m0 = blockIdx.x, m1 = bw - 1 - blockIdx.x;
+  const int nm = (m1 > m0) ? 2 : 1;
+  float2* twm = sh;          // [2][n] exp(-i m phi_j)
+  float2* fk = sh + 2 * n;   // [2][n] F_m(theta_k)
+  const int s = blockIdx.y;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    twm[j] = __ldg(&tw[(j * m0) % n]);
+    twm[n + j] = __ldg(&tw[(j * m1) % n]);
+  }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const float* tb = table + legendre_offset(m, bw);
-  for (int l = m + warp; l < bw; l += nw) {
-    const float* trow = tb + (size_t)(l - m) * n;
+  const float scale = (float)(2.5066282746310002 / (double)n);  // sqrt(2 pi) / 2B
+  const float* S = sig + (size_t)s * n * n;
+  for (int k = warp; k < n; k += nw) {
+    const float* row = S + (size_t)k * n;
+    float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
+    for (int j0 = lane; j0 < n; j0 += 128) {
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = (j0 + 32 * u < n) ? __ldg(&row[j0 + 32 * u]) : 0.f;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int j = j0 + 32 * u;
+        if (j < n) {
+          const float2 w = twm[j], x = twm[n + j];
+          ar = fmaf(v[u], w.x, ar);
+          ai = fmaf(v[u], w.y, ai);
+          br = fmaf(v[u], x.x, br);
+          bi = fmaf(v[u], x.y, bi);
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ar += __shfl_xor_sync(0xffffffffu, ar, o);
+      ai += __shfl_xor_sync(0xffffffffu, ai, o);
+      br += __shfl_xor_sync(0xffffffffu, br, o);
+      bi += __shfl_xor_sync(0xffffffffu, bi, o);
+    }
+    if (lane == 0) {
+      fk[k] = make_float2(ar * scale, ai * scale);
+      fk[n + k] = make_float2(br * scale, bi * scale);
+    }
+  }
+  __syncthreads();
+  const int nl0 = bw - m0;
+  const int ntask = nl0 + (nm == 2 ? bw - m1 : 0);
+  for (int task = warp; task < ntask; task += nw) {
+    const int h = task < nl0 ? 0 : 1;
+    const int m = h ? m1 : m0;
+    const int l = m + (h ? task - nl0 : task);
+    const float* trow = table + legendre_offset(m, bw) + (size_t)(l - m) * n;
+    const float2* f = fk + h * n;
     float ar = 0.f, ai = 0.f;
-    for (int k = lane; k < n; k += 32) {
-      const float t = __ldg(&trow[k]);
-      ar = fmaf(t, fk[k].x, ar);
-      ai = fmaf(t, fk[k].y, ai);
+    for (int k0 = lane; k0 < n; k0 += 128) {
+      float t[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) t[u] = (k0 + 32 * u < n) ? __ldg(&trow[k0 + 32 * u]) : 0.f;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (k0 + 32 * u < n) {
+          const float2 x = f[k0 + 32 * u];
+          ar = fmaf(t[u], x.x, ar);
+          ai = fmaf(t[u], x.y, ai);
+        }
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -124,12 +160,9 @@ __global__ void k_sht_legendre(int bw, const float* __restrict__ table, const fl
 }
 
 cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st) {
-  const int n = 2 * a.bw;
-  dim3 g1(n, a.n_sig);
-  k_sht_phi<<<g1, 128, n * sizeof(float), st>>>(a.bw, a.signal, a.tw, a.fm);
-  dim3 g2(a.bw, a.n_sig);
-  k_sht_legendre<<<g2, 256, n * sizeof(float2), st>>>(a.bw, a.table, a.fm, a.coef);
-  count_launches(2);
+  dim3 g((a.bw + 1) / 2, a.n_sig);
+  k_sht<<<g, kShtThreads, (size_t)4 * 2 * a.bw * sizeof(float2), st>>>(a.bw, a.signal, a.tw, a.table, a.coef);
+  count_launches(1);
   return cudaGetLastError();
 }
 

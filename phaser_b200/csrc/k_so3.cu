@@ -32,7 +32,7 @@ __device__ __forceinline__ float2 prod_conj(float2 a, float2 b, float s) {
 
 // KB betas per thread (k = t, t + ceil(n / KB), ...): the coefficient loads
 // from shared memory serve KB recurrences.
-constexpr int kSynthBetas = 2;
+constexpr int kSynthBetas = 4;
 
 __global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz, const double* __restrict__ btab,
                             float2* __restrict__ S) {

@@ -47,7 +47,6 @@ struct ShtArgs {
   const float* signal;    // [n_sig][2B][2B]
   const float2* tw;       // exp(-2 pi i t / 2B), t in [0, 2B)
   const float* table;     // Legendre table
-  float2* fm;             // scratch [n_sig][B][2B]
   float2* coef;           // [n_sig][B (l)][B (m>=0)]
 };
 cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st);
