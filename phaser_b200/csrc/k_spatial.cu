@@ -373,13 +373,16 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
   __shared__ int s_live[NH];      // packed row r holds a non-zero value
   __shared__ int s_rows[NH];      // compact list of those rows
   __shared__ int s_nrows;
+  __shared__ int s_posN[N], s_posH[NH];  // digit-reversed positions of frequencies
   const int z = blockIdx.x, c = blockIdx.y;
   const float* g = grids + (size_t)c * grid_cstride + (size_t)z * N * N;
   const float* cnt = count ? count + (size_t)z * N * N : nullptr;
   for (int r = threadIdx.x; r < NH; r += blockDim.x) {
     s_live[r] = 0;
     s_flag[r] = rowlive ? (rowlive[z * N + 2 * r] | rowlive[z * N + 2 * r + 1]) : 1;
+    s_posH[r] = fixed_freq2pos<NH>(r);
   }
+  for (int k = threadIdx.x; k < N; k += blockDim.x) s_posN[k] = fixed_freq2pos<N>(k);
   __syncthreads();
   for (int e = threadIdx.x; e < NH * Q; e += blockDim.x) {
     const int r = e / Q, y4 = (e - r * Q) * 4;
@@ -431,8 +434,8 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
   fft_tail<NH, false, true>(W, N, S, pH.tw);               // over r, columns
   for (int e = threadIdx.x; e < NH * H2; e += blockDim.x) {
     const int k = e / H2, ky = e - k * H2;
-    const float2 w1 = W[fixed_freq2pos<NH>(k) * S + fixed_freq2pos<N>(ky)];
-    const float2 w2 = W[fixed_freq2pos<NH>(k == 0 ? 0 : NH - k) * S + fixed_freq2pos<N>(ky == 0 ? 0 : N - ky)];
+    const float2 w1 = W[s_posH[k] * S + s_posN[ky]];
+    const float2 w2 = W[s_posH[k == 0 ? 0 : NH - k] * S + s_posN[ky == 0 ? 0 : N - ky]];
     const float2 A = make_float2(0.5f * (w1.x + w2.x), 0.5f * (w1.y - w2.y));
     const float2 B = make_float2(0.5f * (w1.y + w2.y), -0.5f * (w1.x - w2.x));  // (w1 - conj w2) / 2i
     const float2 tB = cmul(__ldg(&pN.tw[k]), B);
@@ -453,8 +456,14 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
   constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1, S = NF + 1;
   const int H2p = spatial_h2p(N);
   extern __shared__ float2 W[];  // [NH][S]
+  __shared__ int s_posN[N], s_posH[NH];  // digit-reversed positions of frequencies
   const int z = blockIdx.x;
   const float2* X = cspec + (size_t)z * N * H2p;
+  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+    s_posN[k] = fixed_freq2pos<N>(k);
+    if (k < NH) s_posH[k] = fixed_freq2pos<NH>(k);
+  }
+  __syncthreads();
   for (int e = threadIdx.x; e < NH * H2; e += blockDim.x) {
     const int k = e / H2, ky = e - k * H2;
     float2 x0 = X[(size_t)k * H2p + ky];
@@ -468,10 +477,8 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
     const float2 A = make_float2(0.5f * (x0.x + x1.x), 0.5f * (x0.y + x1.y));
     const float2 B = cmul(make_float2(0.5f * (x0.x - x1.x), 0.5f * (x0.y - x1.y)), cconj(__ldg(&pN.tw[k])));
     // W = A + i B at (k, ky); its mirror (-k, -ky) holds conj(A) + i conj(B)
-    W[fixed_freq2pos<NH>(k) * S + fixed_freq2pos<N>(ky)] = make_float2(A.x - B.y, A.y + B.x);
-    if (ky >= 1 && ky < NH)
-      W[fixed_freq2pos<NH>(k == 0 ? 0 : NH - k) * S + fixed_freq2pos<N>(N - ky)] =
-          make_float2(A.x + B.y, -A.y + B.x);
+    W[s_posH[k] * S + s_posN[ky]] = make_float2(A.x - B.y, A.y + B.x);
+    if (ky >= 1 && ky < NH) W[s_posH[k == 0 ? 0 : NH - k] * S + s_posN[N - ky]] = make_float2(A.x + B.y, -A.y + B.x);
   }
   __syncthreads();
   fft_tail<NH, true, true>(W, N, S, pH.tw);    // over r, columns
