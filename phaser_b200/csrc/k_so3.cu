@@ -191,14 +191,18 @@ __global__ void k_so3_c2r(int bw_in, int bw_out, const float2* __restrict__ S, F
   const int k = blockIdx.y;
   const int r0 = blockIdx.x * R;
   const int nr = min(R, n - r0);
+  int* pos = reinterpret_cast<int*>(rows + R * n);  // [n] positions of gamma frequencies
+  int* alpha_of = pos + n;                          // [R] alpha of each row
   for (int e = threadIdx.x; e < R * n; e += blockDim.x) rows[e] = make_float2(0.f, 0.f);
+  for (int b = threadIdx.x; b < n; b += blockDim.x) pos[b] = freq2pos<NF>(b, plan);
+  for (int r = threadIdx.x; r < nr; r += blockDim.x) alpha_of[r] = pos2freq<NF>(r0 + r, plan);
   __syncthreads();
   for (int e = threadIdx.x; e < nr * Bo; e += blockDim.x) {
     const int r = e / Bo, b = e - r * Bo;
     float2* row = rows + r * n;
     const float2 u = b < bw_in ? S[((size_t)k * n + r0 + r) * Bo + b] : make_float2(0.f, 0.f);
-    row[freq2pos<NF>(b, plan)] = cconj(u);
-    if (b > 0) row[freq2pos<NF>(n - b, plan)] = u;
+    row[pos[b]] = cconj(u);
+    if (b > 0) row[pos[n - b]] = u;
   }
   __syncthreads();
   fft_any<NF, true>(rows, R, n, 1, plan);
@@ -209,7 +213,7 @@ __global__ void k_so3_c2r(int bw_in, int bw_out, const float2* __restrict__ S, F
     if (r < nr) {
       const float v = rows[e].x * K;
       const float v2 = v * v;
-      const int alpha = pos2freq<NF>(r0 + r, plan);
+      const int alpha = alpha_of[r];
       const uint32_t idx = ((uint32_t)k * n + (uint32_t)alpha) * n + g;
       const unsigned long long key = pack_argmax(v2, idx);
       best = key > best ? key : best;
@@ -254,8 +258,8 @@ cudaError_t launch_so3_fft(const So3Args& a, cudaStream_t st) {
   dim3 g3((n + 15) / 16, n);
   PHGPU_DISPATCH_N(n,
       k_so3_fft_a<NF><<<g2, 256, (size_t)n * 16 * sizeof(float2), st>>>(a.bw_in, a.bw_out, a.S, *a.plan);
-      k_so3_c2r<NF><<<g3, 256, (size_t)16 * n * sizeof(float2), st>>>(a.bw_in, a.bw_out, a.S, *a.plan,
-                                                                       a.argmax, a.volume));
+      k_so3_c2r<NF><<<g3, 256, (size_t)16 * n * sizeof(float2) + (size_t)(n + 16) * sizeof(int), st>>>(
+          a.bw_in, a.bw_out, a.S, *a.plan, a.argmax, a.volume));
   count_launches(2);
   return cudaGetLastError();
 }

@@ -212,7 +212,9 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
   const int zrows = tma.enabled ? tma.zbox * tma.chunks : N;
   uint64_t* bar = reinterpret_cast<uint64_t*>(tile + (size_t)zrows * rowlen);
   FusionBands* s_bands = reinterpret_cast<FusionBands*>(bar + 2);
+  int* s_kz = reinterpret_cast<int*>(s_bands + 1);  // [N] z frequency of each position
   if (threadIdx.x == 0) *s_bands = a.bands;  // divergent band lookups are cheap in shared memory
+  for (int zp = threadIdx.x; zp < N; zp += blockDim.x) s_kz[zp] = pos2freq<NF>(zp, plan);
   // the bulk copy needs a 128-byte aligned destination (block-uniform test)
   const bool use_tma = tma.enabled && (smem_addr(tile) & 127u) == 0;
   if (use_tma) {
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
       F = row[t];
       G = row[Wt + t];
     } else {
-      const int kz = pos2freq<NF>(zp, plan);
+      const int kz = s_kz[zp];
       const uint32_t klin = ((uint32_t)kz * N + (uint32_t)kx) * (uint32_t)H2 + (uint32_t)(ky0 + t);
       // (klin + nv/2) mod nv with klin < nv
       uint32_t p = klin + (nv >> 1);
@@ -563,7 +565,7 @@ static int fuse_z_tile(int N, int A) {
   int wt = 8;
   const int chunks = (N + 255) / 256;                       // bulk copies of <= 256 z rows
   const size_t rows = (size_t)chunks * ((N + chunks - 1) / chunks);
-  const size_t extra = 16 + sizeof(FusionBands);
+  const size_t extra = 16 + sizeof(FusionBands) + (size_t)N * sizeof(int);
   while (wt > 2 && rows * A * wt * sizeof(float2) + extra > (size_t)kMaxSmem) wt >>= 1;
   return wt;
 }
@@ -639,7 +641,7 @@ cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st) {
       tma = FuseZTma{1, zbox, chunks};
   }
   const size_t rows = (size_t)tma.zbox * tma.chunks;
-  const size_t smB = rows * A * wt * sizeof(float2) + 16 + sizeof(FusionBands);
+  const size_t smB = rows * A * wt * sizeof(float2) + 16 + sizeof(FusionBands) + (size_t)N * sizeof(int);
   if (smB > (size_t)kMaxSmem) return cudaErrorInvalidConfiguration;
   dim3 gB((H2 + wt - 1) / wt, N);
   const int xnat = (spatial_slab_path(N) && a.plan_half) ? 1 : 0;
