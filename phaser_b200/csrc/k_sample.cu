@@ -11,7 +11,8 @@
 //
 // Acceleration structure: points are bucketed on a 32^3 grid over
 // [-1.0625, 1.0625]^3 ordered coarse-cell-major (8^3 coarse cells of 4^3 fine
-// cells), with exact per-cell bounding boxes.  Cells are only pruned when
+// cells); every non-empty coarse cell carries its exact box and a compact list
+// of records {exact box, point range} of its non-empty fine cells.  Cells are only pruned when
 // their box lies beyond the current best distance (with a 1e-5 relative
 // margin so float rounding can never prune the true nearest point), so the
 // search is exact whatever bound it starts from.
@@ -166,47 +167,88 @@ __global__ void k_scatter(int P, const float4* __restrict__ proj, const uint32_t
   sorted[slot] = make_float4(p.x, p.y, p.z, __int_as_float(i));
 }
 
-__device__ __forceinline__ uint32_t ord(float v) { return float_order_bits(v); }
+// Cell records.  For list entry i (non-empty coarse cell clist[i].z) the
+// non-empty fine cells are records frec[2 (64 i + j)], frec[2 (64 i + j) + 1],
+// j < nfine[i], in fine-id order:
+//   {lo.x, lo.y, lo.z, hi.x}, {hi.y, hi.z, start (bits), end (bits)}
+// and the coarse box is cbox[2 i], cbox[2 i + 1] = {lo.xyz, hi.x}, {hi.yz, nfine (bits), 0}.
+// One block per list entry: warps take fine cells, lanes the cell's points.
+constexpr int kRecordThreads = 128;
 
-// Tight boxes of fine and coarse cells: thread per sorted point, warp-segmented
-// min/max over lanes of the same cell, one atomic per segment.  Boxes hold
-// order-preserving bits: lo[c*3+a] (init 0xffffffff), hi[c*3+a] (init 0).
-__global__ void k_cell_bounds(const uint32_t* __restrict__ n_sorted, const float4* __restrict__ sorted,
-                              uint32_t* __restrict__ flo, uint32_t* __restrict__ fhi, uint32_t* __restrict__ clo,
-                              uint32_t* __restrict__ chi) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = i < (int)*n_sorted;
-  float4 p = valid ? sorted[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const uint32_t fk = valid ? cell_key(p.x, p.y, p.z) : 0xffffffffu;
-  const uint32_t v[3] = {ord(p.x), ord(p.y), ord(p.z)};
-  // fine cell segments
-  {
-    const unsigned peers = __match_any_sync(0xffffffffu, fk);
-    const int leader = __ffs(peers) - 1;
+__global__ void __launch_bounds__(kRecordThreads)
+k_cell_records(const uint4* __restrict__ clist, const uint32_t* __restrict__ n_coarse_p,
+               const uint32_t* __restrict__ fstart, const float4* __restrict__ sorted, float4* __restrict__ frec,
+               float4* __restrict__ cbox) {
+  __shared__ int s_fid[64];
+  __shared__ int s_nf;
+  __shared__ float s_box[kRecordThreads / 32][6];
+  const int i = blockIdx.x;
+  if (i >= (int)*n_coarse_p) return;
+  const int c = (int)clist[i].z;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (warp == 0) {  // compact the non-empty fine cells of this coarse cell
+    int base = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int fc = c * 64 + h * 32 + lane;
+      const bool ne = __ldg(&fstart[fc + 1]) > __ldg(&fstart[fc]);
+      const unsigned m = __ballot_sync(0xffffffffu, ne);
+      if (ne) s_fid[base + __popc(m & ((1u << lane) - 1u))] = fc;
+      base += __popc(m);
+    }
+    if (lane == 0) s_nf = base;
+  }
+  __syncthreads();
+  const int nf = s_nf;
+  float wb[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  for (int j = warp; j < nf; j += kRecordThreads / 32) {
+    const int fc = s_fid[j];
+    const uint32_t ps = __ldg(&fstart[fc]), pe = __ldg(&fstart[fc + 1]);
+    float b[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t k = ps + lane; k < pe; k += 32) {
+      const float4 p = sorted[k];
+      b[0] = fminf(b[0], p.x);
+      b[1] = fminf(b[1], p.y);
+      b[2] = fminf(b[2], p.z);
+      b[3] = fmaxf(b[3], p.x);
+      b[4] = fmaxf(b[4], p.y);
+      b[5] = fmaxf(b[5], p.z);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        b[a] = fminf(b[a], __shfl_xor_sync(0xffffffffu, b[a], o));
+        b[3 + a] = fmaxf(b[3 + a], __shfl_xor_sync(0xffffffffu, b[3 + a], o));
+      }
+    }
+    if (lane == 0) {
+      float4* r = frec + 2 * ((size_t)i * 64 + j);
+      r[0] = make_float4(b[0], b[1], b[2], b[3]);
+      r[1] = make_float4(b[4], b[5], __uint_as_float(ps), __uint_as_float(pe));
+    }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const uint32_t mn = __reduce_min_sync(peers, v[a]);
-      const uint32_t mx = __reduce_max_sync(peers, v[a]);
-      if (valid && (int)(threadIdx.x & 31) == leader) {
-        atomicMin(&flo[fk * 3 + a], mn);
-        atomicMax(&fhi[fk * 3 + a], mx);
-      }
+      wb[a] = fminf(wb[a], b[a]);
+      wb[3 + a] = fmaxf(wb[3 + a], b[3 + a]);
     }
   }
-  // coarse cell segments
-  {
-    const uint32_t ck = valid ? fk >> 6 : 0xffffffffu;
-    const unsigned peers = __match_any_sync(0xffffffffu, ck);
-    const int leader = __ffs(peers) - 1;
+  if (lane == 0) {
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const uint32_t mn = __reduce_min_sync(peers, v[a]);
-      const uint32_t mx = __reduce_max_sync(peers, v[a]);
-      if (valid && (int)(threadIdx.x & 31) == leader) {
-        atomicMin(&clo[ck * 3 + a], mn);
-        atomicMax(&chi[ck * 3 + a], mx);
+    for (int a = 0; a < 6; ++a) s_box[warp][a] = wb[a];
+  }
+  __syncthreads();
+  if (t == 0) {
+    float cb[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    for (int w = 0; w < kRecordThreads / 32; ++w) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        cb[a] = fminf(cb[a], s_box[w][a]);
+        cb[3 + a] = fmaxf(cb[3 + a], s_box[w][3 + a]);
       }
     }
+    cbox[2 * i] = make_float4(cb[0], cb[1], cb[2], cb[3]);
+    cbox[2 * i + 1] = make_float4(cb[4], cb[5], __int_as_float(nf), 0.f);
   }
 }
 
@@ -217,15 +259,16 @@ __device__ __forceinline__ float box_lb2(float qx, float qy, float qz, const flo
   return dx * dx + dy * dy + dz * dz;
 }
 
-__device__ __forceinline__ float box_lb2_ord(float qx, float qy, float qz, const uint32_t* lo,
-                                             const uint32_t* hi) {
-  float b[6];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    b[a] = float_from_order_bits(__ldg(&lo[a]));
-    b[3 + a] = float_from_order_bits(__ldg(&hi[a]));
-  }
-  return box_lb2(qx, qy, qz, b);
+// Squared distance from q to a record's box; the record's point range in s, e.
+__device__ __forceinline__ float rec_lb2(float qx, float qy, float qz, const float4* __restrict__ r, uint32_t& s,
+                                         uint32_t& e) {
+  const float4 a = __ldg(&r[0]), b = __ldg(&r[1]);
+  s = __float_as_uint(b.z);
+  e = __float_as_uint(b.w);
+  const float dx = fmaxf(fmaxf(a.x - qx, qx - a.w), 0.0f);
+  const float dy = fmaxf(fmaxf(a.y - qy, qy - b.x), 0.0f);
+  const float dz = fmaxf(fmaxf(a.z - qz, qz - b.y), 0.0f);
+  return dx * dx + dy * dy + dz * dz;
 }
 
 __device__ __forceinline__ float ref_dist2(float qx, float qy, float qz, float4 p) {
@@ -257,50 +300,46 @@ __device__ __forceinline__ void warp_nn_min(float& best, int& bidx) {
 constexpr int kQueryThreads = 256;
 constexpr float kPruneMargin = 0.99999f;  // lower bound * margin must exceed the best to prune
 
-// Best-first scan of one coarse cell: its non-empty fine cells are visited in
-// ascending order of their box lower bound until the bound exceeds the best
-// distance.  best / bidx are warp-uniform on entry and on exit.
-__device__ __forceinline__ void scan_coarse(int cid, float qx, float qy, float qz,
-                                            const float4* __restrict__ sorted,
-                                            const uint32_t* __restrict__ fstart,
-                                            const uint32_t* __restrict__ flo,
-                                            const uint32_t* __restrict__ fhi, float& best, int& bidx) {
+// Scans points [s, e) of the sorted array, four loads in flight per lane.
+__device__ __forceinline__ void scan_points(uint32_t s, uint32_t e, float qx, float qy, float qz,
+                                            const float4* __restrict__ sorted, float& best, int& bidx) {
   const int lane = threadIdx.x & 31;
-  float lb[2];
-  uint32_t fs[2], fe[2];
+  for (uint32_t j = s + lane; j < e; j += 128) {
+    float4 p[4];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int fc = cid * 64 + h * 32 + lane;
-    fs[h] = __ldg(&fstart[fc]);
-    fe[h] = __ldg(&fstart[fc + 1]);
-    lb[h] = fe[h] > fs[h] ? box_lb2_ord(qx, qy, qz, flo + 3 * fc, fhi + 3 * fc) : INFINITY;
-  }
-  // at most 64 picks: every pick retires one fine cell
-  for (int pick = 0; pick < 64; ++pick) {
-    // warp argmin of the remaining lower bounds
-    const int hsel = lb[1] < lb[0] ? 1 : 0;
-    float m = lb[hsel];
-    int who = lane * 2 + hsel;
+    for (int u = 0; u < 4; ++u)
+      if (j + 32 * u < e) p[u] = sorted[j + 32 * u];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const float om = __shfl_xor_sync(0xffffffffu, m, o);
-      const int ow = __shfl_xor_sync(0xffffffffu, who, o);
-      if (om < m || (om == m && ow < who)) {
-        m = om;
-        who = ow;
-      }
-    }
-    if (!(m < INFINITY) || !(m * kPruneMargin <= best)) break;  // done, or nothing within the bound
-    const int src = who >> 1, h = who & 1;
-    const uint32_t s = __shfl_sync(0xffffffffu, h ? fs[1] : fs[0], src);
-    const uint32_t e = __shfl_sync(0xffffffffu, h ? fe[1] : fe[0], src);
-    if (lane == src) lb[h] = INFINITY;
-    for (uint32_t j = s + lane; j < e; j += 32) {
-      const float4 p = sorted[j];
-      nn_update(ref_dist2(qx, qy, qz, p), __float_as_int(p.w), best, bidx);
-    }
-    warp_nn_min(best, bidx);
+    for (int u = 0; u < 4; ++u)
+      if (j + 32 * u < e) nn_update(ref_dist2(qx, qy, qz, p[u]), __float_as_int(p[u].w), best, bidx);
   }
+}
+
+// Opens coarse list entry cc: every fine record within the bound (except the
+// one starting at skip_start) is scanned; lanes keep private minima, the warp
+// minimum is taken at the end.  best / bidx are warp-uniform on entry and exit.
+__device__ __forceinline__ void open_coarse(int cc, int nf, uint32_t skip_start, float qx, float qy, float qz,
+                                            const float4* __restrict__ frec, const float4* __restrict__ sorted,
+                                            float& best, int& bidx) {
+  const int lane = threadIdx.x & 31;
+  const float bound = best;
+  for (int j0 = 0; j0 < nf; j0 += 32) {
+    const int j = j0 + lane;
+    uint32_t s = 0, e = 0;
+    bool in = false;
+    if (j < nf) {
+      const float lb = rec_lb2(qx, qy, qz, frec + 2 * ((size_t)cc * 64 + j), s, e);
+      in = s != skip_start && lb * kPruneMargin <= bound;
+    }
+    unsigned m = __ballot_sync(0xffffffffu, in);
+    while (m) {
+      const int src = __ffs(m) - 1;
+      m &= m - 1;
+      scan_points(__shfl_sync(0xffffffffu, s, src), __shfl_sync(0xffffffffu, e, src), qx, qy, qz, sorted, best,
+                  bidx);
+    }
+  }
+  warp_nn_min(best, bidx);
 }
 
 // Writes the sampled channels {range, intensity, reflectivity, ambient}
@@ -322,93 +361,81 @@ __device__ __forceinline__ void emit_sample(int qi, int nq, float best, int bidx
   if (nn_idx) nn_idx[qi] = ok ? bidx : -1;
 }
 
-// One warp per grid direction (grid-stride).  The bound starts from one
-// representative point per non-empty coarse cell; the coarse cell of the
-// nearest representative is searched first, then every other coarse cell whose
-// box lies within the bound.  Writes the sampled channels {range, intensity,
-// reflectivity, ambient} (float) into out[ch][query] for ch < n_out_ch and the
-// nearest index (or -1) into nn_idx.
-__global__ void __launch_bounds__(kQueryThreads)
-k_nn_query(int nq, const float4* __restrict__ grid, const float4* __restrict__ sorted,
-           const uint32_t* __restrict__ fstart, const uint32_t* __restrict__ flo,
-           const uint32_t* __restrict__ fhi, const uint4* __restrict__ clist,
-           const uint32_t* __restrict__ clo, const uint32_t* __restrict__ chi,
-           const uint32_t* __restrict__ n_coarse_p, float max_sq, const float4* __restrict__ xyzi,
-           const double* __restrict__ range, const float* __restrict__ refl,
-           const float* __restrict__ amb, int n_out_ch, float* __restrict__ out,
-           int32_t* __restrict__ nn_idx) {
-  __shared__ uint32_t s_cid[kCoarseCells];
-  __shared__ float s_box[kCoarseCells * 6];
-  __shared__ float4 s_rep[kCoarseCells];
+// Shared prologue of the query kernels: coarse boxes, fine-record counts and
+// one representative point per non-empty coarse cell.
+struct CoarseSmem {
+  float box[kCoarseCells * 6];
+  int nf[kCoarseCells];
+  float4 rep[kCoarseCells];
+};
+
+__device__ __forceinline__ int load_coarse(CoarseSmem& cs, const uint4* __restrict__ clist,
+                                           const float4* __restrict__ cbox, const uint32_t* __restrict__ n_coarse_p,
+                                           const float4* __restrict__ sorted) {
   const int nc = (int)*n_coarse_p;
   for (int i = threadIdx.x; i < nc; i += blockDim.x) {
-    const uint4 e = clist[i];
-    s_cid[i] = e.z;
-    s_rep[i] = sorted[e.x];
-    for (int a = 0; a < 3; ++a) {
-      s_box[6 * i + a] = float_from_order_bits(clo[e.z * 3 + a]);
-      s_box[6 * i + 3 + a] = float_from_order_bits(chi[e.z * 3 + a]);
-    }
+    const float4 a = cbox[2 * i], b = cbox[2 * i + 1];
+    cs.box[6 * i + 0] = a.x;
+    cs.box[6 * i + 1] = a.y;
+    cs.box[6 * i + 2] = a.z;
+    cs.box[6 * i + 3] = a.w;
+    cs.box[6 * i + 4] = b.x;
+    cs.box[6 * i + 5] = b.y;
+    cs.nf[i] = __float_as_int(b.z);
+    cs.rep[i] = sorted[clist[i].x];
   }
   __syncthreads();
+  return nc;
+}
+
+// Bound from the representatives (lane-parallel), then every coarse cell
+// whose box lies within the bound is opened.
+__device__ __forceinline__ void rep_bound(const CoarseSmem& cs, int nc, float qx, float qy, float qz, float& best,
+                                          int& bidx) {
+  const int lane = threadIdx.x & 31;
+  for (int c = lane; c < nc; c += 32) {
+    const float4 r = cs.rep[c];
+    nn_update(ref_dist2(qx, qy, qz, r), __float_as_int(r.w), best, bidx);
+  }
+  warp_nn_min(best, bidx);
+}
+
+__device__ __forceinline__ void open_within(const CoarseSmem& cs, int nc, uint32_t skip_start, float qx, float qy,
+                                            float qz, const float4* __restrict__ frec,
+                                            const float4* __restrict__ sorted, float& best, int& bidx) {
+  const int lane = threadIdx.x & 31;
+  for (int c0 = 0; c0 < nc; c0 += 32) {
+    const int c = c0 + lane;
+    const bool cand = c < nc && box_lb2(qx, qy, qz, cs.box + 6 * c) * kPruneMargin <= best;
+    unsigned cmask = __ballot_sync(0xffffffffu, cand);
+    while (cmask) {
+      const int cc = c0 + __ffs(cmask) - 1;
+      cmask &= cmask - 1;
+      if (box_lb2(qx, qy, qz, cs.box + 6 * cc) * kPruneMargin > best) continue;  // warp-uniform
+      open_coarse(cc, cs.nf[cc], skip_start, qx, qy, qz, frec, sorted, best, bidx);
+    }
+  }
+}
+
+// One warp per direction of an arbitrary set (grid-stride): bound from the
+// representatives, then the coarse cells within it.
+__global__ void __launch_bounds__(kQueryThreads)
+k_nn_query(int nq, const float4* __restrict__ grid, const float4* __restrict__ sorted,
+           const float4* __restrict__ frec, const uint4* __restrict__ clist, const float4* __restrict__ cbox,
+           const uint32_t* __restrict__ n_coarse_p, float max_sq, const float4* __restrict__ xyzi,
+           const double* __restrict__ range, const float* __restrict__ refl, const float* __restrict__ amb,
+           int n_out_ch, float* __restrict__ out, int32_t* __restrict__ nn_idx) {
+  __shared__ CoarseSmem cs;
+  const int nc = load_coarse(cs, clist, cbox, n_coarse_p, sorted);
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   for (int qi = blockIdx.x * wpb + (threadIdx.x >> 5); qi < nq; qi += gridDim.x * wpb) {
     const float4 q = grid[qi];
     float best = INFINITY;
     int bidx = 0x7fffffff;
-    // representatives: remember which coarse cell gave each lane's best
-    int bcell = -1;
-    for (int c = lane; c < nc; c += 32) {
-      const float4 r = s_rep[c];
-      const float d = ref_dist2(q.x, q.y, q.z, r);
-      const int id = __float_as_int(r.w);
-      if (d < best || (d == best && id < bidx)) {
-        best = d;
-        bidx = id;
-        bcell = c;
-      }
-    }
-    int first = bcell;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const float ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
-      const int oc = __shfl_xor_sync(0xffffffffu, first, o);
-      if (ob < best || (ob == best && oi < bidx)) {
-        best = ob;
-        bidx = oi;
-        first = oc;
-      }
-    }
-    if (first >= 0) scan_coarse((int)s_cid[first], q.x, q.y, q.z, sorted, fstart, flo, fhi, best, bidx);
-    for (int c0 = 0; c0 < nc; c0 += 32) {
-      const int c = c0 + lane;
-      const bool cand = c < nc && c != first && box_lb2(q.x, q.y, q.z, s_box + 6 * c) * kPruneMargin <= best;
-      unsigned cmask = __ballot_sync(0xffffffffu, cand);
-      while (cmask) {
-        const int cc = c0 + __ffs(cmask) - 1;
-        cmask &= cmask - 1;
-        if (box_lb2(q.x, q.y, q.z, s_box + 6 * cc) * kPruneMargin > best) continue;  // warp-uniform
-        scan_coarse((int)s_cid[cc], q.x, q.y, q.z, sorted, fstart, flo, fhi, best, bidx);
-      }
-    }
+    rep_bound(cs, nc, q.x, q.y, q.z, best, bidx);
+    open_within(cs, nc, 0xffffffffu, q.x, q.y, q.z, frec, sorted, best, bidx);
     if (lane == 0) emit_sample(qi, nq, best, bidx, max_sq, xyzi, range, refl, amb, n_out_ch, out, nn_idx);
-  }
-}
-
-// Scans points [s, e) of the sorted array, four loads in flight per lane.
-__device__ __forceinline__ void scan_points(uint32_t s, uint32_t e, float qx, float qy, float qz,
-                                            const float4* __restrict__ sorted, float& best, int& bidx) {
-  const int lane = threadIdx.x & 31;
-  for (uint32_t j = s + lane; j < e; j += 128) {
-    float4 p[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (j + 32 * u < e) p[u] = sorted[j + 32 * u];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (j + 32 * u < e) nn_update(ref_dist2(qx, qy, qz, p[u]), __float_as_int(p[u].w), best, bidx);
   }
 }
 
@@ -432,32 +459,17 @@ __device__ __forceinline__ int nearest_row(const uint32_t* __restrict__ cm, int 
 // points of the nearest occupied bins above and below in columns j-2..j+2
 // (lanes 0..9), then all points of the direction's own fine cell; if no
 // column near it holds any point, one representative per coarse cell.  Then
-// every coarse cell whose box lies within the bound is opened and each of its
-// fine cells within the bound is scanned; lanes keep private minima inside a
-// coarse cell and the warp minimum (the bound for the next) is refreshed after it.
+// every coarse cell whose box lies within the bound is opened.
 __global__ void __launch_bounds__(kQueryThreads)
 k_nn_grid(int n2b, const float4* __restrict__ grid, const float4* __restrict__ proj,
           const uint32_t* __restrict__ binmap, const uint32_t* __restrict__ colmask,
-          const float4* __restrict__ sorted, const uint32_t* __restrict__ fstart,
-          const uint32_t* __restrict__ flo, const uint32_t* __restrict__ fhi, const uint4* __restrict__ clist,
-          const uint32_t* __restrict__ clo, const uint32_t* __restrict__ chi,
-          const uint32_t* __restrict__ n_coarse_p, float max_sq, const float4* __restrict__ xyzi,
-          const double* __restrict__ range, const float* __restrict__ refl, const float* __restrict__ amb,
-          int n_out_ch, float* __restrict__ out, int32_t* __restrict__ nn_idx) {
-  __shared__ uint32_t s_cid[kCoarseCells];
-  __shared__ float s_box[kCoarseCells * 6];
-  __shared__ float4 s_rep[kCoarseCells];
-  const int nc = (int)*n_coarse_p;
-  for (int i = threadIdx.x; i < nc; i += blockDim.x) {
-    const uint4 e = clist[i];
-    s_cid[i] = e.z;
-    s_rep[i] = sorted[e.x];
-    for (int a = 0; a < 3; ++a) {
-      s_box[6 * i + a] = float_from_order_bits(clo[e.z * 3 + a]);
-      s_box[6 * i + 3 + a] = float_from_order_bits(chi[e.z * 3 + a]);
-    }
-  }
-  __syncthreads();
+          const float4* __restrict__ sorted, const uint32_t* __restrict__ fstart, const float4* __restrict__ frec,
+          const uint4* __restrict__ clist, const float4* __restrict__ cbox, const uint32_t* __restrict__ n_coarse_p,
+          float max_sq, const float4* __restrict__ xyzi, const double* __restrict__ range,
+          const float* __restrict__ refl, const float* __restrict__ amb, int n_out_ch, float* __restrict__ out,
+          int32_t* __restrict__ nn_idx) {
+  __shared__ CoarseSmem cs;
+  const int nc = load_coarse(cs, clist, cbox, n_coarse_p, sorted);
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   const int nq = n2b * n2b;
@@ -477,47 +489,11 @@ k_nn_grid(int n2b, const float4* __restrict__ grid, const float4* __restrict__ p
       }
     }
     const uint32_t own = cell_key(q.x, q.y, q.z);
-    scan_points(__ldg(&fstart[own]), __ldg(&fstart[own + 1]), q.x, q.y, q.z, sorted, best, bidx);
+    const uint32_t own_s = __ldg(&fstart[own]), own_e = __ldg(&fstart[own + 1]);
+    scan_points(own_s, own_e, q.x, q.y, q.z, sorted, best, bidx);
     warp_nn_min(best, bidx);
-    if (!(best < INFINITY)) {
-      for (int c = lane; c < nc; c += 32) {
-        const float4 r = s_rep[c];
-        nn_update(ref_dist2(q.x, q.y, q.z, r), __float_as_int(r.w), best, bidx);
-      }
-      warp_nn_min(best, bidx);
-    }
-    for (int c0 = 0; c0 < nc; c0 += 32) {
-      const int c = c0 + lane;
-      const bool cand = c < nc && box_lb2(q.x, q.y, q.z, s_box + 6 * c) * kPruneMargin <= best;
-      unsigned cmask = __ballot_sync(0xffffffffu, cand);
-      while (cmask) {
-        const int cc = c0 + __ffs(cmask) - 1;
-        cmask &= cmask - 1;
-        const int cid = (int)s_cid[cc];
-        uint32_t fs[2], fe[2];
-        bool in[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const uint32_t fc = (uint32_t)(cid * 64 + h * 32 + lane);
-          fs[h] = __ldg(&fstart[fc]);
-          fe[h] = __ldg(&fstart[fc + 1]);
-          in[h] = fe[h] > fs[h] && fc != own &&
-                  box_lb2_ord(q.x, q.y, q.z, flo + 3 * fc, fhi + 3 * fc) * kPruneMargin <= best;
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          unsigned fmask = __ballot_sync(0xffffffffu, in[h]);
-          while (fmask) {
-            const int src = __ffs(fmask) - 1;
-            fmask &= fmask - 1;
-            const uint32_t s1 = __shfl_sync(0xffffffffu, fs[h], src);
-            const uint32_t e1 = __shfl_sync(0xffffffffu, fe[h], src);
-            scan_points(s1, e1, q.x, q.y, q.z, sorted, best, bidx);
-          }
-        }
-        warp_nn_min(best, bidx);
-      }
-    }
+    if (!(best < INFINITY)) rep_bound(cs, nc, q.x, q.y, q.z, best, bidx);
+    open_within(cs, nc, own_e > own_s ? own_s : 0xffffffffu, q.x, q.y, q.z, frec, sorted, best, bidx);
     if (lane == 0) emit_sample(qi, nq, best, bidx, max_sq, xyzi, range, refl, amb, n_out_ch, out, nn_idx);
   }
 }
@@ -535,9 +511,9 @@ size_t sampler_scratch_bytes(int max_points, int max_queries) {
   b += (size_t)kFineCells * sizeof(uint32_t) * 2;   // count, cursor
   b += (size_t)kCoarseCells * sizeof(uint32_t);      // coarse counts
   b += (size_t)(kFineCells + 4) * sizeof(uint32_t);  // start
-  b += (size_t)kFineCells * 6 * sizeof(uint32_t);    // fine boxes
-  b += (size_t)kCoarseCells * sizeof(uint4);
-  b += (size_t)kCoarseCells * 6 * sizeof(uint32_t);
+  b += (size_t)kFineCells * 2 * sizeof(float4);      // fine records
+  b += (size_t)kCoarseCells * sizeof(uint4);         // coarse list
+  b += (size_t)kCoarseCells * 2 * sizeof(float4);    // coarse boxes
   b += 256;
   return b + 20 * 256;  // carve() rounds each of the regions up to 256 bytes
 }
@@ -558,11 +534,9 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   uint32_t* cursor = (uint32_t*)carve(p, (size_t)kFineCells * sizeof(uint32_t));
   uint32_t* ccount = (uint32_t*)carve(p, (size_t)kCoarseCells * sizeof(uint32_t));
   uint32_t* start = (uint32_t*)carve(p, (size_t)(kFineCells + 4) * sizeof(uint32_t));
-  uint32_t* flo = (uint32_t*)carve(p, (size_t)kFineCells * 3 * sizeof(uint32_t));
-  uint32_t* fhi = (uint32_t*)carve(p, (size_t)kFineCells * 3 * sizeof(uint32_t));
+  float4* frec = (float4*)carve(p, (size_t)kFineCells * 2 * sizeof(float4));
   uint4* clist = (uint4*)carve(p, (size_t)kCoarseCells * sizeof(uint4));
-  uint32_t* clo = (uint32_t*)carve(p, (size_t)kCoarseCells * 3 * sizeof(uint32_t));
-  uint32_t* chi = (uint32_t*)carve(p, (size_t)kCoarseCells * 3 * sizeof(uint32_t));
+  float4* cbox = (float4*)carve(p, (size_t)kCoarseCells * 2 * sizeof(float4));
   uint32_t* ncoarse = (uint32_t*)carve(p, 256);
   const int n2b = a.n2b;
   const size_t nbins = (size_t)n2b * n2b, nmask = (size_t)n2b * bin_words(n2b);
@@ -571,10 +545,6 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
 
   // count, cursor and coarse counts are adjacent: one memset
   cudaMemsetAsync(count, 0, (size_t)(2 * kFineCells + kCoarseCells) * sizeof(uint32_t), st);
-  cudaMemsetAsync(flo, 0xff, (size_t)kFineCells * 3 * sizeof(uint32_t), st);
-  cudaMemsetAsync(fhi, 0, (size_t)kFineCells * 3 * sizeof(uint32_t), st);
-  cudaMemsetAsync(clo, 0xff, (size_t)kCoarseCells * 3 * sizeof(uint32_t), st);
-  cudaMemsetAsync(chi, 0, (size_t)kCoarseCells * 3 * sizeof(uint32_t), st);
   if (n2b > 0) {
     cudaMemsetAsync(binmap, 0xff, nbins * sizeof(uint32_t), st);
     cudaMemsetAsync(colmask, 0, nmask * sizeof(uint32_t), st);
@@ -589,20 +559,19 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   ++launched;
   if (P > 0) {
     k_scatter<<<(P + 255) / 256, 256, 0, st>>>(P, proj, key, start, cursor, sorted);
-    k_cell_bounds<<<(P + 255) / 256, 256, 0, st>>>(start + kFineCells, sorted, flo, fhi, clo, chi);
+    k_cell_records<<<kCoarseCells, kRecordThreads, 0, st>>>(clist, ncoarse, start, sorted, frec, cbox);
     launched += 2;
   }
   const int wpb = kQueryThreads / 32;
   int blocks = (a.n_queries + wpb - 1) / wpb;
   if (blocks > 148 * 8) blocks = 148 * 8;
   if (n2b > 0) {
-    k_nn_grid<<<blocks, kQueryThreads, 0, st>>>(n2b, a.grid, proj, binmap, colmask, sorted, start, flo, fhi, clist,
-                                                clo, chi, ncoarse, a.max_sq, a.xyzi, range, a.refl, a.amb,
-                                                a.n_out_ch, a.out, a.nn_idx);
+    k_nn_grid<<<blocks, kQueryThreads, 0, st>>>(n2b, a.grid, proj, binmap, colmask, sorted, start, frec, clist, cbox,
+                                                ncoarse, a.max_sq, a.xyzi, range, a.refl, a.amb, a.n_out_ch, a.out,
+                                                a.nn_idx);
   } else {
-    k_nn_query<<<blocks, kQueryThreads, 0, st>>>(a.n_queries, a.grid, sorted, start, flo, fhi, clist, clo, chi,
-                                                 ncoarse, a.max_sq, a.xyzi, range, a.refl, a.amb, a.n_out_ch,
-                                                 a.out, a.nn_idx);
+    k_nn_query<<<blocks, kQueryThreads, 0, st>>>(a.n_queries, a.grid, sorted, frec, clist, cbox, ncoarse, a.max_sq,
+                                                 a.xyzi, range, a.refl, a.amb, a.n_out_ch, a.out, a.nn_idx);
   }
   ++launched;
   count_launches(launched);
