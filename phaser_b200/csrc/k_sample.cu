@@ -173,7 +173,7 @@ __global__ void k_scatter(int P, const float4* __restrict__ proj, const uint32_t
 //   {lo.x, lo.y, lo.z, hi.x}, {hi.y, hi.z, start (bits), end (bits)}
 // and the coarse box is cbox[2 i], cbox[2 i + 1] = {lo.xyz, hi.x}, {hi.yz, nfine (bits), 0}.
 // One block per list entry: warps take fine cells, lanes the cell's points.
-constexpr int kRecordThreads = 128;
+constexpr int kRecordThreads = 256;
 
 __global__ void __launch_bounds__(kRecordThreads)
 k_cell_records(const uint4* __restrict__ clist, const uint32_t* __restrict__ n_coarse_p,
