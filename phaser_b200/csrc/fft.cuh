@@ -411,6 +411,67 @@ __device__ __forceinline__ void fft_any(float2* buf, int ntrans, int tstride, in
   }
 }
 
+// Column transforms with a column-resident thread mapping: thread tid keeps
+// column t = tid % ntrans and walks the butterflies g, g + groups, ... of each
+// stage (g = tid / ntrans, groups = nthr / ntrans), so the index arithmetic
+// is one division per call instead of one per butterfly, and a warp touches
+// neighbouring columns of one butterfly.  Needs ntrans <= nthr (callers fall
+// back to fft_fixed otherwise).
+template <int N, int R, int L, bool INV>
+__device__ __forceinline__ void fixed_col_stage(float2* buf, int stride, const float2* __restrict__ tw, int t, int g,
+                                                int groups) {
+  constexpr int m = L / R;
+  constexpr int nb = N / R;
+  constexpr int twstep = N / L;
+  if (g >= groups) return;
+  const size_t es = (size_t)m * stride;
+  for (int bf = g; bf < nb; bf += groups) {
+    const int blk = bf / m, j2 = bf - blk * m;
+    float2* base = buf + t + (size_t)(blk * L + j2) * stride;
+    float2 x[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) x[j] = base[j * es];
+    if constexpr (INV) {
+#pragma unroll
+      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], cconj(__ldg(&tw[twstep * j2 * k])));
+      dft_small<R, true>(x);
+    } else {
+      dft_small<R, false>(x);
+#pragma unroll
+      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], __ldg(&tw[twstep * j2 * k]));
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) base[j * es] = x[j];
+  }
+}
+
+template <int N, bool INV, int SI = 0>
+__device__ __forceinline__ void fixed_col_stages(float2* buf, int stride, const float2* __restrict__ tw, int t, int g,
+                                                 int groups) {
+  if constexpr (SI < FixedFft<N>::count) {
+    constexpr int S = INV ? (FixedFft<N>::count - 1 - SI) : SI;
+    fixed_col_stage<N, FixedFft<N>::r[S], fixed_L<N, S>(), INV>(buf, stride, tw, t, g, groups);
+    __syncthreads();
+    fixed_col_stages<N, INV, SI + 1>(buf, stride, tw, t, g, groups);
+  }
+}
+
+// Columns t < ntrans of a [N][stride] buffer (element i of column t at
+// buf[t + i * stride]).  Caller synchronises before; ends with __syncthreads().
+template <int NF, bool INV>
+__device__ __forceinline__ void fft_any_cols(float2* buf, int ntrans, int stride, const FftPlan& p) {
+  const int nthr = blockDim.x;
+  if constexpr (NF > 0) {
+    if (ntrans <= nthr) {
+      const int tid = threadIdx.x;
+      fixed_col_stages<NF, INV>(buf, stride, p.tw, tid % ntrans, tid / ntrans, nthr / ntrans);
+      return;
+    }
+  }
+  fft_any<NF, INV, -2>(buf, ntrans, 1, stride, p);
+}
+
+
 template <int NF>
 __device__ __forceinline__ int freq2pos(int k, const FftPlan& p) {
   if constexpr (NF > 0) {

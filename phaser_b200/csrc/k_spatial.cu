@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
     }
   }
   __syncthreads();
-  fft_any<NF, false, -2>(tile, rowlen, 1, rowlen, plan);
+  fft_any_cols<NF, false>(tile, rowlen, rowlen, plan);
   const int kx = x_natural ? xp : pos2freq<NF>(xp, plan);
   const uint32_t nv = (uint32_t)N * (uint32_t)N * (uint32_t)N;
   // MEAN divides by the total channel count: a product with the reciprocal,
@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
     row[t] = make_float2(F.x * G.x - F.y * (-G.y), F.x * (-G.y) + F.y * G.x);
   }
   __syncthreads();
-  fft_any<NF, true, -2>(tile, Wt, 1, rowlen, plan);
+  fft_any_cols<NF, true>(tile, Wt, rowlen, plan);
   for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
     const int z = e / Wt, t = e - z * Wt;
     if (t < wt) a.cspec[((size_t)z * N + xp) * H2p + ky0 + t] = tile[(size_t)z * rowlen + t];
