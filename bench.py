@@ -135,21 +135,51 @@ def physical_gpu_index(local):
 # ------------------------------------------------------------------ roofline
 
 def stage_bytes(stage, bw, N, C, P):
-    """Algorithmic HBM bytes of one call of a stage (per side where a stage
-    runs per cloud): the minimum each stage must move with its inputs and
-    outputs in HBM (FP32 data, complex64 spectra)."""
+    """Algorithmic HBM bytes of one call of a stage (per cloud / side where a
+    stage runs per side), after the per-unit figures of the survey's
+    measurement section: FP32 data, complex64 spectra, the minimum each stage
+    moves with its inputs and outputs in HBM."""
     nv = N ** 3
     H = N * N * (N // 2 + 1)
     n = 2 * bw
     return {
-        "spatial_fwd": C * nv * 4 + nv * 4 + C * H * 8,      # grids + count in, half spectra out
-        "fuse_z": 2 * C * H * 8 + H * 8,                     # both clouds' spectra in, product out
-        "spatial_inv": H * 8,                                # product in (argmax only, no volume)
-        "so3_synth": n * n * bw * 8,                         # half-spectrum S written
-        "so3_fft": 3 * n * n * bw * 8,                       # S read+write (alpha), read (gamma)
-        "voxelize": P * 20 + (C + 1) * nv * 4,               # points in, grid planes zeroed/updated
-        "s2_sample": P * 20 + 4 * n * n * 4,
+        "s2_sample": P * 20 + 4 * n * n * 4,                 # points in, 4 sample channels out
+        "sht": C * n * n * 4 + C * bw * bw * 8,              # C grids in, C coefficient sets out
+        "fuse_s2": 2 * C * bw * bw * 8 + 2 * bw * bw * 8,    # both sides' coefficients in, fused out
+        "so3_synth": n * n * bw * 8,                         # half spectrum S written (m2 >= 0)
+        "so3_fft": 3 * n * n * bw * 8,                       # S read + write (alpha), read (gamma)
+        "voxelize": P * 20,                                  # points in (voxel updates are scattered)
+        "spatial_fwd": C * (nv * 4 + H * 8),                 # R2C of C grids: read + write
+        "fuse_z": 2 * C * H * 8 + H * 8,                     # both sides' spectra in, product out
+        "spatial_inv": H * 8,                                # product in (argmax fused, no volume)
     }.get(stage)
+
+
+def pair_bytes(bw, N, C, P):
+    """Algorithmic bytes of one served registration (the survey's per-pair
+    total: rotation + translation subtotals)."""
+    n = 2 * bw
+    nv = N ** 3
+    H = N * N * (N // 2 + 1)
+    rot = (2 * P * 20 + 2 * C * n * n * 4 + 2 * C * bw * bw * 8 + (4 * bw ** 3 // 3) * 8 + n ** 3 * 8
+           + 2 * n ** 3 * 8 + n ** 3 * 8)
+    trans = P * 20 + 2 * C * nv * 4 + 2 * C * (nv * 4 + H * 8) + (2 * C * H * 8 + H * 8) + (H * 8 + nv * 4) + nv * 4
+    return rot + trans
+
+
+# DRAM read + write per stage call from the ncu capture summarised in
+# profiles/traffic_register_pair_B100_N200.md (sum over the stage's kernels).
+NCU_TRAFFIC_B100_N200 = {
+    "s2_sample": (2.19 + 0.14 + 2.67 + 2.15 + 5.27) * 1e6,   # project, cell_scan, scatter, records, nn_grid
+    "sht": 4.54e6,
+    "fuse_s2": 0.32e6,
+    "so3_synth": (2.18 + 1.98) * 1e6,
+    "so3_fft": (31.86 + 32.02) * 1e6,
+    "voxelize": (8.25 + 0.83 + 0.31) * 1e6,                  # voxelize + clear
+    "spatial_fwd": (40.77 + 38.67) * 1e6,
+    "fuse_z": (200.54 + 20.29) * 1e6,
+    "spatial_inv": 33.35e6,
+}
 
 
 def measured_peak():
@@ -161,7 +191,11 @@ def measured_peak():
         return 6650.0, "fallback 6.65 TB/s"
 
 
-def roofline(nat, pool, params):
+def roofline(nat, pool, params, served_value):
+    """Per-stage CUDA events (phgpu_profile_*, recorded on each stage's stream)
+    over registrations of the bench workload; the dominant stage is the
+    roofline entry, every stage is listed, and the whole pipeline is rated
+    with the per-pair algorithmic bytes at the served rate."""
     ctx = nat.Context(params)
     ctx.profile(True)
     import torch
@@ -176,19 +210,32 @@ def roofline(nat, pool, params):
         ctx.register_pair(*dev[i % len(dev)])
     st = ctx.profile_read()
     ctx.close()
-    tot = {k: v for k, v in st.items() if v[1] > 0 and k != "upload"}
-    top = max(tot, key=lambda k: tot[k][0])
-    ms, calls = tot[top]
+    bw, N, C = params.spherical_bandwidth, params.spatial_n_voxels, 3
     P = int(np.mean([p.target.xyzi.shape[0] for p in pool]))
-    nb = stage_bytes(top, params.spherical_bandwidth, params.spatial_n_voxels, 3, P)
-    per_call_ms = ms / calls
     peak, src = measured_peak()
-    achieved = nb / (per_call_ms * 1e-3) / 1e9
-    stages = {k: round(v[0] / nrep, 4) for k, v in tot.items()}
-    return {"kernel": top, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": None, "peak_source": src,
-            "algorithmic_bytes_per_launch": nb, "avg_launch_ms": round(per_call_ms, 4),
-            "stage_ms_per_pair": stages}
+    tot = {k: v for k, v in st.items() if v[1] > 0 and k != "upload"}
+    stages = {}
+    for k, (ms, calls) in tot.items():
+        nb = stage_bytes(k, bw, N, C, P)
+        per = ms / calls
+        e = {"ms_per_call": round(per, 4), "calls_per_pair": round(calls / nrep, 2)}
+        if nb:
+            gbs = nb / (per * 1e-3) / 1e9
+            e.update({"algorithmic_bytes": nb, "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)})
+        stages[k] = e
+    top = max(tot, key=lambda k: tot[k][0])
+    e = stages[top]
+    workload_is_bench = (bw, N) == (100, 200)
+    roof = {"kernel": top, "bound": "hbm", "achieved": e.get("achieved_gbs"), "peak": peak, "unit": "GB/s",
+            "frac": e.get("frac"),
+            "traffic": NCU_TRAFFIC_B100_N200.get(top) if workload_is_bench else None,
+            "peak_source": src, "algorithmic_bytes_per_launch": e.get("algorithmic_bytes"),
+            "avg_launch_ms": e["ms_per_call"], "stages": stages}
+    pb = pair_bytes(bw, N, C, P)
+    roof["pipeline"] = {"algorithmic_bytes_per_pair": pb, "achieved_gbs": round(served_value * pb / 1e9, 1),
+                        "frac": round(served_value * pb / 1e9 / peak, 4),
+                        "basis": "served registrations/s x per-pair algorithmic bytes"}
+    return roof
 
 
 # ------------------------------------------------------------------ CPU
@@ -366,7 +413,7 @@ def main():
     barrier()
 
     # ---------------- roofline of the dominant stage (rank 0 context, profiled)
-    roof = roofline(nat, pool, params)
+    roof = roofline(nat, pool, params, value / world)
 
     # ---------------- CPU baseline (rank 0, N = 1)
     cpu = None
