@@ -8,15 +8,16 @@
 // request (a context allocates its buffers).
 //
 // How: the sampler's scratch (projected points, cell keys, sorted points,
-// cell counts and boxes) and the grid directions live in one file-scope
-// __device__ array of fixed size.  The first call on each device, with that
+// cell counts, cell records, direction-bin maps) and the grid directions live
+// in one file-scope __device__ array of fixed size.  The first call on each device, with that
 // device current, looks the array's address up with cudaGetSymbolAddress
 // (this may load the module on that device); it should therefore come before
 // any stream capture.  Later calls reuse the cached address.  Every call runs
 // the same kernels as phgpu_sample_s2 (launch_sample), which clears the
-// parts that must start at zero -- cell counts and cursors, the coarse-cell
-// counter -- and resets the cell boxes with cudaMemsetAsync on the caller's
-// stream; nothing relies on the array's load-time contents.
+// parts that must start at zero -- fine and coarse cell counts, cursors, the
+// direction-bin maps -- with cudaMemsetAsync on the caller's stream and
+// rebuilds everything else from the points; nothing relies on the array's
+// load-time contents or on an earlier call's.
 //
 // One array per device: calls that overlap in time on the same device (two
 // host threads, or two streams with work in flight) race on it.  Serialise
