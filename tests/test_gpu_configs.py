@@ -1,0 +1,132 @@
+"""The benchmark's other configurations as parity cases.
+
+Mixed batch (B from {32, 64, 100, 128}, N from {64, 128, 200}, 32..128 beams):
+every served pose equals the FP64 oracle's (rotation bin and translation voxel
+identical).
+
+Large pair (256 x 4096 LiDAR, ~1M points, B = 256, N = 512 over [-20, 20]^3):
+the FP64 oracle is too slow at this size for whole registrations, so the
+checks are size-independent ones -- every sampled direction's neighbour is a
+nearest point (k-d tree over the oracle's projections, float rounding
+allowed), the N = 512 translation correlation matches the oracle on a sparse
+grid (relative L2 1e-5), and the fused registration equals the composition of
+the public per-stage entry points.
+"""
+import concurrent.futures as cf
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+REL_L2 = 1e-5
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
+
+
+MIXED = [  # (pair k, beams, B, N)
+    (0, 32, 32, 64), (1, 64, 64, 128), (2, 128, 100, 200), (3, 64, 128, 200), (4, 32, 100, 64), (5, 128, 64, 128),
+]
+
+
+def test_mixed_batch_matches_oracle():
+    from phaser_b200 import native as nat, scene
+    pairs = [scene.make_pair(2, k, beams=beams) for k, beams, _, _ in MIXED]
+    params = [nat.default_params(spherical_bandwidth=B, spatial_n_voxels=N, spatial_discretize_lower=-10,
+                                 spatial_discretize_upper=10) for _, _, B, N in MIXED]
+
+    def oracle(i):
+        p, (_, _, B, N) = pairs[i], MIXED[i]
+        return O.register_pair(p.target.xyzi, p.target.reflectivity, p.source.xyzi, p.source.reflectivity, B, N,
+                               -10, 10)
+
+    with cf.ThreadPoolExecutor(max_workers=len(MIXED)) as ex:
+        want = list(ex.map(oracle, range(len(MIXED))))
+    srv = nat.Server(workers=4, device=0, flags=nat.PHGPU_SERVER_BORROW_HOST)
+    tickets = [srv.submit(pr, (p.target.xyzi, p.target.reflectivity), (p.source.xyzi, p.source.reflectivity))
+               for pr, p in zip(params, pairs)]
+    srv.drain()
+    for i, t in enumerate(tickets):
+        pose, _ = srv.poll(t)
+        assert (pose.rot_bin, pose.voxel) == (want[i].rot_bin, want[i].voxel), MIXED[i]
+    srv.close()
+
+
+@pytest.fixture(scope="module")
+def large_pair():
+    from phaser_b200 import scene
+    return scene.workload_pair(4, 0)
+
+
+def test_large_sampling_is_nearest(large_pair):
+    from scipy.spatial import cKDTree
+    from phaser_b200 import native as nat, scene
+    w = scene.WORKLOADS[4]
+    cl = large_pair.target
+    c = nat.Context(spherical_bandwidth=w["bw"], spatial_n_voxels=8, max_points=cl.xyzi.shape[0])
+    c.sample_s2(cl.xyzi, cl.reflectivity, side=0)
+    _, idx = c.samples(0)
+    c.close()
+    proj, _ = O.project(cl.xyzi)
+    proj = proj.astype(np.float64)
+    q = O.dh_grid(w["bw"]).astype(np.float64)
+    ok = np.all(np.isfinite(proj), axis=1)
+    tree = cKDTree(proj[ok])
+    assert (idx >= 0).all()
+    # a seeded subset of directions plus both polar rows (the hardest ones)
+    n2b = 2 * w["bw"]
+    sel = np.unique(np.concatenate([np.random.default_rng(4).choice(n2b * n2b, 32768, replace=False),
+                                    np.arange(n2b), np.arange(n2b * (n2b - 1), n2b * n2b)]))
+    d_gpu = np.linalg.norm(q[sel] - proj[idx[sel]], axis=1)
+    # the chosen point is a nearest one up to float rounding: no point lies
+    # strictly inside its distance
+    inside = tree.query_ball_point(q[sel], d_gpu * (1 - 1e-6) - 1e-9, return_length=True, workers=-1)
+    assert int(np.max(inside)) == 0
+
+
+def test_spatial_n512_sparse_vs_oracle():
+    from phaser_b200 import native as nat
+    N = 512
+    rng = np.random.default_rng(512)
+    f = np.zeros((1, N ** 3))
+    g = np.zeros((1, N ** 3))
+    idx = rng.choice(N ** 3, 40000, replace=False)
+    f[0, idx] = rng.random(40000)
+    g[0, (idx + 7 * N * N + 301 * N + 5) % N ** 3] = f[0, idx] * rng.uniform(0.5, 1.5, 40000)
+    c = nat.Context(spherical_bandwidth=2, spatial_n_voxels=N, spatial_fusion=nat.PHGPU_FUSION_NONE,
+                    flags=nat.PHGPU_FLAG_KEEP_VOLUMES)
+    c.spatial_correlate(list(f), list(g))
+    vox, _, vol = c.spatial_result(volume=True)
+    c.close()
+    ref = O.spatial_correlation(f, g, N, laplace=False)
+    assert rel_l2(vol, ref) <= REL_L2
+    assert vox == O.argmax(ref)
+
+
+def test_large_registration_equals_stage_composition(large_pair):
+    from phaser_b200 import native as nat, scene
+    w = scene.WORKLOADS[4]
+    p = large_pair
+    kw = dict(spherical_bandwidth=w["bw"], spatial_n_voxels=w["n_voxels"], spatial_discretize_lower=w["lo"],
+              spatial_discretize_upper=w["hi"], max_points=max(p.target.xyzi.shape[0], p.source.xyzi.shape[0]))
+    c = nat.Context(**kw)
+    pose = c.register_pair((p.target.xyzi, p.target.reflectivity), (p.source.xyzi, p.source.reflectivity))
+    again = c.register_pair((p.target.xyzi, p.target.reflectivity), (p.source.xyzi, p.source.reflectivity))
+    assert (again.rot_bin, again.voxel) == (pose.rot_bin, pose.voxel)
+    s = nat.Context(**kw)
+    s.sample_s2(p.target.xyzi, p.target.reflectivity, side=0)
+    s.sample_s2(p.source.xyzi, p.source.reflectivity, side=1)
+    s.sph_correlate_sampled()
+    rot_bin, _ = s.sph_result()
+    assert rot_bin == pose.rot_bin
+    s.voxelize(p.target.xyzi, p.target.reflectivity, side=0)
+    s.voxelize(p.source.xyzi, p.source.reflectivity, side=1, T=O.rotation_xyz(*pose.xyz))
+    s.spatial_correlate_voxelized()
+    vox, _ = s.spatial_result()
+    assert vox == pose.voxel
+    c.close()
+    s.close()
