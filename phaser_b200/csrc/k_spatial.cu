@@ -106,38 +106,72 @@ cudaError_t launch_clear_voxels(const uint32_t* lin, int n_points, float* grids,
 }
 
 // ---------------------------------------------------------------- A1
+// mean of a voxel: sum / count, 0 for empty voxels (reference: non-finite -> 0)
+__device__ __forceinline__ float voxel_mean(float v, float c) { return c > 0.0f ? v * __frcp_rn(c) : 0.0f; }
+
 constexpr int kRowsR2C = 16;
 
 // rows r = z*N + x of one channel; out spec[ch][r][ky], ky in [0, N/2].
+// A block takes kRowsR2C rows; rows without any point (row flags of the
+// voxeliser) are written as zeros without being read, and the live rows are
+// transformed two at a time as the real and imaginary parts of one complex
+// row, Z = X0 + i X1, separated afterwards by
+//   X0[k] = (Z[k] + conj Z[-k]) / 2,   X1[k] = (Z[k] - conj Z[-k]) / 2i.
 template <int NF>
 __global__ void k_r2c_y(int N, const float* __restrict__ grid, const float* __restrict__ count,
-                        float2* __restrict__ spec, FftPlan plan) {
-  extern __shared__ float2 rows[];
+                        const uint8_t* __restrict__ rowlive, float2* __restrict__ spec, FftPlan plan) {
+  extern __shared__ float2 rows[];  // [kRowsR2C / 2][n] packed rows, then int pos[n]
   constexpr int R = kRowsR2C;
+  __shared__ int s_slot[R];         // 2 * packed row + part, or -1 for a row without points
+  __shared__ int s_src[R];          // live rows in order
+  __shared__ int s_nlive;
   const int n = NF > 0 ? NF : N;
   const int H2 = n / 2 + 1;
   const int H2p = spatial_h2p(n);
+  int* pos = reinterpret_cast<int*>(rows + (size_t)(R / 2) * n);
   const size_t nrows = (size_t)n * n;
   const size_t r0 = (size_t)blockIdx.x * R;
-  for (int e = threadIdx.x; e < R * n; e += blockDim.x) {
-    const int rr = e / n, y = e - rr * n;
-    const size_t r = r0 + rr;
-    float v = 0.0f;
-    if (r < nrows) {
-      v = grid[r * n + y];
-      if (count) {
-        const float q = v / count[r * n + y];
-        v = isfinite(q) ? q : 0.0f;
+  if (threadIdx.x < 32) {
+    const int rr = threadIdx.x;
+    const bool live = rr < R && r0 + rr < nrows && (!rowlive || rowlive[r0 + rr]);
+    const unsigned m = __ballot_sync(0xffffffffu, live);
+    const int k = __popc(m & ((1u << rr) - 1u));
+    if (rr < R) s_slot[rr] = live ? k : -1;
+    if (live) s_src[k] = rr;
+    if (rr == 0) s_nlive = __popc(m);
+  }
+  for (int k = threadIdx.x; k < n; k += blockDim.x) pos[k] = freq2pos<NF>(k, plan);
+  __syncthreads();
+  const int nlive = s_nlive;
+  const int npk = (nlive + 1) / 2;
+  for (int e = threadIdx.x; e < npk * n; e += blockDim.x) {
+    const int pk = e / n, y = e - pk * n;
+    float v[2] = {0.f, 0.f};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int li = 2 * pk + h;
+      if (li < nlive) {
+        const size_t idx = (r0 + s_src[li]) * n + y;
+        v[h] = count ? voxel_mean(grid[idx], count[idx]) : grid[idx];
       }
     }
-    rows[e] = make_float2(v, 0.0f);
+    rows[e] = make_float2(v[0], v[1]);
   }
   __syncthreads();
-  fft_any<NF, false>(rows, R, n, 1, plan);
+  if (npk > 0) fft_any<NF, false>(rows, npk, n, 1, plan);
   for (int e = threadIdx.x; e < R * H2; e += blockDim.x) {
     const int rr = e / H2, ky = e - rr * H2;
     const size_t r = r0 + rr;
-    if (r < nrows) spec[r * H2p + ky] = rows[rr * n + freq2pos<NF>(ky, plan)];
+    if (r >= nrows) continue;
+    const int sl = s_slot[rr];
+    float2 X = make_float2(0.f, 0.f);
+    if (sl >= 0) {
+      const float2* Z = rows + (size_t)(sl >> 1) * n;
+      const float2 a = Z[pos[ky]], b = Z[pos[ky == 0 ? 0 : n - ky]];
+      X = (sl & 1) ? make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x))  // (a - conj b) / 2i
+                   : make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));  // (a + conj b) / 2
+    }
+    spec[r * H2p + ky] = X;
   }
 }
 
@@ -360,8 +394,6 @@ __global__ void k_c2r_y(int N, const float2* __restrict__ cspec, FftPlan plan,
 //   X[k][ky] = A + w_N^k B,  X[k + N/2][ky] = A - w_N^k B.
 // Output rows are in natural kx order.  Shared rows have the odd stride N + 1.
 
-// mean of a voxel: sum / count, 0 for empty voxels (reference: non-finite -> 0)
-__device__ __forceinline__ float voxel_mean(float v, float c) { return c > 0.0f ? v * __frcp_rn(c) : 0.0f; }
 
 template <int NF>
 __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __restrict__ grids, size_t grid_cstride,
@@ -517,11 +549,11 @@ static cudaError_t allow_max_smem(const void* fn) {
 
 template <int NF>
 static cudaError_t set_attrs() {
-  cudaError_t e = cudaFuncSetAttribute(k_fuse_z<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_r2c_y<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fft_x<NF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fft_x<NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_c2r_y<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  cudaError_t e = allow_max_smem((const void*)k_fuse_z<NF>);
+  if (e == cudaSuccess) e = allow_max_smem((const void*)k_r2c_y<NF>);
+  if (e == cudaSuccess) e = allow_max_smem((const void*)k_fft_x<NF, false>);
+  if (e == cudaSuccess) e = allow_max_smem((const void*)k_fft_x<NF, true>);
+  if (e == cudaSuccess) e = allow_max_smem((const void*)k_c2r_y<NF>);
   return e;
 }
 
@@ -609,8 +641,10 @@ cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t 
     float2* spec = a.spec + (size_t)(side * a.n_data_ch + c) * plane;
     const float* g = grids + (size_t)c * nv;
     dim3 gx((H2 + 15) / 16, N, 1);
+    const uint8_t* rowlive = side == 0 ? a.rowlive_f : a.rowlive_g;
+    const size_t smr = (size_t)(kRowsR2C / 2) * N * sizeof(float2) + (size_t)N * sizeof(int);
     PHGPU_DISPATCH_N(N,
-        k_r2c_y<NF><<<nrowblk, 256, (size_t)kRowsR2C * N * sizeof(float2), st>>>(N, g, count, spec, *a.plan);
+        k_r2c_y<NF><<<nrowblk, 256, smr, st>>>(N, g, count, rowlive, spec, *a.plan);
         k_fft_x<NF, false><<<gx, 256, (size_t)N * 16 * sizeof(float2), st>>>(N, spec, *a.plan));
     count_launches(2);
   }
