@@ -344,36 +344,46 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
 }
 
 // ---------------------------------------------------------------- C2
+// Real inverse over y of kRowsR2C rows with first-occurrence argmax.  A
+// half-complex inverse reads only the real parts of the ky = 0 and ky = N/2
+// terms, so each row is made exactly Hermitian that way, and rows are
+// inverted two at a time as Z = X0 + i X1 (output x0 = Re, x1 = Im).
 template <int NF>
 __global__ void k_c2r_y(int N, const float2* __restrict__ cspec, FftPlan plan,
                         unsigned long long* __restrict__ argmax, float* __restrict__ volume) {
-  extern __shared__ float2 rows[];
+  extern __shared__ float2 rows[];  // [kRowsR2C / 2][n] packed rows, then int pos[n]
   constexpr int R = kRowsR2C;
   const int n = NF > 0 ? NF : N;
   const int H2 = n / 2 + 1;
   const int H2p = spatial_h2p(n);
+  int* pos = reinterpret_cast<int*>(rows + (size_t)(R / 2) * n);
   const size_t nrows = (size_t)n * n;
   const size_t r0 = (size_t)blockIdx.x * R;
-  for (int e = threadIdx.x; e < R * n; e += blockDim.x) rows[e] = make_float2(0.f, 0.f);
+  for (int k = threadIdx.x; k < n; k += blockDim.x) pos[k] = freq2pos<NF>(k, plan);
   __syncthreads();
   const int hmax = (n - 1) / 2;  // last ky with a mirrored partner
-  for (int e = threadIdx.x; e < R * H2; e += blockDim.x) {
-    const int rr = e / H2, ky = e - rr * H2;
-    const size_t r = r0 + rr;
-    if (r >= nrows) continue;
-    const float2 v = cspec[r * H2p + ky];
-    float2* row = rows + rr * n;
-    row[freq2pos<NF>(ky, plan)] = v;
-    if (ky >= 1 && ky <= hmax) row[freq2pos<NF>(n - ky, plan)] = cconj(v);
+  for (int e = threadIdx.x; e < (R / 2) * H2; e += blockDim.x) {
+    const int pk = e / H2, ky = e - pk * H2;
+    const size_t ra = r0 + 2 * pk, rb = ra + 1;
+    float2 a = ra < nrows ? cspec[ra * H2p + ky] : make_float2(0.f, 0.f);
+    float2 b = rb < nrows ? cspec[rb * H2p + ky] : make_float2(0.f, 0.f);
+    if (ky == 0 || 2 * ky == n) {
+      a.y = 0.f;
+      b.y = 0.f;
+    }
+    float2* Z = rows + (size_t)pk * n;
+    Z[pos[ky]] = make_float2(a.x - b.y, a.y + b.x);                                // a + i b
+    if (ky >= 1 && ky <= hmax) Z[pos[n - ky]] = make_float2(a.x + b.y, b.x - a.y);  // conj a + i conj b
   }
   __syncthreads();
-  fft_any<NF, true>(rows, R, n, 1, plan);
+  fft_any<NF, true>(rows, R / 2, n, 1, plan);
   unsigned long long best = 0ull;
   for (int e = threadIdx.x; e < R * n; e += blockDim.x) {
     const int rr = e / n, y = e - rr * n;
     const size_t r = r0 + rr;
     if (r < nrows) {
-      const float v = rows[e].x;
+      const float2 z = rows[(size_t)(rr >> 1) * n + y];
+      const float v = (rr & 1) ? z.y : z.x;
       const uint32_t idx = (uint32_t)(r * n + y);
       const unsigned long long key = pack_argmax(v, idx);
       best = key > best ? key : best;
@@ -598,7 +608,9 @@ static int fuse_z_tile(int N, int A) {
   const int chunks = (N + 255) / 256;                       // bulk copies of <= 256 z rows
   const size_t rows = (size_t)chunks * ((N + chunks - 1) / chunks);
   const size_t extra = 16 + sizeof(FusionBands) + (size_t)N * sizeof(int);
-  while (wt > 2 && rows * A * wt * sizeof(float2) + extra > (size_t)kMaxSmem) wt >>= 1;
+  // narrower tiles until two blocks fit on an SM (one block cannot overlap
+  // its bulk load with its own transforms), at least until the limit is met
+  while (wt > 2 && rows * A * wt * sizeof(float2) + extra > (size_t)kMaxSmem / 2) wt >>= 1;
   return wt;
 }
 
@@ -697,7 +709,8 @@ cudaError_t launch_spatial_inverse(const SpatialArgs& a, cudaStream_t st) {
   const int nrowblk = (int)(((size_t)N * N + kRowsR2C - 1) / kRowsR2C);
   PHGPU_DISPATCH_N(N,
       k_fft_x<NF, true><<<gC, 256, (size_t)N * 16 * sizeof(float2), st>>>(N, a.cspec, *a.plan);
-      k_c2r_y<NF><<<nrowblk, 256, (size_t)kRowsR2C * N * sizeof(float2), st>>>(N, a.cspec, *a.plan, a.argmax, a.volume));
+      k_c2r_y<NF><<<nrowblk, 256, (size_t)(kRowsR2C / 2) * N * sizeof(float2) + (size_t)N * sizeof(int), st>>>(
+          N, a.cspec, *a.plan, a.argmax, a.volume));
   count_launches(2);
   return cudaGetLastError();
 }
