@@ -54,6 +54,8 @@ typedef struct {
   uint32_t max_points;               /* capacity per cloud (grows on demand) */
   uint32_t flags;                    /* PHGPU_FLAG_* */
   int32_t device;                    /* CUDA device ordinal */
+  uint32_t rot_peak_neighbors;       /* bingham_peak_neighbors (0) */
+  uint32_t trans_peak_neighbors;     /* gaussian_peak_neighbors (0) */
 } phgpu_params;
 
 /* A point cloud: x, y, z, intensity as float4 plus optional per-point
@@ -78,6 +80,8 @@ typedef struct {
   uint32_t voxel;       /* argmax of the spatial correlation, [z][x][y] */
   float trans_peak;     /* correlation value at the voxel */
   double trans[3];      /* translation (translation-utils.cc:40-52) */
+  double rot_omega[4];  /* normalised eigenvalues (ascending) of the peak's quaternion scatter matrix */
+  double trans_cov[9];  /* covariance of the peak's translations (row-major) */
 } phgpu_pose;
 
 typedef struct phgpu_ctx phgpu_ctx;
@@ -171,6 +175,35 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
  * translation-utils.cc:40-52). */
 int phgpu_pose_from_bin(uint32_t bin, uint32_t bw_out, double* zyz, double* quat, double* xyz,
                         float* T12);
+/* Peak-neighbourhood statistics (host; the registration calls them when
+ * rot/trans_peak_neighbors > 0 with the volume values of the linear-index
+ * window around the argmax).
+ *
+ * BinghamPeakBasedEval::fitRotationalBinghamDistribution
+ * (phaser_core/src/backend/uncertainty/bingham-peak-based-eval.cc:22-91) with
+ * Bingham::fit / fitToMoment (phaser_common/src/distribution/bingham.cc:239-295):
+ * values[i] weights the quaternion of SO(3) bin first_bin + i (normalised to
+ * sum 1 when count > 1); the scatter matrix sum_i w_i q_i q_i^T is
+ * eigen-decomposed; mode4 (w, x, y, z, w >= 0) is its principal eigenvector --
+ * the mode the reference's estimate returns -- and omega4 its eigenvalues in
+ * ascending order divided by their sum.  xyz3 gets the Euler angles of the
+ * mode (rotation-utils.cc:86-93).  The concentrations, which the reference
+ * fits with an external optimiser, are not computed.
+ *
+ * GaussianPeakBasedEval::fitTranslationalNormalDist (gaussian-peak-based-eval.cc:
+ * 42-101) with Gaussian::setMeanAndCov (phaser_common/src/distribution/
+ * gaussian.cc:47-55): values[i] (normalised to sum 1) weights the translation
+ * of voxel first_voxel + i; mean3 and cov9 (row-major) are the weighted mean
+ * and covariance. */
+int phgpu_bingham_peak(const double* values, uint32_t first_bin, uint32_t count, uint32_t bw_out,
+                       double* mode4, double* omega4, double* xyz3);
+int phgpu_gaussian_peak(const double* values, uint32_t first_voxel, uint32_t count, uint32_t n_voxels,
+                        int32_t lower, int32_t upper, double* mean3, double* cov9);
+/* The linear-index window [first, first + count) the two evaluators take
+ * around an argmax `index` of an n-element volume for k neighbours
+ * (calculateStartEndNeighbor, gaussian-peak-based-eval.cc:31-41). */
+void phgpu_peak_window(uint32_t index, uint32_t n, uint32_t k, uint32_t* first, uint32_t* count);
+
 double phgpu_translation_from_index(double index, uint32_t n_voxels, int32_t lower,
                                     int32_t upper);
 

@@ -92,6 +92,15 @@ def _declare(lib):
     lib.orc_register_pair.argtypes = [_f32p, C.c_size_t, C.c_void_p, _f32p, C.c_size_t, C.c_void_p,
                                       C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                       C.POINTER(Pose), C.c_void_p, C.c_void_p]
+    lib.orc_register_pair_k.argtypes = [_f32p, C.c_size_t, C.c_void_p, _f32p, C.c_size_t, C.c_void_p,
+                                        C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint32, C.c_uint32,
+                                        C.POINTER(Pose), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.orc_peak_window.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint32)]
+    lib.orc_bingham_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]
+    lib.orc_gaussian_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
+                                      C.c_void_p, C.c_void_p]
     lib.orc_num_threads.restype = C.c_int
 
 
@@ -328,7 +337,11 @@ def translation_from_index(idx, n, lo, hi):
     return lib().orc_translation_from_index(float(idx), n, lo, hi)
 
 
-def register_pair(tgt, tgt_refl, src, src_refl, bw, N, lo, hi, max_sq=1e6, want_volumes=False):
+def register_pair(tgt, tgt_refl, src, src_refl, bw, N, lo, hi, max_sq=1e6, want_volumes=False, rot_k=0,
+                  trans_k=0, want_stats=False):
+    """Full registration; with rot_k / trans_k > 0 the Bingham mode and the
+    Gaussian mean of the peak neighbourhoods give the pose.  want_stats adds
+    (omega[4], cov[3x3]) to the returned tuple."""
     tgt = np.ascontiguousarray(tgt, np.float32)
     src = np.ascontiguousarray(src, np.float32)
     tr = None if tgt_refl is None else np.ascontiguousarray(tgt_refl, np.float32)
@@ -336,11 +349,40 @@ def register_pair(tgt, tgt_refl, src, src_refl, bw, N, lo, hi, max_sq=1e6, want_
     pose = Pose()
     rc = np.zeros((2 * bw) ** 3) if want_volumes else None
     tc = np.zeros(N ** 3) if want_volumes else None
-    lib().orc_register_pair(tgt.reshape(-1), tgt.shape[0], _ptr(tr), src.reshape(-1), src.shape[0],
-                            _ptr(sr), bw, N, lo, hi, max_sq, C.byref(pose), _ptr(rc), _ptr(tc))
+    omega, cov = np.zeros(4), np.zeros(9)
+    lib().orc_register_pair_k(tgt.reshape(-1), tgt.shape[0], _ptr(tr), src.reshape(-1), src.shape[0],
+                              _ptr(sr), bw, N, lo, hi, max_sq, int(rot_k), int(trans_k), C.byref(pose), _ptr(rc),
+                              _ptr(tc), omega.ctypes.data, cov.ctypes.data)
+    out = (pose,)
     if want_volumes:
-        return pose, rc, tc
-    return pose
+        out += (rc, tc)
+    if want_stats:
+        out += (omega, cov.reshape(3, 3))
+    return out if len(out) > 1 else pose
+
+
+def peak_window(index, n, k):
+    f, c = C.c_uint32(), C.c_uint32()
+    lib().orc_peak_window(int(index), int(n), int(k), C.byref(f), C.byref(c))
+    return f.value, c.value
+
+
+def bingham_peak(values, first, bw):
+    v = np.ascontiguousarray(values, np.float64)
+    mode, omega, xyz = np.zeros(4), np.zeros(4), np.zeros(3)
+    if lib().orc_bingham_peak(v.ctypes.data, int(first), len(v), int(bw), mode.ctypes.data, omega.ctypes.data,
+                              xyz.ctypes.data) != 0:
+        raise ValueError("no positive weight")
+    return mode, omega, xyz
+
+
+def gaussian_peak(values, first, N, lo, hi):
+    v = np.ascontiguousarray(values, np.float64)
+    mean, cov = np.zeros(3), np.zeros(9)
+    if lib().orc_gaussian_peak(v.ctypes.data, int(first), len(v), int(N), int(lo), int(hi), mean.ctypes.data,
+                               cov.ctypes.data) != 0:
+        raise ValueError("no positive weight sum")
+    return mean, cov.reshape(3, 3)
 
 
 # ------------------------------------------------------ reference (SOFT) side

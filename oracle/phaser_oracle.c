@@ -1057,10 +1057,147 @@ typedef struct {
   double trans[3];
 } orc_pose;
 
+/* ------------------------------------------------------------------------ */
+/* Peak neighbourhoods (bingham_/gaussian_peak_neighbors > 0).               */
+/* ------------------------------------------------------------------------ */
+
+/* GaussianPeakBasedEval::calculateStartEndNeighbor (gaussian-peak-based-    */
+/* eval.cc:31-41): [start, end] around index, one-sided near the ends.       */
+void orc_peak_window(uint32_t index, uint32_t n, uint32_t k, uint32_t* first, uint32_t* count) {
+  const uint32_t start = (k > index) ? index : index - k;
+  const uint32_t end = ((uint64_t)k + index >= n) ? index : index + k;
+  *first = start;
+  *count = end - start + 1u;
+}
+
+/* Symmetric eigenproblem by classical Jacobi (largest off-diagonal pivot).  */
+static void orc_sym_eig(int n, const double* A0, double* w, double* V) {
+  double A[64];
+  for (int i = 0; i < n * n; ++i) A[i] = A0[i];
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) V[i * n + j] = (i == j) ? 1.0 : 0.0;
+  for (int it = 0; it < 500; ++it) {
+    int p = 0, q = 1;
+    double big = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j)
+        if (fabs(A[i * n + j]) > big) {
+          big = fabs(A[i * n + j]);
+          p = i;
+          q = j;
+        }
+    if (big < 1e-300) break;
+    const double phi = 0.5 * atan2(2.0 * A[p * n + q], A[q * n + q] - A[p * n + p]);
+    const double c = cos(phi), s = sin(phi);
+    for (int k = 0; k < n; ++k) {
+      const double kp = A[k * n + p], kq = A[k * n + q];
+      A[k * n + p] = c * kp - s * kq;
+      A[k * n + q] = s * kp + c * kq;
+    }
+    for (int k = 0; k < n; ++k) {
+      const double pk = A[p * n + k], qk = A[q * n + k];
+      A[p * n + k] = c * pk - s * qk;
+      A[q * n + k] = s * pk + c * qk;
+    }
+    for (int k = 0; k < n; ++k) {
+      const double kp = V[k * n + p], kq = V[k * n + q];
+      V[k * n + p] = c * kp - s * kq;
+      V[k * n + q] = s * kp + c * kq;
+    }
+  }
+  for (int i = 0; i < n; ++i) w[i] = A[i * n + i];
+}
+
+/* BinghamPeakBasedEval::retrievePeakNeighbors + Bingham::fit / fitToMoment  */
+/* (bingham-peak-based-eval.cc:59-91, bingham.cc:239-295): moment matrix of  */
+/* the weighted bin quaternions, its eigenvalues sorted ascending and        */
+/* normalised (omega), the mode = eigenvector of the largest one (w >= 0).   */
+int orc_bingham_peak(const double* values, uint32_t first, uint32_t count, uint32_t bw, double* mode,
+                     double* omega, double* xyz) {
+  double sum = 0.0;
+  for (uint32_t i = 0; i < count; ++i) sum += values[i];
+  if (count > 1 && !(sum > 0.0)) return -1;
+  double C[16] = {0};
+  for (uint32_t i = 0; i < count; ++i) {
+    double zyz[3], q[4];
+    orc_bin_to_zyz(first + i, bw, zyz);
+    orc_zyz_to_quat(zyz, q);
+    const double w = (count > 1) ? values[i] / sum : values[i];
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c < 4; ++c) C[r * 4 + c] += q[r] * w * q[c];
+  }
+  for (int r = 0; r < 4; ++r)
+    for (int c = r + 1; c < 4; ++c) C[r * 4 + c] = C[c * 4 + r] = 0.5 * (C[r * 4 + c] + C[c * 4 + r]);
+  double ev[4], V[16];
+  orc_sym_eig(4, C, ev, V);
+  int idx[4] = {0, 1, 2, 3};
+  for (int a = 0; a < 4; ++a)
+    for (int b = a + 1; b < 4; ++b)
+      if (ev[idx[b]] < ev[idx[a]]) {
+        const int t = idx[a];
+        idx[a] = idx[b];
+        idx[b] = t;
+      }
+  double tot = ev[0] + ev[1] + ev[2] + ev[3];
+  for (int i = 0; i < 4; ++i) omega[i] = tot != 0.0 ? ev[idx[i]] / tot : 0.0;
+  const int m = idx[3];
+  double nrm = 0.0;
+  for (int r = 0; r < 4; ++r) nrm += V[r * 4 + m] * V[r * 4 + m];
+  nrm = sqrt(nrm);
+  const double sg = V[0 * 4 + m] < 0 ? -1.0 : 1.0;
+  for (int r = 0; r < 4; ++r) mode[r] = sg * V[r * 4 + m] / nrm;
+  orc_quat_to_xyz(mode, xyz);
+  return 0;
+}
+
+/* GaussianPeakBasedEval::retrievePeakNeighbors + Gaussian::setMeanAndCov    */
+/* (gaussian-peak-based-eval.cc:73-101, gaussian.cc:47-55).                  */
+int orc_gaussian_peak(const double* values, uint32_t first, uint32_t count, uint32_t N, int lo, int hi,
+                      double* mean, double* cov) {
+  double sum = 0.0;
+  for (uint32_t i = 0; i < count; ++i) sum += values[i];
+  if (!(sum > 0.0)) return -1;
+  double* t = (double*)malloc(sizeof(double) * 3 * count);
+  for (int a = 0; a < 3; ++a) mean[a] = 0.0;
+  for (uint32_t i = 0; i < count; ++i) {
+    uint32_t sub[3];
+    orc_ind2sub(first + i, N, N, sub);
+    for (int a = 0; a < 3; ++a) {
+      t[3 * i + a] = orc_translation_from_index((double)sub[a], N, lo, hi);
+      mean[a] += t[3 * i + a] * (values[i] / sum);
+    }
+  }
+  for (int k = 0; k < 9; ++k) cov[k] = 0.0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const double sw = sqrt(values[i] / sum);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) cov[r * 3 + c] += (t[3 * i + r] - mean[r]) * sw * (t[3 * i + c] - mean[c]) * sw;
+  }
+  free(t);
+  return 0;
+}
+
+void orc_register_pair_k(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
+                         const float* src_xyzi, size_t Ps, const float* src_refl,
+                         int bw, int N, int lo, int hi, float max_sq_dist, uint32_t rot_k, uint32_t trans_k,
+                         orc_pose* pose, double* rot_corr, double* trans_corr, double* omega, double* cov);
+
 void orc_register_pair(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
                        const float* src_xyzi, size_t Ps, const float* src_refl,
                        int bw, int N, int lo, int hi, float max_sq_dist,
                        orc_pose* pose, double* rot_corr, double* trans_corr) {
+  double omega[4], cov[9];
+  orc_register_pair_k(tgt_xyzi, Pt, tgt_refl, src_xyzi, Ps, src_refl, bw, N, lo, hi, max_sq_dist, 0, 0, pose,
+                      rot_corr, trans_corr, omega, cov);
+}
+
+/* With rot_k / trans_k > 0 the rotation applied to the source is the mode    */
+/* of the Bingham fit and the translation the mean of the Gaussian fit        */
+/* (sph-opt-registration.cc:58-88).                                           */
+void orc_register_pair_k(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
+                         const float* src_xyzi, size_t Ps, const float* src_refl,
+                         int bw, int N, int lo, int hi, float max_sq_dist, uint32_t rot_k, uint32_t trans_k,
+                         orc_pose* pose, double* rot_corr, double* trans_corr, double* omega, double* cov) {
   const size_t ns = (size_t)4 * bw * bw;
   double* f = (double*)malloc(sizeof(double) * 4 * ns);
   double* h = (double*)malloc(sizeof(double) * 4 * ns);
@@ -1076,6 +1213,13 @@ void orc_register_pair(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
   orc_bin_to_zyz((uint32_t)bin, (uint32_t)bw, pose->zyz);
   orc_zyz_to_quat(pose->zyz, pose->quat);
   orc_quat_to_xyz(pose->quat, pose->xyz);
+  omega[0] = omega[1] = omega[2] = 0.0;
+  omega[3] = 1.0;
+  if (rot_k > 0) {
+    uint32_t first, count;
+    orc_peak_window((uint32_t)bin, (uint32_t)nvol, rot_k, &first, &count);
+    orc_bingham_peak(corr + first, first, count, (uint32_t)bw, pose->quat, omega, pose->xyz);
+  }
   float T[12];
   orc_rotation_xyz((float)pose->xyz[0], (float)pose->xyz[1], (float)pose->xyz[2], T);
   float* rot = (float*)malloc(sizeof(float) * 4 * (Ps ? Ps : 1));
@@ -1095,6 +1239,12 @@ void orc_register_pair(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
   orc_ind2sub((uint32_t)vox, (uint32_t)N, (uint32_t)N, xyz);
   for (int a = 0; a < 3; ++a)
     pose->trans[a] = orc_translation_from_index((double)xyz[a], (uint32_t)N, lo, hi);
+  for (int k = 0; k < 9; ++k) cov[k] = 0.0;
+  if (trans_k > 0) {
+    uint32_t first, count;
+    orc_peak_window((uint32_t)vox, (uint32_t)nv, trans_k, &first, &count);
+    orc_gaussian_peak(tc + first, first, count, (uint32_t)N, lo, hi, pose->trans, cov);
+  }
   if (!rot_corr) free(corr);
   if (!trans_corr) free(tc);
   free(f);

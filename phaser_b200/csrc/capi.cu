@@ -124,17 +124,19 @@ static void quat_product(const double* a, const double* b, double* r) {
   r[3] = a[0] * b[3] + a[3] * b[0] + a[1] * b[2] - a[2] * b[1];
 }
 
-int phgpu_pose_from_bin(uint32_t bin, uint32_t bw_out, double* zyz, double* quat, double* xyz, float* T12) {
-  double z[3], q[4], e[3];
-  bin_to_zyz(bin, bw_out, z);
-  // ConvertZYZtoQuaternion: AngleAxis(a, Z) * AngleAxis(b, Y) * AngleAxis(c, Z)
+// ConvertZYZtoQuaternion: AngleAxis(a, Z) * AngleAxis(b, Y) * AngleAxis(c, Z)
+// (rotation-utils.cc:101-107).
+static void zyz_to_quat(const double* z, double* q) {
   const double qa[4] = {cos(0.5 * z[0]), 0.0, 0.0, sin(0.5 * z[0])};
   const double qb[4] = {cos(0.5 * z[1]), 0.0, sin(0.5 * z[1]), 0.0};
   const double qc[4] = {cos(0.5 * z[2]), 0.0, 0.0, sin(0.5 * z[2])};
   double t[4];
   quat_product(qa, qb, t);
   quat_product(t, qc, q);
-  // ConvertQuaternionToXYZ / fromRotation (rotation-utils.cc:86-93, 190-196)
+}
+
+// ConvertQuaternionToXYZ / fromRotation (rotation-utils.cc:86-93, 190-196).
+static void quat_to_xyz(const double* q, double* e) {
   const double qw = q[0], qx = q[1], qy = q[2], qz = q[3];
   const double r11 = -2 * (qy * qz - qw * qx);
   const double r12 = qw * qw - qx * qx - qy * qy + qz * qz;
@@ -144,10 +146,24 @@ int phgpu_pose_from_bin(uint32_t bin, uint32_t bw_out, double* zyz, double* quat
   e[2] = -atan2(r31, r32);
   e[1] = asin(r21);
   e[0] = atan2(r11, r12);
+}
+
+static void xyz_to_transform(const double* e, float* T12);
+
+int phgpu_pose_from_bin(uint32_t bin, uint32_t bw_out, double* zyz, double* quat, double* xyz, float* T12) {
+  double z[3], q[4], e[3];
+  bin_to_zyz(bin, bw_out, z);
+  zyz_to_quat(z, q);
+  quat_to_xyz(q, e);
   if (zyz) memcpy(zyz, z, sizeof(z));
   if (quat) memcpy(quat, q, sizeof(q));
   if (xyz) memcpy(xyz, e, sizeof(e));
-  if (T12) {
+  if (T12) xyz_to_transform(e, T12);
+  return PHGPU_OK;
+}
+
+static void xyz_to_transform(const double* e, float* T12) {
+  {
     // RotateAroundXYZ: Rx(a) * Ry(b) * Rz(c) in float (rotation-utils.cc:17-24,109-143)
     const float a = (float)e[0], bb = (float)e[1], c = (float)e[2];
     const float ca = cosf(a), sa = sinf(a), cb = cosf(bb), sb = sinf(bb), cc = cosf(c), sc = sinf(c);
@@ -170,6 +186,115 @@ int phgpu_pose_from_bin(uint32_t bin, uint32_t bw_out, double* zyz, double* quat
       T12[4 * i + 3] = 0.0f;
     }
   }
+}
+
+// Cyclic Jacobi eigen-decomposition of a symmetric 4x4 matrix (FP64):
+// eigenvalues in w[i], eigenvectors in the columns of V (V[r * 4 + i]).
+static void jacobi_eig4(const double* A0, double* w, double* V) {
+  double A[16];
+  memcpy(A, A0, sizeof(A));
+  for (int i = 0; i < 16; ++i) V[i] = (i % 5 == 0) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < 4; ++p)
+      for (int q = p + 1; q < 4; ++q) off += A[p * 4 + q] * A[p * 4 + q];
+    if (off < 1e-300) break;
+    for (int p = 0; p < 4; ++p)
+      for (int q = p + 1; q < 4; ++q) {
+        const double apq = A[p * 4 + q];
+        if (fabs(apq) < 1e-300) continue;
+        const double theta = (A[q * 4 + q] - A[p * 4 + p]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < 4; ++k) {  // A = A J (columns p, q)
+          const double akp = A[k * 4 + p], akq = A[k * 4 + q];
+          A[k * 4 + p] = c * akp - sn * akq;
+          A[k * 4 + q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < 4; ++k) {  // A = J^T A (rows p, q)
+          const double apk = A[p * 4 + k], aqk = A[q * 4 + k];
+          A[p * 4 + k] = c * apk - sn * aqk;
+          A[q * 4 + k] = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < 4; ++k) {
+          const double vkp = V[k * 4 + p], vkq = V[k * 4 + q];
+          V[k * 4 + p] = c * vkp - sn * vkq;
+          V[k * 4 + q] = sn * vkp + c * vkq;
+        }
+      }
+  }
+  for (int i = 0; i < 4; ++i) w[i] = A[i * 5];
+}
+
+void phgpu_peak_window(uint32_t index, uint32_t n, uint32_t k, uint32_t* first, uint32_t* count) {
+  const uint32_t start = k > index ? index : index - k;
+  const uint64_t hi = (uint64_t)index + k;
+  const uint32_t end = hi >= n ? index : (uint32_t)hi;
+  if (first) *first = start;
+  if (count) *count = end - start + 1u;
+}
+
+int phgpu_bingham_peak(const double* values, uint32_t first_bin, uint32_t count, uint32_t bw_out, double* mode4,
+                       double* omega4, double* xyz3) {
+  if (!values || count == 0 || bw_out == 0) return PHGPU_ERR_INVALID;
+  double wsum = 0.0;
+  for (uint32_t i = 0; i < count; ++i) wsum += values[i];
+  if (count > 1 && !(wsum > 0.0)) return PHGPU_ERR_INVALID;
+  double C[16] = {0.0};
+  for (uint32_t i = 0; i < count; ++i) {
+    double z[3], q[4];
+    bin_to_zyz(first_bin + i, bw_out, z);
+    zyz_to_quat(z, q);
+    const double w = count > 1 ? values[i] / wsum : values[i];
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c < 4; ++c) C[r * 4 + c] += w * q[r] * q[c];
+  }
+  double ev[4], V[16];
+  jacobi_eig4(C, ev, V);
+  int order[4] = {0, 1, 2, 3};
+  std::sort(order, order + 4, [&](int a, int b) { return ev[a] < ev[b]; });
+  const int top = order[3];
+  double m[4] = {V[0 * 4 + top], V[1 * 4 + top], V[2 * 4 + top], V[3 * 4 + top]};
+  const double nrm = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2] + m[3] * m[3]);
+  const double sg = m[0] < 0 ? -1.0 : 1.0;
+  for (int r = 0; r < 4; ++r) m[r] *= sg / nrm;
+  double esum = 0.0;
+  for (int i = 0; i < 4; ++i) esum += ev[i];
+  if (mode4) memcpy(mode4, m, sizeof(m));
+  if (omega4)
+    for (int i = 0; i < 4; ++i) omega4[i] = esum != 0.0 ? ev[order[i]] / esum : 0.0;
+  if (xyz3) quat_to_xyz(m, xyz3);
+  return PHGPU_OK;
+}
+
+int phgpu_gaussian_peak(const double* values, uint32_t first_voxel, uint32_t count, uint32_t n_voxels,
+                        int32_t lower, int32_t upper, double* mean3, double* cov9) {
+  if (!values || count == 0 || n_voxels == 0) return PHGPU_ERR_INVALID;
+  double wsum = 0.0;
+  for (uint32_t i = 0; i < count; ++i) wsum += values[i];
+  if (!(wsum > 0.0)) return PHGPU_ERR_INVALID;
+  std::vector<double> t(3 * (size_t)count);
+  double mu[3] = {0.0, 0.0, 0.0};
+  for (uint32_t i = 0; i < count; ++i) {
+    const uint32_t v = first_voxel + i, N = n_voxels;
+    // Ind2Sub(i, N, N) (signal-utils.cc:5-19)
+    const uint32_t sub[3] = {(v / N) % N, v % N, v / (N * N)};
+    const double w = values[i] / wsum;
+    for (int a = 0; a < 3; ++a) {
+      t[3 * i + a] = phgpu_translation_from_index((double)sub[a], N, lower, upper);
+      mu[a] += w * t[3 * i + a];
+    }
+  }
+  // the reference scales the centred samples by sqrt(w) (a negative weight
+  // gives NaN there, and here)
+  double cov[9] = {0.0};
+  for (uint32_t i = 0; i < count; ++i) {
+    const double sw = sqrt(values[i] / wsum);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) cov[r * 3 + c] += (sw * (t[3 * i + r] - mu[r])) * (sw * (t[3 * i + c] - mu[c]));
+  }
+  if (mean3) memcpy(mean3, mu, sizeof(mu));
+  if (cov9) memcpy(cov9, cov, sizeof(cov));
   return PHGPU_OK;
 }
 
@@ -444,10 +569,11 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   }
   CKV(dalloc(ctx, &ctx->d_spec, sizeof(float2) * 8 * H));
   CKV(dalloc(ctx, &ctx->d_cspec, sizeof(float2) * H));
-  if (prm->flags & PHGPU_FLAG_KEEP_VOLUMES) {
+  // volumes: kept on request, and needed by the peak-neighbourhood fits
+  if ((prm->flags & PHGPU_FLAG_KEEP_VOLUMES) || prm->rot_peak_neighbors > 0)
     CKV(dalloc(ctx, &ctx->d_rotvol, sizeof(float) * no * no * no));
+  if ((prm->flags & PHGPU_FLAG_KEEP_VOLUMES) || prm->trans_peak_neighbors > 0)
     CKV(dalloc(ctx, &ctx->d_transvol, sizeof(float) * nv));
-  }
   // [0] rotation argmax, [1] translation argmax, [2] kernel status bits (sticky)
   CKV(dalloc(ctx, &ctx->d_argmax, sizeof(unsigned long long) * 3));
   CK(cudaMemset(ctx->d_argmax, 0, sizeof(unsigned long long) * 3));
@@ -876,6 +1002,25 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
   out->rot_peak = float_from_order_bits((uint32_t)(rk >> 32));
   float T[12];
   phgpu_pose_from_bin(out->rot_bin, (uint32_t)ctx->bw_out, out->zyz, out->quat, out->xyz, T);
+  out->rot_omega[0] = out->rot_omega[1] = out->rot_omega[2] = 0.0;
+  out->rot_omega[3] = 1.0;
+  if (ctx->prm.rot_peak_neighbors > 0) {
+    // Bingham fit over the linear-index window of the rotation volume: the
+    // registration rotates the source by the mode (bingham-peak-based-eval.cc,
+    // sph-opt-registration.cc:58-66)
+    const uint32_t no = 2u * (uint32_t)ctx->bw_out;
+    uint32_t first = 0, cnt = 0;
+    phgpu_peak_window(out->rot_bin, no * no * no, ctx->prm.rot_peak_neighbors, &first, &cnt);
+    std::vector<float> wf(cnt);
+    CK(cudaMemcpy(wf.data(), ctx->d_rotvol + first, sizeof(float) * cnt, cudaMemcpyDeviceToHost));
+    std::vector<double> w(wf.begin(), wf.end());
+    if (phgpu_bingham_peak(w.data(), first, cnt, (uint32_t)ctx->bw_out, out->quat, out->rot_omega, out->xyz) !=
+        PHGPU_OK) {
+      ctx->err = "rotation peak neighbourhood has no positive weight";
+      return PHGPU_ERR_STATE;
+    }
+    xyz_to_transform(out->xyz, T);
+  }
   // translation of the rotated source
   CKV(phgpu_run_voxelize(ctx, 1, T, nd_sp, s0));
   {
@@ -909,5 +1054,20 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
   for (int a = 0; a < 3; ++a)
     out->trans[a] = phgpu_translation_from_index((double)xyz[a], N, ctx->prm.spatial_discretize_lower,
                                                  ctx->prm.spatial_discretize_upper);
+  for (int i = 0; i < 9; ++i) out->trans_cov[i] = 0.0;
+  if (ctx->prm.trans_peak_neighbors > 0) {
+    // Gaussian fit over the linear-index window of the translation volume:
+    // the estimate is its mean (gaussian-peak-based-eval.cc, sph-opt-registration.cc:74-88)
+    uint32_t first = 0, cnt = 0;
+    phgpu_peak_window(out->voxel, N * N * N, ctx->prm.trans_peak_neighbors, &first, &cnt);
+    std::vector<float> wf(cnt);
+    CK(cudaMemcpy(wf.data(), ctx->d_transvol + first, sizeof(float) * cnt, cudaMemcpyDeviceToHost));
+    std::vector<double> w(wf.begin(), wf.end());
+    if (phgpu_gaussian_peak(w.data(), first, cnt, N, ctx->prm.spatial_discretize_lower,
+                            ctx->prm.spatial_discretize_upper, out->trans, out->trans_cov) != PHGPU_OK) {
+      ctx->err = "translation peak neighbourhood has no positive weight sum";
+      return PHGPU_ERR_STATE;
+    }
+  }
   return PHGPU_OK;
 }

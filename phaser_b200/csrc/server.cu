@@ -46,13 +46,13 @@ struct Request {
 };
 
 using ShapeKey = std::tuple<uint32_t, uint32_t, uint32_t, int32_t, int32_t, uint32_t, uint32_t, uint32_t,
-                            float, float, uint32_t>;
+                            float, float, uint32_t, uint32_t, uint32_t>;
 
 ShapeKey key_of(const phgpu_params& p) {
   return ShapeKey(p.spherical_bandwidth, p.spherical_zero_padding, p.spatial_n_voxels,
                   p.spatial_discretize_lower, p.spatial_discretize_upper, p.n_channels, p.fusion_levels,
                   p.spherical_fusion * 2 + p.spatial_fusion, p.spatial_low_pass_lower,
-                  p.spatial_low_pass_upper, p.flags);
+                  p.spatial_low_pass_upper, p.flags, p.rot_peak_neighbors, p.trans_peak_neighbors);
 }
 
 // Device bytes of one context (upper estimate used for admission).
@@ -66,7 +66,8 @@ uint64_t estimate_bytes(const phgpu_params& p, uint32_t max_points) {
   b += 2 * 5 * nv * 4;                      // grids
   b += 9 * H * 8;                           // spec + cspec
   b += bw * bw * (bw + 1) * 4;              // Legendre table
-  if (p.flags & PHGPU_FLAG_KEEP_VOLUMES) b += 8 * bo * bo * bo * 4 + nv * 4;
+  if ((p.flags & PHGPU_FLAG_KEEP_VOLUMES) || p.rot_peak_neighbors) b += 8 * bo * bo * bo * 4;
+  if ((p.flags & PHGPU_FLAG_KEEP_VOLUMES) || p.trans_peak_neighbors) b += nv * 4;
   b += 2ull * max_points * (16 + 4 + 4 + 4 + 16 + 8 + 4 + 16) + 2ull * 32768 * 48;
   return b + (8ull << 20);
 }

@@ -46,6 +46,8 @@ class Params(C.Structure):
         ("max_points", C.c_uint32),
         ("flags", C.c_uint32),
         ("device", C.c_int32),
+        ("rot_peak_neighbors", C.c_uint32),
+        ("trans_peak_neighbors", C.c_uint32),
     ]
 
 
@@ -69,12 +71,15 @@ class Pose(C.Structure):
         ("voxel", C.c_uint32),
         ("trans_peak", C.c_float),
         ("trans", C.c_double * 3),
+        ("rot_omega", C.c_double * 4),
+        ("trans_cov", C.c_double * 9),
     ]
 
     def as_dict(self):
         return dict(rot_bin=self.rot_bin, rot_peak=self.rot_peak, zyz=list(self.zyz),
                     quat=list(self.quat), xyz=list(self.xyz), voxel=self.voxel,
-                    trans_peak=self.trans_peak, trans=list(self.trans))
+                    trans_peak=self.trans_peak, trans=list(self.trans), rot_omega=list(self.rot_omega),
+                    trans_cov=list(self.trans_cov))
 
 
 class ServerParams(C.Structure):
@@ -98,7 +103,7 @@ EXPORTED = [
     "phgpu_server_submit", "phgpu_server_poll", "phgpu_server_drain", "phgpu_server_last_error",
     "phgpu_profile_enable", "phgpu_profile_read", "phgpu_profile_stage_count",
     "phgpu_profile_stage_name", "phgpu_launch_count", "phgpu_selftest_fft",
-    "phgpu_sample_s2_noalloc",
+    "phgpu_sample_s2_noalloc", "phgpu_bingham_peak", "phgpu_gaussian_peak", "phgpu_peak_window",
 ]
 
 _LIB = None
@@ -150,6 +155,13 @@ def load(path: str = LIB_PATH):
     lib.phgpu_profile_stage_name.restype = C.c_char_p
     lib.phgpu_profile_stage_name.argtypes = [C.c_int]
     lib.phgpu_launch_count.restype = C.c_ulonglong
+    lib.phgpu_bingham_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]
+    lib.phgpu_gaussian_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int32,
+                                        C.c_void_p, C.c_void_p]
+    lib.phgpu_peak_window.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
+                                      C.POINTER(C.c_uint32)]
+    lib.phgpu_peak_window.restype = None
     lib.phgpu_selftest_fft.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
     lib.phgpu_sample_s2_noalloc.argtypes = [C.POINTER(Params), C.POINTER(Cloud), C.c_void_p, C.c_void_p,
                                             C.c_void_p]
@@ -202,6 +214,37 @@ def sample_s2_noalloc(params: Params, xyzi, reflectivity, ambient, values_dev, n
     c, keep = make_cloud(xyzi, reflectivity, ambient)
     return load().phgpu_sample_s2_noalloc(C.byref(params), C.byref(c), _addr(values_dev), _addr(nn_index_dev),
                                           None if stream is None else stream.cuda_stream)
+
+
+def peak_window(index, n, k):
+    """Linear-index window (first, count) of k neighbours around an argmax."""
+    f, c = C.c_uint32(), C.c_uint32()
+    load().phgpu_peak_window(int(index), int(n), int(k), C.byref(f), C.byref(c))
+    return f.value, c.value
+
+
+def bingham_peak(values, first_bin, bw_out):
+    """Mode quaternion (w, x, y, z), normalised scatter eigenvalues and XYZ
+    angles of the weighted bins first_bin .. first_bin + len(values) - 1."""
+    v = np.ascontiguousarray(values, np.float64)
+    mode, omega, xyz = np.zeros(4), np.zeros(4), np.zeros(3)
+    rc = load().phgpu_bingham_peak(v.ctypes.data, int(first_bin), len(v), int(bw_out), mode.ctypes.data,
+                                   omega.ctypes.data, xyz.ctypes.data)
+    if rc != PHGPU_OK:
+        raise PhgpuError(f"phgpu_bingham_peak failed ({rc})")
+    return mode, omega, xyz
+
+
+def gaussian_peak(values, first_voxel, n_voxels, lower, upper):
+    """Weighted mean and covariance (3x3) of the translations of the voxels
+    first_voxel .. first_voxel + len(values) - 1."""
+    v = np.ascontiguousarray(values, np.float64)
+    mean, cov = np.zeros(3), np.zeros(9)
+    rc = load().phgpu_gaussian_peak(v.ctypes.data, int(first_voxel), len(v), int(n_voxels), int(lower), int(upper),
+                                    mean.ctypes.data, cov.ctypes.data)
+    if rc != PHGPU_OK:
+        raise PhgpuError(f"phgpu_gaussian_peak failed ({rc})")
+    return mean, cov.reshape(3, 3)
 
 
 def selftest_fft(x: np.ndarray, inverse=False, columns=False, engine=2) -> np.ndarray:
