@@ -31,6 +31,13 @@ extern "C" {
 /* fusion modes */
 #define PHGPU_FUSION_LAPLACE 0   /* SphericalCorrelationLaplace / SpatialCorrelationLaplace */
 #define PHGPU_FUSION_NONE 1      /* SphericalCorrelation / SpatialCorrelation (channel 0) */
+/* Low-pass variants: SphericalCorrelationLowPass (spherical-correlation-low-pass.cc:14-59)
+ * correlates channel 0 keeping the B^2 coefficients whose FFT-shifted position
+ * lies in [spherical_low_pass_lower, spherical_low_pass_upper); SpatialCorrelationLowPass
+ * (spatial-correlation-low-pass.cc:40-90) correlates channel 1 keeping the
+ * products whose FFT-shifted N^3 index has all three subscripts in
+ * [spatial_low_pass_lower, min(spatial_low_pass_upper, N)]. */
+#define PHGPU_FUSION_LOW_PASS 2
 
 /* flags */
 #define PHGPU_FLAG_KEEP_VOLUMES 1u /* also keep the full correlation volumes */
@@ -56,6 +63,8 @@ typedef struct {
   int32_t device;                    /* CUDA device ordinal */
   uint32_t rot_peak_neighbors;       /* bingham_peak_neighbors (0) */
   uint32_t trans_peak_neighbors;     /* gaussian_peak_neighbors (0) */
+  uint32_t spherical_low_pass_lower; /* phaser_core_spherical_low_pass_lower_bound (0) */
+  uint32_t spherical_low_pass_upper; /* phaser_core_spherical_low_pass_upper_bound (100000) */
 } phgpu_params;
 
 /* A point cloud: x, y, z, intensity as float4 plus optional per-point

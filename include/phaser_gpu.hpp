@@ -6,6 +6,8 @@
 //   SphericalCorrelationLaplace   .../spherical-correlation-laplace.h
 //   SpatialCorrelation            .../spatial-correlation.h:15-23
 //   SpatialCorrelationLaplace     .../spatial-correlation-laplace.h
+//   SphericalCorrelationLowPass   .../spherical-correlation-low-pass.h
+//   SpatialCorrelationLowPass     .../spatial-correlation-low-pass.h
 //   PhaseAligner                  phaser_core/include/phaser/backend/alignment/phase-aligner.h:17-26
 //   SphOptRegistration            phaser_core/include/phaser/backend/registration/sph-opt-registration.h
 // so a caller swaps the include and the namespace (phaser_gpu instead of
@@ -17,6 +19,7 @@
 #define PHASER_GPU_HPP_
 
 #include <cstdint>
+#include <algorithm>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -136,6 +139,17 @@ class SphericalCorrelationLaplace : public SphericalCorrelation {
   }
 };
 
+// SphericalCorrelationLowPass(bw, zero_padding): channel 0 with the B^2
+// coefficients outside the FFT-shifted band [lower, upper) removed
+// (spherical-correlation-low-pass.cc:14-59); the band comes from
+// base.spherical_low_pass_lower / _upper (the reference's flags).
+class SphericalCorrelationLowPass : public SphericalCorrelation {
+ public:
+  explicit SphericalCorrelationLowPass(const uint32_t bw = 100, const uint32_t zero_padding = 0,
+                                       const phgpu_params& base = default_params())
+      : SphericalCorrelation(bw, zero_padding, PHGPU_FUSION_LOW_PASS, base) {}
+};
+
 // SpatialCorrelation(n_voxels, zero_padding) / SpatialCorrelationLaplace.
 // correlateSignals returns a pointer owned by the object, valid until the next
 // call (spatial-correlation.cc:128-175).
@@ -196,6 +210,42 @@ class SpatialCorrelationLaplace : public SpatialCorrelation {
       : SpatialCorrelation(n_voxels, PHGPU_FUSION_LAPLACE, base) {
     if (zero_padding != 0) throw std::invalid_argument("spatial zero padding is not supported");
   }
+};
+
+// SpatialCorrelationLowPass(n_voxels, zero_padding[, lower, upper]): channel 1
+// of the signals, products kept inside the FFT-shifted cube [lower, upper]^3
+// (spatial-correlation-low-pass.cc:11-98).  Without bounds: the reference's
+// flags, upper clipped to n_voxels.
+class SpatialCorrelationLowPass : public SpatialCorrelation {
+ public:
+  explicit SpatialCorrelationLowPass(const uint32_t n_voxels, const uint32_t zero_padding = 0,
+                                     const phgpu_params& base = default_params())
+      : SpatialCorrelationLowPass(n_voxels, zero_padding,
+                                  base.spatial_low_pass_lower > 0.f ? (uint32_t)base.spatial_low_pass_lower : 0u,
+                                  std::min<uint32_t>(base.spatial_low_pass_upper > 0.f
+                                                         ? (uint32_t)base.spatial_low_pass_upper : 0u,
+                                                     n_voxels),
+                                  base) {}
+  SpatialCorrelationLowPass(const uint32_t n_voxels, const uint32_t zero_padding, const uint32_t lower,
+                            const uint32_t upper, const phgpu_params& base = default_params())
+      : SpatialCorrelation(n_voxels, PHGPU_FUSION_LOW_PASS, with_bounds(base, lower, upper)),
+        lower_(lower), upper_(upper) {
+    if (zero_padding != 0) throw std::invalid_argument("spatial zero padding is not supported");
+  }
+  uint32_t getLowerBound() const noexcept { return lower_; }
+  uint32_t getUpperBound() const noexcept { return upper_; }
+  uint32_t getNumberOfIndices() const noexcept {
+    const uint32_t w = upper_ >= lower_ ? upper_ - lower_ + 1 : 0;
+    return w * w * w;
+  }
+
+ private:
+  static phgpu_params with_bounds(phgpu_params p, uint32_t lower, uint32_t upper) {
+    p.spatial_low_pass_lower = (float)lower;
+    p.spatial_low_pass_upper = (float)upper;
+    return p;
+  }
+  uint32_t lower_, upper_;
 };
 
 // A cloud as the aligner and registration see it: x, y, z, intensity per

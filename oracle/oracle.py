@@ -95,6 +95,9 @@ def _declare(lib):
     lib.orc_register_pair_k.argtypes = [_f32p, C.c_size_t, C.c_void_p, _f32p, C.c_size_t, C.c_void_p,
                                         C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint32, C.c_uint32,
                                         C.POINTER(Pose), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.orc_spherical_correlation_lowpass.argtypes = [C.c_int, C.c_int, _f64p, _f64p, C.c_uint32, C.c_uint32,
+                                                      _f64p]
+    lib.orc_spatial_correlation_lowpass.argtypes = [C.c_int, _f64p, _f64p, C.c_uint32, C.c_uint32, _f64p]
     lib.orc_peak_window.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
                                     C.POINTER(C.c_uint32)]
     lib.orc_bingham_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
@@ -330,6 +333,25 @@ def spatial_correlation(f, g, N, laplace=True, levels=5):
     Cn = f.shape[0] if f.ndim == 2 else 1
     out = np.zeros(N ** 3)
     lib().orc_spatial_correlation(N, Cn, f.reshape(-1), g.reshape(-1), 1 if laplace else 0, levels, out)
+    return out
+
+
+def spherical_correlation_lowpass(f0, g0, bw, lower, upper, bw_out=None):
+    """Low-pass spherical correlation of channel 0 (|z|^2, (2 bw_out)^3)."""
+    bw_out = bw if bw_out is None else bw_out
+    corr = np.zeros((2 * bw_out) ** 3)
+    lib().orc_spherical_correlation_lowpass(bw, bw_out, np.ascontiguousarray(f0, np.float64).reshape(-1),
+                                            np.ascontiguousarray(g0, np.float64).reshape(-1), int(lower), int(upper),
+                                            corr)
+    return corr
+
+
+def spatial_correlation_lowpass(f1, g1, N, lower, upper):
+    """Low-pass spatial correlation of channel 1 grids (N^3 each)."""
+    out = np.zeros(N ** 3)
+    lib().orc_spatial_correlation_lowpass(N, np.ascontiguousarray(f1, np.float64).reshape(-1),
+                                          np.ascontiguousarray(g1, np.float64).reshape(-1), int(lower), int(upper),
+                                          out)
     return out
 
 

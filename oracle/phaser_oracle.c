@@ -1031,6 +1031,97 @@ void orc_spatial_correlation(int N, int C, const double* f, const double* g,
   free(vg);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Low-pass variants, restated literally with the reference's shifts.        */
+/* ------------------------------------------------------------------------ */
+
+/* SignalUtils::FFTShift / IFFTShift (signal-utils.h:29-47): std::rotate.   */
+static void orc_rotate_left(cplx* a, size_t n, size_t s) {
+  if (n == 0 || s % n == 0) return;
+  s %= n;
+  cplx* t = (cplx*)malloc(sizeof(cplx) * n);
+  for (size_t i = 0; i < n; ++i) t[i] = a[(i + s) % n];
+  memcpy(a, t, sizeof(cplx) * n);
+  free(t);
+}
+static void orc_fftshift_c(cplx* a, size_t n) { orc_rotate_left(a, n, (n % 2 == 0) ? (n >> 1) : (n >> 1) + 1); }
+static void orc_ifftshift_c(cplx* a, size_t n) { orc_rotate_left(a, n, n >> 1); }
+
+/* SphericalCorrelationLowPass::correlateSampledSignals (spherical-          */
+/* correlation-low-pass.cc:14-59): channel 0, coefficients shifted, zeroed   */
+/* outside [lower, upper) (both clipped to B^2), shifted back, correlated.   */
+void orc_spherical_correlation_lowpass(int bw, int bw_out, const double* f, const double* g, uint32_t lower,
+                                       uint32_t upper, double* corr) {
+  const size_t nc = (size_t)bw * bw;
+  double *fr = (double*)malloc(sizeof(double) * nc), *fi = (double*)malloc(sizeof(double) * nc);
+  double *gr = (double*)malloc(sizeof(double) * nc), *gi = (double*)malloc(sizeof(double) * nc);
+  orc_sht(f, bw, fr, fi);
+  orc_sht(g, bw, gr, gi);
+  cplx* F = (cplx*)malloc(sizeof(cplx) * nc);
+  cplx* G = (cplx*)malloc(sizeof(cplx) * nc);
+  for (size_t k = 0; k < nc; ++k) {
+    F[k].re = fr[k];
+    F[k].im = fi[k];
+    G[k].re = gr[k];
+    G[k].im = gi[k];
+  }
+  const size_t lo = lower < nc ? lower : nc, hi = upper < nc ? upper : nc;
+  orc_fftshift_c(F, nc);
+  orc_fftshift_c(G, nc);
+  for (size_t i = 0; i < lo; ++i) F[i].re = F[i].im = G[i].re = G[i].im = 0.0;
+  for (size_t i = hi; i < nc; ++i) F[i].re = F[i].im = G[i].re = G[i].im = 0.0;
+  orc_ifftshift_c(F, nc);
+  orc_ifftshift_c(G, nc);
+  for (size_t k = 0; k < nc; ++k) {
+    fr[k] = F[k].re;
+    fi[k] = F[k].im;
+    gr[k] = G[k].re;
+    gi[k] = G[k].im;
+  }
+  const int n = 2 * bw_out;
+  const size_t nv = (size_t)n * n * n;
+  double* vol = (double*)malloc(sizeof(double) * 2 * nv);
+  orc_so3_correlate(bw, bw_out, fr, fi, gr, gi, vol);
+  for (size_t i = 0; i < nv; ++i) corr[i] = vol[2 * i] * vol[2 * i] + vol[2 * i + 1] * vol[2 * i + 1];
+  free(vol);
+  free(fr);
+  free(fi);
+  free(gr);
+  free(gi);
+  free(F);
+  free(G);
+}
+
+/* SpatialCorrelationLowPass::correlateSignals (spatial-correlation-low-     */
+/* pass.cc:40-90): channel 1; the N^3-long half-spectrum buffers are         */
+/* FFT-shifted, the product is formed at Sub2Ind(i, j, k) for i, j, k in     */
+/* [lower, upper] (indices beyond N^3, where the reference's CHECK aborts,   */
+/* are skipped; the product buffer starts at zero), shifted back, inverted.  */
+void orc_spatial_correlation_lowpass(int N, const double* f1, const double* g1, uint32_t lower, uint32_t upper,
+                                     double* out) {
+  const size_t nv = (size_t)N * N * N;
+  cplx* F = (cplx*)calloc(nv, sizeof(cplx));
+  cplx* G = (cplx*)calloc(nv, sizeof(cplx));
+  r2c3d(f1, N, F);
+  r2c3d(g1, N, G);
+  orc_fftshift_c(F, nv);
+  orc_fftshift_c(G, nv);
+  cplx* Cc = (cplx*)calloc(nv, sizeof(cplx));
+  for (uint32_t i = lower; i <= upper; ++i)
+    for (uint32_t j = lower; j <= upper; ++j)
+      for (uint32_t k = lower; k <= upper; ++k) {
+        const uint64_t idx = (uint64_t)(i * (uint32_t)N + j) + (uint64_t)N * N * k;
+        if (idx >= nv) continue;
+        Cc[idx].re = F[idx].re * G[idx].re - F[idx].im * (-G[idx].im);
+        Cc[idx].im = F[idx].re * (-G[idx].im) + F[idx].im * G[idx].re;
+      }
+  orc_ifftshift_c(Cc, nv);
+  c2r3d(Cc, N, out);
+  free(F);
+  free(G);
+  free(Cc);
+}
+
 /* ComputeTranslationFromIndex (translation-utils.cc:40-52). */
 double orc_translation_from_index(double index, uint32_t n_voxels, int lo,
                                   int hi) {

@@ -7,6 +7,8 @@ follow the reference:
   SphericalCorrelationLaplace .../spherical-correlation-laplace.h
   SpatialCorrelation          .../spatial-correlation.h:15-23
   SpatialCorrelationLaplace   .../spatial-correlation-laplace.h
+  SphericalCorrelationLowPass .../spherical-correlation-low-pass.h
+  SpatialCorrelationLowPass   .../spatial-correlation-low-pass.h
   PhaseAligner                phaser_core/include/phaser/backend/alignment/phase-aligner.h:17-26
   SphOptRegistration          phaser_core/include/phaser/backend/registration/sph-opt-registration.h
 
@@ -83,6 +85,21 @@ class SphericalCorrelationLaplace(SphericalCorrelation):
         super().correlateSampledSignals(f, g)
 
 
+class SphericalCorrelationLowPass(SphericalCorrelation):
+    """SphericalCorrelationLowPass(bw, zero_padding): channel 0, coefficients
+    outside the FFT-shifted band [lower, upper) removed
+    (spherical-correlation-low-pass.cc:14-59)."""
+    _fusion = native.PHGPU_FUSION_LOW_PASS
+
+    def __init__(self, bw: int = 100, zero_padding: int = 0, lower: int = 0, upper: int = 100000):
+        self._bw = int(bw)
+        self._bw_out = int(bw) + int(zero_padding)
+        self._ctx = Context(spherical_bandwidth=self._bw, spherical_zero_padding=int(zero_padding),
+                            spatial_n_voxels=4, spherical_fusion=self._fusion, spherical_low_pass_lower=int(lower),
+                            spherical_low_pass_upper=int(upper), flags=native.PHGPU_FLAG_KEEP_VOLUMES)
+        self._have = False
+
+
 class SpatialCorrelation:
     """SpatialCorrelation(n_voxels, zero_padding).correlateSignals(f, g) -> N^3
     correlation (spatial-correlation.cc:128-175)."""
@@ -109,6 +126,31 @@ class SpatialCorrelation:
 
 class SpatialCorrelationLaplace(SpatialCorrelation):
     _fusion = native.PHGPU_FUSION_LAPLACE
+
+
+class SpatialCorrelationLowPass(SpatialCorrelation):
+    """SpatialCorrelationLowPass(n_voxels, zero_padding[, lower, upper]):
+    channel 1 of the signals, products kept inside the FFT-shifted cube
+    [lower, upper]^3 (spatial-correlation-low-pass.cc:11-98)."""
+    _fusion = native.PHGPU_FUSION_LOW_PASS
+
+    def __init__(self, n_voxels: int, zero_padding: int = 0, lower: int = 0, upper: int = 100000):
+        if zero_padding:
+            raise ValueError("spatial zero padding is not supported")
+        self._n = int(n_voxels)
+        self._lower, self._upper = int(lower), min(int(upper), self._n)
+        self._ctx = Context(spherical_bandwidth=2, spatial_n_voxels=self._n, spatial_fusion=self._fusion,
+                            spatial_low_pass_lower=float(self._lower), spatial_low_pass_upper=float(self._upper),
+                            flags=native.PHGPU_FLAG_KEEP_VOLUMES)
+
+    def getLowerBound(self) -> int:
+        return self._lower
+
+    def getUpperBound(self) -> int:
+        return self._upper
+
+    def getNumberOfIndices(self) -> int:
+        return max(0, self._upper - self._lower + 1) ** 3
 
 
 class PhaseAligner:

@@ -394,6 +394,10 @@ int phgpu_params_default(phgpu_params* p) {
   p->max_points = 1u << 18;
   p->flags = 0;
   p->device = 0;
+  p->rot_peak_neighbors = 0;
+  p->trans_peak_neighbors = 0;
+  p->spherical_low_pass_lower = 0;
+  p->spherical_low_pass_upper = 100000;
   return PHGPU_OK;
 }
 
@@ -456,10 +460,11 @@ int phgpu_ctx_create(const phgpu_params* prm, phgpu_ctx** out) {
   const int N = (int)prm->spatial_n_voxels;
   if (bw < 2 || bw > 512 || N < 1 || N > 1024 || prm->spatial_zero_padding != 0 ||
       prm->n_channels < 1 || prm->n_channels > 4 || prm->fusion_levels < 1 ||
-      prm->fusion_levels > (uint32_t)kMaxLevels) {
+      prm->fusion_levels > (uint32_t)kMaxLevels || prm->spherical_fusion > PHGPU_FUSION_LOW_PASS ||
+      prm->spatial_fusion > PHGPU_FUSION_LOW_PASS) {
     g_create_error =
         "unsupported configuration (2 <= bandwidth <= 512, 1 <= n_voxels <= 1024, spatial zero "
-        "padding 0, 1..4 channels, 1..8 fusion levels)";
+        "padding 0, 1..4 channels, 1..8 fusion levels, fusion mode 0..2)";
     return PHGPU_ERR_INVALID;
   }
   phgpu_ctx* ctx = new phgpu_ctx();
@@ -697,6 +702,9 @@ int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStre
   }
   FuseS2Args f;
   f.bw = bw;
+  f.lowpass = (!laplace && ctx->prm.spherical_fusion == PHGPU_FUSION_LOW_PASS) ? 1 : 0;
+  f.lp_lo = std::min<uint32_t>(ctx->prm.spherical_low_pass_lower, (uint32_t)(bw * bw));
+  f.lp_hi = std::min<uint32_t>(ctx->prm.spherical_low_pass_upper, (uint32_t)(bw * bw));
   f.n_data_ch = n_data;
   f.n_total_ch = n_total;
   f.laplace = laplace;
@@ -861,6 +869,11 @@ static SpatialArgs spatial_args(phgpu_ctx* ctx, int n_data, int n_total, int lap
   a.n_data_ch = n_data;
   a.n_total_ch = n_total;
   a.laplace = laplace;
+  a.lowpass = (!laplace && ctx->prm.spatial_fusion == PHGPU_FUSION_LOW_PASS) ? 1 : 0;
+  // the low-pass cube: [lower, min(upper, N)] (spatial-correlation-low-pass.cc:11-19)
+  a.lp_lo = ctx->prm.spatial_low_pass_lower > 0.f ? (uint32_t)ctx->prm.spatial_low_pass_lower : 0u;
+  a.lp_hi = std::min<uint32_t>(ctx->prm.spatial_low_pass_upper > 0.f ? (uint32_t)ctx->prm.spatial_low_pass_upper : 0u,
+                               (uint32_t)ctx->N);
   a.bands = ctx->bands_sp;
   a.grids_f = ctx->d_grids[0];
   a.grids_g = ctx->d_grids[1];
@@ -903,6 +916,10 @@ int phgpu_run_spatial(phgpu_ctx* ctx, int n_data, int n_total, int laplace, int 
 int phgpu_spatial_correlate(phgpu_ctx* ctx, const double* const* f, const double* const* g, uint32_t C) {
   if (!ctx || !f || !g || C < 1 || C > 4) {
     if (ctx) ctx->err = "phgpu_spatial_correlate: 1..4 channels required";
+    return PHGPU_ERR_INVALID;
+  }
+  if (ctx->prm.spatial_fusion == PHGPU_FUSION_LOW_PASS && C < 2) {
+    ctx->err = "the low-pass spatial correlation uses channel 1: at least 2 channels required";
     return PHGPU_ERR_INVALID;
   }
   cudaSetDevice(ctx->prm.device);

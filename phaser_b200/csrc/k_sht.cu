@@ -190,10 +190,9 @@ __global__ void k_fuse_s2(FuseS2Args a) {
   if (m > l || -m > l) return;
   const uint32_t n = (uint32_t)(bw * bw);
   int op = kFuseMax;
-  if (a.laplace) {
-    const uint32_t p = ((uint32_t)sean_index(m, l, bw) + (n >> 1)) % n;
-    op = fusion_op(p, a.bands);
-  }
+  const uint32_t p = ((uint32_t)sean_index(m, l, bw) + (n >> 1)) % n;  // position after FFTShift
+  if (a.laplace) op = fusion_op(p, a.bands);
+  const bool dropped = a.lowpass && (p < a.lp_lo || p >= a.lp_hi);
   for (int side = 0; side < 2; ++side) {
     const float2* base = a.coef + (size_t)side * a.n_data_ch * bw * bw;
     float2 r = make_float2(0.f, 0.f);
@@ -218,6 +217,7 @@ __global__ void k_fuse_s2(FuseS2Args a) {
         }
       }
     }
+    if (dropped) r = make_float2(0.f, 0.f);
     a.fused[((size_t)side * bw + l) * w + mi] = r;
   }
 }

@@ -281,8 +281,9 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
     const int half = Wt >> 1;
     for (int e = threadIdx.x; e < N * A * half; e += blockDim.x) {
       const int z = e / (A * half), rem = e - z * (A * half), ar = rem / half, t2 = rem - ar * half;
-      // arrays: f channels 0..C-1 then g channels; plain mode uses channel 0 of each side
-      const int src = a.laplace ? ar : (ar == 0 ? 0 : C);
+      // arrays: f channels 0..C-1 then g channels; plain mode uses channel 0 of
+      // each side, the low-pass mode channel 1
+      const int src = a.laplace ? ar : (ar == 0 ? a.lowpass : C + a.lowpass);
       const float4 v = *reinterpret_cast<const float4*>(
           a.spec + (size_t)src * plane + ((size_t)z * N + xp) * H2p + ky0 + 2 * t2);
       float2* d = tile + (size_t)z * rowlen + ar * Wt + 2 * t2;
@@ -304,6 +305,20 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
     if (!a.laplace) {
       F = row[t];
       G = row[Wt + t];
+      if (a.lowpass) {
+        // keep the products whose FFT-shifted index p = (i N + j) + N^2 k has
+        // i, j, k in [lp_lo, lp_hi]
+        const int kz = s_kz[zp];
+        const uint32_t klin = ((uint32_t)kz * N + (uint32_t)kx) * (uint32_t)H2 + (uint32_t)(ky0 + t);
+        uint32_t p = klin + (nv >> 1);
+        if (p >= nv || p < klin) p -= nv;
+        const uint32_t n2 = (uint32_t)N * (uint32_t)N, kk = p / n2, rem = p - kk * n2;
+        const uint32_t ii = rem / (uint32_t)N, jj = rem - ii * (uint32_t)N;
+        if (ii < a.lp_lo || ii > a.lp_hi || jj < a.lp_lo || jj > a.lp_hi || kk < a.lp_lo || kk > a.lp_hi) {
+          F = make_float2(0.f, 0.f);
+          G = F;
+        }
+      }
     } else {
       const int kz = s_kz[zp];
       const uint32_t klin = ((uint32_t)kz * N + (uint32_t)kx) * (uint32_t)H2 + (uint32_t)(ky0 + t);
@@ -636,7 +651,7 @@ cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t 
   const size_t nv = (size_t)N * N * N;
   const size_t plane = (size_t)N * N * spatial_h2p(N);
   const float* grids = side == 0 ? a.grids_f : a.grids_g;
-  const int nch = a.laplace ? a.n_data_ch : 1;
+  const int nch = a.laplace ? a.n_data_ch : (a.lowpass ? 2 : 1);
   const float* count = a.grids_are_means ? nullptr : grids + (size_t)a.n_data_ch * nv;
   if (spatial_slab_path(N) && a.plan_half) {
     float2* spec = a.spec + (size_t)(side * a.n_data_ch) * plane;
@@ -681,7 +696,8 @@ cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st) {
                                    (cuuint64_t)N * spatial_h2p(N) * sizeof(float2)};
     const cuuint32_t box[4] = {(cuuint32_t)wt, (cuuint32_t)A, 1u, (cuuint32_t)zbox};
     const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
-    if (enc(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void*)a.spec, dims, strides, box, estr,
+    void* base = (void*)(a.spec + (a.laplace ? 0 : (size_t)a.lowpass * plane));
+    if (enc(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
       tma = FuseZTma{1, zbox, chunks};

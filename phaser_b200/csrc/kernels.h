@@ -56,6 +56,8 @@ struct FuseS2Args {
   int n_data_ch;          // channels with data per side
   int n_total_ch;         // divisor of the channel mean (reference channel count)
   int laplace;            // 0: take channel 0 (plain SphericalCorrelation)
+  int lowpass;            // 1: channel 0, coefficients at shifted positions outside [lp_lo, lp_hi) zeroed
+  uint32_t lp_lo, lp_hi;
   FusionBands bands;      // for n = B^2
   const float2* coef;     // [2][n_data_ch][B][B]   (side-major)
   float2* fused;          // [2][B (l)][2B-1 (m + B - 1)]
@@ -104,6 +106,8 @@ struct SpatialArgs {
   int n_data_ch;          // channels per side with data
   int n_total_ch;         // mean divisor
   int laplace;            // 0: plain SpatialCorrelation on channel 0
+  int lowpass;            // 1 (with laplace 0): channel 1, products outside the shifted cube zeroed
+  uint32_t lp_lo, lp_hi;  // cube [lp_lo, lp_hi]^3 of subscripts
   FusionBands bands;      // for n = N^3
   const float* grids_f;   // [n_data_ch + 1][N^3] target sums + count (normalised here)
   const float* grids_g;   // source

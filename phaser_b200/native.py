@@ -21,6 +21,7 @@ NOALLOC_MAX_POINTS = 1 << 18
 NOALLOC_MAX_BANDWIDTH = 128
 PHGPU_FUSION_LAPLACE = 0
 PHGPU_FUSION_NONE = 1
+PHGPU_FUSION_LOW_PASS = 2
 PHGPU_FLAG_KEEP_VOLUMES = 1
 PHGPU_SERVER_BORROW_HOST = 1
 
@@ -48,6 +49,8 @@ class Params(C.Structure):
         ("device", C.c_int32),
         ("rot_peak_neighbors", C.c_uint32),
         ("trans_peak_neighbors", C.c_uint32),
+        ("spherical_low_pass_lower", C.c_uint32),
+        ("spherical_low_pass_upper", C.c_uint32),
     ]
 
 
