@@ -237,6 +237,51 @@ unsigned long long phgpu_launch_count(void);
  * exp(-2 pi i jk/n), inverse = exp(+2 pi i jk/n), both unnormalised. */
 int phgpu_selftest_fft(int n, int ntrans, int inverse, int columns, int engine, float* data);
 
+/* ------------------------------------------------------------------ ingest
+ * PLY reading (replaces data::PlyHelper::readPlyFromFile +
+ * PointCloud::parsePlyPointCloud, phaser_common/src/common/data/
+ * ply-helper.cc:26-64, phaser_common/src/model/point-cloud.cc:313-348).
+ * field_names: the intensity, reflectivity, ambient and range property names
+ * (the reference's --phaser_ply_*_str flags); NULL, or a NULL entry, selects
+ * the defaults "intensity", "reflectivity", "noise", "range".  x, y, z and
+ * intensity are required (PHGPU_ERR_INVALID otherwise, where the reference
+ * aborts).  Host only; the outputs are typically pinned for the upload. */
+#define PHGPU_PLY_REFLECTIVITY 1u
+#define PHGPU_PLY_AMBIENT 2u
+#define PHGPU_PLY_RANGE 4u
+/* Vertex count and which optional fields exist (PHGPU_PLY_* bits). */
+int phgpu_ply_info(const char* path, const char* const* field_names, uint32_t* n_points, uint32_t* present);
+/* x, y, z, intensity into xyzi (4 floats per point); the optional fields into
+ * their arrays when non-NULL and present (left untouched when absent).
+ * PHGPU_ERR_LIMIT when the file holds more than `capacity` vertices. */
+int phgpu_ply_read(const char* path, const char* const* field_names, float* xyzi, float* reflectivity,
+                   float* ambient, float* range, uint32_t capacity, uint32_t* n_points);
+/* Message of the last failed phgpu_ply_* call on this thread. */
+const char* phgpu_ply_last_error(void);
+
+/* Voxel-grid downsampling on the GPU (replaces preproc::VoxelGridCmd,
+ * phaser_pre/src/commands/voxel-grid-cmd.cc:11-22, i.e. pcl::VoxelGrid with
+ * downsample_all_data on PointXYZI).  Each occupied leaf of the grid
+ * anchored at floor(min / leaf) becomes one point, the float mean of x, y, z
+ * and intensity of its points; leaves come out in increasing leaf index
+ * (x fastest, then y, then z) and points inside a leaf are summed in input
+ * order.  Points with a non-finite coordinate are dropped.  When the leaf
+ * count would overflow int32 the input is returned unchanged (as the
+ * reference does).  Reflectivity and ambient, when given, are averaged over the
+ * same leaves (the reference leaves them unfiltered). */
+typedef struct phgpu_voxel_grid phgpu_voxel_grid;
+int phgpu_voxel_grid_create(uint32_t max_points, int32_t device, phgpu_voxel_grid** out);
+int phgpu_voxel_grid_destroy(phgpu_voxel_grid* vg);
+/* leaf: x, y, z leaf sizes (> 0); min_points_per_voxel: leaves with fewer
+ * points are dropped (pcl::VoxelGrid::setMinimumPointsNumberPerVoxel, 0 by
+ * default).  The outputs hold in->n_points entries at least; out_on_device
+ * says whether they are device (1) or host (0) memory.  Synchronises the
+ * filter's stream before returning *n_out. */
+int phgpu_voxel_grid_filter(phgpu_voxel_grid* vg, const phgpu_cloud* in, const float leaf[3],
+                            uint32_t min_points_per_voxel, float* out_xyzi, float* out_reflectivity,
+                            float* out_ambient, int out_on_device, uint32_t* n_out);
+const char* phgpu_voxel_grid_last_error(const phgpu_voxel_grid* vg);
+
 /* ------------------------------------------------------------------ serving
  * Continuous-batching request server (no reference counterpart: the
  * reference registers one pair at a time, sph-opt-registration.cc:34-47).

@@ -102,6 +102,9 @@ def _declare(lib):
                                     C.POINTER(C.c_uint32)]
     lib.orc_bingham_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
                                      C.c_void_p]
+    lib.orc_voxel_grid.restype = C.c_int64
+    lib.orc_voxel_grid.argtypes = [_f32p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_float, C.c_float, C.c_float,
+                                   C.c_uint32, _f32p, C.c_void_p, C.c_void_p]
     lib.orc_gaussian_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
                                       C.c_void_p, C.c_void_p]
     lib.orc_num_threads.restype = C.c_int
@@ -454,3 +457,22 @@ def ref_register_pair(tgt, tgt_refl, src, src_refl, bw, N, lo, hi, max_sq=1e6, t
                                 src.shape[0], _ptr(sr), bw, N, lo, hi, max_sq, threads,
                                 C.byref(rb), C.byref(vx), pose6)
     return rb.value, vx.value, pose6
+
+
+def voxel_grid(xyzi, leaf=(0.25, 0.25, 0.25), min_points=0, refl=None, amb=None):
+    """pcl::VoxelGrid<PointXYZI> restated in float (orc_voxel_grid): leaf
+    centroids (xyzi, refl, amb) in increasing leaf order; None where the
+    grid leaves PCL's defined int range."""
+    x = np.ascontiguousarray(xyzi, np.float32).reshape(-1, 4)
+    n = x.shape[0]
+    r = None if refl is None else np.ascontiguousarray(refl, np.float32)
+    a = None if amb is None else np.ascontiguousarray(amb, np.float32)
+    out = np.zeros((max(n, 1), 4), np.float32)
+    orf = np.zeros(max(n, 1), np.float32) if r is not None else None
+    oam = np.zeros(max(n, 1), np.float32) if a is not None else None
+    lf = np.broadcast_to(np.asarray(leaf, np.float32), (3,))
+    k = lib().orc_voxel_grid(x, _ptr(r), _ptr(a), n, float(lf[0]), float(lf[1]), float(lf[2]), int(min_points),
+                             out, _ptr(orf), _ptr(oam))
+    if k < 0:
+        return None
+    return out[:k], None if orf is None else orf[:k], None if oam is None else oam[:k]

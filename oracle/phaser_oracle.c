@@ -1352,3 +1352,115 @@ int orc_num_threads(void) {
   return 1;
 #endif
 }
+
+/* ---------------------------------------------------------------- ingest
+ * Voxel-grid downsampling: pcl::VoxelGrid<pcl::PointXYZI>::applyFilter
+ * (PCL 1.8.1, absent from the reference tree; called by
+ * phaser_pre/src/commands/voxel-grid-cmd.cc:11-22 with leaf
+ * --phaser_voxel_grid_leaf_size) restated from PCL's published algorithm in
+ * float arithmetic:
+ *   bounds of x, y, z over finite points; inv = 1/leaf;
+ *   d = int64((max - min) * inv) + 1, output = input when dx*dy*dz > INT32_MAX;
+ *   min_b = int(floor(min * inv)), div_b = int(floor(max * inv)) - min_b + 1;
+ *   leaf = sum_a int(floor(p_a * inv_a) - float(min_b_a)) * (1, div_x, div_x*div_y)_a;
+ *   sort by leaf (stable here: PCL's std::sort leaves the order inside a leaf
+ *   unspecified), float sums of x, y, z, intensity in that order, / float(count);
+ *   leaves with fewer than min_pts points dropped.
+ * Returns the output count, or -1 where PCL's int arithmetic is undefined
+ * (floor(coordinate / leaf) outside int32, more than 2^30 leaves along an
+ * axis, or more than 2^32 - 1 cells).  Non-finite points are dropped. */
+typedef struct {
+  uint32_t key, idx;
+} orc_leaf_pt;
+
+static int orc_cmp_leaf_pt(const void* a, const void* b) {
+  const orc_leaf_pt* x = (const orc_leaf_pt*)a;
+  const orc_leaf_pt* y = (const orc_leaf_pt*)b;
+  if (x->key != y->key) return x->key < y->key ? -1 : 1;
+  return x->idx < y->idx ? -1 : (x->idx > y->idx);
+}
+
+int64_t orc_voxel_grid(const float* xyzi, const float* refl, const float* amb, size_t n, float lx, float ly,
+                       float lz, uint32_t min_pts, float* out, float* out_refl, float* out_amb) {
+  const float inv[3] = {1.0f / lx, 1.0f / ly, 1.0f / lz};
+  float mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
+  size_t n_fin = 0;
+  for (size_t i = 0; i < n; ++i) {
+    const float* p = xyzi + 4 * i;
+    if (!isfinite(p[0]) || !isfinite(p[1]) || !isfinite(p[2])) continue;
+    for (int a = 0; a < 3; ++a) {
+      if (n_fin == 0 || p[a] < mn[a]) mn[a] = p[a];
+      if (n_fin == 0 || p[a] > mx[a]) mx[a] = p[a];
+    }
+    ++n_fin;
+  }
+  if (n_fin == 0) return 0;
+  int overflow = 0, range = 0;
+  long long d[3], div[3];
+  int32_t min_b[3];
+  for (int a = 0; a < 3; ++a) {
+    const float ext = (mx[a] - mn[a]) * inv[a];
+    if (!(ext < 4.0e18f)) {
+      overflow = 1;
+      d[a] = 0;
+    } else {
+      d[a] = (long long)ext + 1;
+    }
+    const float fl = floorf(mn[a] * inv[a]), fh = floorf(mx[a] * inv[a]);
+    if (!(fl >= -2147483648.0f && fh < 2147483648.0f)) range = 1;
+    min_b[a] = range ? 0 : (int32_t)fl;
+    div[a] = range ? 1 : (long long)(int32_t)fh - (long long)(int32_t)fl + 1;
+    if (div[a] > (1ll << 30)) range = 1;
+  }
+  if (!overflow) {
+    if (d[0] > 2147483647ll || d[1] > 2147483647ll || d[2] > 2147483647ll) overflow = 1;
+    else if (d[0] * d[1] > 2147483647ll) overflow = 1;
+    else overflow = d[0] * d[1] * d[2] > 2147483647ll;
+  }
+  if (overflow) {
+    memcpy(out, xyzi, sizeof(float) * 4 * n);
+    if (refl && out_refl) memcpy(out_refl, refl, sizeof(float) * n);
+    if (amb && out_amb) memcpy(out_amb, amb, sizeof(float) * n);
+    return (int64_t)n;
+  }
+  if (range || (unsigned long long)div[0] * (unsigned long long)div[1] * (unsigned long long)div[2] > 0xffffffffull)
+    return -1;
+  const uint32_t mul[3] = {1u, (uint32_t)div[0], (uint32_t)div[0] * (uint32_t)div[1]};
+  orc_leaf_pt* v = (orc_leaf_pt*)malloc(sizeof(orc_leaf_pt) * (n_fin ? n_fin : 1));
+  size_t m = 0;
+  for (size_t i = 0; i < n; ++i) {
+    const float* p = xyzi + 4 * i;
+    if (!isfinite(p[0]) || !isfinite(p[1]) || !isfinite(p[2])) continue;
+    uint32_t key = 0;
+    for (int a = 0; a < 3; ++a) {
+      const int32_t ijk = (int32_t)(floorf(p[a] * inv[a]) - (float)min_b[a]);
+      key += (uint32_t)ijk * mul[a];
+    }
+    v[m].key = key;
+    v[m].idx = (uint32_t)i;
+    ++m;
+  }
+  qsort(v, m, sizeof(orc_leaf_pt), orc_cmp_leaf_pt);
+  int64_t k = 0;
+  for (size_t b = 0; b < m;) {
+    size_t e = b + 1;
+    while (e < m && v[e].key == v[b].key) ++e;
+    if (e - b >= min_pts) {
+      float s[6] = {0, 0, 0, 0, 0, 0};
+      for (size_t j = b; j < e; ++j) {
+        const float* p = xyzi + 4 * (size_t)v[j].idx;
+        for (int c = 0; c < 4; ++c) s[c] += p[c];
+        if (refl) s[4] += refl[v[j].idx];
+        if (amb) s[5] += amb[v[j].idx];
+      }
+      const float cnt = (float)(uint32_t)(e - b);
+      for (int c = 0; c < 4; ++c) out[4 * k + c] = s[c] / cnt;
+      if (refl && out_refl) out_refl[k] = s[4] / cnt;
+      if (amb && out_amb) out_amb[k] = s[5] / cnt;
+      ++k;
+    }
+    b = e;
+  }
+  free(v);
+  return k;
+}

@@ -11,6 +11,8 @@ follow the reference:
   SpatialCorrelationLowPass   .../spatial-correlation-low-pass.h
   PhaseAligner                phaser_core/include/phaser/backend/alignment/phase-aligner.h:17-26
   SphOptRegistration          phaser_core/include/phaser/backend/registration/sph-opt-registration.h
+  PlyHelper / PlyPointCloud   phaser_common/include/phaser/common/data/ply-helper.h, model/ply-point-cloud.h
+  VoxelGridCmd                phaser_pre/include/phaser_pre/commands/voxel-grid-cmd.h
 
 Everything runs on the GPU through libphaser_gpu.so; there is no CPU fallback.
 """
@@ -190,3 +192,68 @@ class SphOptRegistration:
 
     def registerPointCloud(self, cloud_prev, cloud_cur) -> dict:
         return self._ctx.register_pair(cloud_prev, cloud_cur).as_dict()
+
+
+class PlyPointCloud:
+    """The fields PlyHelper reads (phaser_common/src/common/data/
+    ply-helper.cc:26-64), as float32 arrays (the reference keeps doubles and
+    narrows x, y, z, intensity to float when building the cloud)."""
+
+    def __init__(self, xyzi, reflectivity=None, ambient=None, range_=None):
+        self.xyzi, self.reflectivity, self.ambient, self.range = xyzi, reflectivity, ambient, range_
+
+    def getXYZPoints(self):
+        return self.xyzi[:, :3]
+
+    def getIntentsities(self):
+        return self.xyzi[:, 3]
+
+    def getReflectivities(self):
+        return self.reflectivity
+
+    def getAmbientPoints(self):
+        return self.ambient
+
+    def getRange(self):
+        return self.range
+
+    def cloud(self):
+        """(xyzi, reflectivity, ambient): the tuple the registration takes."""
+        return self.xyzi, self.reflectivity, self.ambient
+
+
+class PlyHelper:
+    """PlyHelper::readPlyFromFile; field names default to the reference's
+    --phaser_ply_{intensity,reflectivity,ambient,range}_str flags."""
+
+    def __init__(self, intensity="intensity", reflectivity="reflectivity", ambient="noise", range_="range"):
+        self._names = [intensity, reflectivity, ambient, range_]
+
+    def readPlyFromFile(self, filename, pinned=False) -> PlyPointCloud:
+        d = native.ply_read(filename, self._names, pinned=pinned)
+        return PlyPointCloud(d["xyzi"], d["reflectivity"], d["ambient"], d["range"])
+
+
+class VoxelGridCmd:
+    """VoxelGridCmd::execute (phaser_pre/src/commands/voxel-grid-cmd.cc:11-22):
+    pcl::VoxelGrid with leaf --phaser_voxel_grid_leaf_size (0.25) on the GPU.
+    execute(cloud) returns the filtered (xyzi, reflectivity, ambient) tuple
+    (the reference filters its cloud in place)."""
+
+    def __init__(self, leaf_size=0.25, max_points=1 << 20, device=0, min_points_per_voxel=0):
+        self._leaf = float(leaf_size)
+        self._min = int(min_points_per_voxel)
+        self._vg = None
+        self._cap = int(max_points)
+        self._device = int(device)
+
+    def execute(self, cloud):
+        xyzi = cloud[0]
+        refl = cloud[1] if len(cloud) > 1 else None
+        amb = cloud[2] if len(cloud) > 2 else None
+        n = int(xyzi.shape[0])
+        if self._vg is None or n > self._vg.max_points:
+            if self._vg is not None:
+                self._vg.close()
+            self._vg = native.VoxelGrid(max(self._cap, n), self._device)
+        return self._vg.filter(xyzi, (self._leaf,) * 3, self._min, refl, amb)

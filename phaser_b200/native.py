@@ -107,6 +107,8 @@ EXPORTED = [
     "phgpu_profile_enable", "phgpu_profile_read", "phgpu_profile_stage_count",
     "phgpu_profile_stage_name", "phgpu_launch_count", "phgpu_selftest_fft",
     "phgpu_sample_s2_noalloc", "phgpu_bingham_peak", "phgpu_gaussian_peak", "phgpu_peak_window",
+    "phgpu_ply_info", "phgpu_ply_read", "phgpu_ply_last_error", "phgpu_voxel_grid_create",
+    "phgpu_voxel_grid_destroy", "phgpu_voxel_grid_filter", "phgpu_voxel_grid_last_error",
 ]
 
 _LIB = None
@@ -168,6 +170,17 @@ def load(path: str = LIB_PATH):
     lib.phgpu_selftest_fft.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
     lib.phgpu_sample_s2_noalloc.argtypes = [C.POINTER(Params), C.POINTER(Cloud), C.c_void_p, C.c_void_p,
                                             C.c_void_p]
+    lib.phgpu_ply_info.argtypes = [C.c_char_p, C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    lib.phgpu_ply_read.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_uint32, C.POINTER(C.c_uint32)]
+    lib.phgpu_ply_last_error.restype = C.c_char_p
+    lib.phgpu_ply_last_error.argtypes = []
+    lib.phgpu_voxel_grid_create.argtypes = [C.c_uint32, C.c_int32, C.POINTER(vp)]
+    lib.phgpu_voxel_grid_destroy.argtypes = [vp]
+    lib.phgpu_voxel_grid_filter.argtypes = [vp, C.POINTER(Cloud), C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_int, C.POINTER(C.c_uint32)]
+    lib.phgpu_voxel_grid_last_error.restype = C.c_char_p
+    lib.phgpu_voxel_grid_last_error.argtypes = [vp]
     _LIB = lib
     return lib
 
@@ -193,13 +206,18 @@ def make_cloud(xyzi, reflectivity=None, ambient=None) -> tuple[Cloud, list]:
     """Build a phgpu_cloud from numpy arrays (host) or torch CUDA tensors."""
     keep = []
     on_dev = 0
+    host_tensor = False
     try:
         import torch
-        if isinstance(xyzi, torch.Tensor) and xyzi.is_cuda:
-            on_dev = 1
+        if isinstance(xyzi, torch.Tensor):
+            on_dev = 1 if xyzi.is_cuda else 0
+            # float32 contiguous host tensors (pinned ones included) are read in place
+            host_tensor = not on_dev and all(
+                t is None or (isinstance(t, torch.Tensor) and not t.is_cuda and t.dtype == torch.float32
+                              and t.is_contiguous()) for t in (xyzi, reflectivity, ambient))
     except Exception:  # pragma: no cover - torch is always present here
         pass
-    if not on_dev:
+    if not on_dev and not host_tensor:
         xyzi = np.ascontiguousarray(xyzi, np.float32)
         reflectivity = None if reflectivity is None else np.ascontiguousarray(reflectivity, np.float32)
         ambient = None if ambient is None else np.ascontiguousarray(ambient, np.float32)
@@ -258,6 +276,114 @@ def selftest_fft(x: np.ndarray, inverse=False, columns=False, engine=2) -> np.nd
     if rc != PHGPU_OK:
         raise PhgpuError(f"phgpu_selftest_fft failed ({rc})")
     return a
+
+
+PHGPU_PLY_REFLECTIVITY = 1
+PHGPU_PLY_AMBIENT = 2
+PHGPU_PLY_RANGE = 4
+
+
+def _ply_names(field_names):
+    if field_names is None:
+        return None, None
+    names = [None if f is None else f.encode() for f in field_names]
+    names += [None] * (4 - len(names))
+    arr = (C.c_char_p * 4)(*names[:4])
+    return C.cast(arr, C.c_void_p), arr
+
+
+def ply_info(path, field_names=None):
+    """(vertex count, PHGPU_PLY_* bits of the optional fields present)."""
+    names, keep = _ply_names(field_names)
+    n, present = C.c_uint32(), C.c_uint32()
+    lib = load()
+    rc = lib.phgpu_ply_info(os.fsencode(path), names, C.byref(n), C.byref(present))
+    if rc != PHGPU_OK:
+        raise PhgpuError(f"phgpu_ply_info: {lib.phgpu_ply_last_error().decode()} ({rc})")
+    return n.value, present.value
+
+
+def ply_read(path, field_names=None, pinned=False):
+    """Read a PLY file: dict with xyzi (n x 4 float32) and reflectivity,
+    ambient, range (float32 arrays, or None when the field is absent).
+    field_names: intensity, reflectivity, ambient, range property names
+    (None entries keep "intensity", "reflectivity", "noise", "range").
+    pinned=True returns page-locked torch tensors ready for an async upload."""
+    n, present = ply_info(path, field_names)
+    if pinned:
+        import torch
+
+        def buf(shape):
+            return torch.empty(shape, dtype=torch.float32, pin_memory=True)
+    else:
+        def buf(shape):
+            return np.empty(shape, np.float32)
+    xyzi = buf((n, 4))
+    opt = {k: (buf((n,)) if present & bit else None) for k, bit in
+           (("reflectivity", PHGPU_PLY_REFLECTIVITY), ("ambient", PHGPU_PLY_AMBIENT), ("range", PHGPU_PLY_RANGE))}
+    names, keep = _ply_names(field_names)
+    got = C.c_uint32()
+    lib = load()
+    rc = lib.phgpu_ply_read(os.fsencode(path), names, _addr(xyzi) if n else _addr(buf((1, 4))),
+                            _addr(opt["reflectivity"]), _addr(opt["ambient"]), _addr(opt["range"]), n,
+                            C.byref(got))
+    if rc != PHGPU_OK:
+        raise PhgpuError(f"phgpu_ply_read: {lib.phgpu_ply_last_error().decode()} ({rc})")
+    return dict(xyzi=xyzi, **opt)
+
+
+class VoxelGrid:
+    """GPU pcl::VoxelGrid<PointXYZI> (phgpu_voxel_grid_*): leaf centroids of
+    a cloud, leaves in increasing index order."""
+
+    def __init__(self, max_points: int, device: int = 0):
+        lib = load()
+        h = C.c_void_p()
+        rc = lib.phgpu_voxel_grid_create(int(max_points), int(device), C.byref(h))
+        if rc != PHGPU_OK:
+            raise PhgpuError(f"phgpu_voxel_grid_create: {lib.phgpu_voxel_grid_last_error(None).decode()} ({rc})")
+        self._h = h
+        self.max_points = int(max_points)
+        self.device = int(device)
+
+    def filter(self, xyzi, leaf=(0.25, 0.25, 0.25), min_points_per_voxel=0, reflectivity=None, ambient=None,
+               out_device=False):
+        """Returns (xyzi, reflectivity, ambient) of the leaf centroids (the
+        last two None unless given).  Host inputs give numpy outputs;
+        out_device=True returns CUDA tensors instead."""
+        lib = load()
+        c, keep = make_cloud(xyzi, reflectivity, ambient)
+        n = int(c.n_points)
+        cap = max(n, 1)
+        if out_device:
+            import torch
+            dev = torch.device("cuda", self.device)
+            o = torch.empty((cap, 4), dtype=torch.float32, device=dev)
+            orf = torch.empty(cap, dtype=torch.float32, device=dev) if reflectivity is not None else None
+            oam = torch.empty(cap, dtype=torch.float32, device=dev) if ambient is not None else None
+        else:
+            o = np.empty((cap, 4), np.float32)
+            orf = np.empty(cap, np.float32) if reflectivity is not None else None
+            oam = np.empty(cap, np.float32) if ambient is not None else None
+        lf = np.ascontiguousarray(np.broadcast_to(np.asarray(leaf, np.float32), (3,)))
+        m = C.c_uint32()
+        rc = lib.phgpu_voxel_grid_filter(self._h, C.byref(c), lf.ctypes.data, int(min_points_per_voxel), _addr(o),
+                                         _addr(orf), _addr(oam), 1 if out_device else 0, C.byref(m))
+        if rc != PHGPU_OK:
+            raise PhgpuError(f"phgpu_voxel_grid_filter: {lib.phgpu_voxel_grid_last_error(self._h).decode()} ({rc})")
+        k = m.value
+        return o[:k], None if orf is None else orf[:k], None if oam is None else oam[:k]
+
+    def close(self):
+        if self._h:
+            load().phgpu_voxel_grid_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def launch_count() -> int:
