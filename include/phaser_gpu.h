@@ -51,7 +51,7 @@ typedef struct {
   uint32_t spatial_n_voxels;         /* phaser_core_spatial_n_voxels (100) */
   int32_t spatial_discretize_lower;  /* phaser_core_spatial_discretize_lower (-50) */
   int32_t spatial_discretize_upper;  /* phaser_core_spatial_discretize_upper (50) */
-  uint32_t spatial_zero_padding;     /* phaser_core_spatial_zero_padding (0; only 0 supported) */
+  uint32_t spatial_zero_padding;     /* phaser_core_spatial_zero_padding (0; N + 2 pad <= 1024) */
   float spatial_low_pass_lower;      /* phaser_core_spatial_low_pass_lower_bound (0) */
   float spatial_low_pass_upper;      /* phaser_core_spatial_low_pass_upper_bound (100000) */
   uint32_t n_channels;               /* channel count of the fusion (4) */
@@ -172,8 +172,19 @@ int phgpu_spatial_correlate(phgpu_ctx* ctx, const double* const* f, const double
 /* The same on the grids of the last phgpu_voxelize calls. */
 int phgpu_spatial_correlate_voxelized(phgpu_ctx* ctx);
 /* Result of the last spatial correlation: voxel, value and optionally the
- * N^3 correlation (PhaseAligner::getCorrelation, phase-aligner.cc:133-135). */
+ * correlation (PhaseAligner::getCorrelation, phase-aligner.cc:133-135) of
+ * phgpu_spatial_correlation_size entries.  With spatial_zero_padding p the
+ * correlation lives on M = N + 2p voxels per axis (the voxel decodes with M,
+ * PhaseAligner::getNumberOfVoxels, phase-aligner.cc:137-139), and, as in the
+ * reference, its value depends on the context's previous correlation in the
+ * Laplace mode (the first channel reads the tail the previous call's last
+ * channel left in the shifted buffer); the low-pass mode reproduces the
+ * first call on a fresh reference object. */
 int phgpu_spatial_result(phgpu_ctx* ctx, uint32_t* voxel, float* peak, double* corr_out);
+/* SpatialCorrelation::getCorrelationSize (spatial-correlation.cc:219-221):
+ * N^3, or uint32(N^3 ((N + 2p) / N)^3) in double with padding p (which is
+ * (N + 2p)^3 - 1 for many N, p: the last voxel is then left out). */
+uint32_t phgpu_spatial_correlation_size(const phgpu_ctx* ctx);
 
 /* SphOptRegistration::registerPointCloud (sph-opt-registration.cc:34-47):
  * rotation, then translation of the rotated source. */

@@ -102,6 +102,9 @@ def _declare(lib):
                                     C.POINTER(C.c_uint32)]
     lib.orc_bingham_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
                                      C.c_void_p]
+    lib.orc_spatial_correlation_padded.restype = C.c_uint32
+    lib.orc_spatial_correlation_padded.argtypes = [C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_int, C.c_int,
+                                                   C.c_uint32, C.c_uint32, _f64p, _f64p, _f64p]
     lib.orc_voxel_grid.restype = C.c_int64
     lib.orc_voxel_grid.argtypes = [_f32p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_float, C.c_float, C.c_float,
                                    C.c_uint32, _f32p, C.c_void_p, C.c_void_p]
@@ -476,3 +479,26 @@ def voxel_grid(xyzi, leaf=(0.25, 0.25, 0.25), min_points=0, refl=None, amb=None)
     if k < 0:
         return None
     return out[:k], None if orf is None else orf[:k], None if oam is None else oam[:k]
+
+
+def new_padded_state(N):
+    """Fresh F_ / G_ buffers of a padded SpatialCorrelation (zero at construction)."""
+    return np.zeros(2 * N ** 3), np.zeros(2 * N ** 3)
+
+
+def spatial_correlation_padded(f, g, N, pad, mode=1, levels=5, lower=0, upper=None, state=None):
+    """Literal restatement of the zero-padded spatial correlation
+    (orc_spatial_correlation_padded).  f, g: [C][N^3]; mode 0 plain, 1
+    Laplace, 2 low-pass.  state: (F_, G_) carried between calls (modified in
+    place; fresh when None).  Returns (volume of (N + 2 pad)^3, the
+    reference's correlation length)."""
+    f = np.ascontiguousarray(f, np.float64).reshape(-1, N ** 3)
+    g = np.ascontiguousarray(g, np.float64).reshape(-1, N ** 3)
+    if state is None:
+        state = new_padded_state(N)
+    M = N + 2 * pad
+    out = np.zeros(M ** 3)
+    up = N if upper is None else int(upper)
+    size = lib().orc_spatial_correlation_padded(N, pad, f.shape[0], f.ravel(), g.ravel(), mode, levels, int(lower),
+                                                up, state[0], state[1], out)
+    return out, int(size)

@@ -1464,3 +1464,87 @@ int64_t orc_voxel_grid(const float* xyzi, const float* refl, const float* amb, s
   free(v);
   return k;
 }
+
+/* ---------------------------------------------------------------- padding
+ * Zero-padded spatial correlation, restated literally from
+ * SpatialCorrelation (spatial-correlation.cc:11-45 constructor, 78-83
+ * complexMulSeq, 142-161 complexMulSeqUsingIndices, 163-206 correlateSignals,
+ * 223-230 computeZeroPaddedIndex), SpatialCorrelationLaplace
+ * (spatial-correlation-laplace.cc:17-89) and SpatialCorrelationLowPass
+ * (spatial-correlation-low-pass.cc:40-69), M = N + 2 pad:
+ *   state_f / state_g are the reference's F_ / G_ (N^3 complex, re/im
+ *   interleaved, zero at construction); each r2c writes their first
+ *   N^2 (N/2+1) entries; Laplace and low-pass FFT-shift all N^3 entries,
+ *   copy the shifted buffers out per channel; the product of idx goes to
+ *   Sub2Ind(i+pad, j+pad, k+pad, M, M) of a zeroed M^3 buffer; Laplace and
+ *   low-pass IFFT-shift its first N^3 entries; c2r_3d at M.
+ * mode 0 plain (channel 0 of f/g), 1 Laplace (C channels), 2 low-pass
+ * (channel 1, cube [lower, upper]^3, indices >= N^3 skipped where the
+ * reference aborts).  out: M^3 doubles.  Returns the correlation length the
+ * reference reports, uint32(N^3 * ((M / N)^3)) in double. */
+uint32_t orc_spatial_correlation_padded(int N, int pad, int C, const double* f, const double* g, int mode,
+                                        int levels, uint32_t lower, uint32_t upper, double* state_f,
+                                        double* state_g, double* out) {
+  const size_t nv = (size_t)N * N * N;
+  const int M = N + 2 * pad;
+  const size_t nvM = (size_t)M * M * M;
+  cplx* Fb = (cplx*)state_f;
+  cplx* Gb = (cplx*)state_g;
+  cplx* Cc = (cplx*)calloc(nvM, sizeof(cplx));
+  const size_t H = (size_t)N * N * (N / 2 + 1);
+  cplx* half = (cplx*)malloc(sizeof(cplx) * H);
+  const int nch = mode == 1 ? C : 1;
+  const int ch0 = mode == 2 ? 1 : 0;
+  cplx* Fch = (cplx*)malloc(sizeof(cplx) * nv * nch);
+  cplx* Gch = (cplx*)malloc(sizeof(cplx) * nv * nch);
+  for (int c = 0; c < nch; ++c) {
+    r2c3d(f + nv * (size_t)(ch0 + c), N, half);
+    memcpy(Fb, half, sizeof(cplx) * H);
+    r2c3d(g + nv * (size_t)(ch0 + c), N, half);
+    memcpy(Gb, half, sizeof(cplx) * H);
+    if (mode != 0) {
+      orc_fftshift_c(Fb, nv);
+      orc_fftshift_c(Gb, nv);
+    }
+    memcpy(Fch + nv * c, Fb, sizeof(cplx) * nv);
+    memcpy(Gch + nv * c, Gb, sizeof(cplx) * nv);
+  }
+  cplx* vf = (cplx*)malloc(sizeof(cplx) * nch);
+  cplx* vg = (cplx*)malloc(sizeof(cplx) * nch);
+  for (size_t idx = 0; idx < nv; ++idx) {
+    const uint32_t j = (uint32_t)(idx % N), i = (uint32_t)((idx / N) % N), k = (uint32_t)(idx / ((size_t)N * N));
+    if (mode == 2) {
+      /* the index list Sub2Ind(i, j, k, N, N) over the cube; every listed
+       * index below N^3 decodes back to its own (i, j, k) when upper < N */
+      if (i < lower || i > upper || j < lower || j > upper || k < lower || k > upper) continue;
+    }
+    cplx a, b;
+    if (mode == 1) {
+      for (int c = 0; c < nch; ++c) {
+        vf[c] = Fch[nv * c + idx];
+        vg[c] = Gch[nv * c + idx];
+      }
+      const int rule = orc_fusion_rule((uint32_t)idx, (uint32_t)nv, levels, 4.0f);
+      a = fuse_at(vf, nch, rule);
+      b = fuse_at(vg, nch, rule);
+    } else {
+      a = Fch[idx];
+      b = Gch[idx];
+    }
+    const size_t y = (size_t)(i + pad) * M + (j + pad) + (size_t)M * M * (k + pad);
+    Cc[y].re = a.re * b.re - a.im * (-b.im);
+    Cc[y].im = a.re * (-b.im) + a.im * b.re;
+  }
+  if (mode != 0) orc_ifftshift_c(Cc, nv);
+  c2r3d(Cc, M, out);
+  const double ratio = (double)(uint32_t)M / (double)N;
+  const double factor = ratio * ratio * ratio;
+  const uint32_t size = (uint32_t)((double)(uint32_t)nv * factor);
+  free(Cc);
+  free(half);
+  free(Fch);
+  free(Gch);
+  free(vf);
+  free(vg);
+  return size;
+}

@@ -103,27 +103,29 @@ class SphericalCorrelationLowPass(SphericalCorrelation):
 
 
 class SpatialCorrelation:
-    """SpatialCorrelation(n_voxels, zero_padding).correlateSignals(f, g) -> N^3
-    correlation (spatial-correlation.cc:128-175)."""
+    """SpatialCorrelation(n_voxels, zero_padding).correlateSignals(f, g) ->
+    correlation of getCorrelationSize() values (spatial-correlation.cc:163-206):
+    N^3, or on (N + 2 zero_padding)^3 voxels with padding.  Like the
+    reference object, a padded Laplace correlation depends on the previous
+    call (see phgpu_spatial_result)."""
 
     _fusion = native.PHGPU_FUSION_NONE
 
     def __init__(self, n_voxels: int, zero_padding: int = 0):
-        if zero_padding:
-            raise ValueError("spatial zero padding is not supported")
         self._n = int(n_voxels)
+        self._pad = int(zero_padding)
         self._ctx = Context(spherical_bandwidth=2, spatial_n_voxels=self._n, spatial_fusion=self._fusion,
-                            flags=native.PHGPU_FLAG_KEEP_VOLUMES)
+                            spatial_zero_padding=self._pad, flags=native.PHGPU_FLAG_KEEP_VOLUMES)
 
     def correlateSignals(self, f, g) -> np.ndarray:
         self._ctx.spatial_correlate(list(f), list(g))
         return self._ctx.spatial_result(volume=True)[2]
 
     def getZeroPadding(self) -> int:
-        return 0
+        return self._pad
 
     def getCorrelationSize(self) -> int:
-        return self._n ** 3
+        return int(self._ctx.lib.phgpu_spatial_correlation_size(self._ctx.h))
 
 
 class SpatialCorrelationLaplace(SpatialCorrelation):
@@ -137,13 +139,12 @@ class SpatialCorrelationLowPass(SpatialCorrelation):
     _fusion = native.PHGPU_FUSION_LOW_PASS
 
     def __init__(self, n_voxels: int, zero_padding: int = 0, lower: int = 0, upper: int = 100000):
-        if zero_padding:
-            raise ValueError("spatial zero padding is not supported")
         self._n = int(n_voxels)
+        self._pad = int(zero_padding)
         self._lower, self._upper = int(lower), min(int(upper), self._n)
         self._ctx = Context(spherical_bandwidth=2, spatial_n_voxels=self._n, spatial_fusion=self._fusion,
                             spatial_low_pass_lower=float(self._lower), spatial_low_pass_upper=float(self._upper),
-                            flags=native.PHGPU_FLAG_KEEP_VOLUMES)
+                            spatial_zero_padding=self._pad, flags=native.PHGPU_FLAG_KEEP_VOLUMES)
 
     def getLowerBound(self) -> int:
         return self._lower
@@ -158,10 +159,12 @@ class SpatialCorrelationLowPass(SpatialCorrelation):
 class PhaseAligner:
     """PhaseAligner: voxelise both clouds and correlate (phase-aligner.cc:47-69)."""
 
-    def __init__(self, n_voxels=100, lower=-50, upper=50):
+    def __init__(self, n_voxels=100, lower=-50, upper=50, zero_padding=0):
         self._n, self._lo, self._hi = int(n_voxels), int(lower), int(upper)
+        self._pad = int(zero_padding)
         self._ctx = Context(spherical_bandwidth=2, spatial_n_voxels=self._n, spatial_discretize_lower=self._lo,
-                            spatial_discretize_upper=self._hi, flags=native.PHGPU_FLAG_KEEP_VOLUMES)
+                            spatial_discretize_upper=self._hi, spatial_zero_padding=self._pad,
+                            flags=native.PHGPU_FLAG_KEEP_VOLUMES)
 
     def alignRegistered(self, cloud_prev, cloud_reg):
         """cloud_* = (xyzi, reflectivity) or (xyzi, reflectivity, ambient)."""
@@ -173,7 +176,7 @@ class PhaseAligner:
         return self._ctx.spatial_result(volume=True)[2]
 
     def getNumberOfVoxels(self) -> int:
-        return self._n
+        return self._n + 2 * self._pad
 
     def getLowerBound(self) -> int:
         return self._lo

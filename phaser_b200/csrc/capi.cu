@@ -408,6 +408,7 @@ const char* phgpu_last_error(const phgpu_ctx* ctx) {
 void* phgpu_stream(phgpu_ctx* ctx) { return ctx ? (void*)ctx->s0 : nullptr; }
 
 uint32_t phgpu_sph_bandwidth(const phgpu_ctx* ctx) { return ctx ? (uint32_t)ctx->bw_out : 0u; }
+uint32_t phgpu_spatial_correlation_size(const phgpu_ctx* ctx) { return ctx ? ctx->corr_size : 0u; }
 
 template <typename T>
 static int dalloc(phgpu_ctx* ctx, T** p, size_t bytes) {
@@ -458,13 +459,13 @@ int phgpu_ctx_create(const phgpu_params* prm, phgpu_ctx** out) {
   const int bw = (int)prm->spherical_bandwidth;
   const int bw_out = bw + (int)prm->spherical_zero_padding;
   const int N = (int)prm->spatial_n_voxels;
-  if (bw < 2 || bw > 512 || N < 1 || N > 1024 || prm->spatial_zero_padding != 0 ||
+  if (bw < 2 || bw > 512 || N < 1 || N > 1024 || (uint64_t)N + 2ull * prm->spatial_zero_padding > 1024 ||
       prm->n_channels < 1 || prm->n_channels > 4 || prm->fusion_levels < 1 ||
       prm->fusion_levels > (uint32_t)kMaxLevels || prm->spherical_fusion > PHGPU_FUSION_LOW_PASS ||
       prm->spatial_fusion > PHGPU_FUSION_LOW_PASS) {
     g_create_error =
-        "unsupported configuration (2 <= bandwidth <= 512, 1 <= n_voxels <= 1024, spatial zero "
-        "padding 0, 1..4 channels, 1..8 fusion levels, fusion mode 0..2)";
+        "unsupported configuration (2 <= bandwidth <= 512, 1 <= n_voxels + 2 spatial zero padding <= 1024, "
+        "1..4 channels, 1..8 fusion levels, fusion mode 0..2)";
     return PHGPU_ERR_INVALID;
   }
   phgpu_ctx* ctx = new phgpu_ctx();
@@ -472,6 +473,16 @@ int phgpu_ctx_create(const phgpu_params* prm, phgpu_ctx** out) {
   ctx->bw = bw;
   ctx->bw_out = bw_out;
   ctx->N = N;
+  ctx->pad = (int)prm->spatial_zero_padding;
+  ctx->M = N + 2 * ctx->pad;
+  {
+    // SpatialCorrelation's constructor (spatial-correlation.cc:17-25): the
+    // padded size in double, truncated (M^3 - 1 for many N, pad)
+    const double ratio = (double)(uint32_t)ctx->M / (double)N;
+    const double factor = ratio * ratio * ratio;
+    const uint32_t nv = (uint32_t)N * (uint32_t)N * (uint32_t)N;
+    ctx->corr_size = ctx->pad ? (uint32_t)((double)nv * factor) : nv;
+  }
   if (cudaSetDevice(prm->device) != cudaSuccess) {
     g_create_error = "cudaSetDevice failed";
     delete ctx;
@@ -509,6 +520,19 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
       return PHGPU_ERR_INVALID;
     }
     ctx->has_sp_half = true;
+  }
+  if (ctx->pad) {
+    if (!make_fft_plan(ctx->M, &ctx->plan_pad, &ctx->d_tw_pad[0], &perr)) {
+      ctx->err = perr;
+      return PHGPU_ERR_INVALID;
+    }
+    if (spatial_slab_path(ctx->M)) {
+      if (!make_fft_plan(ctx->M / 2, &ctx->plan_pad_half, &ctx->d_tw_pad[1], &perr)) {
+        ctx->err = perr;
+        return PHGPU_ERR_INVALID;
+      }
+      ctx->has_pad_half = true;
+    }
   }
   ctx->bands_s2 = make_bands((uint32_t)(bw * bw), (int)prm->fusion_levels, 4.0f);
   ctx->bands_sp = make_bands((uint32_t)N * (uint32_t)N * (uint32_t)N, (int)prm->fusion_levels, 4.0f);
@@ -578,7 +602,13 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   if ((prm->flags & PHGPU_FLAG_KEEP_VOLUMES) || prm->rot_peak_neighbors > 0)
     CKV(dalloc(ctx, &ctx->d_rotvol, sizeof(float) * no * no * no));
   if ((prm->flags & PHGPU_FLAG_KEEP_VOLUMES) || prm->trans_peak_neighbors > 0)
-    CKV(dalloc(ctx, &ctx->d_transvol, sizeof(float) * nv));
+    CKV(dalloc(ctx, &ctx->d_transvol, sizeof(float) * (ctx->pad ? (size_t)ctx->M * ctx->M * ctx->M : nv)));
+  if (ctx->pad) {
+    const size_t HM = (size_t)ctx->M * ctx->M * spatial_h2p(ctx->M);
+    CKV(dalloc(ctx, &ctx->d_cspec_pad, sizeof(float2) * HM));
+    if (prm->spatial_fusion == PHGPU_FUSION_LAPLACE)
+      for (int s = 0; s < 2; ++s) CKV(dalloc(ctx, &ctx->d_prev[s], sizeof(float2) * H));
+  }
   // [0] rotation argmax, [1] translation argmax, [2] kernel status bits (sticky)
   CKV(dalloc(ctx, &ctx->d_argmax, sizeof(unsigned long long) * 3));
   CK(cudaMemset(ctx->d_argmax, 0, sizeof(unsigned long long) * 3));
@@ -598,6 +628,8 @@ int phgpu_ctx_destroy(phgpu_ctx* ctx) {
   ctx->allocs.clear();
   for (int i = 0; i < 4; ++i)
     if (ctx->d_tw[i]) cudaFree(ctx->d_tw[i]);
+  for (int i = 0; i < 2; ++i)
+    if (ctx->d_tw_pad[i]) cudaFree(ctx->d_tw_pad[i]);
   if (ctx->h_argmax) cudaFreeHost(ctx->h_argmax);
   for (const ProfRec& r : ctx->prof_recs) {
     cudaEventDestroy(r.a);
@@ -891,12 +923,79 @@ static SpatialArgs spatial_args(phgpu_ctx* ctx, int n_data, int n_total, int lap
   return a;
 }
 
+// Zero-padded product and inverse at M (k_spatial_pad.cu) on the spectra the
+// unpadded forward left in d_spec (both sides); argmax into d_argmax[1].
+static int run_spatial_padded(phgpu_ctx* ctx, const SpatialArgs& a, cudaStream_t st) {
+  const int N = ctx->N, M = ctx->M;
+  const size_t plane = (size_t)N * N * spatial_h2p(N);
+  const int nch = a.laplace ? a.n_data_ch : (a.lowpass ? 2 : 1);
+  {
+    ProfScope ps(ctx, st, PS_FUSE_Z);
+    for (int side = 0; side < 2; ++side)
+      CK(launch_pad_zfft(a.spec + (size_t)side * a.n_data_ch * plane, plane, nch, N, N, N / 2 + 1, 0, ctx->plan_sp,
+                         st));
+    CK(cudaMemsetAsync(ctx->d_cspec_pad, 0, sizeof(float2) * (size_t)M * M * spatial_h2p(M), st));
+    PadArgs pa;
+    pa.N = N;
+    pa.M = M;
+    pa.pad = ctx->pad;
+    pa.mode = a.laplace ? 1 : (a.lowpass ? 2 : 0);
+    pa.n_ch = a.laplace ? a.n_total_ch : 1;
+    pa.n_spec = a.laplace ? a.n_data_ch : 1;
+    pa.spec_ch = a.n_data_ch;
+    pa.first_ch = a.lowpass ? 1 : 0;
+    pa.spec = a.spec;
+    pa.prev_f = (a.laplace && ctx->prev_valid[0]) ? ctx->d_prev[0] : nullptr;
+    pa.prev_g = (a.laplace && ctx->prev_valid[1]) ? ctx->d_prev[1] : nullptr;
+    pa.x_natural_N = (spatial_slab_path(N) && a.plan_half) ? 1 : 0;
+    pa.x_natural_M = ctx->has_pad_half ? 1 : 0;
+    pa.planN = ctx->plan_sp;
+    pa.planM = ctx->plan_pad;
+    pa.bands = ctx->bands_sp;
+    pa.lp_lo = a.lp_lo;
+    pa.lp_hi = a.lp_hi;
+    pa.inv_total = 1.0f / (float)a.n_total_ch;
+    pa.cspec = ctx->d_cspec_pad;
+    CK(launch_pad_fuse(pa, st));
+    if (a.laplace) {
+      // the buffers keep the last channel's shifted spectrum for the next call
+      const int last = a.n_total_ch - 1;
+      for (int side = 0; side < 2; ++side) {
+        ctx->prev_valid[side] = last < a.n_data_ch;
+        if (ctx->prev_valid[side])
+          CK(cudaMemcpyAsync(ctx->d_prev[side], a.spec + (size_t)(side * a.n_data_ch + last) * plane,
+                             sizeof(float2) * plane, cudaMemcpyDeviceToDevice, st));
+      }
+    }
+    CK(launch_pad_zfft(ctx->d_cspec_pad, 0, 1, M, M, M / 2 + 1, 1, ctx->plan_pad, st));
+  }
+  SpatialArgs am = a;
+  am.N = M;
+  am.cspec = ctx->d_cspec_pad;
+  am.plan = &ctx->plan_pad;
+  am.plan_half = ctx->has_pad_half ? &ctx->plan_pad_half : nullptr;
+  am.argmax_limit = ctx->corr_size;
+  CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), st));
+  {
+    ProfScope ps(ctx, st, PS_SPATIAL_INV);
+    CK(launch_spatial_inverse(am, st));
+  }
+  return PHGPU_OK;
+}
+
 int phgpu_run_spatial(phgpu_ctx* ctx, int n_data, int n_total, int laplace, int means, cudaStream_t st) {
   SpatialArgs a = spatial_args(ctx, n_data, n_total, laplace, means);
   {
     ProfScope ps(ctx, st, PS_SPATIAL_FWD);
     CK(launch_spatial_forward(a, 0, st));
     CK(launch_spatial_forward(a, 1, st));
+  }
+  if (ctx->pad) {
+    CKV(run_spatial_padded(ctx, a, st));
+    CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, 2 * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, st));
+    ctx->have_trans = true;
+    return PHGPU_OK;
   }
   CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), st));
   {
@@ -973,7 +1072,7 @@ int phgpu_spatial_result(phgpu_ctx* ctx, uint32_t* voxel, float* peak, double* c
       ctx->err = "volumes not kept (PHGPU_FLAG_KEEP_VOLUMES)";
       return PHGPU_ERR_STATE;
     }
-    const size_t n = (size_t)ctx->N * ctx->N * ctx->N;
+    const size_t n = ctx->corr_size;  // N^3, or the reference's padded correlation length
     std::vector<float> tmp(n);
     CK(cudaMemcpy(tmp.data(), ctx->d_transvol, sizeof(float) * n, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i) corr_out[i] = tmp[i];
@@ -1046,14 +1145,18 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
   }
   CKV(clear_voxelized(ctx, 1, s0));
   CK(cudaStreamWaitEvent(s0, ctx->ev_b, 0));
-  CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), s0));
-  {
-    ProfScope ps(ctx, s0, PS_FUSE_Z);
-    CK(launch_spatial_fuse_z(sa, s0));
-  }
-  {
-    ProfScope ps(ctx, s0, PS_SPATIAL_INV);
-    CK(launch_spatial_inverse(sa, s0));
+  if (ctx->pad) {
+    CKV(run_spatial_padded(ctx, sa, s0));
+  } else {
+    CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), s0));
+    {
+      ProfScope ps(ctx, s0, PS_FUSE_Z);
+      CK(launch_spatial_fuse_z(sa, s0));
+    }
+    {
+      ProfScope ps(ctx, s0, PS_SPATIAL_INV);
+      CK(launch_spatial_inverse(sa, s0));
+    }
   }
   CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, 2 * sizeof(unsigned long long),
                      cudaMemcpyDeviceToHost, s0));
@@ -1066,7 +1169,8 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
   const unsigned long long tk = ctx->h_argmax[1];
   out->voxel = unpack_index(tk);
   out->trans_peak = float_from_order_bits((uint32_t)(tk >> 32));
-  const uint32_t N = (uint32_t)ctx->N;
+  // PhaseAligner::getNumberOfVoxels: N + 2 pad decodes the (padded) voxel
+  const uint32_t N = (uint32_t)(ctx->pad ? ctx->M : ctx->N);
   const uint32_t xyz[3] = {(out->voxel / N) % N, out->voxel % N, out->voxel / (N * N)};
   for (int a = 0; a < 3; ++a)
     out->trans[a] = phgpu_translation_from_index((double)xyz[a], N, ctx->prm.spatial_discretize_lower,
@@ -1076,7 +1180,7 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
     // Gaussian fit over the linear-index window of the translation volume:
     // the estimate is its mean (gaussian-peak-based-eval.cc, sph-opt-registration.cc:74-88)
     uint32_t first = 0, cnt = 0;
-    phgpu_peak_window(out->voxel, N * N * N, ctx->prm.trans_peak_neighbors, &first, &cnt);
+    phgpu_peak_window(out->voxel, ctx->corr_size, ctx->prm.trans_peak_neighbors, &first, &cnt);
     std::vector<float> wf(cnt);
     CK(cudaMemcpy(wf.data(), ctx->d_transvol + first, sizeof(float) * cnt, cudaMemcpyDeviceToHost));
     std::vector<double> w(wf.begin(), wf.end());

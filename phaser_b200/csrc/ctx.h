@@ -73,6 +73,15 @@ struct phgpu_ctx {
   float2* d_spec = nullptr;
   float2* d_cspec = nullptr;
   float* d_transvol = nullptr;
+  // zero-padded translation (spatial_zero_padding > 0): M = N + 2 pad
+  int pad = 0, M = 0;
+  uint32_t corr_size = 0;  // the reference's correlation length uint32(N^3 (M / N)^3) (M^3 or M^3 - 1)
+  phgpu::FftPlan plan_pad, plan_pad_half;
+  bool has_pad_half = false;
+  float2* d_tw_pad[2] = {nullptr, nullptr};
+  float2* d_cspec_pad = nullptr;           // [M][M][H2p(M)]
+  float2* d_prev[2] = {nullptr, nullptr};  // Laplace: last channel spectrum of the previous call, per side
+  bool prev_valid[2] = {false, false};
   int vox_ch[2] = {0, 0};
   // results
   unsigned long long* d_argmax = nullptr;  // [rot, trans]

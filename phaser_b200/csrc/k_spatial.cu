@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
 // inverted two at a time as Z = X0 + i X1 (output x0 = Re, x1 = Im).
 template <int NF>
 __global__ void k_c2r_y(int N, const float2* __restrict__ cspec, FftPlan plan,
-                        unsigned long long* __restrict__ argmax, float* __restrict__ volume) {
+                        unsigned long long* __restrict__ argmax, float* __restrict__ volume, uint32_t limit) {
   extern __shared__ float2 rows[];  // [kRowsR2C / 2][n] packed rows, then int pos[n]
   constexpr int R = kRowsR2C;
   const int n = NF > 0 ? NF : N;
@@ -400,7 +400,7 @@ __global__ void k_c2r_y(int N, const float2* __restrict__ cspec, FftPlan plan,
       const float2 z = rows[(size_t)(rr >> 1) * n + y];
       const float v = (rr & 1) ? z.y : z.x;
       const uint32_t idx = (uint32_t)(r * n + y);
-      const unsigned long long key = pack_argmax(v, idx);
+      const unsigned long long key = idx < limit ? pack_argmax(v, idx) : 0ull;
       best = key > best ? key : best;
       if (volume) volume[idx] = v;
     }
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
 template <int NF>
 __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* __restrict__ cspec, FftPlan pN,
                                                    FftPlan pH, unsigned long long* __restrict__ argmax,
-                                                   float* __restrict__ volume) {
+                                                   float* __restrict__ volume, uint32_t limit) {
   constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1, S = NF + 1;
   const int H2p = spatial_h2p(N);
   extern __shared__ float2 W[];  // [NH][S]
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
     const float a0 = 2.0f * v.x, a1 = 2.0f * v.y;
     const uint32_t i0 = (uint32_t)(((size_t)z * N + 2 * r) * N + y);
     const uint32_t i1 = i0 + N;
-    unsigned long long k0 = pack_argmax(a0, i0), k1 = pack_argmax(a1, i1);
+    unsigned long long k0 = i0 < limit ? pack_argmax(a0, i0) : 0ull, k1 = i1 < limit ? pack_argmax(a1, i1) : 0ull;
     k0 = k1 > k0 ? k1 : k0;
     best = k0 > best ? k0 : best;
     if (volume) {
@@ -714,10 +714,11 @@ cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st) {
 
 cudaError_t launch_spatial_inverse(const SpatialArgs& a, cudaStream_t st) {
   const int N = a.N, H2 = N / 2 + 1;
+  const uint32_t limit = a.argmax_limit ? a.argmax_limit : 0xffffffffu;
   if (spatial_slab_path(N) && a.plan_half) {
     const size_t sm = (size_t)(N / 2) * (N + 1) * sizeof(float2);
     PHGPU_DISPATCH_SLAB(N, k_slab_inv<NF><<<N, tail_threads<NF>(), sm, st>>>(a.cspec, *a.plan, *a.plan_half, a.argmax,
-                                                                             a.volume));
+                                                                             a.volume, limit));
     count_launches(1);
     return cudaGetLastError();
   }
@@ -726,7 +727,7 @@ cudaError_t launch_spatial_inverse(const SpatialArgs& a, cudaStream_t st) {
   PHGPU_DISPATCH_N(N,
       k_fft_x<NF, true><<<gC, 256, (size_t)N * 16 * sizeof(float2), st>>>(N, a.cspec, *a.plan);
       k_c2r_y<NF><<<nrowblk, 256, (size_t)(kRowsR2C / 2) * N * sizeof(float2) + (size_t)N * sizeof(int), st>>>(
-          N, a.cspec, *a.plan, a.argmax, a.volume));
+          N, a.cspec, *a.plan, a.argmax, a.volume, limit));
   count_launches(2);
   return cudaGetLastError();
 }

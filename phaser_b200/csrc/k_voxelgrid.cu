@@ -209,11 +209,15 @@ template <class Op>
 __global__ void __launch_bounds__(kVgThreads) k_flag_count(Op op, uint32_t* __restrict__ counts) {
   const uint32_t n = op.n();
   const uint32_t base = blockIdx.x * kVgTile;
-  uint32_t c = 0;
+  bool f[kVgRounds];  // all of the tile's flags first: one load latency, not one per round
+#pragma unroll
   for (int r = 0; r < kVgRounds; ++r) {
     const uint32_t i = base + r * kVgThreads + threadIdx.x;
-    c += __popc(__ballot_sync(0xffffffffu, i < n && op.flag(i)));
+    f[r] = i < n && op.flag(i);
   }
+  uint32_t c = 0;
+#pragma unroll
+  for (int r = 0; r < kVgRounds; ++r) c += __popc(__ballot_sync(0xffffffffu, f[r]));
   __shared__ uint32_t s[kVgWarps];
   if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = c;
   __syncthreads();
@@ -232,9 +236,16 @@ __global__ void __launch_bounds__(kVgThreads) k_flag_scatter(Op op, const uint32
   __shared__ uint32_t s_w[kVgWarps];
   const int warp = threadIdx.x >> 5;
   uint32_t run = offsets[blockIdx.x];
+  bool fl[kVgRounds];
+#pragma unroll
   for (int r = 0; r < kVgRounds; ++r) {
     const uint32_t i = base + r * kVgThreads + threadIdx.x;
-    const bool f = i < n && op.flag(i);
+    fl[r] = i < n && op.flag(i);
+  }
+#pragma unroll
+  for (int r = 0; r < kVgRounds; ++r) {
+    const uint32_t i = base + r * kVgThreads + threadIdx.x;
+    const bool f = fl[r];
     const uint32_t bal = __ballot_sync(0xffffffffu, f);
     if ((threadIdx.x & 31) == 0) s_w[warp] = __popc(bal);
     __syncthreads();
@@ -317,42 +328,58 @@ __global__ void __launch_bounds__(kVgThreads) k_radix_count(const uint32_t* __re
   s_hist[threadIdx.x] = 0;
   __syncthreads();
   const uint32_t base = blockIdx.x * kVgTile;
+  uint32_t dg[kVgRounds];
+#pragma unroll
   for (int r = 0; r < kVgRounds; ++r) {
     const uint32_t i = base + r * kVgThreads + threadIdx.x;
-    const bool ok = i < n;
-    const uint32_t d = ok ? (keys[i] >> shift) & 0xffu : 0x100u;
+    dg[r] = i < n ? (keys[i] >> shift) & 0xffu : 0x100u;
+  }
+#pragma unroll
+  for (int r = 0; r < kVgRounds; ++r) {
+    const uint32_t d = dg[r];
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    if (ok && (peers & lanemask_lt()) == 0) atomicAdd(&s_hist[d], (uint32_t)__popc(peers));
+    if (d < kBins && (peers & lanemask_lt()) == 0) atomicAdd(&s_hist[d], (uint32_t)__popc(peers));
   }
   __syncthreads();
   counts[threadIdx.x * n_tiles + blockIdx.x] = s_hist[threadIdx.x];
 }
 
-// Per digit: exclusive scan of its tile counts (one warp per digit, lanes own
-// contiguous runs of tiles) and the digit's total.
+// Per digit: exclusive scan of its tile counts in place and the digit's total
+// (one warp per digit; lane l holds tiles c0 + q*32 + l, so every load is one
+// coalesced 128-byte row, and a warp scan per row carries the running sum).
+constexpr int kScanRows = 16;
+
 __global__ void __launch_bounds__(kVgThreads) k_radix_scan(uint32_t* __restrict__ counts, uint32_t n_tiles,
                                                            uint32_t* __restrict__ digit_total) {
   const int lane = threadIdx.x & 31;
   const uint32_t d = blockIdx.x * kVgWarps + (threadIdx.x >> 5);
   uint32_t* row = counts + (size_t)d * n_tiles;
-  const uint32_t chunk = (n_tiles + 31) / 32;
-  const uint32_t b = lane * chunk, e = min(n_tiles, b + chunk);
-  uint32_t sum = 0;
-  for (uint32_t i = b; i < e; ++i) sum += row[i];
-  uint32_t incl = sum;
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
+  uint32_t carry = 0;
+  for (uint32_t c0 = 0; c0 < n_tiles; c0 += 32 * kScanRows) {
+    uint32_t v[kScanRows];
+#pragma unroll
+    for (int q = 0; q < kScanRows; ++q) {
+      const uint32_t i = c0 + q * 32 + lane;
+      v[q] = i < n_tiles ? row[i] : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < kScanRows; ++q) {
+      uint32_t incl = v[q];
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t a = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += a;
+      }
+      const uint32_t i = c0 + q * 32 + lane;
+      if (i < n_tiles) row[i] = carry + incl - v[q];
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
   }
-  uint32_t run = incl - sum;
-  for (uint32_t i = b; i < e; ++i) {
-    const uint32_t v = row[i];
-    row[i] = run;
-    run += v;
-  }
-  if (lane == 31) digit_total[d] = incl;
+  if (lane == 0) digit_total[d] = carry;
 }
 
+// Stable scatter of one tile: items are ranked in tile order into a
+// digit-sorted copy of the tile in shared memory, then written out in that
+// order, so each digit's run of the tile lands in consecutive words.
 __global__ void __launch_bounds__(kVgThreads) k_radix_scatter(const uint32_t* __restrict__ keys_in,
                                                               const uint32_t* __restrict__ vals_in,
                                                               uint32_t* __restrict__ keys_out,
@@ -360,41 +387,77 @@ __global__ void __launch_bounds__(kVgThreads) k_radix_scatter(const uint32_t* __
                                                               int shift, uint32_t n_tiles,
                                                               const uint32_t* __restrict__ offsets,
                                                               const uint32_t* __restrict__ digit_total) {
-  __shared__ uint32_t s_base[kBins];
+  __shared__ uint32_t s_key[kVgTile];
+  __shared__ uint32_t s_val[kVgTile];
+  __shared__ uint32_t s_local[kBins];  // start of each digit in the sorted tile
+  __shared__ uint32_t s_run[kBins];    // next free position of each digit
+  __shared__ uint32_t s_gbase[kBins];  // global position of the tile's first item of each digit
   __shared__ uint32_t s_wc[kVgWarps][kBins];
   const uint32_t n = st->n_valid;
   const uint32_t base = blockIdx.x * kVgTile;
   if (base >= n) return;
+  const uint32_t tile_n = min((uint32_t)kVgTile, n - base);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // digit base = exclusive scan of the digit totals (one block-wide scan)
-  const uint32_t tot = digit_total[threadIdx.x];
-  uint32_t incl = tot;
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  if (lane == 31) s_wc[0][warp] = incl;
-  __syncthreads();
-  uint32_t before = 0;
-  for (int w = 0; w < warp; ++w) before += s_wc[0][w];
-  __syncthreads();
-  s_base[threadIdx.x] = before + incl - tot + offsets[threadIdx.x * n_tiles + blockIdx.x];
-  for (int w = 0; w < kVgWarps; ++w) s_wc[w][threadIdx.x] = 0;
-  __syncthreads();
+  uint32_t k[kVgRounds], v[kVgRounds], dg[kVgRounds];
+#pragma unroll
   for (int r = 0; r < kVgRounds; ++r) {
     const uint32_t i = base + r * kVgThreads + threadIdx.x;
     const bool ok = i < n;
-    const uint32_t k = ok ? keys_in[i] : 0u;
-    const uint32_t d = ok ? (k >> shift) & 0xffu : 0x100u;
+    k[r] = ok ? keys_in[i] : 0u;
+    v[r] = ok ? vals_in[i] : 0u;
+    dg[r] = ok ? (k[r] >> shift) & 0xffu : 0x100u;
+  }
+  s_run[threadIdx.x] = 0;
+  const uint32_t tot = digit_total[threadIdx.x];
+  const uint32_t goff = offsets[threadIdx.x * n_tiles + blockIdx.x];
+  __syncthreads();
+  // tile histogram
+#pragma unroll
+  for (int r = 0; r < kVgRounds; ++r) {
+    const uint32_t peers = __match_any_sync(0xffffffffu, dg[r]);
+    if (dg[r] < kBins && (peers & lanemask_lt()) == 0) atomicAdd(&s_run[dg[r]], (uint32_t)__popc(peers));
+  }
+  __syncthreads();
+  // exclusive scans over the 256 digits: tile histogram and digit totals
+  const uint32_t h = s_run[threadIdx.x];
+  uint32_t ih = h, it = tot;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t a = __shfl_up_sync(0xffffffffu, ih, o);
+    const uint32_t b = __shfl_up_sync(0xffffffffu, it, o);
+    if (lane >= o) {
+      ih += a;
+      it += b;
+    }
+  }
+  if (lane == 31) {
+    s_wc[0][warp] = ih;
+    s_wc[1][warp] = it;
+  }
+  __syncthreads();
+  uint32_t bh = 0, bt = 0;
+  for (int w = 0; w < warp; ++w) {
+    bh += s_wc[0][w];
+    bt += s_wc[1][w];
+  }
+  __syncthreads();
+  s_local[threadIdx.x] = bh + ih - h;
+  s_run[threadIdx.x] = bh + ih - h;
+  s_gbase[threadIdx.x] = bt + it - tot + goff;
+  for (int w = 0; w < kVgWarps; ++w) s_wc[w][threadIdx.x] = 0;
+  __syncthreads();
+  // stable ranks into the sorted tile
+#pragma unroll
+  for (int r = 0; r < kVgRounds; ++r) {
+    const uint32_t d = dg[r];
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const uint32_t rank = __popc(peers & lanemask_lt());
-    if (ok && rank == 0) s_wc[warp][d] = __popc(peers);
+    if (d < kBins && rank == 0) s_wc[warp][d] = __popc(peers);
     __syncthreads();
-    if (ok) {
-      uint32_t pos = s_base[d] + rank;
+    if (d < kBins) {
+      uint32_t pos = s_run[d] + rank;
       for (int w = 0; w < warp; ++w) pos += s_wc[w][d];
-      keys_out[pos] = k;
-      vals_out[pos] = vals_in[i];
+      s_key[pos] = k[r];
+      s_val[pos] = v[r];
     }
     __syncthreads();
     uint32_t t = 0;
@@ -402,8 +465,15 @@ __global__ void __launch_bounds__(kVgThreads) k_radix_scatter(const uint32_t* __
       t += s_wc[w][threadIdx.x];
       s_wc[w][threadIdx.x] = 0;
     }
-    s_base[threadIdx.x] += t;
+    s_run[threadIdx.x] += t;
     __syncthreads();
+  }
+  for (uint32_t L = threadIdx.x; L < tile_n; L += kVgThreads) {
+    const uint32_t key = s_key[L];
+    const uint32_t d = (key >> shift) & 0xffu;
+    const uint32_t g = s_gbase[d] + (L - s_local[d]);
+    keys_out[g] = key;
+    vals_out[g] = s_val[L];
   }
 }
 

@@ -121,12 +121,42 @@ struct SpatialArgs {
   unsigned long long* argmax;
   float* volume;          // optional N^3 correlation, [z][x][y]
   unsigned long long* status;  // bit 0: a bulk-copy wait gave up (result invalid)
+  uint32_t argmax_limit = 0;   // argmax over indices < limit (0: all)
 };
 cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t st);
 cudaError_t launch_spatial_combine(const SpatialArgs& a, cudaStream_t st);
 cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st);   // z FFTs + fusion + cross power
 cudaError_t launch_spatial_inverse(const SpatialArgs& a, cudaStream_t st);  // inverse x + C2R y + argmax
 cudaError_t spatial_init_attributes();  // once per device
+// ------------------------------------------------------------ zero-padded translation
+// The reference's padded spatial correlation (spatial-correlation.cc:11-45,
+// 142-161,223-230): the product of the (fused) N-sized spectra is scattered
+// to computeZeroPaddedIndex positions of an M = N + 2 pad cube and inverted
+// at M.  See k_spatial_pad.cu.
+struct PadArgs {
+  int N, M, pad;
+  int mode;               // 0 plain (channel 0), 1 Laplace fusion, 2 low-pass (channel 1, index cube)
+  int n_ch;               // channels fused per side (mode 1: all channels, zero ones included)
+  int n_spec;             // channels with spectra in spec (mode 1; the others are zero)
+  int spec_ch;            // channels per side in the spec layout
+  int first_ch;           // spec channel read by modes 0 and 2
+  const float2* spec;     // [2][spec_ch][N (z pos)][N (x pos)][H2p]: full 3-D spectra
+  const float2* prev_f;   // last channel of the previous call (mode 1), null = zero
+  const float2* prev_g;
+  int x_natural_N;        // spec x positions: 1 natural, 0 digit-reversed
+  int x_natural_M;        // cspec_pad x positions expected by the inverse at M
+  FftPlan planN, planM;   // z positions (both digit-reversed)
+  FusionBands bands;      // n = N^3
+  uint32_t lp_lo, lp_hi;  // mode 2 index cube
+  float inv_total;        // 1 / channel count (MEAN)
+  float2* cspec;          // [M (z pos)][M (x pos)][H2p(M)], zeroed by the caller
+};
+// Forward (INV = 0) or inverse z transform of n_arrays [n][nx][H2p] arrays
+// (z natural <-> z digit-reversed), columns ky < H.
+cudaError_t launch_pad_zfft(float2* base, size_t array_stride, int n_arrays, int n, int nx, int H, int inverse,
+                            const FftPlan& plan, cudaStream_t st);
+cudaError_t launch_pad_fuse(const PadArgs& a, cudaStream_t st);
+
 // Row length of the half spectra: N/2 + 1 rounded up to 8 complex (64 B).
 __host__ __device__ inline int spatial_h2p(int N) { return ((N / 2 + 1) + 7) / 8 * 8; }
 // True when the fused z-slab kernels handle this N (the slab fits in shared memory).

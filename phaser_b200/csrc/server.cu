@@ -227,6 +227,14 @@ static void copy_cloud(const phgpu_cloud* c, std::vector<float>& xyzi, std::vect
 int phgpu_server_submit(phgpu_server* s, const phgpu_params* params, const phgpu_cloud* target,
                         const phgpu_cloud* source, uint64_t* ticket) {
   if (!s || !params || !target || !source || !ticket) return PHGPU_ERR_INVALID;
+  if (params->spatial_zero_padding != 0) {
+    // the padded correlation carries state from one call to the next (the
+    // previous call's last channel spectrum), so its result would depend on
+    // which requests a worker context served before
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->err = "spatial zero padding is not served (its result depends on the context's previous calls)";
+    return PHGPU_ERR_INVALID;
+  }
   Request* r = new Request();
   r->prm = *params;
   r->tn = target->n_points;

@@ -109,6 +109,7 @@ EXPORTED = [
     "phgpu_sample_s2_noalloc", "phgpu_bingham_peak", "phgpu_gaussian_peak", "phgpu_peak_window",
     "phgpu_ply_info", "phgpu_ply_read", "phgpu_ply_last_error", "phgpu_voxel_grid_create",
     "phgpu_voxel_grid_destroy", "phgpu_voxel_grid_filter", "phgpu_voxel_grid_last_error",
+    "phgpu_spatial_correlation_size",
 ]
 
 _LIB = None
@@ -137,6 +138,8 @@ def load(path: str = LIB_PATH):
     lib.phgpu_sph_result.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_float), vp]
     lib.phgpu_sph_bandwidth.restype = C.c_uint32
     lib.phgpu_sph_bandwidth.argtypes = [vp]
+    lib.phgpu_spatial_correlation_size.restype = C.c_uint32
+    lib.phgpu_spatial_correlation_size.argtypes = [vp]
     lib.phgpu_voxelize.argtypes = [vp, C.POINTER(Cloud), C.c_int, vp]
     lib.phgpu_get_voxel_index.argtypes = [vp, C.c_int, vp, C.c_uint32]
     lib.phgpu_spatial_correlate.argtypes = [vp, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_uint32]
@@ -521,7 +524,7 @@ class Context:
     def spatial_result(self, volume=False):
         v = C.c_uint32()
         pk = C.c_float()
-        vol = np.zeros(self.n_voxels ** 3) if volume else None
+        vol = np.zeros(self.lib.phgpu_spatial_correlation_size(self.h)) if volume else None
         self.check(self.lib.phgpu_spatial_result(self.h, C.byref(v), C.byref(pk),
                                                  None if vol is None else vol.ctypes.data))
         return (v.value, pk.value, vol) if volume else (v.value, pk.value)

@@ -341,7 +341,7 @@ def test_device_resident_inputs(nat, pair0):
 
 def test_invalid_configuration_reports_error(nat):
     with pytest.raises(nat.PhgpuError):
-        nat.Context(spherical_bandwidth=4, spatial_n_voxels=4, spatial_zero_padding=2)
+        nat.Context(spherical_bandwidth=4, spatial_n_voxels=1000, spatial_zero_padding=20)  # N + 2 pad > 1024
     with pytest.raises(nat.PhgpuError):
         nat.Context(spherical_bandwidth=4, spatial_n_voxels=131)  # prime factor above 128
     c = ctx(nat)
