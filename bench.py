@@ -238,6 +238,63 @@ def roofline(nat, pool, params, served_value):
     return roof
 
 
+def ingest(nat, pool, cpu_ok, reps=20):
+    """Ingest (PLY read + VoxelGridCmd) of one bench scan: the scan written as
+    a binary PLY and read into pinned host buffers (phgpu_ply_read), then
+    downsampled with leaf 0.25 (phgpu_voxel_grid_filter).  The filter is
+    synchronous (it returns the leaf count), so its time is the wall time per
+    call: host buffers in and out (copies included) and device-resident
+    buffers.  Algorithmic bytes: 16 per point in (x, y, z, intensity) and 16
+    per leaf out.  CPU: the oracle's single-thread restatement of
+    pcl::VoxelGrid on the same scan."""
+    import tempfile
+    import torch
+    from phaser_b200.profile_ingest import write_ply
+    cl = pool[0].target
+    n = int(cl.xyzi.shape[0])
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "scan.ply")
+        write_ply(path, cl.xyzi, cl.reflectivity)
+        nat.ply_read(path, pinned=True)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            ply = nat.ply_read(path, pinned=True)
+        t_ply = (time.perf_counter() - t0) / 3
+    vg = nat.VoxelGrid(max(1 << 18, n))
+    dev = torch.from_numpy(cl.xyzi).cuda()
+    for _ in range(3):
+        out, _, _ = vg.filter(dev, (0.25,) * 3, out_device=True)
+        vg.filter(ply["xyzi"], (0.25,) * 3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        out, _, _ = vg.filter(dev, (0.25,) * 3, out_device=True)
+    t_dev = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        vg.filter(ply["xyzi"], (0.25,) * 3)
+    t_host = (time.perf_counter() - t0) / reps
+    vg.close()
+    leaves = int(out.shape[0])
+    nb = 16 * n + 16 * leaves
+    peak, src = measured_peak()
+    res = {"workload": f"voxel grid (leaf 0.25 m) of one {n}-point bench scan, read from a binary PLY",
+           "points": n, "leaves": leaves, "ply_read_pinned_ms": round(1e3 * t_ply, 3),
+           "voxel_grid_ms": round(1e3 * t_host, 4), "voxel_grid_device_ms": round(1e3 * t_dev, 4),
+           "points_per_s": round(n / t_host, 1),
+           "roofline": {"bound": "hbm", "achieved": round(nb / t_dev / 1e9, 2), "peak": peak, "unit": "GB/s",
+                        "frac": round(nb / t_dev / 1e9 / peak, 5), "algorithmic_bytes": nb,
+                        "basis": "device-resident call wall time (launch-latency bound at this size)"}}
+    if cpu_ok:
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        for _ in range(3):
+            O.voxel_grid(cl.xyzi, 0.25)
+        res["cpu_baseline"] = {"ms": round(1e3 * (time.perf_counter() - t0) / 3, 3), "cores": 1, "kind": "port",
+                               "sample": "the same scan, oracle restatement of pcl::VoxelGrid"}
+    return res
+
+
 # ------------------------------------------------------------------ CPU
 
 def cpu_reference(pair, w, threads=None):
@@ -415,6 +472,14 @@ def main():
     # ---------------- roofline of the dominant stage (rank 0 context, profiled)
     roof = roofline(nat, pool, params, value / world)
 
+    # ---------------- ingest: PLY read + voxel-grid downsample (rank 0)
+    ing = None
+    if rank == 0:
+        try:
+            ing = ingest(nat, pool, world == 1 and not a.no_cpu_baseline)
+        except Exception as exc:  # the headline line is printed regardless
+            ing = {"error": f"{type(exc).__name__}: {exc}"}
+
     # ---------------- CPU baseline (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -444,6 +509,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": int(launches),
+            "ingest": ing,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

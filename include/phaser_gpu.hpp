@@ -152,13 +152,13 @@ class SphericalCorrelationLowPass : public SphericalCorrelation {
 
 // SpatialCorrelation(n_voxels, zero_padding) / SpatialCorrelationLaplace.
 // correlateSignals returns a pointer owned by the object, valid until the next
-// call (spatial-correlation.cc:128-175).
+// call, to getCorrelationSize() values (spatial-correlation.cc:163-206); with
+// zero padding the correlation covers (n_voxels + 2 zero_padding)^3 voxels.
 class SpatialCorrelation {
  public:
   explicit SpatialCorrelation(const uint32_t n_voxels, const uint32_t zero_padding = 0,
                               const phgpu_params& base = default_params())
-      : n_(n_voxels) {
-    if (zero_padding != 0) throw std::invalid_argument("spatial zero padding is not supported");
+      : n_(n_voxels), pad_(zero_padding) {
     make(base, PHGPU_FUSION_NONE);
   }
   virtual ~SpatialCorrelation() { delete ctx_; }
@@ -168,7 +168,7 @@ class SpatialCorrelation {
       throw std::invalid_argument("correlateSignals: channel counts differ or are zero");
     detail::check(phgpu_spatial_correlate(ctx_->get(), f.data(), g.data(), (uint32_t)f.size()),
                   ctx_->get(), "phgpu_spatial_correlate");
-    c_.resize((size_t)n_ * n_ * n_);
+    c_.resize(getCorrelationSize());
     detail::check(phgpu_spatial_result(ctx_->get(), &peak_voxel_, nullptr, c_.data()), ctx_->get(),
                   "phgpu_spatial_result");
     return c_.data();
@@ -181,23 +181,25 @@ class SpatialCorrelation {
     return correlateSignals(fp, gp);
   }
 #endif
-  uint32_t getZeroPadding() const { return 0; }
-  uint32_t getCorrelationSize() const { return n_ * n_ * n_; }
+  uint32_t getZeroPadding() const { return pad_; }
+  uint32_t getCorrelationSize() const { return phgpu_spatial_correlation_size(ctx_->get()); }
   uint32_t getPeakVoxel() const { return peak_voxel_; }
 
  protected:
-  SpatialCorrelation(const uint32_t n_voxels, int fusion, const phgpu_params& base) : n_(n_voxels) {
+  SpatialCorrelation(const uint32_t n_voxels, const uint32_t zero_padding, int fusion, const phgpu_params& base)
+      : n_(n_voxels), pad_(zero_padding) {
     make(base, fusion);
   }
   void make(const phgpu_params& base, int fusion) {
     phgpu_params p = base;
     p.spatial_n_voxels = n_;
+    p.spatial_zero_padding = pad_;
     p.spatial_fusion = (uint32_t)fusion;
     p.flags |= PHGPU_FLAG_KEEP_VOLUMES;
     if (p.spherical_bandwidth < 2) p.spherical_bandwidth = 2;
     ctx_ = new detail::Context(p);
   }
-  uint32_t n_;
+  uint32_t n_, pad_;
   detail::Context* ctx_ = nullptr;
   std::vector<double> c_;
   uint32_t peak_voxel_ = 0;
@@ -207,9 +209,7 @@ class SpatialCorrelationLaplace : public SpatialCorrelation {
  public:
   explicit SpatialCorrelationLaplace(const uint32_t n_voxels, const uint32_t zero_padding = 0,
                                      const phgpu_params& base = default_params())
-      : SpatialCorrelation(n_voxels, PHGPU_FUSION_LAPLACE, base) {
-    if (zero_padding != 0) throw std::invalid_argument("spatial zero padding is not supported");
-  }
+      : SpatialCorrelation(n_voxels, zero_padding, PHGPU_FUSION_LAPLACE, base) {}
 };
 
 // SpatialCorrelationLowPass(n_voxels, zero_padding[, lower, upper]): channel 1
@@ -228,10 +228,8 @@ class SpatialCorrelationLowPass : public SpatialCorrelation {
                                   base) {}
   SpatialCorrelationLowPass(const uint32_t n_voxels, const uint32_t zero_padding, const uint32_t lower,
                             const uint32_t upper, const phgpu_params& base = default_params())
-      : SpatialCorrelation(n_voxels, PHGPU_FUSION_LOW_PASS, with_bounds(base, lower, upper)),
-        lower_(lower), upper_(upper) {
-    if (zero_padding != 0) throw std::invalid_argument("spatial zero padding is not supported");
-  }
+      : SpatialCorrelation(n_voxels, zero_padding, PHGPU_FUSION_LOW_PASS, with_bounds(base, lower, upper)),
+        lower_(lower), upper_(upper) {}
   uint32_t getLowerBound() const noexcept { return lower_; }
   uint32_t getUpperBound() const noexcept { return upper_; }
   uint32_t getNumberOfIndices() const noexcept {
@@ -275,12 +273,13 @@ class PhaseAligner {
     detail::check(phgpu_spatial_correlate_voxelized(ctx_->get()), ctx_->get(), "phgpu_spatial_correlate");
   }
   std::vector<double> getCorrelation() const {
-    std::vector<double> out((size_t)prm_.spatial_n_voxels * prm_.spatial_n_voxels * prm_.spatial_n_voxels);
+    std::vector<double> out(phgpu_spatial_correlation_size(ctx_->get()));
     detail::check(phgpu_spatial_result(ctx_->get(), nullptr, nullptr, out.data()), ctx_->get(),
                   "phgpu_spatial_result");
     return out;
   }
-  uint32_t getNumberOfVoxels() const noexcept { return prm_.spatial_n_voxels; }
+  // n_voxels + 2 zero padding (phase-aligner.cc:137-139)
+  uint32_t getNumberOfVoxels() const noexcept { return prm_.spatial_n_voxels + 2 * prm_.spatial_zero_padding; }
   // the reference returns the int bounds through uint32 (phase-aligner.cc:141-147)
   uint32_t getLowerBound() const noexcept { return (uint32_t)prm_.spatial_discretize_lower; }
   uint32_t getUpperBound() const noexcept { return (uint32_t)prm_.spatial_discretize_upper; }
