@@ -25,7 +25,7 @@ struct SampleArgs {
   int max_points;       // scratch sizing
   const float4* grid;   // [n_queries] DH grid directions (host-computed)
   int n_queries;
-  int n2b = 0;          // 2B when grid is the 2B x 2B DH grid (bin-seeded search), else 0
+  int n2b = 0;          // 2B: grid is the 2B x 2B DH grid (n_queries = n2b^2)
   float max_sq;         // squared voxel size (rejection threshold)
   int n_out_ch;         // channels written (1..4)
   float* out;           // [n_out_ch][n_queries]

@@ -7,14 +7,14 @@
 // cloud and output buffers on the device and cannot create a phgpu_ctx per
 // request (a context allocates its buffers).
 //
-// How: the sampler's scratch (projected points, cell keys, sorted points,
-// cell counts, cell records, direction-bin maps) and the grid directions live
+// How: the sampler's scratch (projected points, bin keys, bin-sorted points,
+// bin and row counts, bin starts, row tables, occupancy maps) and the grid directions live
 // in one file-scope __device__ array of fixed size.  The first call on each device, with that
 // device current, looks the array's address up with cudaGetSymbolAddress
 // (this may load the module on that device); it should therefore come before
 // any stream capture.  Later calls reuse the cached address.  Every call runs
 // the same kernels as phgpu_sample_s2 (launch_sample), which clears the
-// parts that must start at zero -- fine and coarse cell counts, cursors, the
+// parts that must start at zero -- bin and row counts, cursors, the
 // direction-bin maps -- with cudaMemsetAsync on the caller's stream and
 // rebuilds everything else from the points; nothing relies on the array's
 // load-time contents or on an earlier call's.

@@ -45,12 +45,25 @@ int main() {
     std::printf("sph_laplace_bin %zu %u bw_out %u\n", best, corr.getPeakBin(), corr.getBandwidth());
     if (best != corr.getPeakBin() || vol.size() != 8u * bw * bw * bw) return 2;
   }
+  // zero padding: the correlation covers (n + 2 pad)^3 voxels, of which the
+  // reference reports uint32(n^3 ((n + 2 pad) / n)^3)
+  {
+    std::vector<double> f(27, 0.0), g(27, 0.0);
+    f[0] = 1.0;
+    g[1] = 1.0;
+    SpatialCorrelation corr(3u, 1u);
+    const double ratio = 5.0 / 3.0;
+    const uint32_t want = (uint32_t)(27.0 * (ratio * ratio * ratio));
+    corr.correlateSignals({f.data()}, {g.data()});
+    std::printf("padded_size %u %u\n", corr.getCorrelationSize(), want);
+    if (corr.getCorrelationSize() != want || corr.getZeroPadding() != 1u) return 3;
+  }
   // invalid configuration is reported as an exception, not an abort
   try {
-    SpatialCorrelation bad(4u, 2u);
-    return 3;
-  } catch (const std::invalid_argument&) {
-    std::printf("zero_padding_rejected\n");
+    SpatialCorrelation bad(1000u, 20u);  // n + 2 pad > 1024
+    return 4;
+  } catch (const std::runtime_error&) {
+    std::printf("invalid_configuration_rejected\n");
   }
   std::printf("ok\n");
   return 0;
