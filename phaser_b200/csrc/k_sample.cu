@@ -87,16 +87,22 @@ __global__ void k_project(const float4* __restrict__ xyzi, int P, float4* __rest
 // counts offset by the points of rows < r; row_nxt[r] = first non-empty row
 // >= r (n2b if none), row_prv[r] = last non-empty row < r (-1 if none).
 constexpr int kBinScanThreads = 256;
+constexpr int kMaxGridSide = 1024;  // 2B for B <= 512
 
 __global__ void __launch_bounds__(kBinScanThreads) k_bin_scan(int n2b, const uint32_t* __restrict__ bin_count,
                                                               const uint32_t* __restrict__ row_count,
                                                               uint32_t* __restrict__ bin_start,
                                                               int* __restrict__ row_nxt, int* __restrict__ row_prv) {
+  __shared__ uint32_t s_rows[kMaxGridSide];
   __shared__ uint32_t s_w[kBinScanThreads / 32];
   __shared__ uint32_t s_base;
   const int r = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
   uint32_t part = 0;
-  for (int q = t; q < r; q += kBinScanThreads) part += __ldg(&row_count[q]);
+  for (int q = t; q < n2b; q += kBinScanThreads) {
+    const uint32_t v = __ldg(&row_count[q]);
+    s_rows[q] = v;
+    part += q < r ? v : 0u;
+  }
   for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
   if (lane == 0) s_w[warp] = part;
   __syncthreads();
@@ -105,14 +111,14 @@ __global__ void __launch_bounds__(kBinScanThreads) k_bin_scan(int n2b, const uin
     for (int k = 0; k < kBinScanThreads / 32; ++k) b += s_w[k];
     s_base = b;
     int nx = r;
-    while (nx < n2b && __ldg(&row_count[nx]) == 0u) ++nx;
+    while (nx < n2b && s_rows[nx] == 0u) ++nx;
     row_nxt[r] = nx;
     int pv = r - 1;
-    while (pv >= 0 && __ldg(&row_count[pv]) == 0u) --pv;
+    while (pv >= 0 && s_rows[pv] == 0u) --pv;
     row_prv[r] = pv;
     if (r == n2b - 1) {
       row_nxt[n2b] = n2b;
-      row_prv[n2b] = __ldg(&row_count[r]) ? r : pv;
+      row_prv[n2b] = s_rows[r] ? r : pv;
     }
   }
   __syncthreads();
@@ -392,7 +398,7 @@ static inline char* carve(char*& p, size_t bytes) {
 
 cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   const int n2b = a.n2b;
-  if (n2b <= 0 || (size_t)n2b * n2b != (size_t)a.n_queries) return cudaErrorInvalidValue;
+  if (n2b <= 0 || n2b > kMaxGridSide || (size_t)n2b * n2b != (size_t)a.n_queries) return cudaErrorInvalidValue;
   const size_t nbins = (size_t)n2b * n2b;
   char* p = (char*)a.scratch;
   float4* proj = (float4*)carve(p, (size_t)a.max_points * sizeof(float4));
