@@ -170,14 +170,14 @@ def pair_bytes(bw, N, C, P):
 # DRAM read + write per stage call from the ncu capture summarised in
 # profiles/traffic_register_pair_B100_N200.md (sum over the stage's kernels).
 NCU_TRAFFIC_B100_N200 = {
-    "s2_sample": (2.19 + 0.14 + 2.67 + 2.15 + 5.27) * 1e6,   # project, cell_scan, scatter, records, nn_grid
+    "s2_sample": (2.16 + 0.17 + 2.71 + 4.44) * 1e6,          # project, bin_scan, bin_scatter, nn_rows
     "sht": 4.54e6,
     "fuse_s2": 0.32e6,
-    "so3_synth": (2.18 + 1.98) * 1e6,
+    "so3_synth": (2.20 + 2.00) * 1e6,
     "so3_fft": (31.86 + 32.02) * 1e6,
     "voxelize": (8.25 + 0.83 + 0.31) * 1e6,                  # voxelize + clear
-    "spatial_fwd": (40.77 + 38.67) * 1e6,
-    "fuse_z": (200.54 + 20.29) * 1e6,
+    "spatial_fwd": (40.85 + 38.50) * 1e6,
+    "fuse_z": (200.53 + 20.37) * 1e6,
     "spatial_inv": 33.35e6,
 }
 
