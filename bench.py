@@ -67,9 +67,32 @@ def workload_desc():
                "channels range/intensity/reflectivity")
 
 
+def pool_seeds(rank, n):
+    """Pair seeds of one rank: disjoint across ranks (the pairs are sharded,
+    each rank registers its own)."""
+    return [rank * 1000 + j for j in range(n)]
+
+
 def make_pool(rank, n):
     from phaser_b200 import scene
-    return [scene.workload_pair(WORKLOAD, rank * 1000 + j) for j in range(n)]
+    return [scene.workload_pair(WORKLOAD, k) for k in pool_seeds(rank, n)]
+
+
+def max_over_ranks(x, dist=None, device="cuda"):
+    """Largest value of x over the ranks (the job's time is its slowest
+    rank's); x itself without a process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, steps, pairs_per_step, max_ms):
+    """Whole-job registrations/s: every rank registers steps x pairs_per_step
+    pairs within the slowest rank's window."""
+    return world * steps * pairs_per_step / (max_ms * 1e-3)
 
 
 # ------------------------------------------------------------------ clocks
@@ -382,13 +405,6 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # ---------------- plain GPU pipeline (one pair at a time)
     ctx = nat.Context(params)
     for i in range(W * S):
@@ -404,8 +420,8 @@ def main():
         plain_lat.append(1e3 * (time.perf_counter() - t))
     e1.record()
     e1.synchronize()
-    plain_ms = max_over_ranks(e0.elapsed_time(e1))
-    plain_value = world * K * S / (plain_ms * 1e-3)
+    plain_ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    plain_value = job_rate(world, K, S, plain_ms)
     ctx.close()
 
     # ---------------- served pipeline, device-resident inputs (value)
@@ -437,8 +453,8 @@ def main():
     launches = nat.launch_count() - l0
     time.sleep(0.2)
     clocks = sampler.stop()
-    served_ms = max_over_ranks(e0.elapsed_time(e1))
-    value = world * K * S / (served_ms * 1e-3)
+    served_ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    value = job_rate(world, K, S, served_ms)
 
     # ---------------- e2e: served, pinned host inputs through the public API
     served_round(pinned_np, S)
@@ -448,8 +464,8 @@ def main():
         served_round(pinned_np, S)
     e1.record()
     e1.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = world * K * S / (e2e_ms * 1e-3)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    e2e_value = job_rate(world, K, S, e2e_ms)
 
     # ---------------- open-loop Poisson arrivals at 80% of the served rate
     rate = 0.8 * value / world
