@@ -179,6 +179,16 @@ WORKLOADS = {
 }
 
 
+# Served mix of arrivals (weight, shape): 50 % B = 64 / N = 128, 35 % B = 100 /
+# N = 200, 15 % B = 128 / N = 256, all over [-10, 10]^3 m; scans of the
+# given beam count x 1024 columns, seeds 1000 * 3 + k.
+CONFIG3_MIX = [
+    (0.50, dict(beams=64, bw=64, n_voxels=128, lo=-10, hi=10)),
+    (0.35, dict(beams=128, bw=100, n_voxels=200, lo=-10, hi=10)),
+    (0.15, dict(beams=128, bw=128, n_voxels=256, lo=-10, hi=10)),
+]
+
+
 def workload_pair(workload: int, k: int = 0) -> Pair:
     w = WORKLOADS[workload]
     return make_pair(workload, k, w["beams"], w["cols"], w["reflectivity"])

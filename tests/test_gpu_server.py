@@ -1,6 +1,7 @@
 """Request server (phgpu_server_*): poses of served requests equal those of the
-plain context, for host (copied or borrowed) and device inputs and for
-requests of different shapes in flight together."""
+plain context -- bins, voxels and the correlation values at the peaks -- for
+host (copied or borrowed) and device inputs and for requests of different
+shapes in flight together."""
 import numpy as np
 import pytest
 
@@ -16,7 +17,7 @@ def _reference_poses(nat, params, pairs):
     c = nat.Context(params)
     out = [c.register_pair((p.target.xyzi, None), (p.source.xyzi, None)) for p in pairs]
     c.close()
-    return [(q.rot_bin, q.voxel) for q in out]
+    return [(q.rot_bin, q.voxel, q.rot_peak, q.trans_peak) for q in out]
 
 
 @pytest.mark.parametrize("flags", [0, 1])
@@ -44,7 +45,11 @@ def test_server_matches_context(flags):
     for kind, i, t in tickets:
         pose, lat = srv.poll(t)
         expect = want_small[i] if kind == "small" else want[i]
-        assert (pose.rot_bin, pose.voxel) == expect, (kind, i)
+        assert (pose.rot_bin, pose.voxel) == expect[:2], (kind, i)
+        # the correlation values at the peaks: the same volumes alone and in a
+        # mixed wave (voxel sums are float atomics: equal within 1e-5)
+        assert pose.rot_peak == pytest.approx(expect[2], rel=1e-5), (kind, i)
+        assert pose.trans_peak == pytest.approx(expect[3], rel=1e-5), (kind, i)
         assert lat > 0
     srv.close()
 
