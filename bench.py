@@ -370,6 +370,32 @@ def config3(nat, local, rates=(50, 200, 500, 1000, 2000), seconds=1.0, cap=600):
             "hbm_budget_gb": 150, "server_workers": workers, "inputs": "clouds resident in HBM", "rates": out}
 
 
+def run_script_config(nat, pool, local, reps=10):
+    """One pair at a time with the configuration of the reference's run script
+    (phaser_share/run_phaser_core_driver: B = 150 with spherical zero padding
+    10, N = 201 voxels over [-50, 50]^3 m) on the bench scans, clouds resident
+    in HBM: registrations/s and the latency of one pair."""
+    import torch
+    params = nat.default_params(spherical_bandwidth=150, spherical_zero_padding=10, spatial_n_voxels=201,
+                                spatial_discretize_lower=-50, spatial_discretize_upper=50, max_points=1 << 18,
+                                device=local)
+    ctx = nat.Context(params)
+    dev = [((torch.from_numpy(p.target.xyzi).cuda(), torch.from_numpy(p.target.reflectivity).cuda()),
+            (torch.from_numpy(p.source.xyzi).cuda(), torch.from_numpy(p.source.reflectivity).cuda()))
+           for p in pool]
+    for i in range(3):
+        ctx.register_pair(*dev[i % len(dev)])
+    lat = []
+    for i in range(reps):
+        t0 = time.perf_counter()
+        ctx.register_pair(*dev[i % len(dev)])
+        lat.append(1e3 * (time.perf_counter() - t0))
+    ctx.close()
+    return {"config": "B=150 + spherical zero padding 10 (SO(3) on 320^3), N=201 over [-50,50]^3 m",
+            "plain_gpu_per_s": round(1e3 / float(np.mean(lat)), 2), "p50_ms": round(pct(lat, 50), 3),
+            "p99_ms": round(pct(lat, 99), 3)}
+
+
 # ------------------------------------------------------------------ CPU
 
 def cpu_reference(pair, w, threads=None):
@@ -548,6 +574,14 @@ def main():
         except Exception as exc:  # the headline line is printed regardless
             mix = {"error": f"{type(exc).__name__}: {exc}"}
 
+    # ---------------- the reference run script's configuration (rank 0)
+    rsc = None
+    if rank == 0:
+        try:
+            rsc = run_script_config(nat, pool, local)
+        except Exception as exc:  # the headline line is printed regardless
+            rsc = {"error": f"{type(exc).__name__}: {exc}"}
+
     # ---------------- ingest: PLY read + voxel-grid downsample (rank 0)
     ing = None
     if rank == 0:
@@ -587,6 +621,7 @@ def main():
             "gpu_launches": int(launches),
             "ingest": ing,
             "mixed_arrivals": mix,
+            "run_script_config": rsc,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -182,45 +182,95 @@ __device__ __forceinline__ void fft_stage(float2* buf, int ntrans, int tstride, 
 }
 
 // Radix-R stage for any R <= kMaxGenericRadix (rare lengths with a large prime
-// factor): O(R^2) butterfly through a local buffer, twiddles from the table.
+// factor, e.g. 201 = 3 * 67): the O(R^2) butterfly spread over threads.  A
+// work item is kGenericOuts outputs of one butterfly, summed from the inputs
+// in shared memory with table twiddles (index j * k mod R kept incrementally).
+// Butterflies are processed in rounds of whole butterflies: every item of a
+// round reads, the block synchronises, then writes, so the in-place update
+// never overwrites an input another item still needs.  The inverse stage
+// first multiplies its inputs by the conjugate twiddles in place.  Contains
+// __syncthreads(): every thread of the block must call it.
 constexpr int kMaxGenericRadix = 128;
+constexpr int kGenericOuts = 4;
+
+__device__ __forceinline__ float2* generic_base(float2* buf, int bfi, int ntrans, int nb, int m, int L, int tstride,
+                                                int estride, int& j2) {
+  int t, bf;
+  if (estride == 1) {
+    t = bfi / nb;
+    bf = bfi - t * nb;
+  } else {
+    bf = bfi / ntrans;
+    t = bfi - bf * ntrans;
+  }
+  const int blk = bf / m;
+  j2 = bf - blk * m;
+  return buf + t * tstride + (blk * L + j2) * estride;
+}
 
 template <bool INV>
 __device__ __noinline__ void fft_stage_generic(float2* buf, int R, int ntrans, int tstride, int estride, int n,
                                                int L, const float2* __restrict__ tw, int tid, int nthr) {
   const int m = L / R;
   const int nb = n / R;
-  const int total = ntrans * nb;
+  const int nbf = ntrans * nb;  // butterflies
   const int twstep = n / L;
   const int es = m * estride;
   const int rstep = n / R;
-  float2 x[kMaxGenericRadix];
-  for (int it = tid; it < total; it += nthr) {
-    int t, bf;
-    if (estride == 1) {
-      t = it / nb;
-      bf = it - t * nb;
-    } else {
-      bf = it / ntrans;
-      t = it - bf * ntrans;
+  const int ng = (R + kGenericOuts - 1) / kGenericOuts;  // output groups per butterfly
+  if (INV) {
+    for (int it = tid; it < nbf * R; it += nthr) {
+      const int bfi = it / R, j = it - bfi * R;
+      if (j == 0) continue;
+      int j2;
+      float2* base = generic_base(buf, bfi, ntrans, nb, m, L, tstride, estride, j2);
+      base[j * es] = cmul(base[j * es], cconj(__ldg(&tw[twstep * j2 * j])));
     }
-    const int blk = bf / m;
-    const int j2 = bf - blk * m;
-    float2* base = buf + t * tstride + (blk * L + j2) * estride;
-    for (int j = 0; j < R; ++j) {
-      x[j] = base[j * es];
-      if (INV && j > 0) x[j] = cmul(x[j], cconj(__ldg(&tw[twstep * j2 * j])));
-    }
-    for (int k = 0; k < R; ++k) {
-      float2 acc = x[0];
-      for (int j = 1; j < R; ++j) {
-        float2 w = __ldg(&tw[rstep * ((j * k) % R)]);
-        if (INV) w = cconj(w);
-        acc = cadd(acc, cmul(x[j], w));
+    __syncthreads();
+  }
+  const int bf_round = max(1, nthr / ng);
+  for (int b0 = 0; b0 < nbf; b0 += bf_round) {
+    const int nitems = min(bf_round, nbf - b0) * ng;
+    const bool active = tid < nitems;
+    float2 acc[kGenericOuts];
+    float2* base = nullptr;
+    int j2 = 0, k0 = 0;
+    if (active) {
+      const int bfi = b0 + tid / ng;
+      k0 = (tid - (tid / ng) * ng) * kGenericOuts;
+      base = generic_base(buf, bfi, ntrans, nb, m, L, tstride, estride, j2);
+      int kk[kGenericOuts], mi[kGenericOuts];
+#pragma unroll
+      for (int i = 0; i < kGenericOuts; ++i) {
+        kk[i] = k0 + i < R ? k0 + i : 0;  // padding outputs of the last group stay at index 0
+        mi[i] = 0;
+        acc[i] = base[0];
       }
-      if (!INV && k > 0) acc = cmul(acc, __ldg(&tw[twstep * j2 * k]));
-      base[k * es] = acc;
+      for (int j = 1; j < R; ++j) {
+        const float2 xj = base[j * es];
+#pragma unroll
+        for (int i = 0; i < kGenericOuts; ++i) {
+          mi[i] += kk[i];
+          if (mi[i] >= R) mi[i] -= R;
+          float2 w = __ldg(&tw[rstep * mi[i]]);
+          if (INV) w = cconj(w);
+          acc[i] = cadd(acc[i], cmul(xj, w));
+        }
+      }
     }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < kGenericOuts; ++i) {
+        const int k = k0 + i;
+        if (k < R) {
+          float2 a = acc[i];
+          if (!INV && k > 0) a = cmul(a, __ldg(&tw[twstep * j2 * k]));
+          base[k * es] = a;
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 

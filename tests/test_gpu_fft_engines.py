@@ -23,12 +23,14 @@ def test_fft_engine(engine, n, columns, inverse):
     assert err < 5e-6, err
 
 
-@pytest.mark.parametrize("n", [3, 12, 38, 134, 201])
-def test_fft_runtime_engine_odd_lengths(n):
+@pytest.mark.parametrize("n", [3, 12, 38, 127, 134, 201, 254])
+@pytest.mark.parametrize("columns", [False, True])
+def test_fft_runtime_engine_odd_lengths(n, columns):
+    # large prime factors (19, 67, 127) run through the generic radix stage
     from phaser_b200 import native
     rng = np.random.default_rng(n)
-    x = (rng.standard_normal((4, n)) + 1j * rng.standard_normal((4, n))).astype(np.complex64)
+    x = (rng.standard_normal((7, n)) + 1j * rng.standard_normal((7, n))).astype(np.complex64)
     for inverse in (False, True):
-        y = native.selftest_fft(x, inverse=inverse, columns=False, engine=0)
+        y = native.selftest_fft(x, inverse=inverse, columns=columns, engine=0)
         ref = np.fft.ifft(x.astype(np.complex128), axis=1) * n if inverse else np.fft.fft(x.astype(np.complex128), axis=1)
         assert np.abs(y - ref).max() / np.abs(ref).max() < 5e-6

@@ -293,6 +293,15 @@ def test_register_pair_workload1_full_size(nat, k):
     assert (pose2.rot_bin, pose2.voxel) == (pose.rot_bin, pose.voxel)
 
 
+def test_register_pair_run_script_grid(nat):
+    # the translation grid of the reference's run script
+    # (phaser_share/run_phaser_core_driver: N = 201 voxels over [-50, 50]^3 m,
+    # an odd size on the runtime-plan kernels) with the bench scans at B = 100
+    from phaser_b200 import scene
+    w = dict(scene.WORKLOADS[1], n_voxels=201, lo=-50, hi=50)
+    _register_and_compare(nat, w, scene.workload_pair(1, 0), want_volumes=False)
+
+
 def test_context_reuse_leaves_no_state():
     """Grids are cleared point by point after each registration instead of
     being memset: a context that registered other pairs first must give the
