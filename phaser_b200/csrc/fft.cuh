@@ -183,8 +183,9 @@ __device__ __forceinline__ void fft_stage(float2* buf, int ntrans, int tstride, 
 
 // Radix-R stage for any R <= kMaxGenericRadix (rare lengths with a large prime
 // factor, e.g. 201 = 3 * 67): the O(R^2) butterfly spread over threads.  A
-// work item is kGenericOuts outputs of one butterfly, summed from the inputs
-// in shared memory with table twiddles (index j * k mod R kept incrementally).
+// work item is kGenericOuts outputs of kGenericBfs butterflies, summed from
+// the inputs in shared memory with table twiddles (index j * k mod R kept
+// incrementally).
 // Butterflies are processed in rounds of whole butterflies: every item of a
 // round reads, the block synchronises, then writes, so the in-place update
 // never overwrites an input another item still needs.  The inverse stage
@@ -192,6 +193,7 @@ __device__ __forceinline__ void fft_stage(float2* buf, int ntrans, int tstride, 
 // __syncthreads(): every thread of the block must call it.
 constexpr int kMaxGenericRadix = 128;
 constexpr int kGenericOuts = 4;
+constexpr int kGenericBfs = 4;
 
 __device__ __forceinline__ float2* generic_base(float2* buf, int bfi, int ntrans, int nb, int m, int L, int tstride,
                                                 int estride, int& j2) {
@@ -228,45 +230,64 @@ __device__ __noinline__ void fft_stage_generic(float2* buf, int R, int ntrans, i
     }
     __syncthreads();
   }
-  const int bf_round = max(1, nthr / ng);
-  for (int b0 = 0; b0 < nbf; b0 += bf_round) {
-    const int nitems = min(bf_round, nbf - b0) * ng;
+  // an item: kGenericOuts outputs of kGenericBfs consecutive butterflies (a
+  // twiddle load serves every butterfly, an input load every output)
+  const int nbg = (nbf + kGenericBfs - 1) / kGenericBfs;  // butterfly groups
+  const int grp_round = max(1, nthr / ng);
+  for (int g0 = 0; g0 < nbg; g0 += grp_round) {
+    const int nitems = min(grp_round, nbg - g0) * ng;
     const bool active = tid < nitems;
-    float2 acc[kGenericOuts];
-    float2* base = nullptr;
-    int j2 = 0, k0 = 0;
+    float2 acc[kGenericBfs][kGenericOuts];
+    float2* base[kGenericBfs];
+    int j2[kGenericBfs];
+    bool live[kGenericBfs];
+    int k0 = 0;
     if (active) {
-      const int bfi = b0 + tid / ng;
+      const int grp = g0 + tid / ng;
       k0 = (tid - (tid / ng) * ng) * kGenericOuts;
-      base = generic_base(buf, bfi, ntrans, nb, m, L, tstride, estride, j2);
+#pragma unroll
+      for (int u = 0; u < kGenericBfs; ++u) {
+        const int bfi = grp * kGenericBfs + u;
+        live[u] = bfi < nbf;
+        base[u] = generic_base(buf, live[u] ? bfi : 0, ntrans, nb, m, L, tstride, estride, j2[u]);
+        const float2 x0 = base[u][0];
+#pragma unroll
+        for (int i = 0; i < kGenericOuts; ++i) acc[u][i] = x0;
+      }
       int kk[kGenericOuts], mi[kGenericOuts];
 #pragma unroll
       for (int i = 0; i < kGenericOuts; ++i) {
         kk[i] = k0 + i < R ? k0 + i : 0;  // padding outputs of the last group stay at index 0
         mi[i] = 0;
-        acc[i] = base[0];
       }
       for (int j = 1; j < R; ++j) {
-        const float2 xj = base[j * es];
+        float2 xj[kGenericBfs];
+#pragma unroll
+        for (int u = 0; u < kGenericBfs; ++u) xj[u] = base[u][j * es];
 #pragma unroll
         for (int i = 0; i < kGenericOuts; ++i) {
           mi[i] += kk[i];
           if (mi[i] >= R) mi[i] -= R;
           float2 w = __ldg(&tw[rstep * mi[i]]);
           if (INV) w = cconj(w);
-          acc[i] = cadd(acc[i], cmul(xj, w));
+#pragma unroll
+          for (int u = 0; u < kGenericBfs; ++u) acc[u][i] = cadd(acc[u][i], cmul(xj[u], w));
         }
       }
     }
     __syncthreads();
     if (active) {
 #pragma unroll
-      for (int i = 0; i < kGenericOuts; ++i) {
-        const int k = k0 + i;
-        if (k < R) {
-          float2 a = acc[i];
-          if (!INV && k > 0) a = cmul(a, __ldg(&tw[twstep * j2 * k]));
-          base[k * es] = a;
+      for (int u = 0; u < kGenericBfs; ++u) {
+        if (!live[u]) continue;
+#pragma unroll
+        for (int i = 0; i < kGenericOuts; ++i) {
+          const int k = k0 + i;
+          if (k < R) {
+            float2 a = acc[u][i];
+            if (!INV && k > 0) a = cmul(a, __ldg(&tw[twstep * j2[u] * k]));
+            base[u][k * es] = a;
+          }
         }
       }
     }
