@@ -244,7 +244,7 @@ unsigned long long phgpu_launch_count(void);
  * transforms ntrans sequences of length n (complex interleaved, natural order,
  * sequence-major, in place in `data`) laid out as shared-memory rows or
  * columns; engine 0 = runtime plan, 1 = compile-time plan, 2 = register-tail
- * plan (1 and 2 for n in {32, 64, 100, 128, 200, 256, 512}).  Forward =
+ * plan (1 and 2 for n in {32, 64, 100, 128, 200, 256, 512}; 1 also for 320).  Forward =
  * exp(-2 pi i jk/n), inverse = exp(+2 pi i jk/n), both unnormalised. */
 int phgpu_selftest_fft(int n, int ntrans, int inverse, int columns, int engine, float* data);
 

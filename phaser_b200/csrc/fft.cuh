@@ -369,6 +369,11 @@ struct FixedFft<512> {
   static constexpr int count = 3;
   static constexpr int r[3] = {8, 8, 8};
 };
+template <>
+struct FixedFft<320> {  // 2 bw_out for bw_out = 160 (B = 150 with zero padding 10)
+  static constexpr int count = 3;
+  static constexpr int r[3] = {8, 8, 5};
+};
 
 template <int N>
 constexpr bool fixed_fft_supported() {
@@ -582,6 +587,10 @@ __device__ __forceinline__ int pos2freq(int pos, const FftPlan& p) {
     } break;                                \
     case 512: {                             \
       constexpr int NF = 512;               \
+      __VA_ARGS__;                          \
+    } break;                                \
+    case 320: {                             \
+      constexpr int NF = 320;               \
       __VA_ARGS__;                          \
     } break;                                \
     default: {                              \

@@ -109,6 +109,12 @@ int phgpu_selftest_fft(int n, int ntrans, int inverse, int columns, int engine, 
       PHGPU_SELFTEST_CASE(256)
       PHGPU_SELFTEST_CASE(512)
 #undef PHGPU_SELFTEST_CASE
+      case 320:  // compile-time plan only (no register-tail plan)
+        if (engine == 1)
+          e = run_selftest<320, 1>(n, ntrans, inverse, columns, din, dout, p);
+        else
+          rc = PHGPU_ERR_INVALID;
+        break;
       default:
         rc = PHGPU_ERR_INVALID;
     }

@@ -34,3 +34,15 @@ def test_fft_runtime_engine_odd_lengths(n, columns):
         y = native.selftest_fft(x, inverse=inverse, columns=columns, engine=0)
         ref = np.fft.ifft(x.astype(np.complex128), axis=1) * n if inverse else np.fft.fft(x.astype(np.complex128), axis=1)
         assert np.abs(y - ref).max() / np.abs(ref).max() < 5e-6
+
+
+@pytest.mark.parametrize("columns", [False, True])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_fft_compile_time_plan_320(columns, inverse):
+    # 2 bw_out of the reference run script's rotation (B = 150, padding 10)
+    from phaser_b200 import native
+    rng = np.random.default_rng(320)
+    x = (rng.standard_normal((24, 320)) + 1j * rng.standard_normal((24, 320))).astype(np.complex64)
+    y = native.selftest_fft(x, inverse=inverse, columns=columns, engine=1)
+    ref = np.fft.ifft(x.astype(np.complex128), axis=1) * 320 if inverse else np.fft.fft(x.astype(np.complex128), axis=1)
+    assert np.abs(y - ref).max() / np.abs(ref).max() < 5e-6
