@@ -233,7 +233,7 @@ static cudaError_t so3_attrs() {
 
 cudaError_t so3_init_attributes() {
   cudaError_t e = cudaSuccess;
-  for (int n : {64, 128, 200, 256, 512, 0}) {
+  for (int n : {64, 128, 200, 256, 320, 512, 0}) {  // every length PHGPU_DISPATCH_N instantiates
     cudaError_t r = cudaSuccess;
     PHGPU_DISPATCH_N(n, r = so3_attrs<NF>());
     if (r != cudaSuccess) e = r;

@@ -584,7 +584,7 @@ static cudaError_t set_attrs() {
 
 cudaError_t spatial_init_attributes() {
   cudaError_t e = cudaSuccess;
-  for (int n : {64, 128, 200, 256, 512, 0}) {
+  for (int n : {64, 128, 200, 256, 320, 512, 0}) {  // every length PHGPU_DISPATCH_N instantiates
     cudaError_t r = cudaSuccess;
     PHGPU_DISPATCH_N(n, r = set_attrs<NF>());
     if (r != cudaSuccess) e = r;

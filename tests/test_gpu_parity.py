@@ -136,13 +136,14 @@ def test_spatial_plain_vs_oracle(nat, N):
     assert vox == O.argmax(ref)
 
 
-def test_spatial_shift_property_full_size(nat):
-    # size-independent property at N = 200: every channel of the source is the
-    # target circularly shifted by d voxels -> C(k) = w(k) e^{i k d} with w >= 0
-    # for all three fusion rules, so the correlation peaks exactly at the shift.
-    N = 200
+@pytest.mark.parametrize("N,C", [(200, 3), (320, 2)])
+def test_spatial_shift_property_full_size(nat, N, C):
+    # size-independent property at full size: every channel of the source is
+    # the target circularly shifted by d voxels -> C(k) = w(k) e^{i k d} with
+    # w >= 0 for all three fusion rules, so the correlation peaks exactly at
+    # the shift (N = 320: the compile-time plan of length 320)
     rng = np.random.default_rng(5)
-    f = rng.random((3, N, N, N), dtype=np.float32).astype(np.float64)
+    f = rng.random((C, N, N, N), dtype=np.float32).astype(np.float64)
     d = (17, 181, 3)  # (z, x, y)
     g = np.roll(f, shift=(-d[0], -d[1], -d[2]), axis=(1, 2, 3))
     c = ctx(nat, spatial_n_voxels=N)
@@ -152,7 +153,7 @@ def test_spatial_shift_property_full_size(nat):
 
 
 @pytest.mark.parametrize("bw,pad,C", [(4, 0, 1), (8, 0, 4), (8, 2, 4), (12, 0, 3), (16, 0, 2),
-                                      (16, 3, 4), (32, 0, 4), (25, 0, 3)])
+                                      (16, 3, 4), (32, 0, 4), (25, 0, 3), (8, 152, 2)])
 def test_spherical_vs_oracle(nat, bw, pad, C):
     rng = np.random.default_rng(bw * 100 + pad * 10 + C)
     f = rng.standard_normal((C, 4 * bw * bw))
