@@ -589,6 +589,10 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
     so3_beta_table(bw_out, bt.data());
     CKV(dalloc(ctx, &ctx->d_beta_tab, sizeof(double) * bt.size()));
     CK(cudaMemcpy(ctx->d_beta_tab, bt.data(), sizeof(double) * bt.size(), cudaMemcpyHostToDevice));
+    std::vector<double> wt;
+    so3_wigner_table(bw, wt);
+    CKV(dalloc(ctx, &ctx->d_wig_tab, sizeof(double) * wt.size()));
+    CK(cudaMemcpy(ctx->d_wig_tab, wt.data(), sizeof(double) * wt.size(), cudaMemcpyHostToDevice));
   }
   const size_t nv = (size_t)N * N * N;
   const size_t H = (size_t)N * N * spatial_h2p(N);
@@ -753,6 +757,7 @@ int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStre
   o.bw_out = ctx->bw_out;
   o.fused = ctx->d_fused;
   o.beta_tab = ctx->d_beta_tab;
+  o.wig_tab = ctx->d_wig_tab;
   o.S = ctx->d_S;
   o.plan = &ctx->plan_so3;
   o.argmax = ctx->d_argmax;

@@ -62,6 +62,7 @@ struct phgpu_ctx {
   float2* d_fused = nullptr;
   float2* d_S = nullptr;
   double* d_beta_tab = nullptr;  // [3][2 bw_out] for the Wigner seeds
+  double* d_wig_tab = nullptr;   // Wigner recurrence tables (so3_wigner_table)
   float* d_rotvol = nullptr;
   // translation
   float* d_grids[2] = {nullptr, nullptr};  // [(C+1)][N^3]

@@ -17,6 +17,10 @@
 //   d_{q p} = (-1)^(q-p) d_{p q},  d_{p,-q}(b) = d_{q,-p}(b) = (-1)^(l+p) d_{p q}(pi - b)
 // at beta_k and at the mirrored beta_{2B-1-k}.  Only b = m2 >= 0 is kept
 // (half spectrum); the gamma transform is a Hermitian complex-to-real one.
+#include <math.h>
+
+#include <vector>
+
 #include "kernels.h"
 
 namespace phgpu {
@@ -34,8 +38,45 @@ __device__ __forceinline__ float2 prod_conj(float2 a, float2 b, float s) {
 // from shared memory serve KB recurrences.
 constexpr int kSynthBetas = 4;
 
+// Recurrence factors of the L2-normalised Wigner-d three-term recurrence in
+// l for degrees l < bw_in, from square roots tabulated on the host once per
+// context (so3_wigner_table), so a block's set-up is loads and products:
+//   b_l = sqrt((2l+3)/(2l+1)) (l+1)(2l+1) / (R(l+1,p) R(l+1,q))
+//   a_l = -sqrt((2l+3)/(2l-1)) (l+1)/l R(l,p) R(l,q) / (R(l+1,p) R(l+1,q))
+//   g_l = b_l (-p q / (l(l+1))),   R(l,m) = sqrt(l^2 - m^2)
+// and the seed's log normalisation from log-factorials.
+struct WigTab {
+  const double* s1;   // [B+1][B+1] R(l, m) (0 for m >= l)
+  const double* r1;   // [B+1][B+1] 1 / R(l, m) (0 for m >= l)
+  const double* cl;   // [B+1] sqrt((2l+3)/(2l+1)) (l+1)(2l+1)
+  const double* el;   // [B+1] sqrt((2l+3)/(2l-1)) (l+1)/l (l >= 1)
+  const double* il;   // [B+1] 1/(l(l+1)) (l >= 1)
+  const double* wl;   // [B+1] 2 pi sqrt(2/(2l+1))
+  const double* lq;   // [B+1] log((2q+1)/2)
+  const double* lf;   // [2B+2] log(k!)
+};
+
+__host__ __device__ inline size_t wigner_table_entries(int bw_in) {
+  const size_t b1 = (size_t)bw_in + 1;
+  return 2 * b1 * b1 + 5 * b1 + 2 * b1;
+}
+
+__host__ __device__ inline WigTab wig_tab(const double* t, int bw_in) {
+  const size_t b1 = (size_t)bw_in + 1;
+  WigTab w;
+  w.s1 = t;
+  w.r1 = w.s1 + b1 * b1;
+  w.cl = w.r1 + b1 * b1;
+  w.el = w.cl + b1;
+  w.il = w.el + b1;
+  w.wl = w.il + b1;
+  w.lq = w.wl + b1;
+  w.lf = w.lq + b1;
+  return w;
+}
+
 __global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz, const double* __restrict__ btab,
-                            float2* __restrict__ S) {
+                            const double* __restrict__ wtab, float2* __restrict__ S) {
   extern __shared__ double sm[];
   double* fa = sm;
   double* fb = fa + bw_in;
@@ -49,20 +90,16 @@ __global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz
   const int p = cidx - q * (q + 1) / 2;
   const int nl = bw_in - q;
   const double dp = p, dq = q;
+  const WigTab W = wig_tab(wtab, bw_in);
+  const int b1 = bw_in + 1;
   for (int i = threadIdx.x; i < nl; i += blockDim.x) {
     const int l = q + i;
-    const double dl = l;
-    const double tnext = sqrt(((dl + 1) * (dl + 1) - dp * dp) * ((dl + 1) * (dl + 1) - dq * dq));
-    const double b = sqrt((2 * dl + 3) / (2 * dl + 1)) * (dl + 1) * (2 * dl + 1) / tnext;
+    const double rr = __ldg(&W.r1[(l + 1) * b1 + p]) * __ldg(&W.r1[(l + 1) * b1 + q]);
+    const double b = __ldg(&W.cl[l]) * rr;
     fb[i] = b;
-    gs[i] = (l == 0) ? 0.0 : b * (-dp * dq / (dl * (dl + 1)));
-    double a = 0.0;
-    if (l > 0) {
-      const double tcur = sqrt((dl * dl - dp * dp) * (dl * dl - dq * dq));
-      a = -sqrt((2 * dl + 3) / (2 * dl - 1)) * (dl + 1) / dl * tcur / tnext;
-    }
-    fa[i] = a;
-    const float wn = (float)(2.0 * M_PI * sqrt(2.0 / (2.0 * dl + 1.0)));
+    gs[i] = (l == 0) ? 0.0 : b * (-dp * dq) * __ldg(&W.il[l]);
+    fa[i] = (l == 0) ? 0.0 : -__ldg(&W.el[l]) * __ldg(&W.s1[l * b1 + p]) * __ldg(&W.s1[l * b1 + q]) * rr;
+    const float wn = (float)__ldg(&W.wl[l]);
     const float spq = ((p + q) & 1) ? -wn : wn;
     const float slp = ((l + p) & 1) ? -1.0f : 1.0f;
     // v0: (p, q)
@@ -80,9 +117,8 @@ __global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz
     }
   }
   if (threadIdx.x == 0) {
-    // seed normalisation: 0.5 [log((2q+1)/2) + lgamma(2q+1) - lgamma(q-p+1) - lgamma(q+p+1)]
-    *s_lnorm = 0.5 * (log((2.0 * q + 1.0) / 2.0) + lgamma(2.0 * q + 1.0) - lgamma(dq - dp + 1.0) -
-                      lgamma(dq + dp + 1.0));
+    // seed normalisation: 0.5 [log((2q+1)/2) + log((2q)!) - log((q-p)!) - log((q+p)!)]
+    *s_lnorm = 0.5 * (__ldg(&W.lq[q]) + __ldg(&W.lf[2 * q]) - __ldg(&W.lf[q - p]) - __ldg(&W.lf[q + p]));
   }
   __syncthreads();
   const int n = 2 * bw_out;
@@ -143,6 +179,29 @@ __global__ void k_so3_synth(int bw_in, int bw_out, const float2* __restrict__ fz
       }
     }
   }
+}
+
+void so3_wigner_table(int bw_in, std::vector<double>& tab) {
+  tab.assign(wigner_table_entries(bw_in), 0.0);
+  const WigTab W = wig_tab(tab.data(), bw_in);
+  const int b1 = bw_in + 1;
+  double* s1 = const_cast<double*>(W.s1);
+  double* r1 = const_cast<double*>(W.r1);
+  for (int l = 0; l <= bw_in; ++l)
+    for (int m = 0; m < l; ++m) {
+      const double v = sqrt((double)l * l - (double)m * m);
+      s1[l * b1 + m] = v;
+      r1[l * b1 + m] = 1.0 / v;
+    }
+  for (int l = 0; l <= bw_in; ++l) {
+    const double dl = l;
+    const_cast<double*>(W.cl)[l] = sqrt((2 * dl + 3) / (2 * dl + 1)) * (dl + 1) * (2 * dl + 1);
+    const_cast<double*>(W.el)[l] = l > 0 ? sqrt((2 * dl + 3) / (2 * dl - 1)) * (dl + 1) / dl : 0.0;
+    const_cast<double*>(W.il)[l] = l > 0 ? 1.0 / (dl * (dl + 1)) : 0.0;
+    const_cast<double*>(W.wl)[l] = 2.0 * M_PI * sqrt(2.0 / (2.0 * dl + 1.0));
+    const_cast<double*>(W.lq)[l] = log((2.0 * dl + 1.0) / 2.0);
+  }
+  for (int k = 0; k < 2 * bw_in + 2; ++k) const_cast<double*>(W.lf)[k] = lgamma((double)k + 1.0);
 }
 
 void so3_beta_table(int bw_out, double* tab) {
@@ -247,7 +306,7 @@ cudaError_t launch_so3_synth(const So3Args& a, cudaStream_t st) {
   int thr = (((n + kSynthBetas - 1) / kSynthBetas + 31) / 32) * 32;
   if (thr > 512) thr = 512;
   const size_t sm1 = (size_t)a.bw_in * 3 * sizeof(double) + 2 * sizeof(double) + (size_t)a.bw_in * 4 * sizeof(float2);
-  k_so3_synth<<<ncls, thr, sm1, st>>>(a.bw_in, a.bw_out, a.fused, a.beta_tab, a.S);
+  k_so3_synth<<<ncls, thr, sm1, st>>>(a.bw_in, a.bw_out, a.fused, a.beta_tab, a.wig_tab, a.S);
   count_launches(1);
   return cudaGetLastError();
 }

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <vector>
 
 #include "common.cuh"
 #include "fft.cuh"
@@ -70,6 +71,7 @@ struct So3Args {
   int bw_out;             // output grid 2*bw_out
   const float2* fused;    // [2][bw_in][2 bw_in - 1]
   const double* beta_tab; // [3][2 bw_out]: cos(beta_k), log cos(beta_k / 2), log sin(beta_k / 2)
+  const double* wig_tab;  // so3_wigner_table(bw_in): recurrence square roots, per-degree factors
   float2* S;              // [2 bw_out (beta)][2 bw_out (a)][bw_out (b)]
   const FftPlan* plan;    // length 2 bw_out
   unsigned long long* argmax;  // packed (value^2, index)
@@ -79,6 +81,7 @@ cudaError_t launch_so3_synth(const So3Args& a, cudaStream_t st);  // coefficient
 cudaError_t launch_so3_fft(const So3Args& a, cudaStream_t st);    // alpha FFT + gamma C2R + argmax
 cudaError_t so3_init_attributes();  // once per device
 void so3_beta_table(int bw_out, double* host_tab);  // fills the [3][2 bw_out] beta_tab on the host
+void so3_wigner_table(int bw_in, std::vector<double>& host_tab);  // recurrence tables of the synthesis
 
 // ------------------------------------------------------------ spatial
 struct VoxelArgs {
