@@ -507,6 +507,7 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   CK(cudaEventCreateWithFlags(&ctx->ev_b, cudaEventDisableTiming));
   CK(spatial_init_attributes());
   CK(so3_init_attributes());
+  CK(sht_init_attributes());
   std::string perr;
   if (!make_fft_plan(2 * bw, &ctx->plan_s2, &ctx->d_tw[0], &perr) ||
       !make_fft_plan(2 * bw_out, &ctx->plan_so3, &ctx->d_tw[1], &perr) ||
@@ -579,6 +580,7 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   CK(cudaMemset(ctx->d_samples, 0, sizeof(float) * 2 * 4 * nq));
   for (int s = 0; s < 2; ++s) CKV(dalloc(ctx, &ctx->d_nn[s], sizeof(int32_t) * nq));
   CKV(dalloc(ctx, &ctx->d_coef, sizeof(float2) * 8 * bw * bw));
+  CKV(dalloc(ctx, &ctx->d_fphi, sizeof(float2) * sht_scratch_entries(bw)));
   CKV(dalloc(ctx, &ctx->d_fused, sizeof(float2) * 2 * bw * (2 * bw - 1)));
   CK(cudaMemset(ctx->d_fused, 0, sizeof(float2) * 2 * bw * (2 * bw - 1)));
   const size_t no = (size_t)2 * bw_out;
@@ -725,14 +727,16 @@ int phgpu_get_samples(phgpu_ctx* ctx, int side, double* values, int32_t* nn_inde
 int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st) {
   const int bw = ctx->bw;
   const size_t nq = (size_t)4 * bw * bw;
-  for (int side = 0; side < 2; ++side) {
+  {
     ShtArgs s;
     s.bw = bw;
-    s.n_sig = n_data;
-    s.signal = ctx->d_samples + (size_t)side * 4 * nq;
-    s.tw = ctx->plan_s2.tw;
+    s.n_data = n_data;
+    s.side_stride = 4 * nq;
+    s.signal = ctx->d_samples;
+    s.plan = &ctx->plan_s2;
     s.table = ctx->d_legendre;
-    s.coef = ctx->d_coef + (size_t)side * n_data * bw * bw;
+    s.fphi = ctx->d_fphi;
+    s.coef = ctx->d_coef;
     ProfScope ps(ctx, st, PS_SHT);
     CK(launch_sht(s, st));
   }

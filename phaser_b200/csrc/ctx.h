@@ -58,6 +58,7 @@ struct phgpu_ctx {
   // rotation
   float* d_samples = nullptr;  // [2][4][4B^2]
   int32_t* d_nn[2] = {nullptr, nullptr};
+  float2* d_fphi = nullptr;  // SHT scratch: F_m(theta_k) per signal
   float2* d_coef = nullptr;
   float2* d_fused = nullptr;
   float2* d_S = nullptr;

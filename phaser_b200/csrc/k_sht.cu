@@ -17,6 +17,8 @@
 // LaplacePyramid::fuseChannels (5 levels, divider 4) and shifts back; the
 // fused value at coefficient (l, m) therefore follows the positional rule at
 // p = (seanindex(m, l) + floor(B^2 / 2)) mod B^2.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace phgpu {
@@ -71,98 +73,187 @@ cudaError_t launch_legendre_table(int bw, const double* weights_dev, float* tabl
   return cudaGetLastError();
 }
 
-// Fused transform: block per (order pair {m, B-1-m}, signal), so every block
-// carries B + 1 Legendre degrees.  Phase 1: warps take theta rows k, lanes
-// the phi samples j (four loads in flight), and one pass over a row gives
-// F_m(theta_k) for both orders.  Phase 2: warps take (order, degree) tasks
-// and lanes the rows k of the table.
-constexpr int kShtThreads = 1024;
+// The transform runs in two kernels over both sides' signals at once.
+//
+// k_sht_phi: F_m(theta_k) for every signal, order m < B and row k.  Rows are
+// real, so rows a and b of a block are transformed together as z = x_a + i x_b
+// by one complex FFT (the length's plan; digit-reversed output) and split as
+// X_a[m] = (Z[m] + conj Z[-m]) / 2, X_b[m] = (Z[m] - conj Z[-m]) / 2i.
+//
+// k_sht_leg: block per (order pair {m, B-1-m}, side), so every block carries
+// B + 1 Legendre degrees of one side's channels.  The block's slice of the
+// table (the rows of orders m0 and m1, each order contiguous) is streamed into
+// shared memory by asynchronous copies -- in one piece when it fits, else
+// through two slots, one chunk in flight while the other is consumed -- and
+// each warp takes a degree: one pass over the table row serves every channel.
+constexpr int kPhiRows = 8;  // rows per block: kPhiRows / 2 complex transforms
+constexpr int kPhiThreads = 128;
+constexpr int kLegThreads = 512;
+constexpr int kMaxSig = 4;  // channels per side
+constexpr size_t kShtSmemLimit = (size_t)227 * 1024;
 
-__global__ void __launch_bounds__(kShtThreads) k_sht(int bw, const float* __restrict__ sig,
-                                                     const float2* __restrict__ tw, const float* __restrict__ table,
-                                                     float2* __restrict__ coef) {
+template <int NF>
+__global__ void __launch_bounds__(kPhiThreads) k_sht_phi(int bw, int n_data, size_t side_stride,
+                                                         const float* __restrict__ sig, FftPlan plan,
+                                                         float2* __restrict__ fphi) {
+  extern __shared__ float2 zr[];  // [kPhiRows / 2][n] packed row pairs
+  const int n = 2 * bw;
+  const int s = blockIdx.y, side = s / n_data, c = s - side * n_data;
+  const float* S = sig + side * side_stride + (size_t)c * n * n;
+  const int k0 = blockIdx.x * kPhiRows;
+  const int nr = min(kPhiRows, n - k0);  // even: n and k0 are
+  const int np = nr / 2;
+  for (int e = threadIdx.x; e < np * n; e += blockDim.x) {
+    const int p = e / n, j = e - p * n;
+    const float* r0 = S + (size_t)(k0 + 2 * p) * n;
+    zr[e] = make_float2(__ldg(&r0[j]), __ldg(&r0[n + j]));
+  }
+  __syncthreads();
+  fft_any<NF, false>(zr, np, n, 1, plan);
+  const float half = (float)(0.5 * 2.5066282746310002 / (double)n);  // sqrt(2 pi) / 2B, halved
+  for (int e = threadIdx.x; e < bw * np; e += blockDim.x) {
+    const int m = e / np, p = e - m * np;
+    const float2 za = zr[p * n + freq2pos<NF>(m, plan)];
+    const float2 zb = zr[p * n + freq2pos<NF>(m == 0 ? 0 : n - m, plan)];
+    float2* out = fphi + ((size_t)s * bw + m) * n + k0 + 2 * p;
+    out[0] = make_float2((za.x + zb.x) * half, (za.y - zb.y) * half);
+    out[1] = make_float2((za.y + zb.y) * half, (zb.x - za.x) * half);
+  }
+}
+
+__device__ __forceinline__ void cp_async8(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Copies floats [0, len) of src to dst (len even, both 8-byte aligned: table
+// orders start at even offsets and rows are 2B floats).
+__device__ __forceinline__ void stage_floats(float* dst, const float* src, int len) {
+  for (int i = 2 * (int)threadIdx.x; i < len; i += 2 * (int)blockDim.x) cp_async8(dst + i, src + i);
+}
+
+__global__ void __launch_bounds__(kLegThreads) k_sht_leg(int bw, int n_data, int cr, int nslot,
+                                                         const float* __restrict__ table,
+                                                         const float2* __restrict__ fphi, float2* __restrict__ coef) {
   extern __shared__ float2 sh[];
   const int n = 2 * bw;
   const int m0 = blockIdx.x, m1 = bw - 1 - blockIdx.x;
   const int nm = (m1 > m0) ? 2 : 1;
-  float2* twm = sh;          // [2][n] exp(-i m phi_j)
-  float2* fk = sh + 2 * n;   // [2][n] F_m(theta_k)
-  const int s = blockIdx.y;
-  for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    twm[j] = __ldg(&tw[(j * m0) % n]);
-    twm[n + j] = __ldg(&tw[(j * m1) % n]);
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const float scale = (float)(2.5066282746310002 / (double)n);  // sqrt(2 pi) / 2B
-  const float* S = sig + (size_t)s * n * n;
-  for (int k = warp; k < n; k += nw) {
-    const float* row = S + (size_t)k * n;
-    float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
-    for (int j0 = lane; j0 < n; j0 += 128) {
-      float v[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = (j0 + 32 * u < n) ? __ldg(&row[j0 + 32 * u]) : 0.f;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int j = j0 + 32 * u;
-        if (j < n) {
-          const float2 w = twm[j], x = twm[n + j];
-          ar = fmaf(v[u], w.x, ar);
-          ai = fmaf(v[u], w.y, ai);
-          br = fmaf(v[u], x.x, br);
-          bi = fmaf(v[u], x.y, bi);
-        }
-      }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      ar += __shfl_xor_sync(0xffffffffu, ar, o);
-      ai += __shfl_xor_sync(0xffffffffu, ai, o);
-      br += __shfl_xor_sync(0xffffffffu, br, o);
-      bi += __shfl_xor_sync(0xffffffffu, bi, o);
-    }
-    if (lane == 0) {
-      fk[k] = make_float2(ar * scale, ai * scale);
-      fk[n + k] = make_float2(br * scale, bi * scale);
-    }
-  }
-  __syncthreads();
+  const int side = blockIdx.y;
+  float2* f = sh;                                                       // [n_data][2][n]
+  float* ring = reinterpret_cast<float*>(sh + (size_t)n_data * 2 * n);  // [nslot][cr][n]
+  const size_t slot = (size_t)cr * n;
+  // tasks t < nl0: order m0, degree m0 + t; then order m1, degree m1 + t - nl0
   const int nl0 = bw - m0;
   const int ntask = nl0 + (nm == 2 ? bw - m1 : 0);
-  for (int task = warp; task < ntask; task += nw) {
-    const int h = task < nl0 ? 0 : 1;
+  const float* seg0 = table + legendre_offset(m0, bw);
+  const float* seg1 = table + legendre_offset(m1, bw);
+  auto stage_tasks = [&](float* dst, int t0) {
+    const int t1 = min(t0 + cr, ntask);
+    const int a1 = min(t1, nl0);  // tasks [t0, a1) from order m0
+    if (a1 > t0) stage_floats(dst, seg0 + (size_t)t0 * n, (a1 - t0) * n);
+    const int b0 = max(t0, nl0);  // tasks [b0, t1) from order m1
+    if (t1 > b0) stage_floats(dst + (size_t)(b0 - t0) * n, seg1 + (size_t)(b0 - nl0) * n, (t1 - b0) * n);
+  };
+  stage_tasks(ring, 0);
+  cp_async_commit();
+  for (int e = threadIdx.x; e < n_data * 2 * n; e += blockDim.x) {
+    const int c = e / (2 * n), rem = e - c * 2 * n, h = rem / n, k = rem - h * n;
     const int m = h ? m1 : m0;
-    const int l = m + (h ? task - nl0 : task);
-    const float* trow = table + legendre_offset(m, bw) + (size_t)(l - m) * n;
-    const float2* f = fk + h * n;
-    float ar = 0.f, ai = 0.f;
-    for (int k0 = lane; k0 < n; k0 += 128) {
-      float t[4];
+    f[e] = (h == 0 || nm == 2) ? fphi[(((size_t)side * n_data + c) * bw + m) * n + k] : make_float2(0.f, 0.f);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int nc = (ntask + cr - 1) / cr;
+  for (int c = 0; c < nc; ++c) {
+    if (c + 1 < nc) stage_tasks(ring + ((c + 1) % nslot) * slot, (c + 1) * cr);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const float* chunk = ring + (c % nslot) * slot;
+    for (int i = warp; i < cr && c * cr + i < ntask; i += nw) {
+      const int task = c * cr + i;
+      const int h = task < nl0 ? 0 : 1;
+      const int m = h ? m1 : m0;
+      const int l = m + (h ? task - nl0 : task);
+      const float* trow = chunk + (size_t)i * n;
+      float ar[kMaxSig], ai[kMaxSig];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) t[u] = (k0 + 32 * u < n) ? __ldg(&trow[k0 + 32 * u]) : 0.f;
+      for (int q = 0; q < kMaxSig; ++q) ar[q] = ai[q] = 0.f;
+      for (int k = lane; k < n; k += 32) {
+        const float t = trow[k];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if (k0 + 32 * u < n) {
-          const float2 x = f[k0 + 32 * u];
-          ar = fmaf(t[u], x.x, ar);
-          ai = fmaf(t[u], x.y, ai);
+        for (int q = 0; q < kMaxSig; ++q) {
+          if (q < n_data) {
+            const float2 x = f[((size_t)q * 2 + h) * n + k];
+            ar[q] = fmaf(t, x.x, ar[q]);
+            ai[q] = fmaf(t, x.y, ai[q]);
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kMaxSig; ++q) {
+        if (q < n_data) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            ar[q] += __shfl_xor_sync(0xffffffffu, ar[q], o);
+            ai[q] += __shfl_xor_sync(0xffffffffu, ai[q], o);
+          }
+          if (lane == 0) coef[(((size_t)side * n_data + q) * bw + l) * bw + m] = make_float2(ar[q], ai[q]);
         }
       }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      ar += __shfl_xor_sync(0xffffffffu, ar, o);
-      ai += __shfl_xor_sync(0xffffffffu, ai, o);
-    }
-    if (lane == 0) coef[((size_t)s * bw + l) * bw + m] = make_float2(ar, ai);
+    __syncthreads();  // the slot just read is refilled next iteration
   }
 }
 
+namespace {
+// Table rows per chunk and slots: the whole slice of B + 1 rows in one slot
+// when it fits beside the F rows, else two slots of as many rows as fit.
+bool leg_chunking(int bw, int n_data, int* cr, int* nslot, size_t* smem) {
+  const size_t n = 2 * (size_t)bw;
+  const size_t fixed = (size_t)n_data * 2 * n * sizeof(float2);
+  if (fixed >= kShtSmemLimit) return false;
+  const size_t row = n * sizeof(float);
+  const size_t one = (kShtSmemLimit - fixed) / row;
+  if (one >= (size_t)bw + 1) {
+    *cr = bw + 1;
+    *nslot = 1;
+  } else {
+    *cr = (int)(one / 2);
+    *nslot = 2;
+  }
+  if (*cr < 1) return false;
+  *smem = fixed + (size_t)*nslot * *cr * row;
+  return true;
+}
+}  // namespace
+
+size_t sht_scratch_entries(int bw) { return (size_t)2 * kMaxSig * bw * 2 * bw; }
+
+cudaError_t sht_init_attributes() {
+  return cudaFuncSetAttribute(k_sht_leg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShtSmemLimit);
+}
+
 cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st) {
-  dim3 g((a.bw + 1) / 2, a.n_sig);
-  k_sht<<<g, kShtThreads, (size_t)4 * 2 * a.bw * sizeof(float2), st>>>(a.bw, a.signal, a.tw, a.table, a.coef);
-  count_launches(1);
+  int cr = 0, nslot = 0;
+  size_t sm = 0;
+  if (a.n_data < 1 || a.n_data > kMaxSig || !leg_chunking(a.bw, a.n_data, &cr, &nslot, &sm))
+    return cudaErrorInvalidValue;
+  const int n = 2 * a.bw;
+  if (a.plan->n != n) return cudaErrorInvalidValue;
+  dim3 g1((n + kPhiRows - 1) / kPhiRows, 2 * a.n_data);
+  const size_t sm1 = (size_t)(kPhiRows / 2) * n * sizeof(float2);
+  PHGPU_DISPATCH_N(n, k_sht_phi<NF><<<g1, kPhiThreads, sm1, st>>>(a.bw, a.n_data, a.side_stride, a.signal,
+                                                                   *a.plan, a.fphi));
+  dim3 g2((a.bw + 1) / 2, 2);
+  k_sht_leg<<<g2, kLegThreads, sm, st>>>(a.bw, a.n_data, cr, nslot, a.table, a.fphi, a.coef);
+  count_launches(2);
   return cudaGetLastError();
 }
 

@@ -21,6 +21,7 @@
 
 #include <vector>
 
+#include "fft2.cuh"
 #include "kernels.h"
 
 namespace phgpu {
@@ -225,11 +226,20 @@ __global__ void k_so3_fft_a(int bw_in, int bw_out, float2* __restrict__ S, FftPl
   const int b0 = blockIdx.x * Wt;
   const int wt = min(Wt, bw_in - b0);
   float2* Sk = S + (size_t)k * n * Bo;
-  for (int e = threadIdx.x; e < n * Wt; e += blockDim.x) {
-    const int a = e / Wt, bt = e % Wt;
-    // rows with |m1| >= bw_in are not synthesised: read them as zero
-    const bool row_ok = (a < bw_in) || (a > n - bw_in);
-    tile[e] = (bt < wt && row_ok) ? Sk[(size_t)a * Bo + b0 + bt] : make_float2(0.f, 0.f);
+  // four loads in flight per thread
+  for (int e0 = threadIdx.x; e0 < n * Wt; e0 += 4 * blockDim.x) {
+    float2 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * blockDim.x;
+      const int a = e / Wt, bt = e % Wt;
+      // rows with |m1| >= bw_in are not synthesised: read them as zero
+      const bool row_ok = (a < bw_in) || (a > n - bw_in);
+      v[u] = (e < n * Wt && bt < wt && row_ok) ? Sk[(size_t)a * Bo + b0 + bt] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (e0 + u * blockDim.x < n * Wt) tile[e0 + u * blockDim.x] = v[u];
   }
   __syncthreads();
   fft_any<NF, false, 4>(tile, Wt, 1, Wt, plan);
@@ -282,11 +292,95 @@ __global__ void k_so3_c2r(int bw_in, int bw_out, const float2* __restrict__ S, F
   warp_argmax_commit(best, argmax);
 }
 
+// Rows (alpha) of one block of the packed transform: two Hermitian rows per
+// complex transform.
+template <int NF>
+constexpr int c2r_pair_rows() {
+  return (NF % 40 == 0) ? 40 : 32;
+}
+
+// The same C2R for lengths with a register-tail plan: rows a0 and a1 (two
+// alphas) are inverted by one complex transform of Z = X0 + i X1, whose
+// output is x0 + i x1 since both spectra are Hermitian.  Row a holds
+// X[b] = conj(u_b), X[n - b] = u_b for 0 < b < n/2; its DC term is taken
+// real (its imaginary part only ever reaches the imaginary output, which the
+// real transform discards) and the Nyquist term is zero, as the
+// one-row-per-transform kernel above fills it.
+template <int NF>
+__global__ void __launch_bounds__(256) k_so3_c2r_tail(int bw_in, const float2* __restrict__ S, FftPlan plan,
+                                                     unsigned long long* __restrict__ argmax,
+                                                     float* __restrict__ volume) {
+  constexpr int n = NF, Bo = NF / 2, RB = c2r_pair_rows<NF>(), P = RB / 2, ST = NF + 1;
+  extern __shared__ float2 zrow[];  // [P][ST]
+  __shared__ int s_pos[NF];
+  __shared__ int s_alpha[RB];
+  const int k = blockIdx.y;
+  const int r0 = blockIdx.x * RB;
+  const int nr = min(RB, n - r0);
+  const int np = (nr + 1) >> 1;
+  for (int b = threadIdx.x; b < n; b += blockDim.x) s_pos[b] = fixed_freq2pos<NF>(b);
+  for (int r = threadIdx.x; r < nr; r += blockDim.x) s_alpha[r] = fixed_pos2freq<NF>(r0 + r);
+  __syncthreads();
+  const float2* Sk = S + ((size_t)k * n + r0) * Bo;
+  constexpr int U = 2;  // pairs of loads in flight per thread
+  for (int e0 = threadIdx.x; e0 < np * Bo; e0 += U * blockDim.x) {
+    float2 u0[U], u1[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = e0 + u * blockDim.x;
+      const int p = e / Bo, b = e - p * Bo;
+      const bool ok = e < np * Bo && b < bw_in;
+      u0[u] = ok ? Sk[(size_t)(2 * p) * Bo + b] : make_float2(0.f, 0.f);
+      u1[u] = (ok && 2 * p + 1 < nr) ? Sk[(size_t)(2 * p + 1) * Bo + b] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e >= np * Bo) continue;
+      const int p = e / Bo, b = e - p * Bo;
+      float2* z = zrow + p * ST;
+      if (b == 0) {
+        z[s_pos[0]] = make_float2(u0[u].x, u1[u].x);
+        z[s_pos[Bo]] = make_float2(0.f, 0.f);
+      } else {
+        z[s_pos[b]] = make_float2(u0[u].x + u1[u].y, u1[u].x - u0[u].y);      // conj(u0) + i conj(u1)
+        z[s_pos[n - b]] = make_float2(u0[u].x - u1[u].y, u0[u].y + u1[u].x);  // u0 + i u1
+      }
+    }
+  }
+  __syncthreads();
+  fft_tail<NF, true, false>(zrow, np, ST, plan.tw);
+  const float K = (float)((1.0 / (double)n) * ((double)Bo / M_PI));
+  unsigned long long best = 0ull;
+  for (int e = threadIdx.x; e < np * n; e += blockDim.x) {
+    const int p = e / n, g = e - p * n;
+    const float2 z = zrow[p * ST + g];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = 2 * p + h;
+      if (r < nr) {
+        const float v = (h ? z.y : z.x) * K;
+        const float v2 = v * v;
+        const uint32_t idx = ((uint32_t)k * n + (uint32_t)s_alpha[r]) * n + g;
+        const unsigned long long key = pack_argmax(v2, idx);
+        best = key > best ? key : best;
+        if (volume) volume[idx] = v2;
+      }
+    }
+  }
+  warp_argmax_commit(best, argmax);
+}
+
 template <int NF>
 static cudaError_t so3_attrs() {
   const int m = 227 * 1024;
   cudaError_t e = cudaFuncSetAttribute(k_so3_fft_a<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_so3_c2r<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+  if constexpr (Tail<NF>::ok) {
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_so3_c2r_tail<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (c2r_pair_rows<NF>() / 2) * (NF + 1) * (int)sizeof(float2));
+  }
   return e;
 }
 
@@ -311,14 +405,28 @@ cudaError_t launch_so3_synth(const So3Args& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// The gamma transform: packed pairs on the register-tail engine where the
+// length has a tail plan, one row per transform otherwise.
+template <int NF>
+static void launch_so3_c2r(const So3Args& a, int n, cudaStream_t st) {
+  if constexpr (Tail<NF>::ok) {
+    constexpr int RB = c2r_pair_rows<NF>();
+    dim3 g((n + RB - 1) / RB, n);
+    k_so3_c2r_tail<NF><<<g, 256, (size_t)(RB / 2) * (NF + 1) * sizeof(float2), st>>>(a.bw_in, a.S, *a.plan,
+                                                                                       a.argmax, a.volume);
+  } else {
+    dim3 g((n + 15) / 16, n);
+    k_so3_c2r<NF><<<g, 256, (size_t)16 * n * sizeof(float2) + (size_t)(n + 16) * sizeof(int), st>>>(
+        a.bw_in, a.bw_out, a.S, *a.plan, a.argmax, a.volume);
+  }
+}
+
 cudaError_t launch_so3_fft(const So3Args& a, cudaStream_t st) {
   const int n = 2 * a.bw_out;
   dim3 g2((a.bw_in + 15) / 16, n);
-  dim3 g3((n + 15) / 16, n);
   PHGPU_DISPATCH_N(n,
       k_so3_fft_a<NF><<<g2, 256, (size_t)n * 16 * sizeof(float2), st>>>(a.bw_in, a.bw_out, a.S, *a.plan);
-      k_so3_c2r<NF><<<g3, 256, (size_t)16 * n * sizeof(float2) + (size_t)(n + 16) * sizeof(int), st>>>(
-          a.bw_in, a.bw_out, a.S, *a.plan, a.argmax, a.volume));
+      launch_so3_c2r<NF>(a, n, st));
   count_launches(2);
   return cudaGetLastError();
 }

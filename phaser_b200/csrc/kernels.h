@@ -42,15 +42,20 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st);
 size_t legendre_table_entries(int bw);
 cudaError_t launch_legendre_table(int bw, const double* weights_dev, float* table, cudaStream_t st);
 
+// Both sides at once: signal (side, c) at signal + side * side_stride + c (2B)^2.
 struct ShtArgs {
   int bw;
-  int n_sig;              // signals (sides x channels)
-  const float* signal;    // [n_sig][2B][2B]
-  const float2* tw;       // exp(-2 pi i t / 2B), t in [0, 2B)
+  int n_data;             // channels per side (1..4)
+  size_t side_stride;     // floats between the two sides' grids
+  const float* signal;    // [side][c][2B][2B]
+  const FftPlan* plan;    // length 2B
   const float* table;     // Legendre table
-  float2* coef;           // [n_sig][B (l)][B (m>=0)]
+  float2* fphi;           // scratch [side][c][B (m)][2B (k)], sht_scratch_entries(B) complex
+  float2* coef;           // [side][c][B (l)][B (m>=0)]
 };
+size_t sht_scratch_entries(int bw);
 cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st);
+cudaError_t sht_init_attributes();  // once per device
 
 struct FuseS2Args {
   int bw;

@@ -62,6 +62,7 @@ uint64_t estimate_bytes(const phgpu_params& p, uint32_t max_points) {
   uint64_t b = 0;
   b += 4 * 4 * bw * bw * 2;                 // samples
   b += 8 * bw * bw * 8;                     // coef
+  b += 8 * bw * 2 * bw * 8;                 // SHT scratch
   b += 8 * bo * bo * bo;                    // S
   b += 2 * 5 * nv * 4;                      // grids
   b += 9 * H * 8;                           // spec + cspec
