@@ -158,8 +158,8 @@ def physical_gpu_index(local):
 # ------------------------------------------------------------------ roofline
 
 def stage_bytes(stage, bw, N, C, P):
-    """Algorithmic HBM bytes of one call of a stage (per cloud / side where a
-    stage runs per side), after the per-unit figures of the survey's
+    """Algorithmic HBM bytes of one call of a stage (per cloud where a stage
+    runs per cloud: sampling, voxelisation, the forward spatial transform), after the per-unit figures of the survey's
     measurement section: FP32 data, complex64 spectra, the minimum each stage
     moves with its inputs and outputs in HBM."""
     nv = N ** 3
@@ -167,7 +167,7 @@ def stage_bytes(stage, bw, N, C, P):
     n = 2 * bw
     return {
         "s2_sample": P * 20 + 4 * n * n * 4,                 # points in, 4 sample channels out
-        "sht": C * n * n * 4 + C * bw * bw * 8,              # C grids in, C coefficient sets out
+        "sht": 2 * (C * n * n * 4 + C * bw * bw * 8),        # both sides: C grids in, C coefficient sets out
         "fuse_s2": 2 * C * bw * bw * 8 + 2 * bw * bw * 8,    # both sides' coefficients in, fused out
         "so3_synth": n * n * bw * 8,                         # half spectrum S written (m2 >= 0)
         "so3_fft": 3 * n * n * bw * 8,                       # S read + write (alpha), read (gamma)

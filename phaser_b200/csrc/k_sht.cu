@@ -81,14 +81,19 @@ cudaError_t launch_legendre_table(int bw, const double* weights_dev, float* tabl
 // X_a[m] = (Z[m] + conj Z[-m]) / 2, X_b[m] = (Z[m] - conj Z[-m]) / 2i.
 //
 // k_sht_leg: block per (order pair {m, B-1-m}, side), so every block carries
-// B + 1 Legendre degrees of one side's channels.  The block's slice of the
-// table (the rows of orders m0 and m1, each order contiguous) is streamed into
-// shared memory by asynchronous copies -- in one piece when it fits, else
-// through two slots, one chunk in flight while the other is consumed -- and
-// each warp takes a degree: one pass over the table row serves every channel.
+// B + 1 Legendre degrees of one side's channels: per order, a product of the
+// table rows [degrees x 2B] with the channels' F [2B x channels].  The
+// block's slice of the table (the rows of orders m0 and m1, each order
+// contiguous) is streamed into shared memory by asynchronous copies -- in one
+// piece when it fits, else through two slots, one chunk in flight while the
+// other is consumed.  Thread (degree, quarter of the rows k) accumulates every
+// channel's real and imaginary part from one table load, two k at a time;
+// the four quarters are summed through shared memory.
 constexpr int kPhiRows = 8;  // rows per block: kPhiRows / 2 complex transforms
 constexpr int kPhiThreads = 128;
-constexpr int kLegThreads = 512;
+constexpr int kLegTasks = 128;  // degrees per round
+constexpr int kLegParts = 4;    // threads per degree (quarters of the rows k)
+constexpr int kLegThreads = kLegTasks * kLegParts;
 constexpr int kMaxSig = 4;  // channels per side
 constexpr size_t kShtSmemLimit = (size_t)227 * 1024;
 
@@ -103,10 +108,30 @@ __global__ void __launch_bounds__(kPhiThreads) k_sht_phi(int bw, int n_data, siz
   const int k0 = blockIdx.x * kPhiRows;
   const int nr = min(kPhiRows, n - k0);  // even: n and k0 are
   const int np = nr / 2;
-  for (int e = threadIdx.x; e < np * n; e += blockDim.x) {
-    const int p = e / n, j = e - p * n;
-    const float* r0 = S + (size_t)(k0 + 2 * p) * n;
-    zr[e] = make_float2(__ldg(&r0[j]), __ldg(&r0[n + j]));
+  // items of two neighbouring samples of a row pair (8-byte loads: rows are
+  // 2B floats), all of a thread's loads in flight together
+  const int nh = n / 2;
+  constexpr int U = 4;
+  for (int i0 = threadIdx.x; i0 < np * nh; i0 += U * blockDim.x) {
+    float2 a[U], b[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * blockDim.x;
+      const int p = i / nh, j = 2 * (i - p * nh);
+      const float* r0 = S + (size_t)(k0 + 2 * p) * n + j;
+      const bool ok = i < np * nh;
+      a[u] = ok ? __ldg(reinterpret_cast<const float2*>(r0)) : make_float2(0.f, 0.f);
+      b[u] = ok ? __ldg(reinterpret_cast<const float2*>(r0 + n)) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < np * nh) {
+        const int p = i / nh, j = 2 * (i - p * nh);
+        zr[p * n + j] = make_float2(a[u].x, b[u].x);
+        zr[p * n + j + 1] = make_float2(a[u].y, b[u].y);
+      }
+    }
   }
   __syncthreads();
   fft_any<NF, false>(zr, np, n, 1, plan);
@@ -132,23 +157,20 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Copies floats [0, len) of src to dst (len even, both 8-byte aligned: table
-// orders start at even offsets and rows are 2B floats).
-__device__ __forceinline__ void stage_floats(float* dst, const float* src, int len) {
-  for (int i = 2 * (int)threadIdx.x; i < len; i += 2 * (int)blockDim.x) cp_async8(dst + i, src + i);
-}
 
 __global__ void __launch_bounds__(kLegThreads) k_sht_leg(int bw, int n_data, int cr, int nslot,
                                                          const float* __restrict__ table,
                                                          const float2* __restrict__ fphi, float2* __restrict__ coef) {
   extern __shared__ float2 sh[];
   const int n = 2 * bw;
+  const int rs = n + 2;  // table row stride in shared memory (8-byte aligned, conflict-free 8-byte reads)
   const int m0 = blockIdx.x, m1 = bw - 1 - blockIdx.x;
   const int nm = (m1 > m0) ? 2 : 1;
   const int side = blockIdx.y;
-  float2* f = sh;                                                       // [n_data][2][n]
-  float* ring = reinterpret_cast<float*>(sh + (size_t)n_data * 2 * n);  // [nslot][cr][n]
-  const size_t slot = (size_t)cr * n;
+  float2* f = sh;                                                             // [2][n][kMaxSig]
+  float* part = reinterpret_cast<float*>(sh + (size_t)2 * n * kMaxSig);       // [kLegParts][kLegTasks][2 kMaxSig]
+  float* ring = part + (size_t)kLegParts * kLegTasks * 2 * kMaxSig;           // [nslot][cr][rs]
+  const size_t slot = (size_t)cr * rs;
   // tasks t < nl0: order m0, degree m0 + t; then order m1, degree m1 + t - nl0
   const int nl0 = bw - m0;
   const int ntask = nl0 + (nm == 2 ? bw - m1 : 0);
@@ -156,19 +178,26 @@ __global__ void __launch_bounds__(kLegThreads) k_sht_leg(int bw, int n_data, int
   const float* seg1 = table + legendre_offset(m1, bw);
   auto stage_tasks = [&](float* dst, int t0) {
     const int t1 = min(t0 + cr, ntask);
-    const int a1 = min(t1, nl0);  // tasks [t0, a1) from order m0
-    if (a1 > t0) stage_floats(dst, seg0 + (size_t)t0 * n, (a1 - t0) * n);
-    const int b0 = max(t0, nl0);  // tasks [b0, t1) from order m1
-    if (t1 > b0) stage_floats(dst + (size_t)(b0 - t0) * n, seg1 + (size_t)(b0 - nl0) * n, (t1 - b0) * n);
+    const int rows = t1 - t0, half = n / 2;
+    for (int i = threadIdx.x; i < rows * half; i += blockDim.x) {
+      const int r = i / half, j = 2 * (i - r * half);
+      const int t = t0 + r;
+      const float* src = (t < nl0 ? seg0 + (size_t)t * n : seg1 + (size_t)(t - nl0) * n) + j;
+      cp_async8(dst + (size_t)r * rs + j, src);
+    }
   };
   stage_tasks(ring, 0);
   cp_async_commit();
-  for (int e = threadIdx.x; e < n_data * 2 * n; e += blockDim.x) {
-    const int c = e / (2 * n), rem = e - c * 2 * n, h = rem / n, k = rem - h * n;
+  // F rows of both orders, channels innermost: f[(h n + k) kMaxSig + q]
+  for (int e = threadIdx.x; e < 2 * n * kMaxSig; e += blockDim.x) {
+    const int q = e % kMaxSig, hk = e / kMaxSig, h = hk / n, k = hk - h * n;
     const int m = h ? m1 : m0;
-    f[e] = (h == 0 || nm == 2) ? fphi[(((size_t)side * n_data + c) * bw + m) * n + k] : make_float2(0.f, 0.f);
+    f[e] = (q < n_data && (h == 0 || nm == 2)) ? fphi[(((size_t)side * n_data + q) * bw + m) * n + k]
+                                                : make_float2(0.f, 0.f);
   }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int tl = threadIdx.x % kLegTasks, quarter = threadIdx.x / kLegTasks;
+  const int kq = ((n / 2 + kLegParts - 1) / kLegParts) * 2;  // rows k per quarter (even)
+  const int ka = quarter * kq, kb = min(n, ka + kq);
   const int nc = (ntask + cr - 1) / cr;
   for (int c = 0; c < nc; ++c) {
     if (c + 1 < nc) stage_tasks(ring + ((c + 1) % nslot) * slot, (c + 1) * cr);
@@ -176,39 +205,51 @@ __global__ void __launch_bounds__(kLegThreads) k_sht_leg(int bw, int n_data, int
     cp_async_wait<1>();
     __syncthreads();
     const float* chunk = ring + (c % nslot) * slot;
-    for (int i = warp; i < cr && c * cr + i < ntask; i += nw) {
-      const int task = c * cr + i;
-      const int h = task < nl0 ? 0 : 1;
-      const int m = h ? m1 : m0;
-      const int l = m + (h ? task - nl0 : task);
-      const float* trow = chunk + (size_t)i * n;
-      float ar[kMaxSig], ai[kMaxSig];
+    const int tc = min(cr, ntask - c * cr);  // tasks in this chunk
+    for (int r0 = 0; r0 < tc; r0 += kLegTasks) {
+      const int r = r0 + tl;
+      float acc[2 * kMaxSig];
 #pragma unroll
-      for (int q = 0; q < kMaxSig; ++q) ar[q] = ai[q] = 0.f;
-      for (int k = lane; k < n; k += 32) {
-        const float t = trow[k];
+      for (int q = 0; q < 2 * kMaxSig; ++q) acc[q] = 0.f;
+      if (r < tc) {
+        const int h = c * cr + r < nl0 ? 0 : 1;
+        const float* trow = chunk + (size_t)r * rs;
+        const float4* fh = reinterpret_cast<const float4*>(f + (size_t)h * n * kMaxSig);
+        for (int k = ka; k < kb; k += 2) {
+          const float2 t = *reinterpret_cast<const float2*>(trow + k);
 #pragma unroll
-        for (int q = 0; q < kMaxSig; ++q) {
-          if (q < n_data) {
-            const float2 x = f[((size_t)q * 2 + h) * n + k];
-            ar[q] = fmaf(t, x.x, ar[q]);
-            ai[q] = fmaf(t, x.y, ai[q]);
+          for (int q2 = 0; q2 < kMaxSig / 2; ++q2) {
+            const float4 x0 = fh[(size_t)k * (kMaxSig / 2) + q2];        // channels 2 q2, 2 q2 + 1 at k
+            const float4 x1 = fh[(size_t)(k + 1) * (kMaxSig / 2) + q2];  // at k + 1
+            acc[4 * q2 + 0] = fmaf(t.x, x0.x, fmaf(t.y, x1.x, acc[4 * q2 + 0]));
+            acc[4 * q2 + 1] = fmaf(t.x, x0.y, fmaf(t.y, x1.y, acc[4 * q2 + 1]));
+            acc[4 * q2 + 2] = fmaf(t.x, x0.z, fmaf(t.y, x1.z, acc[4 * q2 + 2]));
+            acc[4 * q2 + 3] = fmaf(t.x, x0.w, fmaf(t.y, x1.w, acc[4 * q2 + 3]));
           }
         }
       }
+      float* pp = part + ((size_t)quarter * kLegTasks + tl) * 2 * kMaxSig;
 #pragma unroll
-      for (int q = 0; q < kMaxSig; ++q) {
-        if (q < n_data) {
+      for (int q = 0; q < 2 * kMaxSig; ++q) pp[q] = acc[q];
+      __syncthreads();
+      // sum the quarters: thread (task, value)
+      for (int e = threadIdx.x; e < kLegTasks * 2 * kMaxSig; e += blockDim.x) {
+        const int rr = e / (2 * kMaxSig), v = e - rr * 2 * kMaxSig, q = v >> 1;
+        const int rt = r0 + rr;
+        if (rt < tc && q < n_data) {
+          float sum = 0.f;
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            ar[q] += __shfl_xor_sync(0xffffffffu, ar[q], o);
-            ai[q] += __shfl_xor_sync(0xffffffffu, ai[q], o);
-          }
-          if (lane == 0) coef[(((size_t)side * n_data + q) * bw + l) * bw + m] = make_float2(ar[q], ai[q]);
+          for (int g = 0; g < kLegParts; ++g) sum += part[((size_t)g * kLegTasks + rr) * 2 * kMaxSig + v];
+          const int task = c * cr + rt;
+          const int h = task < nl0 ? 0 : 1;
+          const int m = h ? m1 : m0;
+          const int l = m + (h ? task - nl0 : task);
+          float* dst = reinterpret_cast<float*>(&coef[(((size_t)side * n_data + q) * bw + l) * bw + m]);
+          dst[v & 1] = sum;
         }
       }
+      __syncthreads();  // partials and (after the last round) the slot are reused
     }
-    __syncthreads();  // the slot just read is refilled next iteration
   }
 }
 
@@ -216,10 +257,11 @@ namespace {
 // Table rows per chunk and slots: the whole slice of B + 1 rows in one slot
 // when it fits beside the F rows, else two slots of as many rows as fit.
 bool leg_chunking(int bw, int n_data, int* cr, int* nslot, size_t* smem) {
+  (void)n_data;
   const size_t n = 2 * (size_t)bw;
-  const size_t fixed = (size_t)n_data * 2 * n * sizeof(float2);
+  const size_t fixed = 2 * n * kMaxSig * sizeof(float2) + (size_t)kLegParts * kLegTasks * 2 * kMaxSig * sizeof(float);
   if (fixed >= kShtSmemLimit) return false;
-  const size_t row = n * sizeof(float);
+  const size_t row = (n + 2) * sizeof(float);
   const size_t one = (kShtSmemLimit - fixed) / row;
   if (one >= (size_t)bw + 1) {
     *cr = bw + 1;
