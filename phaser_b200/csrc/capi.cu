@@ -602,6 +602,8 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
     CKV(dalloc(ctx, &ctx->d_grids[s], sizeof(float) * 5 * nv));
     CKV(dalloc(ctx, &ctx->d_rowlive[s], (size_t)N * N));
   }
+  CKV(dalloc(ctx, &ctx->d_slab_nz, (size_t)8 * N));
+  CK(cudaMemset(ctx->d_slab_nz, 1, (size_t)8 * N));  // nothing known to be zero yet
   CKV(dalloc(ctx, &ctx->d_spec, sizeof(float2) * 8 * H));
   CKV(dalloc(ctx, &ctx->d_cspec, sizeof(float2) * H));
   // volumes: kept on request, and needed by the peak-neighbourhood fits
@@ -922,6 +924,8 @@ static SpatialArgs spatial_args(phgpu_ctx* ctx, int n_data, int n_total, int lap
   // row flags describe voxelised grids only (host-written grids are dense)
   a.rowlive_f = means ? nullptr : ctx->d_rowlive[0];
   a.rowlive_g = means ? nullptr : ctx->d_rowlive[1];
+  // the padded path transforms the spectra in place: no slab stays known-zero
+  a.slab_nz = ctx->pad ? nullptr : ctx->d_slab_nz;
   a.spec = ctx->d_spec;
   a.cspec = ctx->d_cspec;
   a.plan = &ctx->plan_sp;

@@ -68,6 +68,7 @@ struct phgpu_ctx {
   // translation
   float* d_grids[2] = {nullptr, nullptr};  // [(C+1)][N^3]
   uint8_t* d_rowlive[2] = {nullptr, nullptr};  // [N][N] rows holding a point of the last voxelisation
+  uint8_t* d_slab_nz = nullptr;                 // [8][N] spectrum slabs that may be non-zero (k_slab_fwd)
   // leading grid planes (and row flags) known to be zero: a voxelisation whose
   // grids were cleared afterwards leaves them zero, so the next one needs no memset
   int clean_planes[2] = {0, 0};

@@ -424,7 +424,8 @@ template <int NF>
 __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __restrict__ grids, size_t grid_cstride,
                                                    const float* __restrict__ count,
                                                    const uint8_t* __restrict__ rowlive, float2* __restrict__ spec,
-                                                   size_t spec_cstride, FftPlan pN, FftPlan pH) {
+                                                   size_t spec_cstride, FftPlan pN, FftPlan pH,
+                                                   uint8_t* __restrict__ slab_nz) {
   constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1, Q = NF / 4, S = NF + 1;
   const int H2p = spatial_h2p(N);
   extern __shared__ float2 W[];  // [NH][S]
@@ -436,13 +437,20 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
   const int z = blockIdx.x, c = blockIdx.y;
   const float* g = grids + (size_t)c * grid_cstride + (size_t)z * N * N;
   const float* cnt = count ? count + (size_t)z * N * N : nullptr;
+  // slab_nz[c][z]: 0 when this slab of spectrum array c is known to hold zeros
+  uint8_t* nz = slab_nz ? slab_nz + (size_t)c * N + z : nullptr;
+  const int held_nonzero = nz ? *nz : 1;
+  int any_flag = 0;
   for (int r = threadIdx.x; r < NH; r += blockDim.x) {
     s_live[r] = 0;
     s_flag[r] = rowlive ? (rowlive[z * N + 2 * r] | rowlive[z * N + 2 * r + 1]) : 1;
+    any_flag |= s_flag[r];
     s_posH[r] = fixed_freq2pos<NH>(r);
   }
   for (int k = threadIdx.x; k < N; k += blockDim.x) s_posN[k] = fixed_freq2pos<N>(k);
-  __syncthreads();
+  // a slab without a flagged row transforms to zero: nothing to do where the
+  // array already holds zeros there
+  if (!__syncthreads_or(any_flag) && !held_nonzero) return;
   for (int e = threadIdx.x; e < NH * Q; e += blockDim.x) {
     const int r = e / Q, y4 = (e - r * Q) * 4;
     if (!s_flag[r]) {  // no point in either row: skip the loads
@@ -486,8 +494,10 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
       const int k = e / H2, ky = e - k * H2;
       out[(size_t)k * H2p + ky] = make_float2(0.f, 0.f);
     }
+    if (nz && threadIdx.x == 0) *nz = 0;  // every thread read it before the barrier above
     return;
   }
+  if (nz && threadIdx.x == 0) *nz = 1;
   // rows that are all zero stay zero under the y transform
   fft_tail<N, false, false>(W, nrows, S, pN.tw, s_rows);  // over y, live rows
   fft_tail<NH, false, true>(W, N, S, pH.tw);               // over r, columns
@@ -658,8 +668,9 @@ cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t 
     dim3 g(N, nch);
     const size_t sm = (size_t)(N / 2) * (N + 1) * sizeof(float2);
     const uint8_t* rowlive = side == 0 ? a.rowlive_f : a.rowlive_g;
+    uint8_t* nz = a.slab_nz ? a.slab_nz + (size_t)(side * a.n_data_ch) * N : nullptr;
     PHGPU_DISPATCH_SLAB(N, k_slab_fwd<NF><<<g, tail_threads<NF>(), sm, st>>>(grids, nv, count, rowlive, spec, plane,
-                                                                             *a.plan, *a.plan_half));
+                                                                             *a.plan, *a.plan_half, nz));
     count_launches(1);
     return cudaGetLastError();
   }

@@ -122,6 +122,9 @@ struct SpatialArgs {
   int grids_are_means;    // 1: grids already hold values (no count plane)
   const uint8_t* rowlive_f;  // optional row flags of the grids (rows never flagged are all zero)
   const uint8_t* rowlive_g;
+  uint8_t* slab_nz;       // optional [2 n_data_ch][N] per spectrum array: 0 where the z-slab is known
+                          // to hold zeros (the z-slab forward then skips a slab that stays zero,
+                          // and keeps the flags); null: every slab is written
   float2* spec;           // [2 n_data_ch][N (z)][N (x)][H2p (ky)]
   float2* cspec;          // [N][N][H2p]
   const FftPlan* plan;    // length N

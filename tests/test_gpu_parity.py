@@ -336,6 +336,36 @@ def test_context_reuse_leaves_no_state():
     fresh.close()
 
 
+def test_known_zero_slabs_across_scenes():
+    """The z-slab forward skips slabs whose spectra already hold zeros and
+    tracks which may not: a context that first registered a pair lifted by
+    4 m (other occupied slabs) must reproduce a fresh context's translation
+    volume, both right after it and after the plain pair in between."""
+    from phaser_b200 import native, scene
+    w = scene.WORKLOADS[1]
+    kw = dict(spherical_bandwidth=w["bw"], spatial_n_voxels=w["n_voxels"], spatial_discretize_lower=w["lo"],
+              spatial_discretize_upper=w["hi"], flags=native.PHGPU_FLAG_KEEP_VOLUMES)
+    b = scene.workload_pair(1, 0)
+
+    def lifted(xyzi):
+        out = xyzi.copy()
+        out[:, 2] += 4.0
+        return out
+
+    args = lambda p, f=lambda x: x: ((f(p.target.xyzi), p.target.reflectivity),
+                                     (f(p.source.xyzi), p.source.reflectivity))
+    used, fresh_b, fresh_l = native.Context(**kw), native.Context(**kw), native.Context(**kw)
+    fresh_b.register_pair(*args(b))
+    fresh_l.register_pair(*args(b, lifted))
+    vol_b = fresh_b.spatial_result(volume=True)[2]
+    vol_l = fresh_l.spatial_result(volume=True)[2]
+    for pair, f, ref in ((b, lambda x: x, vol_b), (b, lifted, vol_l), (b, lambda x: x, vol_b), (b, lifted, vol_l)):
+        used.register_pair(*args(pair, f))
+        assert rel_l2(used.spatial_result(volume=True)[2], ref) <= 1e-6
+    for c in (used, fresh_b, fresh_l):
+        c.close()
+
+
 def test_device_resident_inputs(nat, pair0):
     import torch
     from phaser_b200 import scene
