@@ -194,13 +194,13 @@ def pair_bytes(bw, N, C, P):
 # profiles/traffic_register_pair_B100_N200.md (sum over the stage's kernels).
 NCU_TRAFFIC_B100_N200 = {
     "s2_sample": (2.16 + 0.17 + 2.71 + 4.44) * 1e6,          # project, bin_scan, bin_scatter, nn_rows
-    "sht": 4.54e6,
+    "sht": (0.98 + 5.01) * 1e6,                              # sht_phi, sht_leg (both clouds)
     "fuse_s2": 0.32e6,
-    "so3_synth": (2.20 + 2.00) * 1e6,
-    "so3_fft": (31.86 + 32.02) * 1e6,
-    "voxelize": (8.25 + 0.83 + 0.31) * 1e6,                  # voxelize + clear
-    "spatial_fwd": (40.85 + 38.50) * 1e6,
-    "fuse_z": (200.53 + 20.37) * 1e6,
+    "so3_synth": (2.43 + 2.15) * 1e6,
+    "so3_fft": (31.86 + 32.03) * 1e6,                        # so3_fft_a, so3_c2r_tail
+    "voxelize": (8.24 + 0.84 + 0.31) * 1e6,                  # voxelize + clear
+    "spatial_fwd": (39.92 + 24.77) * 1e6,
+    "fuse_z": (200.50 + 20.38) * 1e6,
     "spatial_inv": 33.35e6,
 }
 
