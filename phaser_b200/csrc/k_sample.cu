@@ -20,10 +20,14 @@
 // the bound's spherical cap are scanned (the cap's longitude half-width at
 // the row's colatitudes).  A LiDAR scan needs about two rows and fifty
 // points per direction, so the search is a short chain of dependent loads
-// per direction, run for all directions at once.  Bounds are angles with a 1e-4 rad margin and conservative
-// trigonometry, far above the float rounding of the unit vectors, so no
-// point that could be (or tie) the nearest is ever skipped: the search is
-// exact whatever bound it starts from.
+// per direction, run for all directions at once.  The bound is kept as an
+// upper bound hb of hav(beta) = sin^2(beta / 2) of the best distance's angle
+// inflated by 1e-4 rad, and a row's window follows from the haversine law
+//   hav(d) = hav(t - t_q) + sin t sin t_q hav(dphi)
+// with per-row tables (sin of the row edges, hav of the row's colatitude
+// distance) deflated by margins far above the float rounding of the unit
+// vectors, so no point that could be (or tie) the nearest is ever skipped:
+// the search is exact whatever bound it starts from.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -89,10 +93,15 @@ __global__ void k_project(const float4* __restrict__ xyzi, int P, float4* __rest
 constexpr int kBinScanThreads = 256;
 constexpr int kMaxGridSide = 1024;  // 2B for B <= 512
 
+// Also the row tables of the window bound: sin_tab[r] = sin(r w) - 1e-5
+// (clamped at 0) for the row edges r = 0..2B, hav_tab[d] = hav((d - 1/2) w)
+// (1 - 1e-4) for the colatitude distance of a row d >= 1 rows away
+// (hav_tab[0] = 0), w = pi / 2B.
 __global__ void __launch_bounds__(kBinScanThreads) k_bin_scan(int n2b, const uint32_t* __restrict__ bin_count,
                                                               const uint32_t* __restrict__ row_count,
                                                               uint32_t* __restrict__ bin_start,
-                                                              int* __restrict__ row_nxt, int* __restrict__ row_prv) {
+                                                              int* __restrict__ row_nxt, int* __restrict__ row_prv,
+                                                              float* __restrict__ sin_tab, float* __restrict__ hav_tab) {
   __shared__ uint32_t s_rows[kMaxGridSide];
   __shared__ uint32_t s_w[kBinScanThreads / 32];
   __shared__ uint32_t s_base;
@@ -106,6 +115,13 @@ __global__ void __launch_bounds__(kBinScanThreads) k_bin_scan(int n2b, const uin
   for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
   if (lane == 0) s_w[warp] = part;
   __syncthreads();
+  if (t == 32) {
+    const double w = M_PI / (double)n2b;
+    sin_tab[r] = fmaxf((float)sin(r * w) - 1e-5f, 0.0f);
+    if (r == n2b - 1) sin_tab[n2b] = 0.0f;
+    const double h = sin(0.5 * (r - 0.5) * w);
+    hav_tab[r] = r == 0 ? 0.0f : (float)(h * h) * (1.0f - 1e-4f);
+  }
   if (t == 0) {
     uint32_t b = 0;
     for (int k = 0; k < kBinScanThreads / 32; ++k) b += s_w[k];
@@ -204,47 +220,16 @@ __device__ __forceinline__ void emit_sample(int qi, int nq, float best, int bidx
 
 
 // ---------------------------------------------------------------- row sweep
-constexpr float kPi = 3.14159265358979f;
 constexpr float kAngleMargin = 1e-4f;
 
-// Angle bound (radians) of a float squared chord, inflated so that float
-// rounding of the unit vectors cannot hide a nearer point; 4 (> pi) when the
+// Upper bound of sin^2(beta / 2) for the angle beta of a float squared chord
+// inflated by kAngleMargin (sin(asin h + m / 2) <= h + m / 2), so float
+// rounding of the unit vectors cannot hide a nearer point; 2 (> 1) when the
 // chord bounds nothing.
-__device__ __forceinline__ float angle_of_l2(float best) {
-  if (!(best < 3.99f)) return 4.0f;
-  const float h = 0.5f * sqrtf(best) * (1.0f + kAngleMargin);
-  return h >= 1.0f ? 4.0f : 2.0f * asinf(h) + kAngleMargin;
-}
-
-// Largest |phi - phi_q| of the cap of radius beta around q at colatitude t
-// (0 when the circle misses the cap, pi when it lies inside).  f is moved
-// towards -1 by 1e-5 so the ill-conditioned acos near f = 1 errs outwards.
-__device__ __forceinline__ float cap_extent_at(float cq, float sq, float cb, float t) {
-  const float st = sinf(t);
-  if (!(st > 1e-6f)) return kPi;
-  const float f = (cb - cq * cosf(t)) / (sq * st) - 1e-5f;
-  if (f <= -1.0f) return kPi;
-  if (f >= 1.0f) return 0.0f;
-  return acosf(f);
-}
-
-// Largest |phi - phi_q| of any point of colatitude in [a, b] within angle
-// beta of q (colatitude tq): pi when a pole inside the cap makes whole
-// circles of the row range qualify; otherwise the cap's half-width is
-// unimodal in the colatitude (largest at the tangent colatitude
-// acos(cos tq / cos beta)), so the maximum over [a, b] is at an end or there.
-__device__ __noinline__ float row_extent(float tq, float cq, float sq, float beta, float a, float b) {
-  if (beta >= kPi) return kPi;
-  const float bm = beta + kAngleMargin;
-  if (bm >= tq && a <= bm - tq) return kPi;
-  if (bm >= kPi - tq && b >= 2.0f * kPi - bm - tq) return kPi;
-  const float cb = cosf(beta), sb = sinf(beta);
-  float e = fmaxf(cap_extent_at(cq, sq, cb, a), cap_extent_at(cq, sq, cb, b));
-  if (beta < tq && beta < kPi - tq && cb > 0.0f) {
-    const float ts = acosf(fminf(1.0f, fmaxf(-1.0f, cq / cb)));
-    if (ts > a - kAngleMargin && ts < b + kAngleMargin) e = fmaxf(e, asinf(fminf(1.0f, sb / sq * 1.0001f)));
-  }
-  return e + kAngleMargin;
+__device__ __forceinline__ float hav_of_l2(float best) {
+  if (!(best < 3.99f)) return 2.0f;
+  const float s = 0.5f * sqrtf(best) * (1.0f + kAngleMargin) + 0.5f * kAngleMargin;
+  return s >= 1.0f ? 2.0f : s * s;
 }
 
 // Lanes per direction: a group of kGroup lanes strides over the points of a
@@ -291,10 +276,20 @@ __device__ __forceinline__ void group_nn_min(unsigned gmask, float& best, int& b
   }
 }
 
-// Half-width k (in columns) of the cap window of row r: column j +- c holds
-// longitudes at least (c - 1/2) 2w away from phi_q.
-__device__ __forceinline__ int row_window(int r, int n2b, float w, float tq, float cq, float sq, float beta) {
-  const float e = row_extent(tq, cq, sq, beta, (float)r * w, (float)(r + 1) * w);
+// Half-width k (in columns) of the cap window of row r, d rows from the
+// direction's own row: column j +- c holds longitudes at least (c - 1/2) 2w
+// away from phi_q, and a point of the row within the bound has
+//   hav(dphi) <= (hb - hav(row distance)) / (min(sin a, sin b) sin t_q)
+// (sin is concave, so its minimum over the row's colatitudes [a, b] is at an
+// edge).  n2b: the whole row.
+__device__ __forceinline__ int row_window(int r, int d, int n2b, float w, float stq, float hb,
+                                          const float* __restrict__ sin_tab, const float* __restrict__ hav_tab) {
+  if (hb >= 1.0f) return n2b;
+  const float num = hb - __ldg(&hav_tab[d]);
+  const float den = fminf(__ldg(&sin_tab[r]), __ldg(&sin_tab[r + 1])) * stq;
+  if (!(num < den)) return n2b;  // the bound reaches every longitude (or a pole row)
+  if (num <= 0.0f) return 0;
+  const float e = 2.0f * asinf(sqrtf(num / den)) + kAngleMargin;
   const float kf = e / (2.0f * w) + 0.5f;
   return kf >= (float)n2b ? n2b : (int)kf;
 }
@@ -310,37 +305,38 @@ constexpr int kQueryThreads = 256;
 __global__ void __launch_bounds__(kQueryThreads)
 k_nn_rows(int n2b, const float4* __restrict__ grid, const float4* __restrict__ sorted,
           const uint32_t* __restrict__ bin_start, const int* __restrict__ row_nxt, const int* __restrict__ row_prv,
-          float max_sq, const float4* __restrict__ xyzi, const double* __restrict__ range,
-          const float* __restrict__ refl, const float* __restrict__ amb, int n_out_ch, float* __restrict__ out,
-          int32_t* __restrict__ nn_idx) {
+          const float* __restrict__ sin_tab, const float* __restrict__ hav_tab, float max_sq,
+          const float4* __restrict__ xyzi, const double* __restrict__ range, const float* __restrict__ refl,
+          const float* __restrict__ amb, int n_out_ch, float* __restrict__ out, int32_t* __restrict__ nn_idx) {
   const int nq = n2b * n2b;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int qi = tid / kGroup, g = tid % kGroup;
   if (qi >= nq) return;  // whole groups: nq * kGroup threads are launched in full groups
   const unsigned gmask = ((1u << kGroup) - 1u) << ((threadIdx.x & 31) & ~(kGroup - 1));
-  const float w = kPi / (float)n2b;
+  const float w = 3.14159265358979f / (float)n2b;
   const float4 q = __ldg(&grid[qi]);
   const int i = qi / n2b, j = qi - i * n2b;
-  const float tq = ((float)i + 0.5f) * w;
-  const float cq = cosf(tq), sq = sinf(tq);
+  // sin t_q of the direction's colatitude (i + 1/2) w, deflated like the table
+  const float stq = fmaxf(sinf(((float)i + 0.5f) * w) - 1e-5f, 0.0f);
   float best = INFINITY;
   int bidx = 0x7fffffff;
-  float beta = 4.0f;
+  float hb = 2.0f;
   int up = __ldg(&row_nxt[i]), dn = __ldg(&row_prv[i]);
   bool probed = false;
   for (;;) {
-    const float lbu = up < n2b ? fmaxf(((float)(up - i) - 0.5f) * w, 0.0f) : INFINITY;
-    const float lbd = dn >= 0 ? ((float)(i - dn) - 0.5f) * w : INFINITY;
-    const bool take_up = lbu <= lbd;
-    const float lb = take_up ? lbu : lbd;
-    if (!(lb <= beta)) break;
+    if (up >= n2b && dn < 0) break;
+    const int du = up < n2b ? up - i : 0x7fffffff, dd = dn >= 0 ? i - dn : 0x7fffffff;
+    const bool take_up = du <= dd;
+    const int d = take_up ? du : dd;
+    // the row's colatitude distance alone must not exceed the bound
+    if (!(__ldg(&hav_tab[d]) <= hb)) break;
     const int r = take_up ? up : dn;
     if (!probed) {
       const int pw = min(3, n2b);
       scan_cols(r, j - 1, pw, n2b, g, q.x, q.y, q.z, bin_start, sorted, best, bidx);
       group_nn_min(gmask, best, bidx);
-      beta = angle_of_l2(best);
-      const int k = row_window(r, n2b, w, tq, cq, sq, beta);
+      hb = hav_of_l2(best);
+      const int k = row_window(r, d, n2b, w, stq, hb, sin_tab, hav_tab);
       if (2 * k + 1 >= n2b) {
         scan_cols(r, j + 2, n2b - pw, n2b, g, q.x, q.y, q.z, bin_start, sorted, best, bidx);
       } else if (k >= 2) {
@@ -349,14 +345,14 @@ k_nn_rows(int n2b, const float4* __restrict__ grid, const float4* __restrict__ s
       }
       probed = true;
     } else {
-      const int k = row_window(r, n2b, w, tq, cq, sq, beta);
+      const int k = row_window(r, d, n2b, w, stq, hb, sin_tab, hav_tab);
       if (2 * k + 1 >= n2b)
         scan_cols(r, 0, n2b, n2b, g, q.x, q.y, q.z, bin_start, sorted, best, bidx);
       else
         scan_cols(r, j - k, 2 * k + 1, n2b, g, q.x, q.y, q.z, bin_start, sorted, best, bidx);
     }
     group_nn_min(gmask, best, bidx);
-    beta = angle_of_l2(best);
+    hb = hav_of_l2(best);
     if (take_up)
       up = __ldg(&row_nxt[up + 1]);
     else
@@ -387,7 +383,8 @@ size_t sampler_scratch_bytes(int max_points, int max_queries) {
   b += (2 * nbins + (size_t)n2b) * sizeof(uint32_t);             // bin counts, cursors, row counts
   b += (nbins + 1) * sizeof(uint32_t);                           // bin starts
   b += 2 * (size_t)(n2b + 1) * sizeof(int);                      // row tables
-  return b + 8 * 256;  // carve() rounds each region up to 256 bytes
+  b += 2 * (size_t)(n2b + 1) * sizeof(float);                    // window bound tables
+  return b + 10 * 256;  // carve() rounds each region up to 256 bytes
 }
 
 static inline char* carve(char*& p, size_t bytes) {
@@ -412,6 +409,8 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   uint32_t* bin_start = (uint32_t*)carve(p, (nbins + 1) * sizeof(uint32_t));
   int* row_nxt = (int*)carve(p, (size_t)(n2b + 1) * sizeof(int));
   int* row_prv = (int*)carve(p, (size_t)(n2b + 1) * sizeof(int));
+  float* sin_tab = (float*)carve(p, (size_t)(n2b + 1) * sizeof(float));
+  float* hav_tab = (float*)carve(p, (size_t)(n2b + 1) * sizeof(float));
 
   cudaMemsetAsync(counts, 0, (2 * nbins + (size_t)n2b) * sizeof(uint32_t), st);
   const int P = a.n_points;
@@ -420,7 +419,8 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
     k_project<<<(P + 255) / 256, 256, 0, st>>>(a.xyzi, P, proj, range, key, n2b, bin_count, row_count);
     ++launched;
   }
-  k_bin_scan<<<n2b, kBinScanThreads, 0, st>>>(n2b, bin_count, row_count, bin_start, row_nxt, row_prv);
+  k_bin_scan<<<n2b, kBinScanThreads, 0, st>>>(n2b, bin_count, row_count, bin_start, row_nxt, row_prv, sin_tab,
+                                               hav_tab);
   ++launched;
   if (P > 0) {
     k_bin_scatter<<<(P + 255) / 256, 256, 0, st>>>(P, proj, key, bin_start, cursor, sorted);
@@ -428,8 +428,8 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   }
   const size_t q_threads = (size_t)a.n_queries * kGroup;
   k_nn_rows<<<(unsigned)((q_threads + kQueryThreads - 1) / kQueryThreads), kQueryThreads, 0, st>>>(
-      n2b, a.grid, sorted, bin_start, row_nxt, row_prv, a.max_sq, a.xyzi, range, a.refl, a.amb, a.n_out_ch, a.out,
-      a.nn_idx);
+      n2b, a.grid, sorted, bin_start, row_nxt, row_prv, sin_tab, hav_tab, a.max_sq, a.xyzi, range, a.refl, a.amb,
+      a.n_out_ch, a.out, a.nn_idx);
   ++launched;
   count_launches(launched);
   return cudaGetLastError();
