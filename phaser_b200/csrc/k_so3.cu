@@ -351,7 +351,9 @@ __global__ void __launch_bounds__(256) k_so3_c2r_tail(int bw_in, const float2* _
   __syncthreads();
   fft_tail<NF, true, false>(zrow, np, ST, plan.tw);
   const float K = (float)((1.0 / (double)n) * ((double)Bo / M_PI));
-  unsigned long long best = 0ull;
+  // per thread: the largest value, the lowest index among equal ones
+  float bv = -1.0f;
+  uint32_t bi = 0xffffffffu;
   for (int e = threadIdx.x; e < np * n; e += blockDim.x) {
     const int p = e / n, g = e - p * n;
     const float2 z = zrow[p * ST + g];
@@ -362,13 +364,15 @@ __global__ void __launch_bounds__(256) k_so3_c2r_tail(int bw_in, const float2* _
         const float v = (h ? z.y : z.x) * K;
         const float v2 = v * v;
         const uint32_t idx = ((uint32_t)k * n + (uint32_t)s_alpha[r]) * n + g;
-        const unsigned long long key = pack_argmax(v2, idx);
-        best = key > best ? key : best;
+        if (v2 > bv || (v2 == bv && idx < bi)) {
+          bv = v2;
+          bi = idx;
+        }
         if (volume) volume[idx] = v2;
       }
     }
   }
-  warp_argmax_commit(best, argmax);
+  warp_argmax_commit(bi == 0xffffffffu ? 0ull : pack_argmax(bv, bi), argmax);
 }
 
 template <int NF>

@@ -533,10 +533,24 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
     if (k < NH) s_posH[k] = fixed_freq2pos<NH>(k);
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < NH * H2; e += blockDim.x) {
+  // four elements' loads in flight per thread
+  constexpr int U = 4;
+  for (int e0 = threadIdx.x; e0 < NH * H2; e0 += U * blockDim.x) {
+    float2 x0u[U], x1u[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = e0 + u * blockDim.x;
+      const int k = e / H2, ky = e - k * H2;
+      const bool ok = e < NH * H2;
+      x0u[u] = ok ? X[(size_t)k * H2p + ky] : make_float2(0.f, 0.f);
+      x1u[u] = ok ? X[(size_t)(k + NH) * H2p + ky] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+    const int e = e0 + u * blockDim.x;
+    if (e >= NH * H2) break;
     const int k = e / H2, ky = e - k * H2;
-    float2 x0 = X[(size_t)k * H2p + ky];
-    float2 x1 = X[(size_t)(k + NH) * H2p + ky];
+    float2 x0 = x0u[u], x1 = x1u[u];
     if (ky == 0 || ky == NH) {
       const float2 m0 = X[(size_t)(k == 0 ? 0 : N - k) * H2p + ky];  // kx = -k
       const float2 m1 = X[(size_t)(NH - k) * H2p + ky];               // kx = -(k + N/2)
@@ -548,26 +562,35 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
     // W = A + i B at (k, ky); its mirror (-k, -ky) holds conj(A) + i conj(B)
     W[s_posH[k] * S + s_posN[ky]] = make_float2(A.x - B.y, A.y + B.x);
     if (ky >= 1 && ky < NH) W[s_posH[k == 0 ? 0 : NH - k] * S + s_posN[N - ky]] = make_float2(A.x + B.y, -A.y + B.x);
+    }
   }
   __syncthreads();
   fft_tail<NH, true, true>(W, N, S, pH.tw);    // over r, columns
   fft_tail<N, true, false>(W, NH, S, pN.tw);   // over y, rows
-  unsigned long long best = 0ull;
+  // a thread visits its indices in increasing order (i0 < i1 < the next
+  // element's i0): a strictly larger value keeps the first occurrence
+  float bv = -INFINITY;
+  uint32_t bi = 0xffffffffu;
   for (int e = threadIdx.x; e < NH * N; e += blockDim.x) {
     const int r = e / N, y = e - r * N;
     const float2 v = W[r * S + y];
     const float a0 = 2.0f * v.x, a1 = 2.0f * v.y;
     const uint32_t i0 = (uint32_t)(((size_t)z * N + 2 * r) * N + y);
     const uint32_t i1 = i0 + N;
-    unsigned long long k0 = i0 < limit ? pack_argmax(a0, i0) : 0ull, k1 = i1 < limit ? pack_argmax(a1, i1) : 0ull;
-    k0 = k1 > k0 ? k1 : k0;
-    best = k0 > best ? k0 : best;
+    if (i0 < limit && (a0 > bv || bi == 0xffffffffu)) {
+      bv = a0;
+      bi = i0;
+    }
+    if (i1 < limit && (a1 > bv || bi == 0xffffffffu)) {
+      bv = a1;
+      bi = i1;
+    }
     if (volume) {
       volume[i0] = a0;
       volume[i1] = a1;
     }
   }
-  warp_argmax_commit(best, argmax);
+  warp_argmax_commit(bi == 0xffffffffu ? 0ull : pack_argmax(bv, bi), argmax);
 }
 
 // ---------------------------------------------------------------- launchers
