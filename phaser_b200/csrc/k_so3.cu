@@ -310,8 +310,8 @@ template <int NF>
 __global__ void __launch_bounds__(256) k_so3_c2r_tail(int bw_in, const float2* __restrict__ S, FftPlan plan,
                                                      unsigned long long* __restrict__ argmax,
                                                      float* __restrict__ volume) {
-  constexpr int n = NF, Bo = NF / 2, RB = c2r_pair_rows<NF>(), P = RB / 2, ST = NF + 1;
-  extern __shared__ float2 zrow[];  // [P][ST]
+  constexpr int n = NF, Bo = NF / 2, RB = c2r_pair_rows<NF>(), ST = NF + 1;
+  extern __shared__ float2 zrow[];  // [RB / 2][ST]: one row pair per complex transform
   __shared__ int s_pos[NF];
   __shared__ int s_alpha[RB];
   const int k = blockIdx.y;
