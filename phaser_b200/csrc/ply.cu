@@ -270,7 +270,16 @@ int read_body(std::ifstream& in, const Layout& L, const Sinks& s) {
     stride += type_size(ve.props[p].type);
   }
   if (fixed) {
-    // one read of the whole vertex block, then fixed-offset decoding
+    // one read of the whole vertex block, then fixed-offset decoding; when
+    // every requested field is a float32 in host byte order the values are
+    // copied straight (float -> double -> float is exact, so this equals the
+    // general decoding)
+    bool direct = !swap;
+    int off[kFields];
+    for (int f = 0; f < kFields; ++f) {
+      off[f] = L.col[f] >= 0 ? offset[L.col[f]] : -1;
+      if (L.col[f] >= 0 && (f < 4 || s.out[f - 4]) && ve.props[L.col[f]].type != kF32) direct = false;
+    }
     const uint64_t chunk_rows = 1u << 16;
     std::vector<unsigned char> buf(chunk_rows * stride);
     for (uint64_t i0 = 0; i0 < ve.count; i0 += chunk_rows) {
@@ -278,6 +287,16 @@ int read_body(std::ifstream& in, const Layout& L, const Sinks& s) {
       if (!in.read((char*)buf.data(), (std::streamsize)(rows * stride))) {
         g_ply_error = "truncated binary body";
         return PHGPU_ERR_INVALID;
+      }
+      if (direct) {
+        for (uint64_t r = 0; r < rows; ++r) {
+          const unsigned char* b = buf.data() + r * stride;
+          const uint64_t i = i0 + r;
+          for (int c = 0; c < 4; ++c) memcpy(&s.xyzi[4 * i + c], b + off[c], 4);
+          for (int f = 0; f < 3; ++f)
+            if (s.out[f] && off[4 + f] >= 0) memcpy(&s.out[f][i], b + off[4 + f], 4);
+        }
+        continue;
       }
       for (uint64_t r = 0; r < rows; ++r) {
         const unsigned char* b = buf.data() + r * stride;
