@@ -147,6 +147,32 @@ double read_binary(const unsigned char* b, PlyType t, bool swap) {
   }
 }
 
+// Column of `rows` values of type T at `src` + r * stride (host byte order)
+// into dst[r * dst_stride], narrowed as the reference does: to double, then
+// to float.
+template <typename T>
+void decode_column_as(const unsigned char* src, uint64_t rows, int stride, float* dst, int dst_stride) {
+  for (uint64_t r = 0; r < rows; ++r) {
+    T v;
+    memcpy(&v, src + r * stride, sizeof(T));
+    dst[r * dst_stride] = (float)(double)v;
+  }
+}
+
+void decode_column(const unsigned char* src, uint64_t rows, int stride, PlyType t, float* dst, int dst_stride) {
+  switch (t) {
+    case kI8: decode_column_as<int8_t>(src, rows, stride, dst, dst_stride); break;
+    case kU8: decode_column_as<uint8_t>(src, rows, stride, dst, dst_stride); break;
+    case kI16: decode_column_as<int16_t>(src, rows, stride, dst, dst_stride); break;
+    case kU16: decode_column_as<uint16_t>(src, rows, stride, dst, dst_stride); break;
+    case kI32: decode_column_as<int32_t>(src, rows, stride, dst, dst_stride); break;
+    case kU32: decode_column_as<uint32_t>(src, rows, stride, dst, dst_stride); break;
+    case kF32: decode_column_as<float>(src, rows, stride, dst, dst_stride); break;
+    case kF64: decode_column_as<double>(src, rows, stride, dst, dst_stride); break;
+    default: break;
+  }
+}
+
 thread_local std::string g_ply_error;
 
 // The seven requested fields: x, y, z, intensity (required), then
@@ -270,16 +296,9 @@ int read_body(std::ifstream& in, const Layout& L, const Sinks& s) {
     stride += type_size(ve.props[p].type);
   }
   if (fixed) {
-    // one read of the whole vertex block, then fixed-offset decoding; when
-    // every requested field is a float32 in host byte order the values are
-    // copied straight (float -> double -> float is exact, so this equals the
-    // general decoding)
-    bool direct = !swap;
-    int off[kFields];
-    for (int f = 0; f < kFields; ++f) {
-      off[f] = L.col[f] >= 0 ? offset[L.col[f]] : -1;
-      if (L.col[f] >= 0 && (f < 4 || s.out[f - 4]) && ve.props[L.col[f]].type != kF32) direct = false;
-    }
+    // one read of the whole vertex block, then fixed-offset decoding: in host
+    // byte order field by field with the type resolved once per chunk
+    // (decode_column), otherwise value by value
     const uint64_t chunk_rows = 1u << 16;
     std::vector<unsigned char> buf(chunk_rows * stride);
     for (uint64_t i0 = 0; i0 < ve.count; i0 += chunk_rows) {
@@ -288,13 +307,12 @@ int read_body(std::ifstream& in, const Layout& L, const Sinks& s) {
         g_ply_error = "truncated binary body";
         return PHGPU_ERR_INVALID;
       }
-      if (direct) {
-        for (uint64_t r = 0; r < rows; ++r) {
-          const unsigned char* b = buf.data() + r * stride;
-          const uint64_t i = i0 + r;
-          for (int c = 0; c < 4; ++c) memcpy(&s.xyzi[4 * i + c], b + off[c], 4);
-          for (int f = 0; f < 3; ++f)
-            if (s.out[f] && off[4 + f] >= 0) memcpy(&s.out[f][i], b + off[4 + f], 4);
+      if (!swap) {
+        for (int f = 0; f < kFields; ++f) {
+          const int p = L.col[f];
+          if (p < 0 || (f >= 4 && !s.out[f - 4])) continue;
+          float* dst = f < 4 ? s.xyzi + 4 * i0 + f : s.out[f - 4] + i0;
+          decode_column(buf.data() + offset[p], rows, stride, ve.props[p].type, dst, f < 4 ? 4 : 1);
         }
         continue;
       }
