@@ -10,6 +10,9 @@
 //   SpatialCorrelationLowPass     .../spatial-correlation-low-pass.h
 //   PhaseAligner                  phaser_core/include/phaser/backend/alignment/phase-aligner.h:17-26
 //   SphOptRegistration            phaser_core/include/phaser/backend/registration/sph-opt-registration.h
+//   PlyHelper, PlyPointCloud      phaser_common/include/phaser/common/data/ply-helper.h,
+//                                 phaser_common/include/phaser/model/ply-point-cloud.h
+//   VoxelGridCmd                  phaser_pre/include/phaser_pre/commands/voxel-grid-cmd.h
 // so a caller swaps the include and the namespace (phaser_gpu instead of
 // phaser_core).  Errors throw std::runtime_error (the reference aborts through
 // glog CHECKs instead).  Eigen::VectorXd arguments are accepted when Eigen is
@@ -302,6 +305,105 @@ class SphOptRegistration {
 
  private:
   detail::Context ctx_;
+};
+
+// ------------------------------------------------------------------ ingest
+
+// The fields PlyHelper reads (ply-helper.cc:26-64), narrowed to float as the
+// reference's cloud does: x, y, z, intensity interleaved, and the optional
+// reflectivity, ambient ("noise") and range (empty when the file lacks them).
+struct PlyPointCloud {
+  std::vector<float> xyzi;  // [n][4]
+  std::vector<float> reflectivity, ambient, range;
+  size_t size() const noexcept { return xyzi.size() / 4; }
+  const std::vector<float>& getReflectivities() const noexcept { return reflectivity; }
+  const std::vector<float>& getAmbientPoints() const noexcept { return ambient; }
+  const std::vector<float>& getRange() const noexcept { return range; }
+  // x, y, z, intensity + optional channels as the aligner / registration take them
+  CloudView view() const {
+    CloudView v;
+    v.xyzi = xyzi.data();
+    v.reflectivity = reflectivity.empty() ? nullptr : reflectivity.data();
+    v.ambient = ambient.empty() ? nullptr : ambient.data();
+    v.n_points = (uint32_t)size();
+    return v;
+  }
+};
+
+// PlyHelper::readPlyFromFile; the field names default to the reference's
+// --phaser_ply_{intensity,reflectivity,ambient,range}_str flags.
+class PlyHelper {
+ public:
+  explicit PlyHelper(std::string intensity = "intensity", std::string reflectivity = "reflectivity",
+                     std::string ambient = "noise", std::string range = "range")
+      : names_{std::move(intensity), std::move(reflectivity), std::move(ambient), std::move(range)} {}
+  PlyPointCloud readPlyFromFile(const std::string& filename) const {
+    const char* names[4] = {names_[0].c_str(), names_[1].c_str(), names_[2].c_str(), names_[3].c_str()};
+    uint32_t n = 0, present = 0;
+    ply_check(phgpu_ply_info(filename.c_str(), names, &n, &present));
+    PlyPointCloud pc;
+    pc.xyzi.resize((size_t)n * 4);
+    if (present & PHGPU_PLY_REFLECTIVITY) pc.reflectivity.resize(n);
+    if (present & PHGPU_PLY_AMBIENT) pc.ambient.resize(n);
+    if (present & PHGPU_PLY_RANGE) pc.range.resize(n);
+    uint32_t got = 0;
+    ply_check(phgpu_ply_read(filename.c_str(), names, pc.xyzi.data(),
+                             pc.reflectivity.empty() ? nullptr : pc.reflectivity.data(),
+                             pc.ambient.empty() ? nullptr : pc.ambient.data(),
+                             pc.range.empty() ? nullptr : pc.range.data(), n, &got));
+    return pc;
+  }
+
+ private:
+  static void ply_check(int rc) {
+    if (rc != PHGPU_OK) throw std::runtime_error(std::string("phgpu_ply: ") + phgpu_ply_last_error());
+  }
+  std::string names_[4];
+};
+
+// VoxelGridCmd::execute (voxel-grid-cmd.cc:11-22): pcl::VoxelGrid with leaf
+// --phaser_voxel_grid_leaf_size (0.25) on the GPU, filtering the cloud in
+// place (reflectivity and ambient, when present, are averaged over the same
+// leaves; range is per raw point and is dropped).
+class VoxelGridCmd {
+ public:
+  explicit VoxelGridCmd(float leaf_size = 0.25f, int32_t device = 0) : leaf_(leaf_size), device_(device) {}
+  ~VoxelGridCmd() {
+    if (vg_) phgpu_voxel_grid_destroy(vg_);
+  }
+  VoxelGridCmd(const VoxelGridCmd&) = delete;
+  VoxelGridCmd& operator=(const VoxelGridCmd&) = delete;
+  void execute(PlyPointCloud& cloud) {
+    const uint32_t n = (uint32_t)cloud.size();
+    if (!vg_ || n > cap_) {
+      if (vg_) phgpu_voxel_grid_destroy(vg_);
+      vg_ = nullptr;
+      cap_ = std::max<uint32_t>(n, 1u);
+      if (phgpu_voxel_grid_create(cap_, device_, &vg_) != PHGPU_OK)
+        throw std::runtime_error("phgpu_voxel_grid_create failed");
+    }
+    phgpu_cloud in = cloud.view().c();
+    std::vector<float> xyzi((size_t)n * 4), refl(cloud.reflectivity.empty() ? 0 : n),
+        amb(cloud.ambient.empty() ? 0 : n);
+    const float leaf[3] = {leaf_, leaf_, leaf_};
+    uint32_t m = 0;
+    if (phgpu_voxel_grid_filter(vg_, &in, leaf, 0, xyzi.data(), refl.empty() ? nullptr : refl.data(),
+                                amb.empty() ? nullptr : amb.data(), 0, &m) != PHGPU_OK)
+      throw std::runtime_error(std::string("phgpu_voxel_grid_filter: ") + phgpu_voxel_grid_last_error(vg_));
+    xyzi.resize((size_t)m * 4);
+    cloud.xyzi = std::move(xyzi);
+    if (!refl.empty()) refl.resize(m);
+    if (!amb.empty()) amb.resize(m);
+    cloud.reflectivity = std::move(refl);
+    cloud.ambient = std::move(amb);
+    cloud.range.clear();
+  }
+
+ private:
+  float leaf_;
+  int32_t device_;
+  phgpu_voxel_grid* vg_ = nullptr;
+  uint32_t cap_ = 0;
 };
 
 }  // namespace phaser_gpu

@@ -65,6 +65,25 @@ int main() {
   } catch (const std::runtime_error&) {
     std::printf("invalid_configuration_rejected\n");
   }
+  // VoxelGridCmd on a cloud of three points: leaves (0,0,0) and (2,0,0) at
+  // leaf 0.25 (grid anchored at floor(min / leaf)); each leaf's mean is the
+  // in-order float sum divided by the count
+  {
+    PlyPointCloud pc;
+    pc.xyzi = {0.1f, 0.1f, 0.1f, 1.0f, 0.2f, 0.1f, 0.1f, 3.0f, 0.6f, 0.1f, 0.1f, 5.0f};
+    VoxelGridCmd cmd(0.25f);
+    cmd.execute(pc);
+    float sx = 0.0f, sy = 0.0f;
+    sx += 0.1f;
+    sx += 0.2f;
+    sy += 0.1f;
+    sy += 0.1f;
+    const float want[8] = {sx / 2.0f, sy / 2.0f, sy / 2.0f, 2.0f, 0.6f, 0.1f, 0.1f, 5.0f};
+    std::printf("voxel_grid %zu\n", pc.size());
+    if (pc.size() != 2u) return 5;
+    for (int k = 0; k < 8; ++k)
+      if (pc.xyzi[k] != want[k]) return 6;
+  }
   std::printf("ok\n");
   return 0;
 }
