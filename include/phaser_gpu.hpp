@@ -10,6 +10,9 @@
 //   SpatialCorrelationLowPass     .../spatial-correlation-low-pass.h
 //   PhaseAligner                  phaser_core/include/phaser/backend/alignment/phase-aligner.h:17-26
 //   SphOptRegistration            phaser_core/include/phaser/backend/registration/sph-opt-registration.h
+//   SphericalSampler, FunctionValue
+//                                 phaser_common/include/phaser/common/spherical-sampler.h,
+//                                 phaser_common/include/phaser/model/function-value.h
 //   PlyHelper, PlyPointCloud      phaser_common/include/phaser/common/data/ply-helper.h,
 //                                 phaser_common/include/phaser/model/ply-point-cloud.h
 //   VoxelGridCmd                  phaser_pre/include/phaser_pre/commands/voxel-grid-cmd.h
@@ -23,6 +26,7 @@
 
 #include <cstdint>
 #include <algorithm>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -305,6 +309,61 @@ class SphOptRegistration {
 
  private:
   detail::Context ctx_;
+};
+
+// ------------------------------------------------------------------ S^2 sampling
+
+// One direction's sample (model::FunctionValue): the values of the nearest
+// cloud point (the 1-NN sampler feeds each direction one point), 0 when the
+// nearest point lies beyond the rejection radius (nn_index -1).
+struct FunctionValue {
+  double range = 0.0, intensity = 0.0, reflectivity = 0.0, ambient = 0.0;
+  int32_t nn_index = -1;
+  double getAveragedRange() const noexcept { return range; }
+  double getAveragedIntensity() const noexcept { return intensity; }
+  double getAveragedReflectivity() const noexcept { return reflectivity; }
+  double getAveragedAmbientNoise() const noexcept { return ambient; }
+};
+
+// SphericalSampler::sampleUniformly (spherical-sampler.cc:20-27): the 2B x 2B
+// Driscoll-Healy directions, [theta][phi] order, each sampled by its nearest
+// point of the cloud's projection on the unit sphere.  The rejection radius
+// comes from the parameters as in a context.
+class SphericalSampler {
+ public:
+  explicit SphericalSampler(int bandwith, const phgpu_params& base = default_params()) : base_(base) {
+    initialize(bandwith);
+  }
+  void initialize(int bandwith) {
+    phgpu_params p = base_;
+    p.spherical_bandwidth = (uint32_t)bandwith;
+    p.spherical_zero_padding = 0;
+    ctx_.reset(new detail::Context(p));
+    bw_ = bandwith;
+  }
+  int getInitializedBandwith() const noexcept { return bw_; }
+  void sampleUniformly(const CloudView& cloud, std::vector<FunctionValue>* grid) {
+    phgpu_cloud c = cloud.c();
+    detail::check(phgpu_sample_s2(ctx_->get(), &c, 0), ctx_->get(), "phgpu_sample_s2");
+    const size_t nq = (size_t)4 * bw_ * bw_;
+    std::vector<double> v(4 * nq);
+    std::vector<int32_t> nn(nq);
+    detail::check(phgpu_get_samples(ctx_->get(), 0, v.data(), nn.data()), ctx_->get(), "phgpu_get_samples");
+    grid->assign(nq, FunctionValue());
+    for (size_t q = 0; q < nq; ++q) {
+      FunctionValue& f = (*grid)[q];
+      f.range = v[q];
+      f.intensity = v[nq + q];
+      f.reflectivity = v[2 * nq + q];
+      f.ambient = v[3 * nq + q];
+      f.nn_index = nn[q];
+    }
+  }
+
+ private:
+  phgpu_params base_;
+  std::unique_ptr<detail::Context> ctx_;
+  int bw_ = 0;
 };
 
 // ------------------------------------------------------------------ ingest

@@ -65,6 +65,23 @@ int main() {
   } catch (const std::runtime_error&) {
     std::printf("invalid_configuration_rejected\n");
   }
+  // SphericalSampler on a one-point cloud: every direction's nearest point is
+  // that point (the default rejection radius is 1000 m), range |p| = 3
+  {
+    const float xyzi[4] = {3.0f, 0.0f, 0.0f, 5.0f};
+    CloudView cv;
+    cv.xyzi = xyzi;
+    cv.n_points = 1;
+    SphericalSampler sampler(8);
+    std::vector<FunctionValue> grid;
+    sampler.sampleUniformly(cv, &grid);
+    std::printf("sampler %zu bw %d\n", grid.size(), sampler.getInitializedBandwith());
+    if (grid.size() != 4u * 8u * 8u) return 7;
+    for (const FunctionValue& f : grid)
+      if (f.nn_index != 0 || f.getAveragedRange() != 3.0 || f.getAveragedIntensity() != 5.0 ||
+          f.getAveragedReflectivity() != 0.0)
+        return 8;
+  }
   // VoxelGridCmd on a cloud of three points: leaves (0,0,0) and (2,0,0) at
   // leaf 0.25 (grid anchored at floor(min / leaf)); each leaf's mean is the
   // in-order float sum divided by the count
