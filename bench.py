@@ -623,7 +623,8 @@ def main():
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         dt, kind = cpu_reference(pool[0], w)
         cpu = {"value": round(1.0 / dt, 4), "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
-               "sample": "1 pair of the B=100/N=200 workload, all host threads"}
+               "sample": "1 pair of the B=100/N=200 workload, all host threads; SOFT sources with the "
+                         "project's FP64 FFTW-API shim (no FFTW3 library in the image)"}
 
     if rank == 0:
         line = {
