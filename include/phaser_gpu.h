@@ -42,6 +42,15 @@ extern "C" {
 /* flags */
 #define PHGPU_FLAG_KEEP_VOLUMES 1u /* also keep the full correlation volumes */
 
+/* Arithmetic of the SO(3) synthesis (the Wigner-d sums over l):
+ * FP32: CUDA-core FP32 sums of d-values from an FP64 recurrence run per call;
+ * TF32X3 / BF16X3: tensor-core sums over a Wigner-d table generated once per
+ * context in FP64 and stored as FP32, each product split as hi*hi + hi*lo +
+ * lo*hi of TF32 or BF16 parts with FP32 accumulation (bandwidth <= 256). */
+#define PHGPU_PRECISION_FP32 0
+#define PHGPU_PRECISION_TF32X3 1
+#define PHGPU_PRECISION_BF16X3 2
+
 /* Configuration; names and defaults follow the reference's gflags
  * (phaser_common/src/common/core-gflags.cc:6-40,
  *  phaser_common/src/model/point-cloud.cc:19-20). */
@@ -65,6 +74,7 @@ typedef struct {
   uint32_t trans_peak_neighbors;     /* gaussian_peak_neighbors (0) */
   uint32_t spherical_low_pass_lower; /* phaser_core_spherical_low_pass_lower_bound (0) */
   uint32_t spherical_low_pass_upper; /* phaser_core_spherical_low_pass_upper_bound (100000) */
+  uint32_t precision;                /* PHGPU_PRECISION_* of the SO(3) synthesis (FP32) */
 } phgpu_params;
 
 /* A point cloud: x, y, z, intensity as float4 plus optional per-point
@@ -187,9 +197,17 @@ int phgpu_spatial_result(phgpu_ctx* ctx, uint32_t* voxel, float* peak, double* c
 uint32_t phgpu_spatial_correlation_size(const phgpu_ctx* ctx);
 
 /* SphOptRegistration::registerPointCloud (sph-opt-registration.cc:34-47):
- * rotation, then translation of the rotated source. */
+ * rotation, then translation of the rotated source.  The rotation pose and the
+ * source's transform are computed on the device, so the pair runs as one
+ * asynchronous chain with a single read-back; the host then recomputes the
+ * transform from the bin and, should any bit differ (the two sides' double
+ * trig functions may round differently), redoes the translation with the
+ * host's transform.  With rot_peak_neighbors > 0 or spatial zero padding the
+ * transform comes from the host. */
 int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_cloud* source,
                         phgpu_pose* out);
+/* Translations phgpu_register_pair redid with the host transform on ctx. */
+unsigned long long phgpu_pose_reruns(const phgpu_ctx* ctx);
 
 /* Host pose arithmetic of the reference (rotation-utils.cc:86-143, 197-208;
  * translation-utils.cc:40-52). */
@@ -296,35 +314,60 @@ const char* phgpu_voxel_grid_last_error(const phgpu_voxel_grid* vg);
 /* ------------------------------------------------------------------ serving
  * Continuous-batching request server (no reference counterpart: the
  * reference registers one pair at a time, sph-opt-registration.cc:34-47).
- * Requests of different (bandwidth, voxel grid) shapes are admitted against an
- * HBM budget, grouped by shape into waves and run on device-resident state. */
+ * Requests are grouped by shape (bandwidth, voxel grid, fusion, precision and
+ * the clouds' optional channels) into waves of up to max_wave pairs; a wave is
+ * one CUDA graph launch over device-resident per-slot state, with each SO(3)
+ * stage batched across the wave (the tensor-core synthesis reads the shape's
+ * Wigner-d table once per wave).  `lanes` waves run concurrently, so requests
+ * that arrive while one wave is on the GPU join the next.  Executors (the
+ * per-shape slot sets) are admitted against the HBM budget; idle ones are
+ * evicted, least recently used first, when a new shape needs the memory. */
 typedef struct phgpu_server phgpu_server;
 
 typedef struct {
-  uint64_t hbm_budget_bytes;   /* admission budget */
-  uint32_t max_wave;           /* pairs per wave and shape */
-  uint32_t max_points;         /* capacity per cloud */
+  uint64_t hbm_budget_bytes;   /* admission budget (150 GB when 0) */
+  uint32_t max_wave;           /* pairs per wave (16 when 0; at most 32) */
+  uint32_t max_points;         /* capacity per cloud (2^18 when 0); larger clouds are refused */
   int32_t device;
   uint32_t flags;              /* PHGPU_SERVER_* */
+  uint32_t lanes;              /* waves in flight at once (2 when 0) */
 } phgpu_server_params;
 
 /* Host clouds are read in place by the worker (copied to the device inside the
- * request, asynchronously when the memory is pinned) instead of being copied
- * at submit; the caller keeps them valid until the ticket completes. */
+ * wave, asynchronously when the memory is pinned) instead of being copied at
+ * submit; the caller keeps them valid until the ticket completes. */
 #define PHGPU_SERVER_BORROW_HOST 1u
+
+typedef struct {
+  uint64_t waves;           /* waves run */
+  uint64_t requests;        /* requests completed in waves */
+  uint64_t graph_captures;  /* CUDA graphs captured (one per executor and wave size) */
+  uint64_t evictions;       /* executors evicted to admit another shape */
+  uint64_t pose_reruns;     /* translations redone with the host transform */
+  uint64_t executors;       /* executors resident now */
+  uint64_t bytes_in_use;    /* device bytes of the resident executors */
+} phgpu_server_stats;
 
 int phgpu_server_create(const phgpu_server_params* params, phgpu_server** out);
 int phgpu_server_destroy(phgpu_server* srv);
-/* Submits one pair; params gives the shape (bandwidth, voxels, bounds).  Host
- * clouds are copied before the call returns (unless PHGPU_SERVER_BORROW_HOST);
- * device clouds (on_device = 1 for both) are read in place and must stay
- * valid until the ticket completes.  *ticket identifies the request. */
+/* Submits one pair; params gives the shape (bandwidth, voxels, bounds,
+ * precision).  Host clouds are copied before the call returns (unless
+ * PHGPU_SERVER_BORROW_HOST); device clouds (on_device = 1 for both) are read in
+ * place and must stay valid until the ticket completes.  Spatial zero padding
+ * is refused (PHGPU_ERR_INVALID), clouds above max_points too (PHGPU_ERR_LIMIT).
+ * *ticket identifies the request. */
 int phgpu_server_submit(phgpu_server* srv, const phgpu_params* params, const phgpu_cloud* target,
                         const phgpu_cloud* source, uint64_t* ticket);
 /* Non-blocking: 1 and the pose when the ticket finished, 0 otherwise. */
 int phgpu_server_poll(phgpu_server* srv, uint64_t ticket, phgpu_pose* out, double* latency_ms);
+/* The same, also copying the request's correlation volumes ((2 bw_out)^3 and
+ * N^3 floats, layouts as phgpu_sph_result / phgpu_spatial_result) when it was
+ * submitted with PHGPU_FLAG_KEEP_VOLUMES; either pointer may be NULL. */
+int phgpu_server_poll_volumes(phgpu_server* srv, uint64_t ticket, phgpu_pose* out, double* latency_ms,
+                              float* rot_volume, float* trans_volume);
 /* Blocks until every submitted request finished. */
 int phgpu_server_drain(phgpu_server* srv);
+int phgpu_server_get_stats(phgpu_server* srv, phgpu_server_stats* out);
 const char* phgpu_server_last_error(const phgpu_server* srv);
 
 #ifdef __cplusplus

@@ -831,11 +831,18 @@ void orc_quat_to_xyz(const double* q, double* xyz) {
   xyz[0] = atan2(r11, r12);
 }
 
-/* Rx(a) * Ry(b) * Rz(c) as float 3x4 (rows), createTransformationAround*. */
+/* Rx(a) * Ry(b) * Rz(c) as float 3x4 (rows), createTransformationAround*
+ * (phaser_common/src/common/rotation-utils.cc:109-143).  std::cos(float) and
+ * std::sin(float) are taken as their correctly rounded values (evaluated in
+ * double, rounded once): the reference's libm is not pinned, and glibc 2.39's
+ * cosf / sinf differ from the correctly rounded value on ~1.3% of inputs. */
+static float cr_cosf(float x) { return (float)cos((double)x); }
+static float cr_sinf(float x) { return (float)sin((double)x); }
+
 void orc_rotation_xyz(float a, float b, float c, float* T) {
-  const float ca = cosf(a), sa = sinf(a);
-  const float cb = cosf(b), sb = sinf(b);
-  const float cc = cosf(c), sc = sinf(c);
+  const float ca = cr_cosf(a), sa = cr_sinf(a);
+  const float cb = cr_cosf(b), sb = cr_sinf(b);
+  const float cc = cr_cosf(c), sc = cr_sinf(c);
   float X[3][3] = {{1, 0, 0}, {0, ca, -sa}, {0, sa, ca}};
   float Y[3][3] = {{cb, 0, sb}, {0, 1, 0}, {-sb, 0, cb}};
   float Z[3][3] = {{cc, sc, 0}, {-sc, cc, 0}, {0, 0, 1}};

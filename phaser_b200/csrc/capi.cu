@@ -29,6 +29,15 @@ static thread_local std::string g_create_error;
     }                                                                              \
   } while (0)
 
+#define CKC(c, expr)                                                               \
+  do {                                                                             \
+    cudaError_t _e = (expr);                                                       \
+    if (_e != cudaSuccess) {                                                       \
+      (c)->err = std::string(#expr) + ": " + cudaGetErrorString(_e);               \
+      return PHGPU_ERR_CUDA;                                                       \
+    }                                                                              \
+  } while (0)
+
 #define CKV(expr)                                                                  \
   do {                                                                             \
     int _r = (expr);                                                               \
@@ -164,9 +173,12 @@ int phgpu_pose_from_bin(uint32_t bin, uint32_t bw_out, double* zyz, double* quat
 
 static void xyz_to_transform(const double* e, float* T12) {
   {
-    // RotateAroundXYZ: Rx(a) * Ry(b) * Rz(c) in float (rotation-utils.cc:17-24,109-143)
+    // RotateAroundXYZ: Rx(a) * Ry(b) * Rz(c) in float (rotation-utils.cc:17-24,109-143);
+    // float cos / sin correctly rounded (double evaluation, one rounding), as
+    // the device pose kernel (k_pose.cu) computes them
     const float a = (float)e[0], bb = (float)e[1], c = (float)e[2];
-    const float ca = cosf(a), sa = sinf(a), cb = cosf(bb), sb = sinf(bb), cc = cosf(c), sc = sinf(c);
+    const float ca = (float)cos((double)a), sa = (float)sin((double)a), cb = (float)cos((double)bb),
+                sb = (float)sin((double)bb), cc = (float)cos((double)c), sc = (float)sin((double)c);
     const float X[3][3] = {{1, 0, 0}, {0, ca, -sa}, {0, sa, ca}};
     const float Y[3][3] = {{cb, 0, sb}, {0, 1, 0}, {-sb, 0, cb}};
     const float Z[3][3] = {{cc, sc, 0}, {-sc, cc, 0}, {0, 0, 1}};
@@ -374,6 +386,8 @@ int phgpu_profile_stage_count(void) { return PS_COUNT; }
 
 unsigned long long phgpu_launch_count(void) { return g_launch_count.load(); }
 
+unsigned long long phgpu_pose_reruns(const phgpu_ctx* ctx) { return ctx ? ctx->pose_reruns : 0ull; }
+
 // ------------------------------------------------------------------ context
 
 int phgpu_params_default(phgpu_params* p) {
@@ -398,6 +412,7 @@ int phgpu_params_default(phgpu_params* p) {
   p->trans_peak_neighbors = 0;
   p->spherical_low_pass_lower = 0;
   p->spherical_low_pass_upper = 100000;
+  p->precision = PHGPU_PRECISION_FP32;
   return PHGPU_OK;
 }
 
@@ -462,10 +477,10 @@ int phgpu_ctx_create(const phgpu_params* prm, phgpu_ctx** out) {
   if (bw < 2 || bw > 512 || N < 1 || N > 1024 || (uint64_t)N + 2ull * prm->spatial_zero_padding > 1024 ||
       prm->n_channels < 1 || prm->n_channels > 4 || prm->fusion_levels < 1 ||
       prm->fusion_levels > (uint32_t)kMaxLevels || prm->spherical_fusion > PHGPU_FUSION_LOW_PASS ||
-      prm->spatial_fusion > PHGPU_FUSION_LOW_PASS) {
+      prm->spatial_fusion > PHGPU_FUSION_LOW_PASS || prm->precision > PHGPU_PRECISION_BF16X3) {
     g_create_error =
         "unsupported configuration (2 <= bandwidth <= 512, 1 <= n_voxels + 2 spatial zero padding <= 1024, "
-        "1..4 channels, 1..8 fusion levels, fusion mode 0..2)";
+        "1..4 channels, 1..8 fusion levels, fusion mode 0..2, precision 0..2)";
     return PHGPU_ERR_INVALID;
   }
   phgpu_ctx* ctx = new phgpu_ctx();
@@ -596,6 +611,19 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
     CKV(dalloc(ctx, &ctx->d_wig_tab, sizeof(double) * wt.size()));
     CK(cudaMemcpy(ctx->d_wig_tab, wt.data(), sizeof(double) * wt.size(), cudaMemcpyHostToDevice));
   }
+  if (prm->precision != PHGPU_PRECISION_FP32) {
+    // tensor-core synthesis: the Wigner-d table, generated once in FP64
+    if (!so3_tc_supported(bw_out, 1, (int)prm->precision)) {
+      ctx->err = "the tensor-core SO(3) synthesis supports bandwidth + spherical zero padding <= 256";
+      return PHGPU_ERR_INVALID;
+    }
+    std::vector<size_t> off;
+    const size_t nf = so3_table_layout(bw, bw_out, &off);
+    CKV(dalloc(ctx, &ctx->d_class_off, sizeof(size_t) * off.size()));
+    CK(cudaMemcpy(ctx->d_class_off, off.data(), sizeof(size_t) * off.size(), cudaMemcpyHostToDevice));
+    CKV(dalloc(ctx, &ctx->d_wtable, sizeof(float) * nf));
+    CK(launch_so3_table(bw, bw_out, ctx->d_beta_tab, ctx->d_wig_tab, ctx->d_class_off, ctx->d_wtable, ctx->s0));
+  }
   const size_t nv = (size_t)N * N * N;
   const size_t H = (size_t)N * N * spatial_h2p(N);
   for (int s = 0; s < 2; ++s) {
@@ -621,6 +649,11 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   CKV(dalloc(ctx, &ctx->d_argmax, sizeof(unsigned long long) * 3));
   CK(cudaMemset(ctx->d_argmax, 0, sizeof(unsigned long long) * 3));
   CK(cudaMallocHost((void**)&ctx->h_argmax, sizeof(unsigned long long) * 3));
+  CKV(dalloc(ctx, &ctx->d_T, sizeof(float) * 16));
+  CK(cudaMallocHost((void**)&ctx->h_T, sizeof(float) * 16));
+  CKV(dalloc(ctx, &ctx->d_np, sizeof(uint32_t) * 2));
+  CK(cudaMemset(ctx->d_np, 0, sizeof(uint32_t) * 2));
+  CK(cudaMallocHost((void**)&ctx->h_np, sizeof(uint32_t) * 2));
   ctx->h_argmax[0] = ctx->h_argmax[1] = ctx->h_argmax[2] = 0ull;
   CKV(ensure_cloud_capacity(ctx, prm->max_points ? prm->max_points : (1u << 18)));
   CK(cudaStreamSynchronize(ctx->s0));
@@ -639,6 +672,8 @@ int phgpu_ctx_destroy(phgpu_ctx* ctx) {
   for (int i = 0; i < 2; ++i)
     if (ctx->d_tw_pad[i]) cudaFree(ctx->d_tw_pad[i]);
   if (ctx->h_argmax) cudaFreeHost(ctx->h_argmax);
+  if (ctx->h_T) cudaFreeHost(ctx->h_T);
+  if (ctx->h_np) cudaFreeHost(ctx->h_np);
   for (const ProfRec& r : ctx->prof_recs) {
     cudaEventDestroy(r.a);
     cudaEventDestroy(r.b);
@@ -672,6 +707,10 @@ int phgpu_upload_cloud(phgpu_ctx* ctx, const phgpu_cloud* c, int side, cudaStrea
   ctx->np[side] = c->n_points;
   ctx->has_refl[side] = c->reflectivity != nullptr;
   ctx->has_amb[side] = c->ambient != nullptr;
+  if (ctx->dev_counts) {
+    ctx->h_np[side] = c->n_points;
+    CK(cudaMemcpyAsync(ctx->d_np + side, ctx->h_np + side, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  }
   return PHGPU_OK;
 }
 
@@ -680,7 +719,8 @@ static int run_sample(phgpu_ctx* ctx, int side, cudaStream_t st) {
   a.xyzi = ctx->d_xyzi[side];
   a.refl = ctx->has_refl[side] ? ctx->d_refl[side] : nullptr;
   a.amb = ctx->has_amb[side] ? ctx->d_amb[side] : nullptr;
-  a.n_points = (int)ctx->np[side];
+  a.n_points = ctx->dev_counts ? (int)ctx->cap_points : (int)ctx->np[side];
+  a.n_dev = ctx->dev_counts ? ctx->d_np + side : nullptr;
   a.max_points = (int)ctx->cap_points;
   a.grid = ctx->d_grid;
   a.n_queries = 4 * ctx->bw * ctx->bw;
@@ -725,8 +765,35 @@ int phgpu_get_samples(phgpu_ctx* ctx, int side, double* values, int32_t* nn_inde
   return PHGPU_OK;
 }
 
+// SO(3) launch arguments of this context alone (a batch of one request).
+So3Args so3_args(phgpu_ctx* ctx) {
+  So3Args o;
+  memset(&o, 0, sizeof(o));
+  o.bw_in = ctx->bw;
+  o.bw_out = ctx->bw_out;
+  o.beta_tab = ctx->d_beta_tab;
+  o.wig_tab = ctx->d_wig_tab;
+  o.plan = &ctx->plan_so3;
+  o.batch.count = 1;
+  o.batch.fused[0] = ctx->d_fused;
+  o.batch.out[0].S = ctx->d_S;
+  o.batch.out[0].argmax = ctx->d_argmax;
+  o.batch.out[0].volume = ctx->d_rotvol;
+  return o;
+}
+
+So3Table so3_table(phgpu_ctx* ctx) {
+  So3Table t;
+  t.table = ctx->d_wtable;
+  t.class_off = ctx->d_class_off;
+  t.precision = (int)ctx->prm.precision;
+  return t;
+}
+
 // Spherical correlation of the sample grids currently in d_samples.
-int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st) {
+// SHT of both sides' sample grids and their fusion (up to the fused spectra);
+// resets the rotation argmax.
+int phgpu_run_sph_front(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st) {
   const int bw = ctx->bw;
   const size_t nq = (size_t)4 * bw * bw;
   {
@@ -758,26 +825,50 @@ int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStre
     CK(launch_fuse_s2(f, st));
   }
   CK(cudaMemsetAsync(ctx->d_argmax, 0, sizeof(unsigned long long), st));
-  So3Args o;
-  o.bw_in = bw;
-  o.bw_out = ctx->bw_out;
-  o.fused = ctx->d_fused;
-  o.beta_tab = ctx->d_beta_tab;
-  o.wig_tab = ctx->d_wig_tab;
-  o.S = ctx->d_S;
-  o.plan = &ctx->plan_so3;
-  o.argmax = ctx->d_argmax;
-  o.volume = ctx->d_rotvol;
+  return PHGPU_OK;
+}
+
+// SO(3) synthesis, angle transforms and argmax of the fused spectra of
+// ctx[0..k) (one shape) on stream st: one batched launch per stage.  The
+// tensor-core synthesis reads `table` (null: the FP32 synthesis).
+int phgpu_run_so3_batch(phgpu_ctx* const* ctx, int k, const So3Table* table, cudaStream_t st) {
+  if (k < 1 || k > kMaxWave) return PHGPU_ERR_INVALID;
+  So3Args o = so3_args(ctx[0]);
+  o.batch.count = k;
+  for (int i = 0; i < k; ++i) {
+    o.batch.fused[i] = ctx[i]->d_fused;
+    o.batch.out[i].S = ctx[i]->d_S;
+    o.batch.out[i].argmax = ctx[i]->d_argmax;
+    o.batch.out[i].volume = ctx[i]->d_rotvol;
+  }
+  phgpu_ctx* c0 = ctx[0];
   {
-    ProfScope ps(ctx, st, PS_SO3_SYNTH);
-    CK(launch_so3_synth(o, st));
+    ProfScope ps(c0, st, PS_SO3_SYNTH);
+    if (table) {
+      if (launch_so3_synth_tc(o, *table, c0->d_argmax + 2, st) != cudaSuccess) {
+        c0->err = "tensor-core SO(3) synthesis launch failed";
+        return PHGPU_ERR_CUDA;
+      }
+    } else {
+      CKC(c0, launch_so3_synth(o, st));
+    }
   }
   {
-    ProfScope ps(ctx, st, PS_SO3_FFT);
-    CK(launch_so3_fft(o, st));
+    ProfScope ps(c0, st, PS_SO3_FFT);
+    CKC(c0, launch_so3_fft(o, st));
   }
+  for (int i = 0; i < k; ++i) ctx[i]->have_rot = true;
+  return PHGPU_OK;
+}
+
+// Spherical correlation of the sample grids currently in d_samples; the bin
+// and status are read back to h_argmax[0], [2].
+int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st) {
+  CKV(phgpu_run_sph_front(ctx, n_data, n_total, laplace, st));
+  So3Table t = so3_table(ctx);
+  CKV(phgpu_run_so3_batch(&ctx, 1, ctx->prm.precision != PHGPU_PRECISION_FP32 ? &t : nullptr, st));
   CK(cudaMemcpyAsync(ctx->h_argmax, ctx->d_argmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-  ctx->have_rot = true;
+  CK(cudaMemcpyAsync(ctx->h_argmax + 2, ctx->d_argmax + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   return PHGPU_OK;
 }
 
@@ -824,6 +915,10 @@ int phgpu_sph_result(phgpu_ctx* ctx, uint32_t* bin, float* peak, double* corr_ou
   }
   cudaSetDevice(ctx->prm.device);
   CK(cudaStreamSynchronize(ctx->s0));
+  if (ctx->h_argmax[2] & 2ull) {
+    ctx->err = "a wait in the tensor-core SO(3) synthesis timed out";
+    return PHGPU_ERR_CUDA;
+  }
   const unsigned long long k = ctx->h_argmax[0];
   if (bin) *bin = unpack_index(k);
   if (peak) *peak = float_from_order_bits((uint32_t)(k >> 32));
@@ -843,7 +938,8 @@ int phgpu_sph_result(phgpu_ctx* ctx, uint32_t* bin, float* peak, double* corr_ou
 // Spatial channel count with data: {intensity, range} always, + reflectivity, + ambient.
 static int sp_channels(int has_refl, int has_amb) { return has_amb ? 4 : (has_refl ? 3 : 2); }
 
-int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, cudaStream_t st) {
+int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, cudaStream_t st,
+                       const float* T_dev) {
   const size_t nv = (size_t)ctx->N * ctx->N * ctx->N;
   if (ctx->clean_planes[side] < n_data + 1) {
     CK(cudaMemsetAsync(ctx->d_grids[side], 0, sizeof(float) * (n_data + 1) * nv, st));
@@ -854,7 +950,8 @@ int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, c
   v.xyzi = ctx->d_xyzi[side];
   v.refl = ctx->has_refl[side] ? ctx->d_refl[side] : nullptr;
   v.amb = ctx->has_amb[side] ? ctx->d_amb[side] : nullptr;
-  v.n_points = (int)ctx->np[side];
+  v.n_points = ctx->dev_counts ? (int)ctx->cap_points : (int)ctx->np[side];
+  v.n_dev = ctx->dev_counts ? ctx->d_np + side : nullptr;
   v.N = ctx->N;
   v.edges = ctx->d_edges;
   v.has_T = T12 ? 1 : 0;
@@ -863,6 +960,7 @@ int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, c
   v.grids = ctx->d_grids[side];
   v.lin_out = ctx->d_lin[side];
   v.rowlive = ctx->d_rowlive[side];
+  v.T_dev = T_dev;
   {
     ProfScope ps(ctx, st, PS_VOXELIZE);
     CK(launch_voxelize(v, st));
@@ -879,8 +977,9 @@ int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, c
 static int clear_voxelized(phgpu_ctx* ctx, int side, cudaStream_t st) {
   const int planes = ctx->vox_ch[side] + 1;
   const size_t nv = (size_t)ctx->N * ctx->N * ctx->N;
-  CK(launch_clear_voxels(ctx->d_lin[side], (int)ctx->np[side], ctx->d_grids[side], nv, planes,
-                         ctx->d_rowlive[side], ctx->N, st));
+  CK(launch_clear_voxels(ctx->d_lin[side], ctx->dev_counts ? (int)ctx->cap_points : (int)ctx->np[side],
+                         ctx->d_grids[side], nv, planes, ctx->d_rowlive[side], ctx->N, st,
+                         ctx->dev_counts ? ctx->d_np + side : nullptr));
   ctx->clean_planes[side] = planes;
   ctx->grids_live[side] = false;
   return PHGPU_OK;
@@ -1073,7 +1172,7 @@ int phgpu_spatial_result(phgpu_ctx* ctx, uint32_t* voxel, float* peak, double* c
   }
   cudaSetDevice(ctx->prm.device);
   CK(cudaStreamSynchronize(ctx->s0));
-  if (ctx->h_argmax[2]) {
+  if (ctx->h_argmax[2] & 1ull) {
     ctx->err = "a bulk-copy wait in the translation kernels timed out";
     return PHGPU_ERR_CUDA;
   }
@@ -1095,41 +1194,75 @@ int phgpu_spatial_result(phgpu_ctx* ctx, uint32_t* voxel, float* peak, double* c
 
 // ------------------------------------------------------------------ pipeline
 
-int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_cloud* source,
-                        phgpu_pose* out) {
-  if (!ctx || !target || !source || !out) return PHGPU_ERR_INVALID;
-  cudaSetDevice(ctx->prm.device);
+PairPlan pair_plan(const phgpu_ctx* ctx, bool t_refl, bool t_amb, bool s_refl, bool s_amb) {
+  PairPlan pp;
+  pp.laplace_s2 = ctx->prm.spherical_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
+  pp.laplace_sp = ctx->prm.spatial_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
+  pp.nd_s2 = std::max(t_amb ? 4 : (t_refl ? 3 : 2), s_amb ? 4 : (s_refl ? 3 : 2));
+  pp.nd_sp = sp_channels(t_refl || s_refl, t_amb || s_amb);
+  return pp;
+}
+
+int phgpu_pair_front(phgpu_ctx* ctx, const PairPlan& pp) {
   cudaStream_t s0 = ctx->s0, s1 = ctx->s1;
-  {
-    ProfScope ps(ctx, s0, PS_UPLOAD);
-    CKV(phgpu_upload_cloud(ctx, target, 0, s0));
-    CKV(phgpu_upload_cloud(ctx, source, 1, s0));
-  }
-  const int laplace_s2 = ctx->prm.spherical_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
-  const int laplace_sp = ctx->prm.spatial_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
-  const int nd_s2 = std::max(s2_channels(target), s2_channels(source));
-  const int nd_sp = sp_channels(target->reflectivity || source->reflectivity,
-                                target->ambient || source->ambient);
   // target translation side overlaps the rotation stage
   CK(cudaEventRecord(ctx->ev_a, s0));
   CK(cudaStreamWaitEvent(s1, ctx->ev_a, 0));
-  CKV(phgpu_run_voxelize(ctx, 0, nullptr, nd_sp, s1));
-  SpatialArgs sa = spatial_args(ctx, nd_sp, (int)ctx->prm.n_channels, laplace_sp, 0);
+  CKV(phgpu_run_voxelize(ctx, 0, nullptr, pp.nd_sp, s1));
+  const SpatialArgs sa = spatial_args(ctx, pp.nd_sp, (int)ctx->prm.n_channels, pp.laplace_sp, 0);
   {
     ProfScope ps(ctx, s1, PS_SPATIAL_FWD);
     CK(launch_spatial_forward(sa, 0, s1));
   }
   CKV(clear_voxelized(ctx, 0, s1));
   CK(cudaEventRecord(ctx->ev_b, s1));
-  // rotation
+  // rotation up to the fused spectra
   CKV(run_sample(ctx, 0, s0));
   CKV(run_sample(ctx, 1, s0));
-  CKV(phgpu_run_sph(ctx, laplace_s2 ? nd_s2 : 1, (int)ctx->prm.n_channels, laplace_s2, s0));
-  CK(cudaStreamSynchronize(s0));
+  CKV(phgpu_run_sph_front(ctx, pp.laplace_s2 ? pp.nd_s2 : 1, (int)ctx->prm.n_channels, pp.laplace_s2, s0));
+  return PHGPU_OK;
+}
+
+int phgpu_pair_back(phgpu_ctx* ctx, const PairPlan& pp, const float* T, const float* T_dev) {
+  cudaStream_t s0 = ctx->s0;
+  const SpatialArgs sa = spatial_args(ctx, pp.nd_sp, (int)ctx->prm.n_channels, pp.laplace_sp, 0);
+  CKV(phgpu_run_voxelize(ctx, 1, T, pp.nd_sp, s0, T_dev));
+  {
+    ProfScope ps(ctx, s0, PS_SPATIAL_FWD);
+    CK(launch_spatial_forward(sa, 1, s0));
+  }
+  CKV(clear_voxelized(ctx, 1, s0));
+  CK(cudaStreamWaitEvent(s0, ctx->ev_b, 0));
+  if (ctx->pad) {
+    CKV(run_spatial_padded(ctx, sa, s0));
+  } else {
+    CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), s0));
+    {
+      ProfScope ps(ctx, s0, PS_FUSE_Z);
+      CK(launch_spatial_fuse_z(sa, s0));
+    }
+    {
+      ProfScope ps(ctx, s0, PS_SPATIAL_INV);
+      CK(launch_spatial_inverse(sa, s0));
+    }
+  }
+  // one read-back: rotation key, translation key, status (and the device transform)
+  CK(cudaMemcpyAsync(ctx->h_argmax, ctx->d_argmax, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s0));
+  if (T_dev) CK(cudaMemcpyAsync(ctx->h_T, T_dev, 12 * sizeof(float), cudaMemcpyDeviceToHost, s0));
+  ctx->have_trans = true;
+  return PHGPU_OK;
+}
+
+int phgpu_pair_finish(phgpu_ctx* ctx, const PairPlan& pp, bool device_pose, phgpu_pose* out) {
+  cudaStream_t s0 = ctx->s0;
+  if (ctx->h_argmax[2] & 2ull) {
+    ctx->err = "a wait in the tensor-core SO(3) synthesis timed out";
+    return PHGPU_ERR_CUDA;
+  }
+  float T[12];
   const unsigned long long rk = ctx->h_argmax[0];
   out->rot_bin = unpack_index(rk);
   out->rot_peak = float_from_order_bits((uint32_t)(rk >> 32));
-  float T[12];
   phgpu_pose_from_bin(out->rot_bin, (uint32_t)ctx->bw_out, out->zyz, out->quat, out->xyz, T);
   out->rot_omega[0] = out->rot_omega[1] = out->rot_omega[2] = 0.0;
   out->rot_omega[3] = 1.0;
@@ -1150,32 +1283,15 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
     }
     xyz_to_transform(out->xyz, T);
   }
-  // translation of the rotated source
-  CKV(phgpu_run_voxelize(ctx, 1, T, nd_sp, s0));
-  {
-    ProfScope ps(ctx, s0, PS_SPATIAL_FWD);
-    CK(launch_spatial_forward(sa, 1, s0));
+  if (!device_pose || memcmp(T, ctx->h_T, sizeof(T)) != 0) {
+    // translation with the host's transform: the host-pose cases, or a device
+    // transform that differs in some bit from the host restatement (the two
+    // sides' double trig functions may round differently)
+    if (device_pose) ++ctx->pose_reruns;
+    CKV(phgpu_pair_back(ctx, pp, T, nullptr));
+    CK(cudaStreamSynchronize(s0));
   }
-  CKV(clear_voxelized(ctx, 1, s0));
-  CK(cudaStreamWaitEvent(s0, ctx->ev_b, 0));
-  if (ctx->pad) {
-    CKV(run_spatial_padded(ctx, sa, s0));
-  } else {
-    CK(cudaMemsetAsync(ctx->d_argmax + 1, 0, sizeof(unsigned long long), s0));
-    {
-      ProfScope ps(ctx, s0, PS_FUSE_Z);
-      CK(launch_spatial_fuse_z(sa, s0));
-    }
-    {
-      ProfScope ps(ctx, s0, PS_SPATIAL_INV);
-      CK(launch_spatial_inverse(sa, s0));
-    }
-  }
-  CK(cudaMemcpyAsync(ctx->h_argmax + 1, ctx->d_argmax + 1, 2 * sizeof(unsigned long long),
-                     cudaMemcpyDeviceToHost, s0));
-  ctx->have_trans = true;
-  CK(cudaStreamSynchronize(s0));
-  if (ctx->h_argmax[2]) {
+  if (ctx->h_argmax[2] & 1ull) {
     ctx->err = "a bulk-copy wait in the translation kernels timed out";
     return PHGPU_ERR_CUDA;
   }
@@ -1204,4 +1320,42 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
     }
   }
   return PHGPU_OK;
+}
+
+bool pair_device_pose(const phgpu_ctx* ctx) { return ctx->prm.rot_peak_neighbors == 0 && ctx->pad == 0; }
+
+int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_cloud* source,
+                        phgpu_pose* out) {
+  if (!ctx || !target || !source || !out) return PHGPU_ERR_INVALID;
+  cudaSetDevice(ctx->prm.device);
+  cudaStream_t s0 = ctx->s0;
+  {
+    ProfScope ps(ctx, s0, PS_UPLOAD);
+    CKV(phgpu_upload_cloud(ctx, target, 0, s0));
+    CKV(phgpu_upload_cloud(ctx, source, 1, s0));
+  }
+  const PairPlan pp = pair_plan(ctx, target->reflectivity, target->ambient, source->reflectivity, source->ambient);
+  CKV(phgpu_pair_front(ctx, pp));
+  So3Table t = so3_table(ctx);
+  CKV(phgpu_run_so3_batch(&ctx, 1, ctx->prm.precision != PHGPU_PRECISION_FP32 ? &t : nullptr, s0));
+  // The rotation pose and the source's transform are computed on the device
+  // and the translation follows without a host round trip.  A peak
+  // neighbourhood fit (host, FP64) or the padded correlation (whose Laplace
+  // mode carries state from one call to the next, so it cannot be redone)
+  // take the transform from the host instead.
+  const bool device_pose = pair_device_pose(ctx);
+  if (device_pose) {
+    PoseBatch pb;
+    memset(&pb, 0, sizeof(pb));
+    pb.count = 1;
+    pb.bw_out = (uint32_t)ctx->bw_out;
+    pb.argmax[0] = ctx->d_argmax;
+    pb.T[0] = ctx->d_T;
+    CK(launch_pose(pb, s0));
+    CKV(phgpu_pair_back(ctx, pp, nullptr, ctx->d_T));
+  } else {
+    CK(cudaMemcpyAsync(ctx->h_argmax, ctx->d_argmax, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s0));
+  }
+  CK(cudaStreamSynchronize(s0));
+  return phgpu_pair_finish(ctx, pp, device_pose, out);
 }

@@ -64,6 +64,8 @@ struct phgpu_ctx {
   float2* d_S = nullptr;
   double* d_beta_tab = nullptr;  // [3][2 bw_out] for the Wigner seeds
   double* d_wig_tab = nullptr;   // Wigner recurrence tables (so3_wigner_table)
+  float* d_wtable = nullptr;     // Wigner-d values of the tensor-core synthesis (precision != FP32)
+  size_t* d_class_off = nullptr; // per-class offsets into d_wtable
   float* d_rotvol = nullptr;
   // translation
   float* d_grids[2] = {nullptr, nullptr};  // [(C+1)][N^3]
@@ -89,6 +91,14 @@ struct phgpu_ctx {
   // results
   unsigned long long* d_argmax = nullptr;  // [rot, trans]
   unsigned long long* h_argmax = nullptr;  // pinned
+  float* d_T = nullptr;                    // [12] source transform of the device pose kernel
+  float* h_T = nullptr;                    // pinned copy of d_T
+  unsigned long long pose_reruns = 0;      // translations redone with the host transform
+  // point counts read by the kernels from device memory (the server's waves,
+  // whose captured graphs take any count up to the capacity)
+  bool dev_counts = false;
+  uint32_t* d_np = nullptr;  // [2]
+  uint32_t* h_np = nullptr;  // [2] pinned
   bool sampled[2] = {false, false};
   bool voxelized[2] = {false, false};
   bool have_rot = false, have_trans = false;
@@ -116,8 +126,28 @@ struct ProfScope {
 int phgpu_ctx_init(phgpu_ctx* ctx);
 int phgpu_upload_cloud(phgpu_ctx* ctx, const phgpu_cloud* c, int side, cudaStream_t st);
 int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st);
-int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, cudaStream_t st);
+int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, cudaStream_t st,
+                       const float* T_dev = nullptr);
 int phgpu_run_spatial(phgpu_ctx* ctx, int n_data, int n_total, int laplace, int means, cudaStream_t st);
+phgpu::So3Args so3_args(phgpu_ctx* ctx);
+int phgpu_run_sph_front(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st);
+int phgpu_run_so3_batch(phgpu_ctx* const* ctx, int k, const phgpu::So3Table* table, cudaStream_t st);
+
+// One registration split for the server's waves: the front half on the
+// context's streams (target translation side on s1, sampling + SHT + fusion
+// on s0), the SO(3) stage (phgpu_run_so3_batch, batched across a wave), the
+// pose kernel, the back half on s0 (source translation with the device or a
+// host transform, one read-back into h_argmax / h_T) and the host finish
+// (pose from the bin, transform check, peak neighbourhoods).
+struct PairPlan {
+  int nd_s2, nd_sp, laplace_s2, laplace_sp;
+};
+PairPlan pair_plan(const phgpu_ctx* ctx, bool t_refl, bool t_amb, bool s_refl, bool s_amb);
+int phgpu_pair_front(phgpu_ctx* ctx, const PairPlan& pp);
+int phgpu_pair_back(phgpu_ctx* ctx, const PairPlan& pp, const float* T, const float* T_dev);
+int phgpu_pair_finish(phgpu_ctx* ctx, const PairPlan& pp, bool device_pose, phgpu_pose* out);
+bool pair_device_pose(const phgpu_ctx* ctx);
+phgpu::So3Table so3_table(phgpu_ctx* ctx);
 
 namespace phgpu {
 bool make_fft_plan(int n, FftPlan* p, float2** d_tw, std::string* err);

@@ -45,9 +45,10 @@ __device__ __forceinline__ float atan2_f(float y, float x) { return (float)atan2
 // Projection of every point, its bin and the per-bin and per-row counts.
 __global__ void k_project(const float4* __restrict__ xyzi, int P, float4* __restrict__ proj,
                           double* __restrict__ range, uint32_t* __restrict__ key, int n2b,
-                          uint32_t* __restrict__ bin_count, uint32_t* __restrict__ row_count) {
+                          uint32_t* __restrict__ bin_count, uint32_t* __restrict__ row_count,
+                          const uint32_t* __restrict__ P_dev) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P) return;
+  if (i >= (P_dev ? (int)*P_dev : P)) return;
   const float4 p = xyzi[i];
   const float sxy = __fadd_rn(__fmul_rn(p.x, p.x), __fmul_rn(p.y, p.y));
   const double dist_xy = (double)sqrtf(sxy);
@@ -165,9 +166,9 @@ __global__ void __launch_bounds__(kBinScanThreads) k_bin_scan(int n2b, const uin
 // Counting-sort scatter: sorted[k] = {x, y, z, point index (bits)}.
 __global__ void k_bin_scatter(int P, const float4* __restrict__ proj, const uint32_t* __restrict__ key,
                               const uint32_t* __restrict__ bin_start, uint32_t* __restrict__ cursor,
-                              float4* __restrict__ sorted) {
+                              float4* __restrict__ sorted, const uint32_t* __restrict__ P_dev) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P) return;
+  if (i >= (P_dev ? (int)*P_dev : P)) return;
   const uint32_t k = key[i];
   if (k == 0xffffffffu) return;
   const unsigned act = __activemask();
@@ -416,14 +417,14 @@ cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st) {
   const int P = a.n_points;
   int launched = 0;
   if (P > 0) {
-    k_project<<<(P + 255) / 256, 256, 0, st>>>(a.xyzi, P, proj, range, key, n2b, bin_count, row_count);
+    k_project<<<(P + 255) / 256, 256, 0, st>>>(a.xyzi, P, proj, range, key, n2b, bin_count, row_count, a.n_dev);
     ++launched;
   }
   k_bin_scan<<<n2b, kBinScanThreads, 0, st>>>(n2b, bin_count, row_count, bin_start, row_nxt, row_prv, sin_tab,
                                                hav_tab);
   ++launched;
   if (P > 0) {
-    k_bin_scatter<<<(P + 255) / 256, 256, 0, st>>>(P, proj, key, bin_start, cursor, sorted);
+    k_bin_scatter<<<(P + 255) / 256, 256, 0, st>>>(P, proj, key, bin_start, cursor, sorted, a.n_dev);
     ++launched;
   }
   const size_t q_threads = (size_t)a.n_queries * kGroup;

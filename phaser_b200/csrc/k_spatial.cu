@@ -45,12 +45,21 @@ __device__ __forceinline__ int histc_bin(float x, const float* __restrict__ E, i
 
 __global__ void k_voxelize(VoxelArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n_points) return;
+  const int np = a.n_dev ? (int)*a.n_dev : a.n_points;
+  if (i >= np) return;
   const float4 p = a.xyzi[i];
   float x = p.x, y = p.y, z = p.z;
-  if (a.has_T) {
+  if (a.has_T || a.T_dev) {
     // PCL 1.8 transformPointCloud order ((T0 x + T1 y) + T2 z) + T3
-    const float* T = a.T;
+    float Tl[12];
+    if (a.T_dev) {
+#pragma unroll
+      for (int k = 0; k < 12; ++k) Tl[k] = __ldg(&a.T_dev[k]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 12; ++k) Tl[k] = a.T[k];
+    }
+    const float* T = Tl;
     const float nx = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(T[0], x), __fmul_rn(T[1], y)), __fmul_rn(T[2], z)), T[3]);
     const float ny = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(T[4], x), __fmul_rn(T[5], y)), __fmul_rn(T[6], z)), T[7]);
     const float nz = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(T[8], x), __fmul_rn(T[9], y)), __fmul_rn(T[10], z)), T[11]);
@@ -87,9 +96,9 @@ cudaError_t launch_voxelize(const VoxelArgs& a, cudaStream_t st) {
 }
 
 __global__ void k_clear_voxels(const uint32_t* __restrict__ lin, int n_points, float* __restrict__ grids, size_t nv,
-                               int n_planes, uint8_t* __restrict__ rowlive, int N) {
+                               int n_planes, uint8_t* __restrict__ rowlive, int N, const uint32_t* __restrict__ n_dev) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_points) return;
+  if (i >= (n_dev ? (int)*n_dev : n_points)) return;
   const uint32_t l = lin[i];
   if (l == 0xffffffffu) return;
   for (int p = 0; p < n_planes; ++p) grids[(size_t)p * nv + l] = 0.0f;
@@ -97,9 +106,9 @@ __global__ void k_clear_voxels(const uint32_t* __restrict__ lin, int n_points, f
 }
 
 cudaError_t launch_clear_voxels(const uint32_t* lin, int n_points, float* grids, size_t nv, int n_planes,
-                                uint8_t* rowlive, int N, cudaStream_t st) {
+                                uint8_t* rowlive, int N, cudaStream_t st, const uint32_t* n_dev) {
   if (n_points > 0) {
-    k_clear_voxels<<<(n_points + 255) / 256, 256, 0, st>>>(lin, n_points, grids, nv, n_planes, rowlive, N);
+    k_clear_voxels<<<(n_points + 255) / 256, 256, 0, st>>>(lin, n_points, grids, nv, n_planes, rowlive, N, n_dev);
     count_launches(1);
   }
   return cudaGetLastError();

@@ -32,6 +32,7 @@ struct SampleArgs {
   float* out;           // [n_out_ch][n_queries]
   int32_t* nn_idx;      // [n_queries] or null
   void* scratch;        // sampler_scratch_bytes(max_points, >= n_queries)
+  const uint32_t* n_dev = nullptr;  // when set: the point count is read from device memory (n_points = capacity)
 };
 size_t sampler_scratch_bytes(int max_points, int max_queries);
 cudaError_t launch_sample(const SampleArgs& a, cudaStream_t st);
@@ -71,22 +72,61 @@ struct FuseS2Args {
 cudaError_t launch_fuse_s2(const FuseS2Args& a, cudaStream_t st);
 
 // ------------------------------------------------------------ SO(3)
+// Requests of one shape processed by one launch (a wave of the server).
+constexpr int kMaxWave = 32;
+struct So3Out {
+  float2* S;                   // [2 bw_out (a)][bw_out (b)][2 bw_out (beta)]
+  unsigned long long* argmax;  // packed (value^2, index)
+  float* volume;               // optional (2 bw_out)^3 |z|^2, [beta][alpha][gamma]
+};
+struct So3Batch {
+  int count;                      // requests (1..kMaxWave)
+  const float2* fused[kMaxWave];  // [2][bw_in][2 bw_in - 1] per request
+  So3Out out[kMaxWave];
+};
 struct So3Args {
   int bw_in;              // degree limit
   int bw_out;             // output grid 2*bw_out
-  const float2* fused;    // [2][bw_in][2 bw_in - 1]
   const double* beta_tab; // [3][2 bw_out]: cos(beta_k), log cos(beta_k / 2), log sin(beta_k / 2)
   const double* wig_tab;  // so3_wigner_table(bw_in): recurrence square roots, per-degree factors
-  float2* S;              // [2 bw_out (beta)][2 bw_out (a)][bw_out (b)]
   const FftPlan* plan;    // length 2 bw_out
-  unsigned long long* argmax;  // packed (value^2, index)
-  float* volume;          // optional (2 bw_out)^3 |z|^2, [beta][alpha][gamma]
+  So3Batch batch;
 };
-cudaError_t launch_so3_synth(const So3Args& a, cudaStream_t st);  // coefficient product + Wigner synthesis
+cudaError_t launch_so3_synth(const So3Args& a, cudaStream_t st);  // coefficient product + FP32 Wigner synthesis
 cudaError_t launch_so3_fft(const So3Args& a, cudaStream_t st);    // alpha FFT + gamma C2R + argmax
 cudaError_t so3_init_attributes();  // once per device
 void so3_beta_table(int bw_out, double* host_tab);  // fills the [3][2 bw_out] beta_tab on the host
 void so3_wigner_table(int bw_in, std::vector<double>& host_tab);  // recurrence tables of the synthesis
+
+// Tensor-core synthesis (k_so3_tc.cu) from a Wigner-d table generated once in
+// FP64 and stored as FP32: per order class (p, q) a [nl_pad / 4][2 bw_out][4]
+// block (nl_pad = bw_in - q rounded up to 8), i.e. 16-byte groups of four
+// degrees for every beta, the operand layout of the matrix instructions.
+enum So3Precision { kSo3Fp32 = 0, kSo3Tf32x3 = 1, kSo3Bf16x3 = 2 };
+struct So3Table {
+  const float* table;       // Wigner-d values of every class
+  const size_t* class_off;  // [classes] float offset of each class's block
+  int precision;            // kSo3Tf32x3 or kSo3Bf16x3
+};
+// Offsets of every class's block (host) and the table's float count.
+size_t so3_table_layout(int bw_in, int bw_out, std::vector<size_t>* class_off);
+cudaError_t launch_so3_table(int bw_in, int bw_out, const double* beta_tab, const double* wig_tab,
+                             const size_t* class_off, float* table, cudaStream_t st);
+// Whether a launch of `count` requests fits the tensor-core kernel's shared
+// and tensor memory (bw_out <= 256, count <= kMaxWave).
+bool so3_tc_supported(int bw_out, int count, int precision);
+cudaError_t launch_so3_synth_tc(const So3Args& a, const So3Table& t, unsigned long long* status, cudaStream_t st);
+cudaError_t so3_tc_init_attributes();
+
+// Rotation pose of each request's SO(3) argmax on the device (k_pose.cu):
+// T[r] receives the float 3x4 transform RotateAroundXYZ applies to the source.
+struct PoseBatch {
+  int count;
+  uint32_t bw_out;
+  const unsigned long long* argmax[kMaxWave];
+  float* T[kMaxWave];  // 12 floats each
+};
+cudaError_t launch_pose(const PoseBatch& b, cudaStream_t st);
 
 // ------------------------------------------------------------ spatial
 struct VoxelArgs {
@@ -102,12 +142,14 @@ struct VoxelArgs {
   float* grids;           // [n_data_ch + 1][N^3] sums, last = count
   uint32_t* lin_out;      // optional per-point linear index (or 0xffffffff)
   uint8_t* rowlive;       // optional [N (z)][N (x)]: set to 1 for every row a point lands in
+  const float* T_dev = nullptr;     // when set: the 3x4 transform is read from device memory (has_T ignored)
+  const uint32_t* n_dev = nullptr;  // when set: the point count is read from device memory (n_points = capacity)
 };
 cudaError_t launch_voxelize(const VoxelArgs& a, cudaStream_t st);
 // Zeroes what one voxelisation wrote: planes [0, n_planes) at every point's
 // voxel (lin[i] != 0xffffffff) and the point's row flag.
 cudaError_t launch_clear_voxels(const uint32_t* lin, int n_points, float* grids, size_t nv, int n_planes,
-                                uint8_t* rowlive, int N, cudaStream_t st);
+                                uint8_t* rowlive, int N, cudaStream_t st, const uint32_t* n_dev = nullptr);
 
 struct SpatialArgs {
   int N;

@@ -1,18 +1,37 @@
 // Continuous-batching request server (C ABI phgpu_server_*).
 //
-// Requests of any (bandwidth, voxel grid) shape are queued on submit; worker
-// threads take them as soon as they are free.  Each worker owns device-resident
-// contexts (tables, plans, buffers) per shape, created on demand and admitted
-// against the HBM budget; an idle context of another shape is evicted when the
-// budget would be exceeded.  Every worker drives its own CUDA streams, so the
-// kernels of requests that arrive while others run overlap on the device.
+// Requests are queued on submit.  Worker threads ("lanes") take the oldest
+// request and every queued request of the same shape and channel layout, up to
+// max_wave, and run them as one wave on an executor of that shape:
+//
+//   * an executor owns one device-resident context per slot (grids, spectra,
+//     plans; point counts read from device memory) and, for the tensor-core
+//     precisions, shares the shape's Wigner-d table with the other executors of
+//     that bandwidth;
+//   * a wave of k requests is one CUDA graph launch, captured the first time an
+//     executor runs k requests: the k pairs' front halves (target translation
+//     side, sampling, SHT, fusion) on their own streams, one batched launch of
+//     each SO(3) stage (synthesis on the tensor cores, angle transforms,
+//     argmax) and of the pose kernel, then the k source translations, each
+//     ending in one read-back of its keys and transform;
+//   * the clouds are copied into the slots before the launch (device-resident
+//     clouds device to device, host clouds from pinned or pageable memory).
+//
+// Lanes run waves concurrently, so requests that arrive while a wave is on the
+// GPU are admitted into the next wave on another executor and overlap with it.
+// Executors are admitted against the HBM budget with their allocators' byte
+// counts; when a new one does not fit, idle executors of any shape are evicted
+// (least recently used first), and a lane waits only while some other lane's
+// wave holds the memory it needs -- which always finishes.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstring>
 #include <deque>
-#include <list>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -23,6 +42,8 @@
 #include "../../include/phaser_gpu.h"
 #include "ctx.h"
 
+using namespace phgpu;
+
 namespace {
 
 using Clock = std::chrono::steady_clock;
@@ -30,48 +51,71 @@ using Clock = std::chrono::steady_clock;
 struct Request {
   uint64_t ticket = 0;
   phgpu_params prm;
-  // device-resident inputs (and host inputs under PHGPU_SERVER_BORROW_HOST)
-  // are used in place: the caller keeps them alive until the ticket
-  // completes; other host inputs are copied at submit
-  phgpu_cloud tdev{}, sdev{};
-  bool in_place = false;
+  phgpu_cloud t{}, s{};  // what the worker reads (in place, or the copies below)
   std::vector<float> txyzi, trefl, tamb, sxyzi, srefl, samb;
-  uint32_t tn = 0, sn = 0;
-  bool t_refl = false, t_amb = false, s_refl = false, s_amb = false;
   phgpu_pose pose;
   int status = PHGPU_OK;
   std::string err;
   Clock::time_point t_submit, t_done;
   bool done = false;
+  bool want_volumes = false;
+  std::vector<float> rot_vol, trans_vol;
 };
 
-using ShapeKey = std::tuple<uint32_t, uint32_t, uint32_t, int32_t, int32_t, uint32_t, uint32_t, uint32_t,
-                            float, float, uint32_t, uint32_t, uint32_t>;
+using ShapeKey = std::tuple<uint32_t, uint32_t, uint32_t, int32_t, int32_t, uint32_t, uint32_t, uint32_t, float,
+                            float, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t, int>;
 
-ShapeKey key_of(const phgpu_params& p) {
-  return ShapeKey(p.spherical_bandwidth, p.spherical_zero_padding, p.spatial_n_voxels,
-                  p.spatial_discretize_lower, p.spatial_discretize_upper, p.n_channels, p.fusion_levels,
-                  p.spherical_fusion * 2 + p.spatial_fusion, p.spatial_low_pass_lower,
-                  p.spatial_low_pass_upper, p.flags, p.rot_peak_neighbors, p.trans_peak_neighbors);
+// Everything that decides a wave's buffers and captured graph: the shape and
+// fusion parameters and which optional channels each cloud carries.
+ShapeKey key_of(const phgpu_params& p, const phgpu_cloud& t, const phgpu_cloud& s) {
+  const int sig = (t.reflectivity ? 1 : 0) | (t.ambient ? 2 : 0) | (s.reflectivity ? 4 : 0) | (s.ambient ? 8 : 0);
+  return ShapeKey(p.spherical_bandwidth, p.spherical_zero_padding, p.spatial_n_voxels, p.spatial_discretize_lower,
+                  p.spatial_discretize_upper, p.n_channels, p.fusion_levels, p.spherical_fusion * 4 + p.spatial_fusion,
+                  p.spatial_low_pass_lower, p.spatial_low_pass_upper, p.flags & PHGPU_FLAG_KEEP_VOLUMES,
+                  p.rot_peak_neighbors, p.trans_peak_neighbors,
+                  p.spherical_low_pass_lower, p.spherical_low_pass_upper, p.precision, sig);
 }
 
-// Device bytes of one context (upper estimate used for admission).
-uint64_t estimate_bytes(const phgpu_params& p, uint32_t max_points) {
+// Device bytes of one slot before any exists (an upper estimate; executors
+// are then accounted with their allocators' counts).
+uint64_t estimate_slot_bytes(const phgpu_params& p, uint32_t max_points) {
   const uint64_t bw = p.spherical_bandwidth, bo = bw + p.spherical_zero_padding, N = p.spatial_n_voxels;
   const uint64_t nv = N * N * N, H = N * N * ((N / 2 + 1 + 7) / 8 * 8);
   uint64_t b = 0;
-  b += 4 * 4 * bw * bw * 2;                 // samples
-  b += 8 * bw * bw * 8;                     // coef
-  b += 8 * bw * 2 * bw * 8;                 // SHT scratch
-  b += 8 * bo * bo * bo;                    // S
-  b += 2 * 5 * nv * 4;                      // grids
-  b += 9 * H * 8;                           // spec + cspec
-  b += bw * bw * (bw + 1) * 4;              // Legendre table
-  if ((p.flags & PHGPU_FLAG_KEEP_VOLUMES) || p.rot_peak_neighbors) b += 8 * bo * bo * bo * 4;
-  if ((p.flags & PHGPU_FLAG_KEEP_VOLUMES) || p.trans_peak_neighbors) b += nv * 4;
+  b += 4 * 4 * bw * bw * 2 + 8 * bw * bw * 8 + 8 * bw * 2 * bw * 8;  // samples, coefficients, SHT scratch
+  b += 8 * bo * bo * bo;                                           // S
+  b += 2 * 5 * nv * 4 + 9 * H * 8;                                 // grids, spectra
+  b += bw * bw * (bw + 1) * 4;                                     // Legendre table
+  if (p.flags & PHGPU_FLAG_KEEP_VOLUMES || p.rot_peak_neighbors) b += 8 * bo * bo * bo * 4;
+  if (p.flags & PHGPU_FLAG_KEEP_VOLUMES || p.trans_peak_neighbors) b += nv * 4;
   b += 2ull * max_points * (16 + 4 + 4 + 4 + 16 + 8 + 4 + 16) + 2ull * 32768 * 48;
   return b + (8ull << 20);
 }
+
+// A Wigner-d table shared by the executors of one (bandwidth, output bandwidth).
+struct Table {
+  float* d_tab = nullptr;
+  size_t* d_off = nullptr;
+  uint64_t bytes = 0;
+  int refs = 0;
+};
+
+struct Executor {
+  ShapeKey key;
+  phgpu_params prm;
+  PairPlan pp{};
+  int kmax = 1;
+  bool graphs = true;  // waves replay captured graphs (device pose path)
+  std::vector<phgpu_ctx*> slots;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_mid = nullptr, ev_done = nullptr;
+  std::vector<cudaEvent_t> ev_join;
+  std::vector<cudaGraphExec_t> exec;  // [k] wave of k requests
+  std::shared_ptr<Table> table;
+  uint64_t bytes = 0;
+  bool busy = false;
+  Clock::time_point last_used;
+};
 
 }  // namespace
 
@@ -82,89 +126,384 @@ struct phgpu_server {
   std::deque<Request*> queue;
   std::unordered_map<uint64_t, Request*> reqs;
   std::vector<std::thread> workers;
+  std::vector<std::unique_ptr<Executor>> execs;
+  std::map<std::pair<uint32_t, uint32_t>, std::weak_ptr<Table>> tables;
+  std::map<ShapeKey, uint64_t> measured_bytes;  // bytes of an executor of each key (allocator counts)
   uint64_t next_ticket = 1;
   uint64_t used_bytes = 0;
   size_t in_flight = 0;
   bool stop = false;
   std::string err;
+  phgpu_server_stats stats{};
 
-  struct Owned {
-    ShapeKey key;
-    phgpu_ctx* ctx;
-    uint64_t bytes;
-  };
+  // ---------------------------------------------------------------- executors
 
-  void worker_main(int wid) {
-    cudaSetDevice(prm.device);
-    std::list<Owned> owned;  // most recently used first
+  // mu held on entry and exit; released while CUDA objects are created.
+  Executor* acquire(const ShapeKey& key, const phgpu_params& rp, int want, std::unique_lock<std::mutex>& lk,
+                    int* rc, std::string* why) {
     for (;;) {
-      Request* r = nullptr;
+      for (auto& e : execs)
+        if (!e->busy && e->key == key) {
+          e->busy = true;
+          return e.get();
+        }
+      const int kmax = std::max(1, std::min<int>((int)prm.max_wave, kMaxWave));
+      auto mb = measured_bytes.find(key);
+      const uint64_t need =
+          mb != measured_bytes.end() ? mb->second : estimate_slot_bytes(rp, prm.max_points) * (uint64_t)kmax;
+      // evict idle executors (any shape, least recently used first) until the new one fits
+      while (used_bytes + need > prm.hbm_budget_bytes) {
+        Executor* lru = nullptr;
+        for (auto& e : execs)
+          if (!e->busy && (!lru || e->last_used < lru->last_used)) lru = e.get();
+        if (!lru) break;
+        lru->busy = true;
+        lk.unlock();
+        destroy_exec(lru);
+        lk.lock();
+        used_bytes -= lru->bytes;
+        execs.erase(std::find_if(execs.begin(), execs.end(), [&](auto& e) { return e.get() == lru; }));
+        ++stats.evictions;
+      }
+      if (used_bytes + need <= prm.hbm_budget_bytes || used_bytes == 0) {
+        used_bytes += need;  // reserved; corrected to the allocators' count below
+        auto ex = std::make_unique<Executor>();
+        Executor* e = ex.get();
+        e->key = key;
+        e->prm = rp;
+        e->busy = true;
+        e->kmax = kmax;
+        execs.push_back(std::move(ex));
+        lk.unlock();
+        const int r = create_exec(e, why);
+        lk.lock();
+        used_bytes -= need;
+        if (r != PHGPU_OK) {
+          execs.erase(std::find_if(execs.begin(), execs.end(), [&](auto& x) { return x.get() == e; }));
+          *rc = r;
+          cv_budget.notify_all();
+          return nullptr;
+        }
+        used_bytes += e->bytes;
+        measured_bytes[key] = e->bytes;
+        return e;
+      }
+      // every executor is busy in another lane's wave: wait for one to finish
+      cv_budget.wait(lk);
+      if (stop) {
+        *rc = PHGPU_ERR_STATE;
+        *why = "server stopped";
+        return nullptr;
+      }
+    }
+    (void)want;
+  }
+
+  void release(Executor* e) {
+    e->busy = false;
+    e->last_used = Clock::now();
+    cv_budget.notify_all();
+  }
+
+  int create_exec(Executor* e, std::string* why) {
+    cudaSetDevice(prm.device);
+    phgpu_params p = e->prm;
+    p.max_points = prm.max_points;
+    p.device = prm.device;
+    p.precision = PHGPU_PRECISION_FP32;  // the executor owns the shape's table
+    const int bw_out = (int)(p.spherical_bandwidth + p.spherical_zero_padding);
+    if (e->prm.precision != PHGPU_PRECISION_FP32)
+      while (e->kmax > 1 && !so3_tc_supported(bw_out, e->kmax, (int)e->prm.precision)) --e->kmax;
+    e->graphs = e->prm.rot_peak_neighbors == 0 && e->prm.spatial_zero_padding == 0;
+    for (int i = 0; i < e->kmax; ++i) {
+      phgpu_ctx* c = nullptr;
+      const int rc = phgpu_ctx_create(&p, &c);
+      if (rc != PHGPU_OK) {
+        *why = phgpu_last_error(nullptr);
+        destroy_exec(e);
+        return rc;
+      }
+      e->slots.push_back(c);
+      e->bytes += c->device_bytes;
+      // point counts from device memory (any count up to the capacity replays
+      // the same graph); grids zeroed once, the graph's clears keep them so
+      c->dev_counts = true;
+      const size_t nv = (size_t)c->N * c->N * c->N;
+      for (int s = 0; s < 2; ++s) {
+        if (cudaMemset(c->d_grids[s], 0, sizeof(float) * 5 * nv) != cudaSuccess ||
+            cudaMemset(c->d_rowlive[s], 0, (size_t)c->N * c->N) != cudaSuccess) {
+          *why = "grid initialisation failed";
+          destroy_exec(e);
+          return PHGPU_ERR_CUDA;
+        }
+        c->clean_planes[s] = 5;
+      }
+    }
+    if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_mid, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_done, cudaEventDisableTiming) != cudaSuccess) {
+      *why = "stream / event creation failed";
+      destroy_exec(e);
+      return PHGPU_ERR_CUDA;
+    }
+    e->ev_join.assign(e->kmax, nullptr);
+    for (auto& ev : e->ev_join) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    e->exec.assign(e->kmax + 1, nullptr);
+    if (e->prm.precision != PHGPU_PRECISION_FP32) {
+      const int rc = attach_table(e, why);
+      if (rc != PHGPU_OK) {
+        destroy_exec(e);
+        return rc;
+      }
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+      *why = "executor set-up failed";
+      destroy_exec(e);
+      return PHGPU_ERR_CUDA;
+    }
+    return PHGPU_OK;
+  }
+
+  // The shape's Wigner-d table, shared with other executors of the bandwidth.
+  int attach_table(Executor* e, std::string* why) {
+    phgpu_ctx* c = e->slots[0];
+    const auto tk = std::make_pair((uint32_t)c->bw, (uint32_t)c->bw_out);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = tables.find(tk);
+      if (it != tables.end()) e->table = it->second.lock();
+    }
+    if (e->table) return PHGPU_OK;
+    auto t = std::make_shared<Table>();
+    std::vector<size_t> off;
+    const size_t nf = so3_table_layout(c->bw, c->bw_out, &off);
+    if (cudaMalloc((void**)&t->d_off, sizeof(size_t) * off.size()) != cudaSuccess ||
+        cudaMalloc((void**)&t->d_tab, sizeof(float) * nf) != cudaSuccess) {
+      if (t->d_off) cudaFree(t->d_off);
+      *why = "Wigner-d table allocation failed";
+      return PHGPU_ERR_MEMORY;
+    }
+    t->bytes = sizeof(size_t) * off.size() + sizeof(float) * nf;
+    if (cudaMemcpy(t->d_off, off.data(), sizeof(size_t) * off.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        launch_so3_table(c->bw, c->bw_out, c->d_beta_tab, c->d_wig_tab, t->d_off, t->d_tab, e->st) != cudaSuccess) {
+      cudaFree(t->d_off);
+      cudaFree(t->d_tab);
+      *why = "Wigner-d table generation failed";
+      return PHGPU_ERR_CUDA;
+    }
+    e->bytes += t->bytes;
+    e->table = t;
+    std::lock_guard<std::mutex> lk(mu);
+    tables[tk] = t;
+    return PHGPU_OK;
+  }
+
+  void destroy_exec(Executor* e) {
+    cudaSetDevice(prm.device);
+    if (e->st) cudaStreamSynchronize(e->st);
+    for (auto& g : e->exec)
+      if (g) cudaGraphExecDestroy(g);
+    e->exec.clear();
+    for (auto* c : e->slots) phgpu_ctx_destroy(c);
+    e->slots.clear();
+    for (auto& ev : e->ev_join)
+      if (ev) cudaEventDestroy(ev);
+    e->ev_join.clear();
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+    if (e->ev_mid) cudaEventDestroy(e->ev_mid);
+    if (e->ev_done) cudaEventDestroy(e->ev_done);
+    if (e->st) cudaStreamDestroy(e->st);
+    e->ev_fork = e->ev_mid = e->ev_done = nullptr;
+    e->st = nullptr;
+    if (e->table) {
+      if (e->table.use_count() == 1) {
+        cudaFree(e->table->d_tab);
+        cudaFree(e->table->d_off);
+      }
+      e->table.reset();
+    }
+  }
+
+  // ---------------------------------------------------------------- waves
+
+  // Enqueues a wave of k requests already staged in slots [0, k) on the
+  // executor's streams (captured into a graph, or run directly).
+  int enqueue_wave(Executor* e, int k) {
+    std::vector<phgpu_ctx*> sl(e->slots.begin(), e->slots.begin() + k);
+    phgpu_ctx* c0 = sl[0];
+    if (cudaEventRecord(e->ev_fork, e->st) != cudaSuccess) return PHGPU_ERR_CUDA;
+    for (int i = 0; i < k; ++i) {
+      if (cudaStreamWaitEvent(sl[i]->s0, e->ev_fork, 0) != cudaSuccess) return PHGPU_ERR_CUDA;
+      const int rc = phgpu_pair_front(sl[i], e->pp);
+      if (rc != PHGPU_OK) return rc;
+      if (cudaEventRecord(e->ev_join[i], sl[i]->s0) != cudaSuccess ||
+          cudaStreamWaitEvent(e->st, e->ev_join[i], 0) != cudaSuccess)
+        return PHGPU_ERR_CUDA;
+    }
+    So3Table tab;
+    if (e->table) {
+      tab.table = e->table->d_tab;
+      tab.class_off = e->table->d_off;
+      tab.precision = (int)e->prm.precision;
+    }
+    int rc = phgpu_run_so3_batch(sl.data(), k, e->table ? &tab : nullptr, e->st);
+    if (rc != PHGPU_OK) return rc;
+    PoseBatch pb;
+    memset(&pb, 0, sizeof(pb));
+    pb.count = k;
+    pb.bw_out = (uint32_t)c0->bw_out;
+    for (int i = 0; i < k; ++i) {
+      pb.argmax[i] = sl[i]->d_argmax;
+      pb.T[i] = sl[i]->d_T;
+    }
+    if (launch_pose(pb, e->st) != cudaSuccess || cudaEventRecord(e->ev_mid, e->st) != cudaSuccess)
+      return PHGPU_ERR_CUDA;
+    for (int i = 0; i < k; ++i) {
+      if (cudaStreamWaitEvent(sl[i]->s0, e->ev_mid, 0) != cudaSuccess) return PHGPU_ERR_CUDA;
+      rc = phgpu_pair_back(sl[i], e->pp, nullptr, sl[i]->d_T);
+      if (rc != PHGPU_OK) return rc;
+      if (cudaEventRecord(e->ev_join[i], sl[i]->s0) != cudaSuccess ||
+          cudaStreamWaitEvent(e->st, e->ev_join[i], 0) != cudaSuccess)
+        return PHGPU_ERR_CUDA;
+    }
+    return PHGPU_OK;
+  }
+
+  int capture(Executor* e, int k, std::string* why) {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      *why = "stream capture could not start";
+      return PHGPU_ERR_CUDA;
+    }
+    const int rc = enqueue_wave(e, k);
+    const cudaError_t ce = cudaStreamEndCapture(e->st, &g);
+    if (rc != PHGPU_OK || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      *why = rc != PHGPU_OK ? std::string("wave capture: ") + phgpu_last_error(e->slots[0])
+                            : std::string("wave capture: ") + cudaGetErrorString(ce);
+      cudaGetLastError();
+      return PHGPU_ERR_CUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&e->exec[k], g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      e->exec[k] = nullptr;
+      *why = std::string("graph instantiation: ") + cudaGetErrorString(ie);
+      return PHGPU_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    ++stats.graph_captures;
+    return PHGPU_OK;
+  }
+
+  void run_wave(Executor* e, std::vector<Request*>& wave) {
+    cudaSetDevice(prm.device);
+    const int k = (int)wave.size();
+    std::string why;
+    int rc = PHGPU_OK;
+    e->pp = pair_plan(e->slots[0], wave[0]->t.reflectivity, wave[0]->t.ambient, wave[0]->s.reflectivity,
+                      wave[0]->s.ambient);
+    if (!e->graphs) {
+      // host-pose registrations (peak neighbourhoods): one at a time
+      for (int i = 0; i < k; ++i) {
+        Request* r = wave[i];
+        r->status = phgpu_register_pair(e->slots[0], &r->t, &r->s, &r->pose);
+        if (r->status != PHGPU_OK) r->err = phgpu_last_error(e->slots[0]);
+        if (r->status == PHGPU_OK && r->want_volumes) copy_volumes(e->slots[0], r);
+      }
+      std::lock_guard<std::mutex> lk(mu);
+      ++stats.waves;
+      stats.requests += (uint64_t)k;
+      return;
+    }
+    for (int i = 0; i < k && rc == PHGPU_OK; ++i) {
+      rc = phgpu_upload_cloud(e->slots[i], &wave[i]->t, 0, e->st);
+      if (rc == PHGPU_OK) rc = phgpu_upload_cloud(e->slots[i], &wave[i]->s, 1, e->st);
+      if (rc != PHGPU_OK) why = phgpu_last_error(e->slots[i]);
+    }
+    if (rc == PHGPU_OK && !e->exec[k]) rc = capture(e, k, &why);
+    if (rc == PHGPU_OK) {
+      if (cudaGraphLaunch(e->exec[k], e->st) != cudaSuccess || cudaEventRecord(e->ev_done, e->st) != cudaSuccess ||
+          cudaEventSynchronize(e->ev_done) != cudaSuccess) {
+        rc = PHGPU_ERR_CUDA;
+        why = std::string("wave: ") + cudaGetErrorString(cudaGetLastError());
+      }
+    }
+    uint64_t reruns = 0;
+    for (int i = 0; i < k; ++i) {
+      Request* r = wave[i];
+      if (rc != PHGPU_OK) {
+        r->status = rc;
+        r->err = why;
+        continue;
+      }
+      phgpu_ctx* c = e->slots[i];
+      const uint64_t before = c->pose_reruns;
+      r->status = phgpu_pair_finish(c, e->pp, true, &r->pose);
+      reruns += c->pose_reruns - before;
+      if (r->status != PHGPU_OK) r->err = phgpu_last_error(c);
+      if (r->status == PHGPU_OK && r->want_volumes) copy_volumes(c, r);
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    ++stats.waves;
+    stats.requests += (uint64_t)k;
+    stats.pose_reruns += reruns;
+  }
+
+  static void copy_volumes(phgpu_ctx* c, Request* r) {
+    const size_t nr = (size_t)8 * c->bw_out * c->bw_out * c->bw_out;
+    const size_t nt = (size_t)c->N * c->N * c->N;
+    r->rot_vol.resize(nr);
+    r->trans_vol.resize(nt);
+    if (c->d_rotvol) cudaMemcpy(r->rot_vol.data(), c->d_rotvol, sizeof(float) * nr, cudaMemcpyDeviceToHost);
+    if (c->d_transvol) cudaMemcpy(r->trans_vol.data(), c->d_transvol, sizeof(float) * nt, cudaMemcpyDeviceToHost);
+  }
+
+  void worker_main() {
+    cudaSetDevice(prm.device);
+    for (;;) {
+      std::vector<Request*> wave;
+      ShapeKey key;
       {
         std::unique_lock<std::mutex> lk(mu);
         cv_work.wait(lk, [&] { return stop || !queue.empty(); });
         if (stop && queue.empty()) break;
-        r = queue.front();
-        queue.pop_front();
-      }
-      const ShapeKey k = key_of(r->prm);
-      phgpu_ctx* ctx = nullptr;
-      for (auto it = owned.begin(); it != owned.end(); ++it) {
-        if (it->key == k) {
-          ctx = it->ctx;
-          owned.splice(owned.begin(), owned, it);
-          break;
-        }
-      }
-      if (!ctx) {
-        phgpu_params p = r->prm;
-        p.max_points = std::max<uint32_t>(prm.max_points, std::max(r->tn, r->sn));
-        p.device = prm.device;
-        const uint64_t need = estimate_bytes(p, p.max_points);
-        {
-          std::unique_lock<std::mutex> lk(mu);
-          // evict this worker's least recently used contexts until the request fits
-          while (used_bytes + need > prm.hbm_budget_bytes && !owned.empty()) {
-            Owned o = owned.back();
-            owned.pop_back();
-            lk.unlock();
-            phgpu_ctx_destroy(o.ctx);
-            lk.lock();
-            used_bytes -= o.bytes;
-            cv_budget.notify_all();
+        // the oldest request and every queued request of its key, up to max_wave
+        Request* first = queue.front();
+        key = key_of(first->prm, first->t, first->s);
+        const size_t kmax = std::max<uint32_t>(1u, std::min<uint32_t>(prm.max_wave, kMaxWave));
+        for (auto it = queue.begin(); it != queue.end() && wave.size() < kmax;) {
+          if (key_of((*it)->prm, (*it)->t, (*it)->s) == key) {
+            wave.push_back(*it);
+            it = queue.erase(it);
+          } else {
+            ++it;
           }
-          // wait for other workers to release memory
-          cv_budget.wait(lk, [&] { return stop || used_bytes + need <= prm.hbm_budget_bytes || used_bytes == 0; });
-          used_bytes += need;
         }
-        int rc = phgpu_ctx_create(&p, &ctx);
-        if (rc != PHGPU_OK) {
-          std::lock_guard<std::mutex> lk(mu);
-          used_bytes -= need;
-          r->status = rc;
-          r->err = phgpu_last_error(nullptr);
-          finish(r);
+        int rc = PHGPU_OK;
+        std::string why;
+        Executor* e = acquire(key, first->prm, (int)wave.size(), lk, &rc, &why);
+        if (!e) {
+          for (Request* r : wave) {
+            r->status = rc;
+            r->err = why;
+            finish(r);
+          }
           continue;
         }
-        owned.push_front(Owned{k, ctx, need});
+        // an executor may hold fewer slots than the wave (shared / tensor memory)
+        if ((int)wave.size() > e->kmax) {
+          for (size_t i = wave.size(); i-- > (size_t)e->kmax;) queue.push_front(wave[i]);
+          wave.resize(e->kmax);
+          cv_work.notify_one();
+        }
+        lk.unlock();
+        run_wave(e, wave);
+        lk.lock();
+        release(e);
+        for (Request* r : wave) finish(r);
       }
-      phgpu_cloud t{r->txyzi.data(), r->t_refl ? r->trefl.data() : nullptr,
-                    r->t_amb ? r->tamb.data() : nullptr, r->tn, 0};
-      phgpu_cloud s{r->sxyzi.data(), r->s_refl ? r->srefl.data() : nullptr,
-                    r->s_amb ? r->samb.data() : nullptr, r->sn, 0};
-      if (r->in_place) {
-        t = r->tdev;
-        s = r->sdev;
-      }
-      const int rc = phgpu_register_pair(ctx, &t, &s, &r->pose);
-      std::lock_guard<std::mutex> lk(mu);
-      r->status = rc;
-      if (rc != PHGPU_OK) r->err = phgpu_last_error(ctx);
-      finish(r);
-    }
-    std::lock_guard<std::mutex> lk(mu);
-    for (auto& o : owned) {
-      phgpu_ctx_destroy(o.ctx);
-      used_bytes -= o.bytes;
     }
   }
 
@@ -185,10 +524,12 @@ int phgpu_server_create(const phgpu_server_params* params, phgpu_server** out) {
   if (!params || !out) return PHGPU_ERR_INVALID;
   phgpu_server* s = new phgpu_server();
   s->prm = *params;
-  if (s->prm.max_wave == 0) s->prm.max_wave = 4;
+  if (s->prm.max_wave == 0) s->prm.max_wave = 16;
+  if (s->prm.max_wave > (uint32_t)kMaxWave) s->prm.max_wave = kMaxWave;
   if (s->prm.max_points == 0) s->prm.max_points = 1u << 18;
   if (s->prm.hbm_budget_bytes == 0) s->prm.hbm_budget_bytes = 150ull << 30;
-  for (uint32_t w = 0; w < s->prm.max_wave; ++w) s->workers.emplace_back(&phgpu_server::worker_main, s, (int)w);
+  if (s->prm.lanes == 0) s->prm.lanes = 2;
+  for (uint32_t w = 0; w < s->prm.lanes; ++w) s->workers.emplace_back(&phgpu_server::worker_main, s);
   *out = s;
   return PHGPU_OK;
 }
@@ -202,27 +543,29 @@ int phgpu_server_destroy(phgpu_server* s) {
   s->cv_work.notify_all();
   s->cv_budget.notify_all();
   for (auto& t : s->workers) t.join();
+  for (auto& e : s->execs) s->destroy_exec(e.get());
+  s->execs.clear();
   for (auto& kv : s->reqs) delete kv.second;
   delete s;
   return PHGPU_OK;
 }
 
 static void copy_cloud(const phgpu_cloud* c, std::vector<float>& xyzi, std::vector<float>& refl,
-                       std::vector<float>& amb, bool& has_refl, bool& has_amb) {
+                       std::vector<float>& amb, phgpu_cloud* dst) {
   const size_t n = c->n_points;
   xyzi.resize(4 * n);
   const cudaMemcpyKind k = c->on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
   if (n) cudaMemcpy(xyzi.data(), c->xyzi, sizeof(float) * 4 * n, k);
-  has_refl = c->reflectivity != nullptr;
-  has_amb = c->ambient != nullptr;
-  if (has_refl) {
+  if (c->reflectivity) {
     refl.resize(n);
     if (n) cudaMemcpy(refl.data(), c->reflectivity, sizeof(float) * n, k);
   }
-  if (has_amb) {
+  if (c->ambient) {
     amb.resize(n);
     if (n) cudaMemcpy(amb.data(), c->ambient, sizeof(float) * n, k);
   }
+  *dst = phgpu_cloud{xyzi.data(), c->reflectivity ? refl.data() : nullptr, c->ambient ? amb.data() : nullptr,
+                     c->n_points, 0};
 }
 
 int phgpu_server_submit(phgpu_server* s, const phgpu_params* params, const phgpu_cloud* target,
@@ -231,22 +574,30 @@ int phgpu_server_submit(phgpu_server* s, const phgpu_params* params, const phgpu
   if (params->spatial_zero_padding != 0) {
     // the padded correlation carries state from one call to the next (the
     // previous call's last channel spectrum), so its result would depend on
-    // which requests a worker context served before
+    // which requests a slot served before
     std::lock_guard<std::mutex> lk(s->mu);
     s->err = "spatial zero padding is not served (its result depends on the context's previous calls)";
     return PHGPU_ERR_INVALID;
   }
+  if (target->n_points > s->prm.max_points || source->n_points > s->prm.max_points) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->err = "cloud larger than the server's max_points";
+    return PHGPU_ERR_LIMIT;
+  }
+  if (target->on_device != source->on_device) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->err = "both clouds must be on the device or both on the host";
+    return PHGPU_ERR_INVALID;
+  }
   Request* r = new Request();
   r->prm = *params;
-  r->tn = target->n_points;
-  r->sn = source->n_points;
-  if ((target->on_device && source->on_device) || (s->prm.flags & PHGPU_SERVER_BORROW_HOST)) {
-    r->in_place = true;
-    r->tdev = *target;
-    r->sdev = *source;
+  r->want_volumes = (params->flags & PHGPU_FLAG_KEEP_VOLUMES) != 0;
+  if (target->on_device || (s->prm.flags & PHGPU_SERVER_BORROW_HOST)) {
+    r->t = *target;
+    r->s = *source;
   } else {
-    copy_cloud(target, r->txyzi, r->trefl, r->tamb, r->t_refl, r->t_amb);
-    copy_cloud(source, r->sxyzi, r->srefl, r->samb, r->s_refl, r->s_amb);
+    copy_cloud(target, r->txyzi, r->trefl, r->tamb, &r->t);
+    copy_cloud(source, r->sxyzi, r->srefl, r->samb, &r->s);
   }
   r->t_submit = Clock::now();
   {
@@ -265,7 +616,8 @@ int phgpu_server_submit(phgpu_server* s, const phgpu_params* params, const phgpu
   return PHGPU_OK;
 }
 
-int phgpu_server_poll(phgpu_server* s, uint64_t ticket, phgpu_pose* out, double* latency_ms) {
+int phgpu_server_poll_volumes(phgpu_server* s, uint64_t ticket, phgpu_pose* out, double* latency_ms,
+                              float* rot_volume, float* trans_volume) {
   if (!s) return PHGPU_ERR_INVALID;
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->reqs.find(ticket);
@@ -282,6 +634,12 @@ int phgpu_server_poll(phgpu_server* s, uint64_t ticket, phgpu_pose* out, double*
     delete r;
     return st;
   }
+  if ((rot_volume || trans_volume) && !r->want_volumes) {
+    s->err = "volumes were not kept (submit with PHGPU_FLAG_KEEP_VOLUMES)";
+    return PHGPU_ERR_STATE;
+  }
+  if (rot_volume) memcpy(rot_volume, r->rot_vol.data(), sizeof(float) * r->rot_vol.size());
+  if (trans_volume) memcpy(trans_volume, r->trans_vol.data(), sizeof(float) * r->trans_vol.size());
   if (out) *out = r->pose;
   if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
   s->reqs.erase(it);
@@ -289,10 +647,23 @@ int phgpu_server_poll(phgpu_server* s, uint64_t ticket, phgpu_pose* out, double*
   return 1;
 }
 
+int phgpu_server_poll(phgpu_server* s, uint64_t ticket, phgpu_pose* out, double* latency_ms) {
+  return phgpu_server_poll_volumes(s, ticket, out, latency_ms, nullptr, nullptr);
+}
+
 int phgpu_server_drain(phgpu_server* s) {
   if (!s) return PHGPU_ERR_INVALID;
   std::unique_lock<std::mutex> lk(s->mu);
   s->cv_done.wait(lk, [&] { return s->in_flight == 0; });
+  return PHGPU_OK;
+}
+
+int phgpu_server_get_stats(phgpu_server* s, phgpu_server_stats* out) {
+  if (!s || !out) return PHGPU_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = s->stats;
+  out->executors = (uint64_t)s->execs.size();
+  out->bytes_in_use = s->used_bytes;
   return PHGPU_OK;
 }
 

@@ -24,6 +24,9 @@ PHGPU_FUSION_NONE = 1
 PHGPU_FUSION_LOW_PASS = 2
 PHGPU_FLAG_KEEP_VOLUMES = 1
 PHGPU_SERVER_BORROW_HOST = 1
+PHGPU_PRECISION_FP32 = 0
+PHGPU_PRECISION_TF32X3 = 1
+PHGPU_PRECISION_BF16X3 = 2
 
 
 class PhgpuError(RuntimeError):
@@ -51,6 +54,7 @@ class Params(C.Structure):
         ("trans_peak_neighbors", C.c_uint32),
         ("spherical_low_pass_lower", C.c_uint32),
         ("spherical_low_pass_upper", C.c_uint32),
+        ("precision", C.c_uint32),
     ]
 
 
@@ -92,7 +96,16 @@ class ServerParams(C.Structure):
         ("max_points", C.c_uint32),
         ("device", C.c_int32),
         ("flags", C.c_uint32),
+        ("lanes", C.c_uint32),
     ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("waves", "requests", "graph_captures", "evictions", "pose_reruns",
+                                          "executors", "bytes_in_use")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
 # every symbol the header declares (checked by the CPU tests)
@@ -109,7 +122,8 @@ EXPORTED = [
     "phgpu_sample_s2_noalloc", "phgpu_bingham_peak", "phgpu_gaussian_peak", "phgpu_peak_window",
     "phgpu_ply_info", "phgpu_ply_read", "phgpu_ply_last_error", "phgpu_voxel_grid_create",
     "phgpu_voxel_grid_destroy", "phgpu_voxel_grid_filter", "phgpu_voxel_grid_last_error",
-    "phgpu_spatial_correlation_size",
+    "phgpu_spatial_correlation_size", "phgpu_pose_reruns", "phgpu_server_poll_volumes",
+    "phgpu_server_get_stats",
 ]
 
 _LIB = None
@@ -155,6 +169,8 @@ def load(path: str = LIB_PATH):
                                         C.POINTER(C.c_uint64)]
     lib.phgpu_server_poll.argtypes = [vp, C.c_uint64, C.POINTER(Pose), C.POINTER(C.c_double)]
     lib.phgpu_server_drain.argtypes = [vp]
+    lib.phgpu_server_poll_volumes.argtypes = [vp, C.c_uint64, C.POINTER(Pose), C.POINTER(C.c_double), vp, vp]
+    lib.phgpu_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
     lib.phgpu_server_last_error.restype = C.c_char_p
     lib.phgpu_server_last_error.argtypes = [vp]
     lib.phgpu_profile_enable.argtypes = [vp, C.c_int]
@@ -163,6 +179,8 @@ def load(path: str = LIB_PATH):
     lib.phgpu_profile_stage_name.restype = C.c_char_p
     lib.phgpu_profile_stage_name.argtypes = [C.c_int]
     lib.phgpu_launch_count.restype = C.c_ulonglong
+    lib.phgpu_pose_reruns.restype = C.c_ulonglong
+    lib.phgpu_pose_reruns.argtypes = [vp]
     lib.phgpu_bingham_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
                                        C.c_void_p]
     lib.phgpu_gaussian_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int32,
@@ -530,6 +548,10 @@ class Context:
         return (v.value, pk.value, vol) if volume else (v.value, pk.value)
 
     # ---- full pipeline
+    def pose_reruns(self) -> int:
+        """Translations register_pair redid with the host transform."""
+        return int(self.lib.phgpu_pose_reruns(self.h))
+
     def register_pair(self, target, source) -> Pose:
         """target/source: (xyzi, reflectivity) tuples of numpy arrays or torch CUDA tensors."""
         ct, k1 = make_cloud(*target)
@@ -540,18 +562,20 @@ class Context:
 
 
 class Server:
-    """Continuous-batching request server (C ABI phgpu_server_*)."""
+    """Continuous-batching request server (C ABI phgpu_server_*): waves of up
+    to max_wave same-shape pairs, `lanes` waves in flight."""
 
-    def __init__(self, workers=4, hbm_budget_bytes=150 << 30, max_points=1 << 18, device=0, flags=0):
+    def __init__(self, max_wave=16, hbm_budget_bytes=150 << 30, max_points=1 << 18, device=0, flags=0, lanes=2):
         lib = load()
         self.lib = lib
-        sp = ServerParams(int(hbm_budget_bytes), int(workers), int(max_points), int(device), int(flags))
+        sp = ServerParams(int(hbm_budget_bytes), int(max_wave), int(max_points), int(device), int(flags), int(lanes))
         h = C.c_void_p()
         rc = lib.phgpu_server_create(C.byref(sp), C.byref(h))
         if rc != PHGPU_OK:
             raise PhgpuError(f"phgpu_server_create failed ({rc})")
         self.h = h
         self._keep = {}
+        self._vol = {}
         self._borrow = bool(int(flags) & PHGPU_SERVER_BORROW_HOST)
 
     def submit(self, params: Params, target, source) -> int:
@@ -563,18 +587,41 @@ class Server:
             raise PhgpuError(f"submit failed ({rc}): {self.lib.phgpu_server_last_error(self.h).decode()}")
         if (ct.on_device and cs.on_device) or self._borrow:
             self._keep[t.value] = (k1, k2)  # read in place until the ticket completes
+        if params.flags & PHGPU_FLAG_KEEP_VOLUMES:
+            bo = params.spherical_bandwidth + params.spherical_zero_padding
+            self._vol[t.value] = ((2 * bo) ** 3, params.spatial_n_voxels ** 3)
         return t.value
 
-    def poll(self, ticket):
+    def poll(self, ticket, volumes=False):
+        """None while running; (pose, latency_ms) when done, plus the rotation
+        and translation volumes when volumes=True (submitted with
+        PHGPU_FLAG_KEEP_VOLUMES)."""
         pose = Pose()
         lat = C.c_double()
-        rc = self.lib.phgpu_server_poll(self.h, C.c_uint64(ticket), C.byref(pose), C.byref(lat))
+        rv = tv = None
+        if volumes:
+            nr, nt = self._vol[ticket]
+            rv = np.zeros(nr, np.float32)
+            tv = np.zeros(nt, np.float32)
+        rc = self.lib.phgpu_server_poll_volumes(self.h, C.c_uint64(ticket), C.byref(pose), C.byref(lat),
+                                                rv.ctypes.data if volumes else None,
+                                                tv.ctypes.data if volumes else None)
         if rc < 0:
             raise PhgpuError(f"request {ticket} failed ({rc}): {self.lib.phgpu_server_last_error(self.h).decode()}")
         if rc == 0:
             return None
         self._keep.pop(ticket, None)
+        self._vol.pop(ticket, None)
+        if volumes:
+            return pose, lat.value, rv, tv
         return pose, lat.value
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        rc = self.lib.phgpu_server_get_stats(self.h, C.byref(st))
+        if rc != PHGPU_OK:
+            raise PhgpuError(f"stats failed ({rc})")
+        return st.as_dict()
 
     def drain(self):
         rc = self.lib.phgpu_server_drain(self.h)

@@ -46,7 +46,7 @@ def test_mixed_batch_matches_oracle():
 
     with cf.ThreadPoolExecutor(max_workers=len(MIXED)) as ex:
         want = list(ex.map(oracle, range(len(MIXED))))
-    srv = nat.Server(workers=4, device=0, flags=nat.PHGPU_SERVER_BORROW_HOST)
+    srv = nat.Server(max_wave=8, lanes=2, device=0, flags=nat.PHGPU_SERVER_BORROW_HOST)
     tickets = [srv.submit(pr, (p.target.xyzi, p.target.reflectivity), (p.source.xyzi, p.source.reflectivity))
                for pr, p in zip(params, pairs)]
     srv.drain()

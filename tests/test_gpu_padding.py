@@ -117,7 +117,7 @@ def test_padded_registration_decodes_on_padded_grid():
 def test_padding_not_served():
     from phaser_b200 import native as nat, scene
     pair = scene.workload_pair(0, 0)
-    srv = nat.Server(workers=1, device=0)
+    srv = nat.Server(max_wave=1, lanes=1, device=0)
     p = nat.default_params(spherical_bandwidth=8, spatial_n_voxels=16, spatial_zero_padding=2)
     with pytest.raises(nat.PhgpuError):
         srv.submit(p, (pair.target.xyzi, None), (pair.source.xyzi, None))
