@@ -51,6 +51,16 @@ def parse():
     ap.add_argument("--lanes", type=int, default=2, help="waves in flight at once")
     ap.add_argument("--pool", type=int, default=4, help="distinct synthetic pairs per rank")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", choices=["pair", "served", "ingest"], default=None,
+                    help="run a small program for an ncu capture and exit: `pair` registers --pairs pairs of "
+                         "--workload one at a time (plain), `served` runs --pairs pairs through the server in "
+                         "waves, `ingest` reads one scan from a PLY and voxel-grid filters it --calls times")
+    ap.add_argument("--workload", type=int, default=WORKLOAD)
+    ap.add_argument("--pairs", type=int, default=2)
+    ap.add_argument("--calls", type=int, default=4)
+    ap.add_argument("--precision", type=int, default=0, help="--profile pair: PHGPU_PRECISION_* of the context")
+    ap.add_argument("--no-cpu-throughput", action="store_true",
+                    help="reference arm: skip the nproc single-threaded processes leg")
     return ap.parse_args()
 
 
@@ -301,7 +311,7 @@ def ingest(nat, pool, cpu_ok, reps=20):
     pcl::VoxelGrid on the same scan."""
     import tempfile
     import torch
-    from phaser_b200.profile_ingest import write_ply
+    from phaser_b200.scene import write_ply
     cl = pool[0].target
     n = int(cl.xyzi.shape[0])
     with tempfile.TemporaryDirectory() as d:
@@ -428,18 +438,59 @@ def run_script_config(nat, pool, local, reps=10):
 
 # ------------------------------------------------------------------ CPU
 
-def cpu_reference(pair, w, threads=None):
+# FFTW threads the reference registration plans with
+# (phaser_core/src/backend/registration/sph-opt-registration.cc:29-30).
+REF_FFT_THREADS = 12
+
+CPU_PATH = ("SOFT 2.0 sources of the reference (unmodified) + project FP64 FFTW-API shim (no FFTW3 library in "
+            "the image) + restated phaser_core glue, kd-tree NN")
+
+
+def config_desc(desc, world):
+    """The `config` both arms print (identical, so the driver can pair them)."""
+    return {"workload": desc, "l2": "per-pair working set ~1 GB > 126 MB L2 (no flush needed)",
+            "parallelism": f"replicas x{world}, pairs sharded per rank"}
+
+
+def cpu_reference(pair, w, threads=REF_FFT_THREADS):
+    """One registration on the host cores through the reference path (the
+    oracle port when oracle/_ref is absent): seconds, kind, (bin, voxel)."""
     from oracle import oracle as O
     kind = "reference" if O.ref_available() else "port"
     t0 = time.perf_counter()
     if kind == "reference":
-        O.ref_register_pair(pair.target.xyzi, pair.target.reflectivity, pair.source.xyzi,
-                            pair.source.reflectivity, w["bw"], w["n_voxels"], w["lo"], w["hi"],
-                            threads=threads)
+        rb, vx, _ = O.ref_register_pair(pair.target.xyzi, pair.target.reflectivity, pair.source.xyzi,
+                                        pair.source.reflectivity, w["bw"], w["n_voxels"], w["lo"], w["hi"],
+                                        threads=threads)
     else:
-        O.register_pair(pair.target.xyzi, pair.target.reflectivity, pair.source.xyzi,
-                        pair.source.reflectivity, w["bw"], w["n_voxels"], w["lo"], w["hi"])
-    return time.perf_counter() - t0, kind
+        pose = O.register_pair(pair.target.xyzi, pair.target.reflectivity, pair.source.xyzi,
+                               pair.source.reflectivity, w["bw"], w["n_voxels"], w["lo"], w["hi"])
+        rb, vx = pose.rot_bin, pose.voxel
+    return time.perf_counter() - t0, kind, (int(rb), int(vx))
+
+
+def _throughput_worker(k):
+    """One single-threaded reference registration of pair k (spawned process):
+    wall-clock start and end of the registration alone."""
+    sys.path.insert(0, ROOT)
+    from phaser_b200 import scene
+    w = scene.WORKLOADS[WORKLOAD]
+    pair = scene.workload_pair(WORKLOAD, k)
+    t0 = time.time()
+    cpu_reference(pair, w, threads=1)
+    return t0, time.time()
+
+
+def cpu_throughput(n_proc):
+    """nproc independent single-threaded registrations of distinct pairs at
+    once: the aggregate rate over the span from the first start to the last
+    end."""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(n_proc) as pool:
+        spans = pool.map(_throughput_worker, list(range(100, 100 + n_proc)))
+    wall = max(b for _, b in spans) - min(a for a, _ in spans)
+    return {"value": round(n_proc / wall, 4), "unit": UNIT, "processes": n_proc, "threads_per_process": 1,
+            "wall_s": round(wall, 2), "sample": f"{n_proc} distinct pairs of the workload, one per process"}
 
 
 def run_reference(a, world, rank):
@@ -449,26 +500,84 @@ def run_reference(a, world, rank):
     pool = make_pool(0, 1)
     lat = []
     kind = "reference"
+    bins = None
     for i in range(a.warmup + a.steps):
-        dt, kind = cpu_reference(pool[0], w)
+        dt, kind, bins = cpu_reference(pool[0], w)
         if i >= a.warmup:
             lat.append(dt)
     T = sum(lat)
     v = a.steps / T
     cores = os.cpu_count()
+    thr = cpu_throughput(cores) if not a.no_cpu_throughput else None
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(1e3 * T / a.steps, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded room scans)",
-        "config": {"workload": desc, "pairs_per_step": 1, "path": "SOFT 2.0 sources of the reference + "
-                   "project FFTW-API shim + restated phaser_core glue, kd-tree NN, OpenMP threads"},
-        "latency_ms": {"p50": round(1e3 * pct(lat, 50), 2), "p99": round(1e3 * pct(lat, 99), 2)},
-        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": "1 pair of the B=100/N=200 workload per step"},
+        "data": "synthetic (seeded room scans)", "config": config_desc(desc, world), "pairs_per_step": 1,
+        "path": CPU_PATH,
+        "latency_ms": {"p50": round(1e3 * pct(lat, 50), 2), "p99": round(1e3 * pct(lat, 99), 2),
+                       "threads": REF_FFT_THREADS},
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": REF_FFT_THREADS, "kind": kind,
+                         "sample": f"1 pair of the workload per step (seed {pool_seeds(0, 1)[0]}), FFTs on "
+                                   f"{REF_FFT_THREADS} threads as the reference plans them, {cores} host threads"},
+        "cpu_throughput": thr,
+        "parity": {"pair_seed": pool_seeds(0, 1)[0], "rot_bin": bins[0], "voxel": bins[1]},
         "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ profiling programs
+
+def run_profile(a):
+    """The small programs the committed ncu summaries are captured on (one GPU,
+    a few launches of each kernel): prints one JSON line."""
+    import torch
+    from phaser_b200 import native as nat, scene
+    nat.load()
+    w = scene.WORKLOADS[a.workload]
+    p = scene.workload_pair(a.workload, 0)
+    cap = max(1 << 18, p.target.xyzi.shape[0], p.source.xyzi.shape[0])
+    params = nat.default_params(spherical_bandwidth=w["bw"], spatial_n_voxels=w["n_voxels"],
+                                spatial_discretize_lower=w["lo"], spatial_discretize_upper=w["hi"], max_points=cap,
+                                precision=a.precision)
+    clouds = ((p.target.xyzi, p.target.reflectivity), (p.source.xyzi, p.source.reflectivity))
+    out = {"profile": a.profile, "workload": a.workload}
+    if a.profile == "pair":
+        ctx = nat.Context(params)
+        pose = None
+        for _ in range(a.pairs):
+            pose = ctx.register_pair(*clouds)
+        out.update({"rot_bin": pose.rot_bin, "voxel": pose.voxel, "pairs": a.pairs})
+        ctx.close()
+    elif a.profile == "served":
+        params.precision = nat.PHGPU_PRECISION_TF32X3
+        dev = tuple((torch.from_numpy(x).cuda(), torch.from_numpy(r).cuda()) for x, r in clouds)
+        srv = nat.Server(max_wave=a.max_wave, lanes=1, max_points=cap)
+        tickets = [srv.submit(params, *dev) for _ in range(a.pairs)]
+        srv.drain()
+        poses = [srv.poll(t)[0] for t in tickets]
+        out.update({"rot_bin": poses[0].rot_bin, "voxel": poses[0].voxel, "pairs": a.pairs, "server": srv.stats()})
+        srv.close()
+    else:
+        import tempfile
+        cl = p.target
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "scan.ply")
+            scene.write_ply(path, cl.xyzi, cl.reflectivity)
+            ply = nat.ply_read(path, pinned=True)
+        vg = nat.VoxelGrid(max(1 << 18, len(cl.xyzi)))
+        dv = torch.from_numpy(cl.xyzi).cuda()
+        leaves = 0
+        for _ in range(a.calls):
+            o, _, _ = vg.filter(dv, (0.25,) * 3, out_device=True)
+            vg.filter(ply["xyzi"], (0.25,) * 3, reflectivity=ply["reflectivity"])
+            leaves = int(o.shape[0])
+        vg.close()
+        out.update({"points": len(cl.xyzi), "leaves": leaves, "calls": 2 * a.calls})
+    torch.cuda.synchronize()
+    print(json.dumps(out), flush=True)
     return 0
 
 
@@ -481,6 +590,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         return run_reference(a, world, rank)
+    if a.profile:
+        return run_profile(a)
 
     import torch
     torch.cuda.set_device(local)
@@ -530,6 +641,7 @@ def main():
     e1.synchronize()
     plain_ms = max_over_ranks(e0.elapsed_time(e1), dist)
     plain_value = job_rate(world, K, S, plain_ms)
+    plain_pose0 = ctx.register_pair(*dev[0])
     ctx.close()
 
     # ---------------- served pipeline, device-resident inputs (value)
@@ -594,6 +706,9 @@ def main():
         tick.append(srv.submit(sparams, *dev[i % len(dev)]))
     srv.drain()
     open_lat = [srv.poll(t)[1] for t in tick]
+    t0 = srv.submit(sparams, *dev[0])
+    srv.drain()
+    served_pose0 = srv.poll(t0)[0]
     server_stats = srv.stats()
     srv.close()
     barrier()
@@ -625,13 +740,21 @@ def main():
         except Exception as exc:  # the headline line is printed regardless
             ing = {"error": f"{type(exc).__name__}: {exc}"}
 
-    # ---------------- CPU baseline (rank 0, N = 1)
+    # ---------------- CPU baseline and reference parity (rank 0, N = 1): the
+    # reference path on the first pool pair; the GPU's plain and served poses
+    # of that pair must equal its bin and voxel
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        dt, kind = cpu_reference(pool[0], w)
-        cpu = {"value": round(1.0 / dt, 4), "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
-               "sample": "1 pair of the B=100/N=200 workload, all host threads; SOFT sources with the "
-                         "project's FP64 FFTW-API shim (no FFTW3 library in the image)"}
+        dt, kind, bins = cpu_reference(pool[0], w)
+        cpu = {"value": round(1.0 / dt, 4), "unit": UNIT, "cores": REF_FFT_THREADS, "kind": kind,
+               "sample": f"1 pair of the workload (seed {pool_seeds(rank, 1)[0]}), FFTs on {REF_FFT_THREADS} threads "
+                         f"as the reference plans them; {CPU_PATH}"}
+        gp = [(q.rot_bin, q.voxel) for q in (plain_pose0, served_pose0)]
+        parity = {"pair_seed": pool_seeds(rank, 1)[0], "reference": {"rot_bin": bins[0], "voxel": bins[1]},
+                  "plain": {"rot_bin": gp[0][0], "voxel": gp[0][1]},
+                  "served": {"rot_bin": gp[1][0], "voxel": gp[1][1]},
+                  "equal": all(g == bins for g in gp)}
 
     if rank == 0:
         line = {
@@ -639,10 +762,8 @@ def main():
             "warmup": W, "ms_per_step": round(served_ms / K, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
             "data": "synthetic (seeded room scans, 128x1024 LiDAR)",
-            "config": {"workload": desc, "pairs_per_step": S, "pairs_per_rank": K * S,
-                       "max_wave": a.max_wave, "lanes": a.lanes, "distinct_pairs": a.pool,
-                       "l2": "per-pair working set ~1 GB > 126 MB L2 (no flush needed)",
-                       "parallelism": f"replicas x{world}, pairs sharded per rank"},
+            "config": config_desc(desc, world), "pairs_per_step": S, "pairs_per_rank": K * S,
+            "server": {"max_wave": a.max_wave, "lanes": a.lanes}, "distinct_pairs": a.pool,
             "served": {"value": round(value, 2), "precision": "tf32x3 tensor-core Wigner-d synthesis",
                        "server_stats": server_stats, "p50_ms": round(pct(served_lat, 50), 3),
                        "p99_ms": round(pct(served_lat, 99), 3), "latency": "closed-loop batches of pairs_per_step",
@@ -654,6 +775,7 @@ def main():
                     "d2h_bytes_per_step": 16 * S},
             "roofline": roof,
             "cpu_baseline": cpu,
+            "reference_parity": parity,
             "clocks": clocks,
             "gpu_launches": int(launches),
             "ingest": ing,
@@ -664,6 +786,9 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    if parity is not None and not parity["equal"]:
+        print("GPU poses differ from the reference path on the checked pair", file=sys.stderr)
+        return 1
     return 0
 
 

@@ -38,6 +38,12 @@ extern "C" {
  * products whose FFT-shifted N^3 index has all three subscripts in
  * [spatial_low_pass_lower, min(spatial_low_pass_upper, N)]. */
 #define PHGPU_FUSION_LOW_PASS 2
+/* SphRegistration's single signal (spherical only; sph-registration.cc:166-198
+ * with SphericalCorrelation::correlateSignals, spherical-correlation.cc:54-67,
+ * 103-112): the sampled grids are mixed as 0.6 * intensity + 0.4 * range (in
+ * double) and correlated as one channel without fusion.  Host sample arrays
+ * (phgpu_sph_correlate, correlateSampledSignals) are taken as given: channel 0. */
+#define PHGPU_FUSION_MIX 3
 
 /* flags */
 #define PHGPU_FLAG_KEEP_VOLUMES 1u /* also keep the full correlation volumes */
@@ -145,7 +151,10 @@ int phgpu_get_samples(phgpu_ctx* ctx, int side, double* values, int32_t* nn_inde
  * PHGPU_NOALLOC_MAX_POINTS returns PHGPU_ERR_LIMIT; calls that overlap on
  * one device race on the array.  The first call on each device looks the
  * array up (and may load the module there): make it before any stream
- * capture. */
+ * capture.  A call whose bandwidth differs from the previous call's on that
+ * device also copies the grid directions into the array (host to device, on
+ * `stream`).  After cudaDeviceReset of a device, do not call this again in
+ * the same process: the looked-up address belonged to the destroyed context. */
 #define PHGPU_NOALLOC_MAX_POINTS (1 << 18)
 #define PHGPU_NOALLOC_MAX_BANDWIDTH 128
 int phgpu_sample_s2_noalloc(const phgpu_params* params, const phgpu_cloud* cloud, float* values_dev,
@@ -258,14 +267,6 @@ const char* phgpu_profile_stage_name(int stage);
 /* Kernels launched by this library since it was loaded (all contexts). */
 unsigned long long phgpu_launch_count(void);
 
-/* Self-test of the shared-memory FFT engines (no reference counterpart):
- * transforms ntrans sequences of length n (complex interleaved, natural order,
- * sequence-major, in place in `data`) laid out as shared-memory rows or
- * columns; engine 0 = runtime plan, 1 = compile-time plan, 2 = register-tail
- * plan (1 and 2 for n in {32, 64, 100, 128, 200, 256, 512}; 1 also for 320).  Forward =
- * exp(-2 pi i jk/n), inverse = exp(+2 pi i jk/n), both unnormalised. */
-int phgpu_selftest_fft(int n, int ntrans, int inverse, int columns, int engine, float* data);
-
 /* ------------------------------------------------------------------ ingest
  * PLY reading (replaces data::PlyHelper::readPlyFromFile +
  * PointCloud::parsePlyPointCloud, phaser_common/src/common/data/
@@ -342,6 +343,8 @@ typedef struct {
   uint64_t waves;           /* waves run */
   uint64_t requests;        /* requests completed in waves */
   uint64_t graph_captures;  /* CUDA graphs captured (one per executor and wave size) */
+  uint64_t direct_waves;    /* waves launched without a graph (their capture was invalidated by other
+                               CUDA work of the process that synchronised the device) */
   uint64_t evictions;       /* executors evicted to admit another shape */
   uint64_t pose_reruns;     /* translations redone with the host transform */
   uint64_t executors;       /* executors resident now */

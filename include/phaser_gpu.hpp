@@ -71,6 +71,18 @@ class Context {
 };
 }  // namespace detail
 
+// One direction's sample (model::FunctionValue): the values of the nearest
+// cloud point (the 1-NN sampler feeds each direction one point), 0 when the
+// nearest point lies beyond the rejection radius (nn_index -1).
+struct FunctionValue {
+  double range = 0.0, intensity = 0.0, reflectivity = 0.0, ambient = 0.0;
+  int32_t nn_index = -1;
+  double getAveragedRange() const noexcept { return range; }
+  double getAveragedIntensity() const noexcept { return intensity; }
+  double getAveragedReflectivity() const noexcept { return reflectivity; }
+  double getAveragedAmbientNoise() const noexcept { return ambient; }
+};
+
 // SphericalCorrelation(bw, zero_padding): single-signal correlation
 // (correlateSampledSignals uses the first channel, spherical-correlation.cc:69-80).
 class SphericalCorrelation {
@@ -96,6 +108,21 @@ class SphericalCorrelation {
     detail::check(phgpu_sph_correlate(ctx_->get(), fp.data(), gp.data(), (uint32_t)nc), ctx_->get(),
                   "phgpu_sph_correlate");
     have_ = true;
+  }
+
+  // SphericalCorrelation::correlateSignals (spherical-correlation.cc:54-67):
+  // one signal per side, 0.6 * intensity + 0.4 * range of every direction
+  // (retrieveInterpolation, :103-112), correlated by correlateSampledSignals
+  // (virtual, as in the reference: the Laplace class refuses one channel).
+  void correlateSignals(const std::vector<FunctionValue>& f1, const std::vector<FunctionValue>& f2) {
+    SampledSignal a, b;
+    retrieveInterpolation(f1, &a);
+    retrieveInterpolation(f2, &b);
+    correlateSampledSignals({a}, {b});
+  }
+  static void retrieveInterpolation(const std::vector<FunctionValue>& f, SampledSignal* out) {
+    out->reserve(out->size() + f.size());
+    for (const FunctionValue& v : f) out->push_back(0.6 * v.getAveragedIntensity() + 0.4 * v.getAveragedRange());
   }
 
   // |z|^2 over the (2 bw_out)^3 grid, [beta][alpha][gamma].
@@ -311,19 +338,29 @@ class SphOptRegistration {
   detail::Context ctx_;
 };
 
-// ------------------------------------------------------------------ S^2 sampling
+// SphRegistration::registerPointCloud (sph-registration.cc:82-198): rotation
+// from the single 0.6 intensity + 0.4 range signal of the sampled directions
+// with the plain SphericalCorrelation, then the PhaseAligner translation of
+// the rotated cloud (prev = target, cur = source).
+class SphRegistration {
+ public:
+  explicit SphRegistration(const phgpu_params& base = default_params()) : ctx_(mix_params(base)) {}
+  phgpu_pose registerPointCloud(const CloudView& cloud_prev, const CloudView& cloud_cur) {
+    phgpu_cloud t = cloud_prev.c(), s = cloud_cur.c();
+    phgpu_pose pose;
+    detail::check(phgpu_register_pair(ctx_.get(), &t, &s, &pose), ctx_.get(), "phgpu_register_pair");
+    return pose;
+  }
 
-// One direction's sample (model::FunctionValue): the values of the nearest
-// cloud point (the 1-NN sampler feeds each direction one point), 0 when the
-// nearest point lies beyond the rejection radius (nn_index -1).
-struct FunctionValue {
-  double range = 0.0, intensity = 0.0, reflectivity = 0.0, ambient = 0.0;
-  int32_t nn_index = -1;
-  double getAveragedRange() const noexcept { return range; }
-  double getAveragedIntensity() const noexcept { return intensity; }
-  double getAveragedReflectivity() const noexcept { return reflectivity; }
-  double getAveragedAmbientNoise() const noexcept { return ambient; }
+ private:
+  static phgpu_params mix_params(phgpu_params p) {
+    p.spherical_fusion = PHGPU_FUSION_MIX;
+    return p;
+  }
+  detail::Context ctx_;
 };
+
+// ------------------------------------------------------------------ S^2 sampling
 
 // SphericalSampler::sampleUniformly (spherical-sampler.cc:20-27): the 2B x 2B
 // Driscoll-Healy directions, [theta][phi] order, each sampled by its nearest

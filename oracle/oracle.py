@@ -43,7 +43,9 @@ class Pose(C.Structure):
 def build(ref: bool = True) -> None:
     """Compile the oracle (and, when the reference tree exists, oracle/_ref)."""
     targets = ["all"]
-    ref_root = os.environ.get("PHASER_REF_ROOT", "/root/reference")
+    # the reference tree beside the repository unless PHASER_REF_ROOT names it
+    ref_root = os.environ.get("PHASER_REF_ROOT",
+                              os.path.abspath(os.path.join(HERE, os.pardir, os.pardir, "reference")))
     if ref and os.path.isdir(os.path.join(ref_root, "phaser_core", "lib", "SOFT")):
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", HERE, f"REF_ROOT={ref_root}"] + targets,
@@ -95,6 +97,11 @@ def _declare(lib):
     lib.orc_register_pair_k.argtypes = [_f32p, C.c_size_t, C.c_void_p, _f32p, C.c_size_t, C.c_void_p,
                                         C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint32, C.c_uint32,
                                         C.POINTER(Pose), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.orc_mix_signal.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
+    lib.orc_register_pair_mode.argtypes = [_f32p, C.c_size_t, C.c_void_p, _f32p, C.c_size_t, C.c_void_p,
+                                           C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint32, C.c_uint32,
+                                           C.c_int, C.POINTER(Pose), C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p]
     lib.orc_spherical_correlation_lowpass.argtypes = [C.c_int, C.c_int, _f64p, _f64p, C.c_uint32, C.c_uint32,
                                                       _f64p]
     lib.orc_spatial_correlation_lowpass.argtypes = [C.c_int, _f64p, _f64p, C.c_uint32, C.c_uint32, _f64p]
@@ -143,6 +150,11 @@ def ref_lib():
                                            C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                            C.c_float, C.c_int, C.POINTER(C.c_uint32),
                                            C.POINTER(C.c_uint32), _f64p]
+        _REF.ref_register_pair_mode.restype = C.c_int
+        _REF.ref_register_pair_mode.argtypes = [_f32p, C.c_size_t, C.c_void_p, _f32p, C.c_size_t,
+                                                C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                C.c_float, C.c_int, C.c_int, C.POINTER(C.c_uint32),
+                                                C.POINTER(C.c_uint32), _f64p]
     return _REF
 
 
@@ -366,10 +378,11 @@ def translation_from_index(idx, n, lo, hi):
 
 
 def register_pair(tgt, tgt_refl, src, src_refl, bw, N, lo, hi, max_sq=1e6, want_volumes=False, rot_k=0,
-                  trans_k=0, want_stats=False):
+                  trans_k=0, want_stats=False, sph_mode=0):
     """Full registration; with rot_k / trans_k > 0 the Bingham mode and the
     Gaussian mean of the peak neighbourhoods give the pose.  want_stats adds
-    (omega[4], cov[3x3]) to the returned tuple."""
+    (omega[4], cov[3x3]) to the returned tuple.  sph_mode 1: SphRegistration's
+    single 0.6 intensity + 0.4 range signal instead of the Laplace fusion."""
     tgt = np.ascontiguousarray(tgt, np.float32)
     src = np.ascontiguousarray(src, np.float32)
     tr = None if tgt_refl is None else np.ascontiguousarray(tgt_refl, np.float32)
@@ -378,9 +391,9 @@ def register_pair(tgt, tgt_refl, src, src_refl, bw, N, lo, hi, max_sq=1e6, want_
     rc = np.zeros((2 * bw) ** 3) if want_volumes else None
     tc = np.zeros(N ** 3) if want_volumes else None
     omega, cov = np.zeros(4), np.zeros(9)
-    lib().orc_register_pair_k(tgt.reshape(-1), tgt.shape[0], _ptr(tr), src.reshape(-1), src.shape[0],
-                              _ptr(sr), bw, N, lo, hi, max_sq, int(rot_k), int(trans_k), C.byref(pose), _ptr(rc),
-                              _ptr(tc), omega.ctypes.data, cov.ctypes.data)
+    lib().orc_register_pair_mode(tgt.reshape(-1), tgt.shape[0], _ptr(tr), src.reshape(-1), src.shape[0],
+                                 _ptr(sr), bw, N, lo, hi, max_sq, int(rot_k), int(trans_k), int(sph_mode),
+                                 C.byref(pose), _ptr(rc), _ptr(tc), omega.ctypes.data, cov.ctypes.data)
     out = (pose,)
     if want_volumes:
         out += (rc, tc)
@@ -447,7 +460,7 @@ def ref_spatial_correlation(f, g, N, laplace=True):
     return out
 
 
-def ref_register_pair(tgt, tgt_refl, src, src_refl, bw, N, lo, hi, max_sq=1e6, threads=None):
+def ref_register_pair(tgt, tgt_refl, src, src_refl, bw, N, lo, hi, max_sq=1e6, threads=None, sph_mode=0):
     tgt = np.ascontiguousarray(tgt, np.float32)
     src = np.ascontiguousarray(src, np.float32)
     tr = None if tgt_refl is None else np.ascontiguousarray(tgt_refl, np.float32)
@@ -456,9 +469,9 @@ def ref_register_pair(tgt, tgt_refl, src, src_refl, bw, N, lo, hi, max_sq=1e6, t
     rb = C.c_uint32()
     vx = C.c_uint32()
     pose6 = np.zeros(6)
-    ref_lib().ref_register_pair(tgt.reshape(-1), tgt.shape[0], _ptr(tr), src.reshape(-1),
-                                src.shape[0], _ptr(sr), bw, N, lo, hi, max_sq, threads,
-                                C.byref(rb), C.byref(vx), pose6)
+    ref_lib().ref_register_pair_mode(tgt.reshape(-1), tgt.shape[0], _ptr(tr), src.reshape(-1),
+                                     src.shape[0], _ptr(sr), bw, N, lo, hi, max_sq, threads, int(sph_mode),
+                                     C.byref(rb), C.byref(vx), pose6)
     return rb.value, vx.value, pose6
 
 

@@ -890,10 +890,21 @@ void orc_transform(float* xyzi, size_t P, const float* T) {
 /* 71-131; phaser_core/include/igl/histc.cpp:34-73).                        */
 /* ------------------------------------------------------------------------ */
 
+/* Eigen::VectorXf::LinSpaced(N, lo, hi) of Eigen >= 3.3 (the eigen_catkin
+ * version phaser builds against; Eigen's published linspaced_op for floats):
+ * step = (hi - lo) / (N - 1) in float; when |hi| < |lo| the entries count
+ * down from the high end, e[0] = lo, e[i] = hi - (N - 1 - i) step, otherwise
+ * up from the low end, e[i] = lo + i step, e[N - 1] = hi. */
 void orc_edges(int N, int lo, int hi, float* e) {
   const float flo = (float)lo, fhi = (float)hi;
   const float step = (N == 1) ? 0.0f : (fhi - flo) / (float)(N - 1);
-  for (int i = 0; i < N; ++i) e[i] = (i == N - 1) ? fhi : (flo + (float)i * step);
+  const int flip = fabsf(fhi) < fabsf(flo);
+  for (int i = 0; i < N; ++i) {
+    if (flip)
+      e[i] = (i == 0) ? flo : (fhi - (float)(N - 1 - i) * step);
+    else
+      e[i] = (i == N - 1) ? fhi : (flo + (float)i * step);
+  }
 }
 
 static int32_t histc1(float xf, const float* E, int N) {
@@ -1279,6 +1290,11 @@ void orc_register_pair_k(const float* tgt_xyzi, size_t Pt, const float* tgt_refl
                          const float* src_xyzi, size_t Ps, const float* src_refl,
                          int bw, int N, int lo, int hi, float max_sq_dist, uint32_t rot_k, uint32_t trans_k,
                          orc_pose* pose, double* rot_corr, double* trans_corr, double* omega, double* cov);
+void orc_register_pair_mode(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
+                            const float* src_xyzi, size_t Ps, const float* src_refl,
+                            int bw, int N, int lo, int hi, float max_sq_dist, uint32_t rot_k, uint32_t trans_k,
+                            int sph_mode, orc_pose* pose, double* rot_corr, double* trans_corr, double* omega,
+                            double* cov);
 
 void orc_register_pair(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
                        const float* src_xyzi, size_t Ps, const float* src_refl,
@@ -1289,13 +1305,31 @@ void orc_register_pair(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
                       rot_corr, trans_corr, omega, cov);
 }
 
-/* With rot_k / trans_k > 0 the rotation applied to the source is the mode    */
-/* of the Bingham fit and the translation the mean of the Gaussian fit        */
-/* (sph-opt-registration.cc:58-88).                                           */
 void orc_register_pair_k(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
                          const float* src_xyzi, size_t Ps, const float* src_refl,
                          int bw, int N, int lo, int hi, float max_sq_dist, uint32_t rot_k, uint32_t trans_k,
                          orc_pose* pose, double* rot_corr, double* trans_corr, double* omega, double* cov) {
+  orc_register_pair_mode(tgt_xyzi, Pt, tgt_refl, src_xyzi, Ps, src_refl, bw, N, lo, hi, max_sq_dist, rot_k,
+                         trans_k, 0, pose, rot_corr, trans_corr, omega, cov);
+}
+
+/* SphericalCorrelation::retrieveInterpolation (spherical-correlation.cc:
+ * 103-112): one signal 0.6 * intensity + 0.4 * range per direction, from the
+ * sample channels {range, intensity, ...} of n directions. */
+void orc_mix_signal(const double* samples, size_t n, double* out) {
+  for (size_t i = 0; i < n; ++i) out[i] = 0.6 * samples[n + i] + 0.4 * samples[i];
+}
+
+/* With rot_k / trans_k > 0 the rotation applied to the source is the mode    */
+/* of the Bingham fit and the translation the mean of the Gaussian fit        */
+/* (sph-opt-registration.cc:58-88).  sph_mode 0: SphOptRegistration (4        */
+/* channels, Laplace fusion); 1: SphRegistration (sph-registration.cc:166-198: */
+/* the single 0.6 I + 0.4 R signal, plain SphericalCorrelation).              */
+void orc_register_pair_mode(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
+                            const float* src_xyzi, size_t Ps, const float* src_refl,
+                            int bw, int N, int lo, int hi, float max_sq_dist, uint32_t rot_k, uint32_t trans_k,
+                            int sph_mode, orc_pose* pose, double* rot_corr, double* trans_corr, double* omega,
+                            double* cov) {
   const size_t ns = (size_t)4 * bw * bw;
   double* f = (double*)malloc(sizeof(double) * 4 * ns);
   double* h = (double*)malloc(sizeof(double) * 4 * ns);
@@ -1304,7 +1338,17 @@ void orc_register_pair_k(const float* tgt_xyzi, size_t Pt, const float* tgt_refl
   const int n = 2 * bw;
   const size_t nvol = (size_t)n * n * n;
   double* corr = rot_corr ? rot_corr : (double*)malloc(sizeof(double) * nvol);
-  orc_spherical_correlation(bw, bw, 4, f, h, 5, corr, NULL, NULL);
+  if (sph_mode == 1) {
+    double* fm = (double*)malloc(sizeof(double) * ns);
+    double* hm = (double*)malloc(sizeof(double) * ns);
+    orc_mix_signal(f, ns, fm);
+    orc_mix_signal(h, ns, hm);
+    orc_spherical_correlation(bw, bw, 1, fm, hm, 5, corr, NULL, NULL);
+    free(fm);
+    free(hm);
+  } else {
+    orc_spherical_correlation(bw, bw, 4, f, h, 5, corr, NULL, NULL);
+  }
   const uint64_t bin = orc_argmax(corr, nvol);
   pose->rot_bin = (uint32_t)bin;
   pose->rot_peak = corr[bin];

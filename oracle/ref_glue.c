@@ -438,12 +438,29 @@ static void ref_sample_cloud(const float* xyzi, size_t P, const float* refl, int
   free(t.node_right);
 }
 
+int ref_register_pair_mode(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
+                           const float* src_xyzi, size_t Ps, const float* src_refl,
+                           int bw, int N, int lo, int hi, float max_sq, int threads, int sph_mode,
+                           uint32_t* rot_bin, uint32_t* voxel, double* pose6);
+
 /* Whole registration on the CPU: returns rotation bin and translation voxel;
  * pose6 = {x, y, z rotation angles (XYZ), tx, ty, tz}. */
 int ref_register_pair(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
                       const float* src_xyzi, size_t Ps, const float* src_refl,
                       int bw, int N, int lo, int hi, float max_sq, int threads,
                       uint32_t* rot_bin, uint32_t* voxel, double* pose6) {
+  return ref_register_pair_mode(tgt_xyzi, Pt, tgt_refl, src_xyzi, Ps, src_refl, bw, N, lo, hi, max_sq, threads,
+                                0, rot_bin, voxel, pose6);
+}
+
+/* sph_mode 0: SphOptRegistration (sph-opt-registration.cc:34-132: four
+ * channels, SphericalCorrelationLaplace); 1: SphRegistration
+ * (sph-registration.cc:82-198: SphericalCorrelation::correlateSignals on the
+ * 0.6 intensity + 0.4 range signal of each direction). */
+int ref_register_pair_mode(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
+                           const float* src_xyzi, size_t Ps, const float* src_refl,
+                           int bw, int N, int lo, int hi, float max_sq, int threads, int sph_mode,
+                           uint32_t* rot_bin, uint32_t* voxel, double* pose6) {
   fftw_plan_with_nthreads(threads);
   const size_t ns = (size_t)4 * bw * bw;
   double* f = (double*)malloc(sizeof(double) * 4 * ns);
@@ -452,7 +469,15 @@ int ref_register_pair(const float* tgt_xyzi, size_t Pt, const float* tgt_refl,
   ref_sample_cloud(src_xyzi, Ps, src_refl, bw, max_sq, h);
   const long nvol = 8L * bw * bw * bw;
   double* corr = (double*)malloc(sizeof(double) * nvol);
-  ref_spherical_correlation(bw, bw, 4, f, h, corr, NULL);
+  if (sph_mode == 1) {
+    for (size_t i = 0; i < ns; ++i) {
+      f[i] = 0.6 * f[ns + i] + 0.4 * f[i];
+      h[i] = 0.6 * h[ns + i] + 0.4 * h[i];
+    }
+    ref_spherical_correlation(bw, bw, 1, f, h, corr, NULL);
+  } else {
+    ref_spherical_correlation(bw, bw, 4, f, h, corr, NULL);
+  }
   const uint64_t bin = orc_argmax(corr, (uint64_t)nvol);
   double zyz[3], q[4], xyz[3];
   orc_bin_to_zyz((uint32_t)bin, (uint32_t)bw, zyz);

@@ -476,11 +476,11 @@ int phgpu_ctx_create(const phgpu_params* prm, phgpu_ctx** out) {
   const int N = (int)prm->spatial_n_voxels;
   if (bw < 2 || bw > 512 || N < 1 || N > 1024 || (uint64_t)N + 2ull * prm->spatial_zero_padding > 1024 ||
       prm->n_channels < 1 || prm->n_channels > 4 || prm->fusion_levels < 1 ||
-      prm->fusion_levels > (uint32_t)kMaxLevels || prm->spherical_fusion > PHGPU_FUSION_LOW_PASS ||
-      prm->spatial_fusion > PHGPU_FUSION_LOW_PASS || prm->precision > PHGPU_PRECISION_BF16X3) {
+      prm->fusion_levels > (uint32_t)kMaxLevels || prm->spherical_fusion > PHGPU_FUSION_MIX || prm->spatial_fusion > PHGPU_FUSION_LOW_PASS ||
+      prm->precision > PHGPU_PRECISION_BF16X3) {
     g_create_error =
         "unsupported configuration (2 <= bandwidth <= 512, 1 <= n_voxels + 2 spatial zero padding <= 1024, "
-        "1..4 channels, 1..8 fusion levels, fusion mode 0..2, precision 0..2)";
+        "1..4 channels, 1..8 fusion levels, spherical fusion 0..3, spatial fusion 0..2, precision 0..2)";
     return PHGPU_ERR_INVALID;
   }
   phgpu_ctx* ctx = new phgpu_ctx();
@@ -578,11 +578,18 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   CK(cudaMemcpy(ctx->d_weights, w.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
   CKV(dalloc(ctx, &ctx->d_legendre, sizeof(float) * legendre_table_entries(bw)));
   CK(launch_legendre_table(bw, ctx->d_weights, ctx->d_legendre, ctx->s0));
-  // histc edges (phase-aligner.cc:27-30): float LinSpaced
+  // histc edges (phase-aligner.cc:27-30): float LinSpaced of Eigen >= 3.3,
+  // which counts down from the high end when |hi| < |lo|
   std::vector<float> e(N);
   const float flo = (float)prm->spatial_discretize_lower, fhi = (float)prm->spatial_discretize_upper;
   const float step = (N == 1) ? 0.0f : (fhi - flo) / (float)(N - 1);
-  for (int i = 0; i < N; ++i) e[i] = (i == N - 1) ? fhi : (flo + (float)i * step);
+  const bool flip = fabsf(fhi) < fabsf(flo);
+  for (int i = 0; i < N; ++i) {
+    if (flip)
+      e[i] = (i == 0) ? flo : (fhi - (float)(N - 1 - i) * step);
+    else
+      e[i] = (i == N - 1) ? fhi : (flo + (float)i * step);
+  }
   CKV(dalloc(ctx, &ctx->d_edges, sizeof(float) * N));
   CK(cudaMemcpy(ctx->d_edges, e.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
   // squared voxel size of the sampler rejection (point-cloud.cc:66-72)
@@ -593,6 +600,7 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   const size_t nq = (size_t)4 * bw * bw;
   CKV(dalloc(ctx, &ctx->d_samples, sizeof(float) * 2 * 4 * nq));
   CK(cudaMemset(ctx->d_samples, 0, sizeof(float) * 2 * 4 * nq));
+  if (prm->spherical_fusion == PHGPU_FUSION_MIX) CKV(dalloc(ctx, &ctx->d_mix, sizeof(float) * 2 * nq));
   for (int s = 0; s < 2; ++s) CKV(dalloc(ctx, &ctx->d_nn[s], sizeof(int32_t) * nq));
   CKV(dalloc(ctx, &ctx->d_coef, sizeof(float2) * 8 * bw * bw));
   CKV(dalloc(ctx, &ctx->d_fphi, sizeof(float2) * sht_scratch_entries(bw)));
@@ -793,15 +801,16 @@ So3Table so3_table(phgpu_ctx* ctx) {
 // Spherical correlation of the sample grids currently in d_samples.
 // SHT of both sides' sample grids and their fusion (up to the fused spectra);
 // resets the rotation argmax.
-int phgpu_run_sph_front(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st) {
+int phgpu_run_sph_front(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st, bool mix) {
   const int bw = ctx->bw;
   const size_t nq = (size_t)4 * bw * bw;
+  if (mix) CK(launch_mix_signal(ctx->d_samples, 4 * nq, (int)nq, ctx->d_mix, st));
   {
     ShtArgs s;
     s.bw = bw;
-    s.n_data = n_data;
-    s.side_stride = 4 * nq;
-    s.signal = ctx->d_samples;
+    s.n_data = mix ? 1 : n_data;
+    s.side_stride = mix ? nq : 4 * nq;
+    s.signal = mix ? ctx->d_mix : ctx->d_samples;
     s.plan = &ctx->plan_s2;
     s.table = ctx->d_legendre;
     s.fphi = ctx->d_fphi;
@@ -863,8 +872,8 @@ int phgpu_run_so3_batch(phgpu_ctx* const* ctx, int k, const So3Table* table, cud
 
 // Spherical correlation of the sample grids currently in d_samples; the bin
 // and status are read back to h_argmax[0], [2].
-int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st) {
-  CKV(phgpu_run_sph_front(ctx, n_data, n_total, laplace, st));
+int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st, bool mix) {
+  CKV(phgpu_run_sph_front(ctx, n_data, n_total, laplace, st, mix));
   So3Table t = so3_table(ctx);
   CKV(phgpu_run_so3_batch(&ctx, 1, ctx->prm.precision != PHGPU_PRECISION_FP32 ? &t : nullptr, st));
   CK(cudaMemcpyAsync(ctx->h_argmax, ctx->d_argmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
@@ -902,7 +911,8 @@ int phgpu_sph_correlate_sampled(phgpu_ctx* ctx) {
   const int nd = std::max(ctx->has_amb[0] || ctx->has_amb[1] ? 4 : 0,
                           ctx->has_refl[0] || ctx->has_refl[1] ? 3 : 2);
   const int laplace = ctx->prm.spherical_fusion == PHGPU_FUSION_LAPLACE ? 1 : 0;
-  CKV(phgpu_run_sph(ctx, laplace ? nd : 1, (int)ctx->prm.n_channels, laplace, ctx->s0));
+  CKV(phgpu_run_sph(ctx, laplace ? nd : 1, (int)ctx->prm.n_channels, laplace, ctx->s0,
+                    ctx->prm.spherical_fusion == PHGPU_FUSION_MIX));
   CK(cudaStreamSynchronize(ctx->s0));
   return PHGPU_OK;
 }
@@ -1219,7 +1229,8 @@ int phgpu_pair_front(phgpu_ctx* ctx, const PairPlan& pp) {
   // rotation up to the fused spectra
   CKV(run_sample(ctx, 0, s0));
   CKV(run_sample(ctx, 1, s0));
-  CKV(phgpu_run_sph_front(ctx, pp.laplace_s2 ? pp.nd_s2 : 1, (int)ctx->prm.n_channels, pp.laplace_s2, s0));
+  CKV(phgpu_run_sph_front(ctx, pp.laplace_s2 ? pp.nd_s2 : 1, (int)ctx->prm.n_channels, pp.laplace_s2, s0,
+                          ctx->prm.spherical_fusion == PHGPU_FUSION_MIX));
   return PHGPU_OK;
 }
 

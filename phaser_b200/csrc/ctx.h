@@ -57,6 +57,7 @@ struct phgpu_ctx {
   int has_refl[2] = {0, 0}, has_amb[2] = {0, 0};
   // rotation
   float* d_samples = nullptr;  // [2][4][4B^2]
+  float* d_mix = nullptr;      // [2][4B^2] single signal of PHGPU_FUSION_MIX
   int32_t* d_nn[2] = {nullptr, nullptr};
   float2* d_fphi = nullptr;  // SHT scratch: F_m(theta_k) per signal
   float2* d_coef = nullptr;
@@ -125,12 +126,12 @@ struct ProfScope {
 
 int phgpu_ctx_init(phgpu_ctx* ctx);
 int phgpu_upload_cloud(phgpu_ctx* ctx, const phgpu_cloud* c, int side, cudaStream_t st);
-int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st);
+int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st, bool mix = false);
 int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, cudaStream_t st,
                        const float* T_dev = nullptr);
 int phgpu_run_spatial(phgpu_ctx* ctx, int n_data, int n_total, int laplace, int means, cudaStream_t st);
 phgpu::So3Args so3_args(phgpu_ctx* ctx);
-int phgpu_run_sph_front(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st);
+int phgpu_run_sph_front(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st, bool mix = false);
 int phgpu_run_so3_batch(phgpu_ctx* const* ctx, int k, const phgpu::So3Table* table, cudaStream_t st);
 
 // One registration split for the server's waves: the front half on the

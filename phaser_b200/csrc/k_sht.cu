@@ -355,6 +355,24 @@ __global__ void k_fuse_s2(FuseS2Args a) {
   }
 }
 
+// SphRegistration's single signal (SphericalCorrelation::retrieveInterpolation,
+// phaser_core/src/backend/correlation/spherical-correlation.cc:103-112):
+// 0.6 * intensity + 0.4 * range of every direction, in double, for both
+// sides; samples [side][c][n] with channels {range, intensity, ...}.
+__global__ void k_mix_signal(const float* __restrict__ samples, size_t side_stride, int n, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 2 * n) return;
+  const int side = i / n, k = i - side * n;
+  const float* s = samples + (size_t)side * side_stride;
+  out[i] = (float)__dadd_rn(__dmul_rn(0.6, (double)s[n + k]), __dmul_rn(0.4, (double)s[k]));
+}
+
+cudaError_t launch_mix_signal(const float* samples, size_t side_stride, int n, float* out, cudaStream_t st) {
+  k_mix_signal<<<(2 * n + 255) / 256, 256, 0, st>>>(samples, side_stride, n, out);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fuse_s2(const FuseS2Args& a, cudaStream_t st) {
   const int tot = a.bw * (2 * a.bw - 1);
   k_fuse_s2<<<(tot + 255) / 256, 256, 0, st>>>(a);

@@ -576,8 +576,8 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
   __syncthreads();
   fft_tail<NH, true, true>(W, N, S, pH.tw);    // over r, columns
   fft_tail<N, true, false>(W, NH, S, pN.tw);   // over y, rows
-  // a thread visits its indices in increasing order (i0 < i1 < the next
-  // element's i0): a strictly larger value keeps the first occurrence
+  // per thread: the largest value, the lowest index among equal ones (the
+  // reference's first occurrence, whatever order the thread visits them in)
   float bv = -INFINITY;
   uint32_t bi = 0xffffffffu;
   for (int e = threadIdx.x; e < NH * N; e += blockDim.x) {
@@ -586,11 +586,11 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
     const float a0 = 2.0f * v.x, a1 = 2.0f * v.y;
     const uint32_t i0 = (uint32_t)(((size_t)z * N + 2 * r) * N + y);
     const uint32_t i1 = i0 + N;
-    if (i0 < limit && (a0 > bv || bi == 0xffffffffu)) {
+    if (i0 < limit && (a0 > bv || (a0 == bv && i0 < bi) || bi == 0xffffffffu)) {
       bv = a0;
       bi = i0;
     }
-    if (i1 < limit && (a1 > bv || bi == 0xffffffffu)) {
+    if (i1 < limit && (a1 > bv || (a1 == bv && i1 < bi) || bi == 0xffffffffu)) {
       bv = a1;
       bi = i1;
     }
@@ -624,6 +624,21 @@ static cudaError_t set_attrs() {
   return e;
 }
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
 cudaError_t spatial_init_attributes() {
   cudaError_t e = cudaSuccess;
   for (int n : {64, 128, 200, 256, 320, 512, 0}) {  // every length PHGPU_DISPATCH_N instantiates
@@ -636,6 +651,8 @@ cudaError_t spatial_init_attributes() {
     cudaError_t r = allow_max_smem(fn);
     if (r != cudaSuccess) e = r;
   }
+  // look the tensor-map encoder up now, not first inside a stream capture
+  encode_tiled();
   return e;
 }
 
@@ -673,21 +690,6 @@ static int fuse_z_tile(int N, int A) {
 
 // cuTensorMapEncodeTiled through the runtime (no link against the driver
 // library); null when unavailable, in which case the element loader is used.
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-static EncodeTiledFn encode_tiled() {
-  static EncodeTiledFn fn = [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess)
-      p = nullptr;
-    return reinterpret_cast<EncodeTiledFn>(p);
-  }();
-  return fn;
-}
-
 cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t st) {
   const int N = a.N, H2 = N / 2 + 1;
   const size_t nv = (size_t)N * N * N;

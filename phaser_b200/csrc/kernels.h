@@ -70,6 +70,8 @@ struct FuseS2Args {
   float2* fused;          // [2][B (l)][2B-1 (m + B - 1)]
 };
 cudaError_t launch_fuse_s2(const FuseS2Args& a, cudaStream_t st);
+// out[side][k] = 0.6 * intensity + 0.4 * range of samples [side][c][n] (n = 4B^2)
+cudaError_t launch_mix_signal(const float* samples, size_t side_stride, int n, float* out, cudaStream_t st);
 
 // ------------------------------------------------------------ SO(3)
 // Requests of one shape processed by one launch (a wave of the server).

@@ -111,6 +111,7 @@ struct Executor {
   cudaEvent_t ev_fork = nullptr, ev_mid = nullptr, ev_done = nullptr;
   std::vector<cudaEvent_t> ev_join;
   std::vector<cudaGraphExec_t> exec;  // [k] wave of k requests
+  std::vector<int> capture_failures;  // [k] captures of a k-request wave that were invalidated
   std::shared_ptr<Table> table;
   uint64_t bytes = 0;
   bool busy = false;
@@ -129,6 +130,10 @@ struct phgpu_server {
   std::vector<std::unique_ptr<Executor>> execs;
   std::map<std::pair<uint32_t, uint32_t>, std::weak_ptr<Table>> tables;
   std::map<ShapeKey, uint64_t> measured_bytes;  // bytes of an executor of each key (allocator counts)
+  // Held while a lane captures a wave graph and while an executor is created or
+  // destroyed: allocation, frees and synchronous set-up calls synchronise the
+  // device, which would invalidate a capture running in another lane.
+  std::mutex cuda_excl;
   uint64_t next_ticket = 1;
   uint64_t used_bytes = 0;
   size_t in_flight = 0;
@@ -159,7 +164,10 @@ struct phgpu_server {
         if (!lru) break;
         lru->busy = true;
         lk.unlock();
-        destroy_exec(lru);
+        {
+          std::lock_guard<std::mutex> ex(cuda_excl);
+          destroy_exec(lru);
+        }
         lk.lock();
         used_bytes -= lru->bytes;
         execs.erase(std::find_if(execs.begin(), execs.end(), [&](auto& e) { return e.get() == lru; }));
@@ -175,7 +183,11 @@ struct phgpu_server {
         e->kmax = kmax;
         execs.push_back(std::move(ex));
         lk.unlock();
-        const int r = create_exec(e, why);
+        int r;
+        {
+          std::lock_guard<std::mutex> ex(cuda_excl);
+          r = create_exec(e, why);
+        }
         lk.lock();
         used_bytes -= need;
         if (r != PHGPU_OK) {
@@ -257,11 +269,12 @@ struct phgpu_server {
         return rc;
       }
     }
-    if (cudaDeviceSynchronize() != cudaSuccess) {
+    if (cudaStreamSynchronize(e->st) != cudaSuccess) {
       *why = "executor set-up failed";
       destroy_exec(e);
       return PHGPU_ERR_CUDA;
     }
+    e->capture_failures.assign(e->kmax + 1, 0);
     return PHGPU_OK;
   }
 
@@ -371,6 +384,7 @@ struct phgpu_server {
   }
 
   int capture(Executor* e, int k, std::string* why) {
+    std::lock_guard<std::mutex> ex(cuda_excl);
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
       *why = "stream capture could not start";
@@ -422,12 +436,38 @@ struct phgpu_server {
       if (rc == PHGPU_OK) rc = phgpu_upload_cloud(e->slots[i], &wave[i]->s, 1, e->st);
       if (rc != PHGPU_OK) why = phgpu_last_error(e->slots[i]);
     }
-    if (rc == PHGPU_OK && !e->exec[k]) rc = capture(e, k, &why);
+    // capture the graph of a k-request wave on first use; CUDA work of other
+    // threads of the process that synchronises the device invalidates a
+    // capture, so after a failed capture the wave runs uncaptured (the same
+    // launches) and capturing is retried on later waves (twice at most)
+    bool direct = false;
+    if (rc == PHGPU_OK && !e->exec[k]) {
+      if (e->capture_failures[k] < 2 && capture(e, k, &why) == PHGPU_OK) {
+        why.clear();
+      } else {
+        ++e->capture_failures[k];
+        direct = true;
+        why.clear();
+        cudaGetLastError();
+      }
+    }
     if (rc == PHGPU_OK) {
-      if (cudaGraphLaunch(e->exec[k], e->st) != cudaSuccess || cudaEventRecord(e->ev_done, e->st) != cudaSuccess ||
-          cudaEventSynchronize(e->ev_done) != cudaSuccess) {
+      cudaError_t ce = cudaSuccess;
+      if (direct) {
+        rc = enqueue_wave(e, k);
+        if (rc != PHGPU_OK) why = phgpu_last_error(e->slots[0]);
+      } else {
+        ce = cudaGraphLaunch(e->exec[k], e->st);
+      }
+      if (rc == PHGPU_OK && ce == cudaSuccess) ce = cudaEventRecord(e->ev_done, e->st);
+      if (rc == PHGPU_OK && ce == cudaSuccess) ce = cudaEventSynchronize(e->ev_done);
+      if (rc == PHGPU_OK && ce != cudaSuccess) {
         rc = PHGPU_ERR_CUDA;
-        why = std::string("wave: ") + cudaGetErrorString(cudaGetLastError());
+        why = std::string("wave: ") + cudaGetErrorString(ce);
+      }
+      if (direct) {
+        std::lock_guard<std::mutex> lk(mu);
+        ++stats.direct_waves;
       }
     }
     uint64_t reruns = 0;

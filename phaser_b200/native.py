@@ -24,6 +24,7 @@ PHGPU_FUSION_NONE = 1
 PHGPU_FUSION_LOW_PASS = 2
 PHGPU_FLAG_KEEP_VOLUMES = 1
 PHGPU_SERVER_BORROW_HOST = 1
+PHGPU_FUSION_MIX = 3
 PHGPU_PRECISION_FP32 = 0
 PHGPU_PRECISION_TF32X3 = 1
 PHGPU_PRECISION_BF16X3 = 2
@@ -101,7 +102,7 @@ class ServerParams(C.Structure):
 
 
 class ServerStats(C.Structure):
-    _fields_ = [(n, C.c_uint64) for n in ("waves", "requests", "graph_captures", "evictions", "pose_reruns",
+    _fields_ = [(n, C.c_uint64) for n in ("waves", "requests", "graph_captures", "direct_waves", "evictions", "pose_reruns",
                                           "executors", "bytes_in_use")]
 
     def as_dict(self):
@@ -118,7 +119,7 @@ EXPORTED = [
     "phgpu_translation_from_index", "phgpu_server_create", "phgpu_server_destroy",
     "phgpu_server_submit", "phgpu_server_poll", "phgpu_server_drain", "phgpu_server_last_error",
     "phgpu_profile_enable", "phgpu_profile_read", "phgpu_profile_stage_count",
-    "phgpu_profile_stage_name", "phgpu_launch_count", "phgpu_selftest_fft",
+    "phgpu_profile_stage_name", "phgpu_launch_count",
     "phgpu_sample_s2_noalloc", "phgpu_bingham_peak", "phgpu_gaussian_peak", "phgpu_peak_window",
     "phgpu_ply_info", "phgpu_ply_read", "phgpu_ply_last_error", "phgpu_voxel_grid_create",
     "phgpu_voxel_grid_destroy", "phgpu_voxel_grid_filter", "phgpu_voxel_grid_last_error",
@@ -188,7 +189,6 @@ def load(path: str = LIB_PATH):
     lib.phgpu_peak_window.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
                                       C.POINTER(C.c_uint32)]
     lib.phgpu_peak_window.restype = None
-    lib.phgpu_selftest_fft.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
     lib.phgpu_sample_s2_noalloc.argtypes = [C.POINTER(Params), C.POINTER(Cloud), C.c_void_p, C.c_void_p,
                                             C.c_void_p]
     lib.phgpu_ply_info.argtypes = [C.c_char_p, C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
@@ -223,8 +223,29 @@ def _addr(a):
     return a.data_ptr()
 
 
+def _check_device_tensor(name, t, dtype, min_numel, device):
+    """A CUDA tensor the C ABI may write or read `min_numel` elements of."""
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise ValueError(f"{name}: expected a CUDA tensor")
+    if t.dtype != dtype:
+        raise ValueError(f"{name}: expected dtype {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name}: expected a contiguous tensor")
+    if t.numel() < min_numel:
+        raise ValueError(f"{name}: {t.numel()} elements, at least {min_numel} needed")
+    if device is not None and t.device != device:
+        raise ValueError(f"{name}: on {t.device}, expected {device}")
+
+
 def make_cloud(xyzi, reflectivity=None, ambient=None) -> tuple[Cloud, list]:
-    """Build a phgpu_cloud from numpy arrays (host) or torch CUDA tensors."""
+    """Build a phgpu_cloud from numpy arrays (host) or torch tensors.
+
+    CUDA tensors are passed to the device code as they are, so they are
+    checked first: xyzi float32 contiguous of shape (n, 4), reflectivity /
+    ambient None or float32 contiguous with at least n elements on the same
+    device (ValueError otherwise).  Host inputs are converted to contiguous
+    float32 and must have shape (n, 4) too."""
     keep = []
     on_dev = 0
     host_tensor = False
@@ -238,10 +259,26 @@ def make_cloud(xyzi, reflectivity=None, ambient=None) -> tuple[Cloud, list]:
                               and t.is_contiguous()) for t in (xyzi, reflectivity, ambient))
     except Exception:  # pragma: no cover - torch is always present here
         pass
-    if not on_dev and not host_tensor:
+    if on_dev:
+        import torch
+        if xyzi.dim() != 2 or xyzi.shape[1] != 4:
+            raise ValueError(f"xyzi: expected shape (n, 4), got {tuple(xyzi.shape)}")
+        _check_device_tensor("xyzi", xyzi, torch.float32, 4 * xyzi.shape[0], None)
+        for name, t in (("reflectivity", reflectivity), ("ambient", ambient)):
+            if t is not None:
+                _check_device_tensor(name, t, torch.float32, xyzi.shape[0], xyzi.device)
+    elif not host_tensor:
         xyzi = np.ascontiguousarray(xyzi, np.float32)
         reflectivity = None if reflectivity is None else np.ascontiguousarray(reflectivity, np.float32)
         ambient = None if ambient is None else np.ascontiguousarray(ambient, np.float32)
+    if not on_dev:
+        if xyzi.ndim != 2 or xyzi.shape[1] != 4:
+            raise ValueError(f"xyzi: expected shape (n, 4), got {tuple(xyzi.shape)}")
+        for name, t in (("reflectivity", reflectivity), ("ambient", ambient)):
+            if t is not None and (t.ndim != 1 or t.shape[0] < xyzi.shape[0]):
+                raise ValueError(f"{name}: expected at least {xyzi.shape[0]} values")
+            if t is not None and getattr(t, "is_cuda", False):
+                raise ValueError(f"{name}: on the device while xyzi is on the host")
     keep += [xyzi, reflectivity, ambient]
     n = int(xyzi.shape[0])
     c = Cloud(_addr(xyzi), _addr(reflectivity), _addr(ambient), n, on_dev)
@@ -252,8 +289,18 @@ def sample_s2_noalloc(params: Params, xyzi, reflectivity, ambient, values_dev, n
                       stream=None) -> int:
     """phgpu_sample_s2_noalloc on device tensors; returns the status code.
     values_dev: float32 CUDA tensor of 4 * 4bw^2, nn_index_dev: int32 of 4bw^2
-    or None; stream: a torch.cuda.Stream (None = legacy default stream)."""
+    or None; stream: a torch.cuda.Stream (None = legacy default stream).
+    Every tensor is checked before the call (ValueError): the cloud as in
+    make_cloud and on the device, the outputs on the cloud's device with
+    enough elements of the right type."""
+    import torch
+    if not (isinstance(xyzi, torch.Tensor) and xyzi.is_cuda):
+        raise ValueError("xyzi: phgpu_sample_s2_noalloc reads a CUDA tensor")
     c, keep = make_cloud(xyzi, reflectivity, ambient)
+    nq = 4 * params.spherical_bandwidth * params.spherical_bandwidth
+    _check_device_tensor("values_dev", values_dev, torch.float32, 4 * nq, xyzi.device)
+    if nn_index_dev is not None:
+        _check_device_tensor("nn_index_dev", nn_index_dev, torch.int32, nq, xyzi.device)
     return load().phgpu_sample_s2_noalloc(C.byref(params), C.byref(c), _addr(values_dev), _addr(nn_index_dev),
                                           None if stream is None else stream.cuda_stream)
 
@@ -287,16 +334,6 @@ def gaussian_peak(values, first_voxel, n_voxels, lower, upper):
     if rc != PHGPU_OK:
         raise PhgpuError(f"phgpu_gaussian_peak failed ({rc})")
     return mean, cov.reshape(3, 3)
-
-
-def selftest_fft(x: np.ndarray, inverse=False, columns=False, engine=2) -> np.ndarray:
-    """Run one of the shared-memory FFT engines on x (complex, [ntrans, n])."""
-    a = np.ascontiguousarray(x, np.complex64).copy()
-    ntrans, n = a.shape
-    rc = load().phgpu_selftest_fft(n, ntrans, 1 if inverse else 0, 1 if columns else 0, engine, a.ctypes.data)
-    if rc != PHGPU_OK:
-        raise PhgpuError(f"phgpu_selftest_fft failed ({rc})")
-    return a
 
 
 PHGPU_PLY_REFLECTIVITY = 1

@@ -192,3 +192,19 @@ CONFIG3_MIX = [
 def workload_pair(workload: int, k: int = 0) -> Pair:
     w = WORKLOADS[workload]
     return make_pair(workload, k, w["beams"], w["cols"], w["reflectivity"])
+
+
+def write_ply(path, xyzi, reflectivity=None):
+    """A scan as a binary little-endian PLY with the reference reader's field
+    names (x, y, z, intensity[, reflectivity]), float32."""
+    cols = [("x", 0), ("y", 1), ("z", 2), ("intensity", 3)]
+    head = ["ply", "format binary_little_endian 1.0", f"element vertex {len(xyzi)}"]
+    head += [f"property float {n}" for n, _ in cols]
+    data = [np.asarray(xyzi, np.float32)]
+    if reflectivity is not None:
+        head.append("property float reflectivity")
+        data.append(np.asarray(reflectivity, np.float32)[:, None])
+    head.append("end_header")
+    with open(path, "wb") as f:
+        f.write(("\n".join(head) + "\n").encode())
+        f.write(np.concatenate(data, axis=1).astype("<f4").tobytes())

@@ -82,6 +82,50 @@ int main() {
           f.getAveragedReflectivity() != 0.0)
         return 8;
   }
+  // SphRegistration's single signal: SphericalCorrelation::correlateSignals on
+  // the sampled FunctionValues of two clouds gives the bin SphRegistration
+  // registers them with; the Laplace class refuses the single signal
+  {
+    std::vector<float> a, b;
+    unsigned s = 777;
+    for (int i = 0; i < 3000; ++i) {
+      float p[4];
+      for (float& v : p) {
+        s = s * 1103515245u + 12345u;
+        v = ((s >> 8) & 0xffff) / 65535.0f * 8.0f - 4.0f;
+      }
+      p[3] = std::fabs(p[3]) / 4.0f;
+      a.insert(a.end(), p, p + 4);
+      b.insert(b.end(), {p[1], -p[0], p[2] + 0.5f, p[3]});  // rotated by 90 degrees about z, shifted
+    }
+    CloudView ca, cb;
+    ca.xyzi = a.data();
+    ca.n_points = 3000;
+    cb.xyzi = b.data();
+    cb.n_points = 3000;
+    phgpu_params prm = default_params();
+    prm.spherical_bandwidth = 16;
+    prm.spatial_n_voxels = 32;
+    prm.spatial_discretize_lower = -10;
+    prm.spatial_discretize_upper = 10;
+    SphericalSampler sampler(16, prm);
+    std::vector<FunctionValue> fa, fb;
+    sampler.sampleUniformly(ca, &fa);
+    sampler.sampleUniformly(cb, &fb);
+    SphericalCorrelation corr(16u, 0u, prm);
+    corr.correlateSignals(fa, fb);
+    SphRegistration reg(prm);
+    const phgpu_pose pose = reg.registerPointCloud(ca, cb);
+    std::printf("sph_registration_bin %u %u\n", corr.getPeakBin(), pose.rot_bin);
+    if (corr.getPeakBin() != pose.rot_bin) return 9;
+    SphericalCorrelationLaplace lap(16u, 0u, prm);
+    try {
+      lap.correlateSignals(fa, fb);
+      return 10;
+    } catch (const std::invalid_argument&) {
+      std::printf("laplace_refuses_single_signal\n");
+    }
+  }
   // VoxelGridCmd on a cloud of three points: leaves (0,0,0) and (2,0,0) at
   // leaf 0.25 (grid anchored at floor(min / leaf)); each leaf's mean is the
   // in-order float sum divided by the count

@@ -1,4 +1,10 @@
-// Self-test of the shared-memory FFT engines (phgpu_selftest_fft): one block
+// Test-only library (built by tests/test_gpu_fft_engines.py, linked against
+// the product library for the FFT plans): self-test of the shared-memory FFT
+// engines, phgpu_selftest_fft(n, ntrans, inverse, columns, engine, data),
+// which transforms ntrans sequences of length n (complex interleaved, natural
+// order, sequence-major, in place in `data`); engine 0 = runtime plan,
+// 1 = compile-time plan, 2 = register-tail plan.  Forward = exp(-2 pi i jk/n),
+// inverse = exp(+2 pi i jk/n), both unnormalised.  One block
 // transforms `ntrans` sequences of length n held in shared memory as rows
 // (stride n + 1) or columns (stride ntrans), through the runtime plan, the
 // compile-time plan or the register-tail plan.  Input and output are in
@@ -7,10 +13,13 @@
 
 #include <string>
 
-#include "../../include/phaser_gpu.h"
-#include "ctx.h"
+#include "phaser_gpu.h"
 #include "fft2.cuh"
 #include "kernels.h"
+
+namespace phgpu {
+bool make_fft_plan(int n, FftPlan* p, float2** d_tw, std::string* err);
+}
 
 namespace phgpu {
 

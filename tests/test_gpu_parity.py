@@ -255,6 +255,19 @@ def test_voxel_index_exact_with_edge_cases(nat, pair0):
     assert np.array_equal(lin, O.voxel_index(O.transform(pair0.source.xyzi, T), N, lo, hi))
 
 
+@pytest.mark.parametrize("N,lo,hi", [(64, -50, 40), (100, -20, 7), (50, 3, -9)])
+def test_voxel_index_exact_asymmetric_range(nat, pair0, N, lo, hi):
+    # |upper| < |lower|: Eigen's LinSpaced counts the edges down from the
+    # upper bound (and a reversed range, upper < lower, has no inside points)
+    c = ctx(nat, spatial_n_voxels=N, spatial_discretize_lower=lo, spatial_discretize_upper=hi)
+    e = O.edges(N, lo, hi)
+    edge = np.stack([np.array([v, v, v, 1.0], np.float32) for v in e[:: max(1, N // 8)]])
+    pts = np.concatenate([pair0.target.xyzi * np.float32(2.0), edge])
+    c.voxelize(pts, None, side=0)
+    lin = c.voxel_index(0, pts.shape[0])
+    assert np.array_equal(lin, O.voxel_index(pts, N, lo, hi))
+
+
 def _register_and_compare(nat, w, pair, want_volumes):
     c = ctx(nat, spherical_bandwidth=w["bw"], spatial_n_voxels=w["n_voxels"],
             spatial_discretize_lower=w["lo"], spatial_discretize_upper=w["hi"],

@@ -81,3 +81,23 @@ def test_context_creation_without_gpu_raises(native):
         pytest.skip("GPU present")
     with pytest.raises(native.PhgpuError):
         native.Context(spherical_bandwidth=8, spatial_n_voxels=8)
+
+
+def test_make_cloud_rejects_bad_host_inputs(native):
+    # arrays the C ABI would read out of bounds are refused before the call
+    good = np.zeros((10, 4), np.float32)
+    c, _ = native.make_cloud(good)
+    assert c.n_points == 10 and c.on_device == 0
+    with pytest.raises(ValueError):
+        native.make_cloud(np.zeros((10, 3), np.float32))
+    with pytest.raises(ValueError):
+        native.make_cloud(good, reflectivity=np.zeros(9, np.float32))
+    with pytest.raises(ValueError):
+        native.make_cloud(good, ambient=np.zeros((10, 2), np.float32))
+
+
+def test_noalloc_wrapper_rejects_host_cloud(native):
+    import torch
+    p = native.default_params(spherical_bandwidth=8)
+    with pytest.raises(ValueError):
+        native.sample_s2_noalloc(p, torch.zeros(10, 4), None, None, torch.zeros(4 * 256))

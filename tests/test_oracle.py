@@ -163,8 +163,47 @@ def test_histc_edges_and_aliasing():
     assert lin[3] == 0xFFFFFFFF
 
 
+@pytest.mark.parametrize("N,lo,hi", [(200, -10, 10), (64, -50, 40), (7, -3, 1), (101, 5, -7), (13, 0, 3)])
+def test_edges_follow_eigen_linspaced(N, lo, hi):
+    # Eigen >= 3.3 LinSpaced (float): counted down from hi when |hi| < |lo|
+    # (e[0] = lo, e[i] = hi - (N - 1 - i) step), up from lo otherwise
+    # (e[N - 1] = hi); step = (hi - lo) / (N - 1) in float
+    e = O.edges(N, lo, hi)
+    f32 = np.float32
+    step = (f32(hi) - f32(lo)) / f32(N - 1)
+    if abs(hi) < abs(lo):
+        want = [f32(lo)] + [f32(hi) - f32(N - 1 - i) * step for i in range(1, N)]
+    else:
+        want = [f32(lo) + f32(i) * step for i in range(N - 1)] + [f32(hi)]
+    np.testing.assert_array_equal(e, np.array(want, np.float32))
+    assert e[0] == f32(lo) and e[-1] == f32(hi)
+
+
 def test_translation_from_index():
     # translation-utils.cc:40-52, width = |lo| + |hi| + 1
     assert O.translation_from_index(0, 200, -10, 10) == 0.0
     assert O.translation_from_index(5, 200, -10, 10) == pytest.approx(5 * 21 / 200)
     assert O.translation_from_index(150, 200, -10, 10) == pytest.approx(-50 * 21 / 200)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("sph_mode", [0, 1])
+def test_oracle_registration_equals_reference_path(sph_mode):
+    # SphOptRegistration (mode 0) and SphRegistration's single 0.6 I + 0.4 R
+    # signal (mode 1): the FP64 restatement and the reference's SOFT sources
+    # driven by the restated glue give the same bin, voxel and pose
+    from phaser_b200 import scene
+    pair = scene.make_pair(0, 9, beams=16, cols=256)
+    args = (pair.target.xyzi, pair.target.reflectivity, pair.source.xyzi, pair.source.reflectivity, 8, 16, -10, 10)
+    rb, vx, pose6 = O.ref_register_pair(*args, threads=2, sph_mode=sph_mode)
+    pose = O.register_pair(*args, sph_mode=sph_mode)
+    assert (pose.rot_bin, pose.voxel) == (rb, vx)
+    assert list(pose.xyz) == list(pose6[:3]) and list(pose.trans) == list(pose6[3:])
+
+
+def test_mix_signal_is_the_reference_weighting():
+    # retrieveInterpolation (spherical-correlation.cc:103-112)
+    s = np.arange(8, dtype=np.float64).reshape(2, 4)  # channels {range, intensity}, 4 directions
+    out = np.zeros(4)
+    O.lib().orc_mix_signal(s.reshape(-1).ctypes.data, 4, out.ctypes.data)
+    np.testing.assert_array_equal(out, 0.6 * s[1] + 0.4 * s[0])
