@@ -201,47 +201,14 @@ def pair_bytes(bw, N, C, P):
     return rot + trans
 
 
-# DRAM read + write per stage call from the ncu capture summarised in
-# profiles/traffic_register_pair_B100_N200.md (sum over the stage's kernels).
-NCU_TRAFFIC_B100_N200 = {
-    "s2_sample": (2.16 + 0.17 + 2.71 + 4.44) * 1e6,          # project, bin_scan, bin_scatter, nn_rows
-    "sht": (0.98 + 5.01) * 1e6,                              # sht_phi, sht_leg (both clouds)
-    "fuse_s2": 0.32e6,
-    "so3_synth": (2.43 + 2.15) * 1e6,
-    "so3_fft": (31.86 + 32.03) * 1e6,                        # so3_fft_a, so3_c2r_tail
-    "voxelize": (8.24 + 0.84 + 0.31) * 1e6,                  # voxelize + clear
-    "spatial_fwd": (39.92 + 24.77) * 1e6,
-    "fuse_z": (200.50 + 20.38) * 1e6,
-    "spatial_inv": 33.35e6,
-}
-
-
-# Device-time share (%) of each stage's kernels in the same capture's launch
-# list (profiles/launches_register_pair_B100_N200.md; launches serialised, so
-# the overlap of the two clouds' streams, which the per-stage CUDA events
-# include, does not inflate any stage).
-NCU_SHARE_B100_N200 = {
-    "s2_sample": 9.1 + 2.8 + 2.7 + 1.8,                      # nn_rows, project, bin_scan, bin_scatter
-    "sht": 2.0 + 1.2,                                         # sht_leg, sht_phi
-    "fuse_s2": 1.3,
-    "so3_synth": 8.7,
-    "so3_fft": 5.3 + 3.6,                                     # so3_c2r_tail, so3_fft_a
-    "voxelize": 3.7 + 2.0,                                    # voxelize, clear_voxels
-    "spatial_fwd": 22.7,
-    "fuse_z": 21.4,
-    "spatial_inv": 8.8,
-}
-
-
-def dominant_stage(stage_ms, workload_is_bench):
-    """The stage the top-level roofline entry describes: on the bench workload
-    the one whose kernels take the largest share of device time in the ncu
-    launch list, otherwise the one with the largest event time."""
-    if workload_is_bench:
-        known = [k for k in stage_ms if k in NCU_SHARE_B100_N200]
-        if known:
-            return max(known, key=lambda k: NCU_SHARE_B100_N200[k])
-    return max(stage_ms, key=lambda k: stage_ms[k])
+# DRAM read + write per stage call (sum over the stage's kernels; per cloud for
+# the per-cloud stages), B = 100 / N = 200 workload, from one-kernel ncu
+# captures of the current kernels:
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#       --clock-control none -k regex:<kernel> -s <n> -c 1
+#       python bench.py --profile pair --workload 1 --pairs 2 --precision 1
+# None where no capture exists.
+NCU_TRAFFIC_B100_N200 = {}
 
 
 def measured_peak():
@@ -253,13 +220,18 @@ def measured_peak():
         return 6650.0, "fallback 6.65 TB/s"
 
 
-def roofline(nat, pool, params, served_value):
-    """Per-stage CUDA events (phgpu_profile_*, recorded on each stage's stream)
-    over registrations of the bench workload; the dominant stage is the
-    roofline entry, every stage is listed, and the whole pipeline is rated
-    with the per-pair algorithmic bytes at the served rate."""
+def roofline(nat, pool, params, tuning, served_value):
+    """Per-stage device time from CUDA events recorded on each stage's stream
+    while both halves of a registration run on one stream (so no two stages'
+    events overlap), on a context of the served form (tensor-core synthesis,
+    its tuning) registering the bench pairs one at a time.  Each stage is rated
+    by its algorithmic bytes (frac) and, where an ncu capture measured it, by
+    its DRAM traffic (frac_actual); the top-level entry is the stage with the
+    largest device time.  The whole pipeline is rated with the per-pair
+    algorithmic bytes at the served rate."""
     ctx = nat.Context(params)
-    ctx.profile(True)
+    ctx.set_tuning(tuning)
+    ctx.profile(True, serial=True)
     import torch
     dev = [((torch.from_numpy(p.target.xyzi).cuda(), torch.from_numpy(p.target.reflectivity).cuda()),
             (torch.from_numpy(p.source.xyzi).cuda(), torch.from_numpy(p.source.reflectivity).cuda()))
@@ -267,7 +239,7 @@ def roofline(nat, pool, params, served_value):
     for i in range(2):
         ctx.register_pair(*dev[i % len(dev)])
     ctx.profile_read()
-    nrep = 6
+    nrep = 8
     for i in range(nrep):
         ctx.register_pair(*dev[i % len(dev)])
     st = ctx.profile_read()
@@ -276,26 +248,32 @@ def roofline(nat, pool, params, served_value):
     P = int(np.mean([p.target.xyzi.shape[0] for p in pool]))
     peak, src = measured_peak()
     tot = {k: v for k, v in st.items() if v[1] > 0 and k != "upload"}
+    workload_is_bench = (bw, N) == (100, 200)
     stages = {}
     for k, (ms, calls) in tot.items():
         nb = stage_bytes(k, bw, N, C, P)
         per = ms / calls
-        e = {"ms_per_call": round(per, 4), "calls_per_pair": round(calls / nrep, 2)}
+        e = {"ms_per_call": round(per, 4), "calls_per_pair": round(calls / nrep, 2),
+             "ms_per_pair": round(ms / nrep, 4)}
         if nb:
             gbs = nb / (per * 1e-3) / 1e9
             e.update({"algorithmic_bytes": nb, "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)})
+        tr = NCU_TRAFFIC_B100_N200.get(k) if workload_is_bench else None
+        if tr:
+            e.update({"traffic": tr, "traffic_gbs": round(tr / (per * 1e-3) / 1e9, 1),
+                      "frac_actual": round(tr / (per * 1e-3) / 1e9 / peak, 4)})
         stages[k] = e
-    workload_is_bench = (bw, N) == (100, 200)
-    top = dominant_stage({k: v[0] for k, v in tot.items()}, workload_is_bench)
+    top = max(stages, key=lambda k: stages[k]["ms_per_pair"])
     e = stages[top]
     roof = {"kernel": top, "bound": "hbm", "achieved": e.get("achieved_gbs"), "peak": peak, "unit": "GB/s",
-            "frac": e.get("frac"),
-            "traffic": NCU_TRAFFIC_B100_N200.get(top) if workload_is_bench else None,
+            "frac": e.get("frac"), "traffic": e.get("traffic"), "frac_actual": e.get("frac_actual"),
             "peak_source": src, "algorithmic_bytes_per_launch": e.get("algorithmic_bytes"),
-            "avg_launch_ms": e["ms_per_call"], "stages": stages}
+            "avg_launch_ms": e["ms_per_call"], "timing": "CUDA events, stages serialised on one stream",
+            "stages": stages}
     pb = pair_bytes(bw, N, C, P)
     roof["pipeline"] = {"algorithmic_bytes_per_pair": pb, "achieved_gbs": round(served_value * pb / 1e9, 1),
                         "frac": round(served_value * pb / 1e9 / peak, 4),
+                        "device_ms_per_pair_serialised": round(sum(v["ms_per_pair"] for v in stages.values()), 4),
                         "basis": "served registrations/s x per-pair algorithmic bytes"}
     return roof
 
@@ -624,8 +602,18 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    # ---------------- autotuned launch parameters of both forms (cached per
+    # shape and device; the search times candidates on one pool pair)
+    from phaser_b200 import tuning as tuning_cache
+    sparams = nat.default_params(spherical_bandwidth=w["bw"], spatial_n_voxels=w["n_voxels"],
+                                 spatial_discretize_lower=w["lo"], spatial_discretize_upper=w["hi"],
+                                 max_points=1 << 18, device=local, precision=nat.PHGPU_PRECISION_TF32X3)
+    tuned_plain = tuning_cache.tuned(params, *dev[0])
+    tuned_served = tuning_cache.tuned(sparams, *dev[0])
+
     # ---------------- plain GPU pipeline (one pair at a time)
     ctx = nat.Context(params)
+    ctx.set_tuning(tuned_plain["tuning"])
     for i in range(W * S):
         ctx.register_pair(*dev[i % len(dev)])
     barrier()
@@ -649,9 +637,7 @@ def main():
     srv = nat.Server(max_wave=a.max_wave, lanes=a.lanes, hbm_budget_bytes=150 << 30, device=local,
                      flags=nat.PHGPU_SERVER_BORROW_HOST)
     # the served form: tensor-core (split-TF32) Wigner-d synthesis, batched per wave
-    sparams = nat.default_params(spherical_bandwidth=w["bw"], spatial_n_voxels=w["n_voxels"],
-                                 spatial_discretize_lower=w["lo"], spatial_discretize_upper=w["hi"],
-                                 max_points=1 << 18, device=local, precision=nat.PHGPU_PRECISION_TF32X3)
+    srv.set_tuning(sparams, tuned_served["tuning"])
 
     def served_round(inputs, n):
         tickets = [srv.submit(sparams, *inputs[i % len(inputs)]) for i in range(n)]
@@ -714,7 +700,7 @@ def main():
     barrier()
 
     # ---------------- roofline of the dominant stage (rank 0 context, profiled)
-    roof = roofline(nat, pool, params, value / world)
+    roof = roofline(nat, pool, sparams, tuned_served["tuning"], value / world)
 
     # ---------------- mixed shapes under Poisson arrivals (rank 0)
     mix = None
@@ -778,6 +764,7 @@ def main():
             "reference_parity": parity,
             "clocks": clocks,
             "gpu_launches": int(launches),
+            "tuning": {"plain": tuned_plain, "served": tuned_served},
             "ingest": ing,
             "mixed_arrivals": mix,
             "run_script_config": rsc,

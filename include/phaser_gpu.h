@@ -254,10 +254,38 @@ void phgpu_peak_window(uint32_t index, uint32_t n, uint32_t k, uint32_t* first, 
 double phgpu_translation_from_index(double index, uint32_t n_voxels, int32_t lower,
                                     int32_t upper);
 
+/* ------------------------------------------------------------------ tuning
+ * Launch parameters chosen per shape by the project's autotuner (no reference
+ * counterpart: the reference plans its FFTs with FFTW_ESTIMATE on every call,
+ * spherical-correlation.cc:122-206).  0 selects the built-in default.  Every
+ * value gives the same results except radix_order, which reorders the stages
+ * of runtime FFT plans (lengths other than 64, 128, 200, 256, 320 and 512) and
+ * so their FP32 rounding. */
+typedef struct {
+  uint32_t fuse_z_tile;    /* ky columns per block of the translation z pass: 2, 4, 8, 16 */
+  uint32_t so3_beta_tile;  /* betas per block of the SO(3) alpha transform: 8, 16, 32 */
+  uint32_t tc_chunk;       /* degrees per chunk of the tensor-core synthesis: 16, 32 */
+  uint32_t radix_order;    /* runtime FFT plans: 0 radix 8 first, 1 radix 4 first, 2 odd radices first */
+} phgpu_tuning;
+int phgpu_tuning_get(const phgpu_ctx* ctx, phgpu_tuning* out);
+/* PHGPU_ERR_INVALID for a value the context's shape cannot take. */
+int phgpu_tuning_set(phgpu_ctx* ctx, const phgpu_tuning* t);
+/* Coordinate search: the candidates of each parameter in turn, each timed on
+ * `reps` registrations of the given pair (after one warm-up) with this
+ * context's buffers by the per-stage CUDA events of the stage the parameter
+ * affects (the whole registration for the radix order).  Keeps the fastest on
+ * ctx and returns it with the registration's device time in ms (sum of the
+ * stage events) under it. */
+int phgpu_autotune(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_cloud* source, uint32_t reps,
+                   phgpu_tuning* best, double* ms_per_pair);
+
 /* ------------------------------------------------------------------ tracing
  * Per-stage device time measured with CUDA events on each stage's launching
  * stream (the reference times stages on the host clock,
  * phaser_common/include/phaser/common/statistic-utils.h:10-18). */
+/* enable 1: events on each stage's own stream (the two clouds' stages of a
+ * registration overlap, and so do their events); 2: the registration's two
+ * streams serialised on one, so every stage's events time it alone. */
 int phgpu_profile_enable(phgpu_ctx* ctx, int enable);
 /* Accumulated milliseconds and call counts per stage since the last read
  * (synchronises the context's streams; resets the accumulators). */
@@ -371,6 +399,9 @@ int phgpu_server_poll_volumes(phgpu_server* srv, uint64_t ticket, phgpu_pose* ou
 /* Blocks until every submitted request finished. */
 int phgpu_server_drain(phgpu_server* srv);
 int phgpu_server_get_stats(phgpu_server* srv, phgpu_server_stats* out);
+/* Tuning the server applies to executors created afterwards for the shape of
+ * `shape` (bandwidth, spherical zero padding, voxels, precision). */
+int phgpu_server_set_tuning(phgpu_server* srv, const phgpu_params* shape, const phgpu_tuning* t);
 const char* phgpu_server_last_error(const phgpu_server* srv);
 
 #ifdef __cplusplus

@@ -75,7 +75,7 @@ def _declare(lib):
     lib.orc_wigner_column.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, _f64p]
     lib.orc_so3_correlate.argtypes = [C.c_int, C.c_int, _f64p, _f64p, _f64p, _f64p, _f64p]
     lib.orc_spherical_correlation.argtypes = [C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_int,
-                                              _f64p, C.c_void_p, C.c_void_p]
+                                              C.c_void_p, C.c_void_p, C.c_void_p]
     lib.orc_spherical_volume.argtypes = [C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_int, _f64p]
     lib.orc_argmax.restype = C.c_uint64
     lib.orc_argmax.argtypes = [_f64p, C.c_uint64]
@@ -97,6 +97,8 @@ def _declare(lib):
     lib.orc_register_pair_k.argtypes = [_f32p, C.c_size_t, C.c_void_p, _f32p, C.c_size_t, C.c_void_p,
                                         C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint32, C.c_uint32,
                                         C.POINTER(Pose), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.orc_so3_correlate_slices.argtypes = [C.c_int, C.c_int, _f64p, _f64p, _f64p, _f64p, C.c_int, C.c_void_p,
+                                             _f64p]
     lib.orc_mix_signal.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
     lib.orc_register_pair_mode.argtypes = [_f32p, C.c_size_t, C.c_void_p, _f32p, C.c_size_t, C.c_void_p,
                                            C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint32, C.c_uint32,
@@ -279,11 +281,32 @@ def spherical_correlation(f, g, bw, bw_out=None, levels=5, return_fused=False):
     corr = np.zeros(n ** 3)
     ff = np.zeros(2 * bw * bw)
     gg = np.zeros(2 * bw * bw)
-    lib().orc_spherical_correlation(bw, bw_out, Cn, f.reshape(-1), g.reshape(-1), levels, corr,
+    lib().orc_spherical_correlation(bw, bw_out, Cn, f.reshape(-1), g.reshape(-1), levels, _ptr(corr),
                                     ff.ctypes.data_as(C.c_void_p), gg.ctypes.data_as(C.c_void_p))
     if return_fused:
         return corr, ff.view(np.complex128), gg.view(np.complex128)
     return corr
+
+
+def spherical_correlation_slices(f, g, bw, ks, bw_out=None, levels=5):
+    """|z|^2 of the Laplace-fused correlation at beta indices ks only:
+    [len(ks)][2 bw_out (alpha)][2 bw_out (gamma)], FP64."""
+    bw_out = bw if bw_out is None else bw_out
+    f = np.ascontiguousarray(f, np.float64)
+    g = np.ascontiguousarray(g, np.float64)
+    nc = bw * bw
+    ff = np.zeros(2 * nc)
+    gg = np.zeros(2 * nc)
+    # the fused spectra alone (no correlation volume)
+    lib().orc_spherical_correlation(bw, bw_out, f.shape[0], f.reshape(-1), g.reshape(-1), levels, None,
+                                    ff.ctypes.data_as(C.c_void_p), gg.ctypes.data_as(C.c_void_p))
+    ks = np.ascontiguousarray(ks, np.int32)
+    n = 2 * bw_out
+    out = np.zeros(len(ks) * n * n)
+    lib().orc_so3_correlate_slices(bw, bw_out, np.ascontiguousarray(ff[0::2]), np.ascontiguousarray(ff[1::2]),
+                                   np.ascontiguousarray(gg[0::2]), np.ascontiguousarray(gg[1::2]), len(ks),
+                                   ks.ctypes.data, out)
+    return out.reshape(len(ks), n, n)
 
 
 def spherical_volume(f, g, bw, bw_out=None, levels=5):

@@ -731,13 +731,16 @@ void orc_spherical_correlation(int bw, int bw_out, int C, const double* f,
       fused_g_re_im[2 * k + 1] = Gf_im[k];
     }
   }
-  const int n = 2 * bw_out;
-  const size_t nv = (size_t)n * n * n;
-  double* vol = (double*)malloc(sizeof(double) * 2 * nv);
-  orc_so3_correlate(bw, bw_out, Ff_re, Ff_im, Gf_re, Gf_im, vol);
-  for (size_t i = 0; i < nv; ++i)
-    corr[i] = vol[2 * i] * vol[2 * i] + vol[2 * i + 1] * vol[2 * i + 1];
-  free(vol);
+  /* corr NULL: the fused spectra alone */
+  if (corr) {
+    const int n = 2 * bw_out;
+    const size_t nv = (size_t)n * n * n;
+    double* vol = (double*)malloc(sizeof(double) * 2 * nv);
+    orc_so3_correlate(bw, bw_out, Ff_re, Ff_im, Gf_re, Gf_im, vol);
+    for (size_t i = 0; i < nv; ++i)
+      corr[i] = vol[2 * i] * vol[2 * i] + vol[2 * i + 1] * vol[2 * i + 1];
+    free(vol);
+  }
   free(fr);
   free(fi);
   free(gr);
@@ -746,6 +749,93 @@ void orc_spherical_correlation(int bw, int bw_out, int C, const double* f,
   free(Ff_im);
   free(Gf_re);
   free(Gf_im);
+}
+
+/* |z|^2 of the correlation at the listed beta indices only (the same
+ * coefficient product, Wigner-d recurrence and angle transforms as
+ * orc_so3_correlate, restricted to nk slices: [nk][alpha][gamma]), from the
+ * fused spectra of orc_spherical_correlation.  For bandwidths whose full
+ * FP64 volume is too large to evaluate. */
+void orc_so3_correlate_slices(int bw_in, int bw_out, const double* f_re, const double* f_im, const double* h_re,
+                              const double* h_im, int nk, const int* ks, double* out) {
+  const int n = 2 * bw_out;
+  const size_t n2 = (size_t)n * n;
+  cplx* sl_all = (cplx*)calloc((size_t)nk * n2, sizeof(cplx));
+#pragma omp parallel
+  {
+    double* d = (double*)malloc(sizeof(double) * (bw_in > 0 ? bw_in : 1));
+    double* fa = (double*)malloc(sizeof(double) * (bw_in + 1));
+    double* fb = (double*)malloc(sizeof(double) * (bw_in + 1));
+    double* sh = (double*)malloc(sizeof(double) * (bw_in + 1));
+#pragma omp for schedule(dynamic, 1)
+    for (int ai = 0; ai < 2 * bw_in - 1; ++ai) {
+      const int a = ai - (bw_in - 1);
+      for (int b = -(bw_in - 1); b <= bw_in - 1; ++b) {
+        if (!in_half(a, b)) continue;
+        const int j0 = abs(a) > abs(b) ? abs(a) : abs(b);
+        if (j0 >= bw_in) continue;
+        const int aidx = (a + n) % n, bidx = (b + n) % n;
+        const int caidx = (-a + n) % n, cbidx = (-b + n) % n;
+        wig_coeffs(a, b, bw_in, fa, fb, sh);
+        for (int s = 0; s < nk; ++s) {
+          const int k = ks[s];
+          const double beta = M_PI * (2.0 * k + 1.0) / (4.0 * bw_out);
+          wig_run(a, b, bw_in, beta, fa, fb, sh, d);
+          double sr = 0.0, si = 0.0;
+          for (int l = j0; l < bw_in; ++l) {
+            const int i1 = orc_seanindex(-a, l, bw_in);
+            const int i2 = orc_seanindex(-b, l, bw_in);
+            const double fr = f_re[i1], fi = f_im[i1];
+            const double sg = ((a + b) & 1) ? -1.0 : 1.0;
+            const double pr = sg * h_re[i2], pi = sg * -h_im[i2];
+            const double wn = 2.0 * M_PI * sqrt(2.0 / (2.0 * l + 1.0));
+            sr += wn * (fr * pr - fi * pi) * d[l - j0];
+            si += wn * (fr * pi + fi * pr) * d[l - j0];
+          }
+          cplx* sl = sl_all + (size_t)s * n2;
+          sl[(size_t)aidx * n + bidx].re = sr;
+          sl[(size_t)aidx * n + bidx].im = si;
+          if (!(a == 0 && b == 0)) {
+            sl[(size_t)caidx * n + cbidx].re = sr;
+            sl[(size_t)caidx * n + cbidx].im = -si;
+          }
+        }
+      }
+    }
+    free(d);
+    free(fa);
+    free(fb);
+    free(sh);
+  }
+  orc_fft_plan p;
+  plan_init(&p, n);
+  const double sc = (1.0 / (double)n) * ((double)bw_out / M_PI);
+#pragma omp parallel
+  {
+    cplx* row = (cplx*)malloc(sizeof(cplx) * n);
+    cplx* scr = (cplx*)malloc(sizeof(cplx) * n);
+#pragma omp for
+    for (int s = 0; s < nk; ++s) {
+      cplx* sl = sl_all + (size_t)s * n2;
+      for (int ai = 0; ai < n; ++ai) {
+        memcpy(row, sl + (size_t)ai * n, sizeof(cplx) * n);
+        fft_exec(&p, row, scr, -1);
+        memcpy(sl + (size_t)ai * n, row, sizeof(cplx) * n);
+      }
+      for (int bi = 0; bi < n; ++bi) {
+        for (int ai = 0; ai < n; ++ai) row[ai] = sl[(size_t)ai * n + bi];
+        fft_exec(&p, row, scr, -1);
+        for (int ai = 0; ai < n; ++ai) {
+          const double re = row[ai].re * sc, im = row[ai].im * sc;
+          out[(size_t)s * n2 + (size_t)ai * n + bi] = re * re + im * im;
+        }
+      }
+    }
+    free(row);
+    free(scr);
+  }
+  plan_free(&p);
+  free(sl_all);
 }
 
 /* Raw signed volume (real part) for error measurements. */

@@ -48,12 +48,18 @@ static thread_local std::string g_create_error;
 
 namespace phgpu {
 
-bool make_fft_plan(int n, FftPlan* p, float2** d_tw, std::string* err) {
-  memset(p, 0, sizeof(*p));
-  p->n = n;
+// Radix preference orders of runtime FFT plans (a tuned parameter): radix 8
+// first; radix 4 first; odd radices first.
+static const int kRadixOrders[3][8] = {{8, 4, 2, 5, 3, 7, 11, 13}, {4, 2, 8, 5, 3, 7, 11, 13},
+                                       {5, 3, 7, 11, 13, 8, 4, 2}};
+
+// Stages of a runtime plan of length n in radix order `order`; false when n
+// has a prime factor above the generic radix limit.
+bool fft_plan_radices(int n, int order, FftPlan* p) {
+  const int* pref = kRadixOrders[(order >= 0 && order < 3) ? order : 0];
   int m = n, ns = 0;
-  const int order[] = {8, 4, 2, 5, 3, 7, 11, 13};
-  for (int r : order) {
+  for (int i = 0; i < 8; ++i) {
+    const int r = pref[i];
     while (m % r == 0 && ns < kMaxFftStages) {
       p->radix[ns++] = r;
       m /= r;
@@ -65,16 +71,23 @@ bool make_fft_plan(int n, FftPlan* p, float2** d_tw, std::string* err) {
       m /= r;
     }
   }
-  if (m != 1 || n < 1) {
-    *err = "FFT length " + std::to_string(n) + " has a prime factor above " +
-           std::to_string(kMaxGenericRadix) + " (unsupported)";
-    return false;
-  }
+  if (m != 1 || n < 1) return false;
+  p->n = n;
   p->nstage = ns;
   int L = n;
   for (int s = 0; s < ns; ++s) {
     p->L[s] = L;
     L /= p->radix[s];
+  }
+  return true;
+}
+
+bool make_fft_plan(int n, FftPlan* p, float2** d_tw, std::string* err) {
+  memset(p, 0, sizeof(*p));
+  if (!fft_plan_radices(n, 0, p)) {
+    *err = "FFT length " + std::to_string(n) + " has a prime factor above " +
+           std::to_string(kMaxGenericRadix) + " (unsupported)";
+    return false;
   }
   std::vector<float2> tw(n);
   for (int t = 0; t < n; ++t) {
@@ -351,6 +364,7 @@ static const char* kStageNames[PS_COUNT] = {"upload", "s2_sample", "sht", "fuse_
 int phgpu_profile_enable(phgpu_ctx* ctx, int enable) {
   if (!ctx) return PHGPU_ERR_INVALID;
   ctx->prof_on = enable != 0;
+  ctx->prof_serial = enable == 2;
   return PHGPU_OK;
 }
 
@@ -787,6 +801,8 @@ So3Args so3_args(phgpu_ctx* ctx) {
   o.batch.out[0].S = ctx->d_S;
   o.batch.out[0].argmax = ctx->d_argmax;
   o.batch.out[0].volume = ctx->d_rotvol;
+  o.beta_tile = (int)ctx->tune.so3_beta_tile;
+  o.tc_chunk = (int)ctx->tune.tc_chunk;
   return o;
 }
 
@@ -1042,6 +1058,7 @@ static SpatialArgs spatial_args(phgpu_ctx* ctx, int n_data, int n_total, int lap
   a.argmax = ctx->d_argmax + 1;
   a.status = ctx->d_argmax + 2;
   a.volume = ctx->d_transvol;
+  a.fuse_tile = (int)ctx->tune.fuse_z_tile;
   return a;
 }
 
@@ -1214,7 +1231,9 @@ PairPlan pair_plan(const phgpu_ctx* ctx, bool t_refl, bool t_amb, bool s_refl, b
 }
 
 int phgpu_pair_front(phgpu_ctx* ctx, const PairPlan& pp) {
-  cudaStream_t s0 = ctx->s0, s1 = ctx->s1;
+  // serialised profiling: the target's translation side on s0 as well, so the
+  // per-stage events do not overlap
+  cudaStream_t s0 = ctx->s0, s1 = ctx->prof_serial ? ctx->s0 : ctx->s1;
   // target translation side overlaps the rotation stage
   CK(cudaEventRecord(ctx->ev_a, s0));
   CK(cudaStreamWaitEvent(s1, ctx->ev_a, 0));

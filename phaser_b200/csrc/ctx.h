@@ -95,6 +95,7 @@ struct phgpu_ctx {
   float* d_T = nullptr;                    // [12] source transform of the device pose kernel
   float* h_T = nullptr;                    // pinned copy of d_T
   unsigned long long pose_reruns = 0;      // translations redone with the host transform
+  phgpu_tuning tune{};                     // launch parameters (0 = built-in defaults)
   // point counts read by the kernels from device memory (the server's waves,
   // whose captured graphs take any count up to the capacity)
   bool dev_counts = false;
@@ -105,6 +106,7 @@ struct phgpu_ctx {
   bool have_rot = false, have_trans = false;
   // profiler
   bool prof_on = false;
+  bool prof_serial = false;  // profiling with both halves of a registration on one stream
   std::vector<ProfRec> prof_recs;
   std::vector<cudaEvent_t> ev_pool;
   double prof_ms[PS_COUNT] = {0};
@@ -152,5 +154,6 @@ phgpu::So3Table so3_table(phgpu_ctx* ctx);
 
 namespace phgpu {
 bool make_fft_plan(int n, FftPlan* p, float2** d_tw, std::string* err);
+bool fft_plan_radices(int n, int order, FftPlan* p);
 FusionBands make_bands(uint32_t n, int levels, float div);
 }  // namespace phgpu

@@ -137,13 +137,12 @@ void so3_beta_table(int bw_out, double* tab) {
   }
 }
 
-// Forward DFT over a (alpha) for one b and a tile of Wt betas.
-constexpr int kFftABetas = 16;
-
-template <int NF>
+// Forward DFT over a (alpha) for one b and a tile of Wt = 2^LOG2W betas
+// (8, 16 or 32: a tuned parameter, 16 by default).
+template <int NF, int LOG2W>
 __global__ void k_so3_fft_a(int bw_in, int bw_out, So3Batch bt, FftPlan plan) {
   extern __shared__ float2 tile[];  // [a][beta tile]
-  constexpr int Wt = kFftABetas;
+  constexpr int Wt = 1 << LOG2W;
   const int n = NF > 0 ? NF : 2 * bw_out;
   const int Bo = n / 2;
   const int b = blockIdx.y;
@@ -167,7 +166,7 @@ __global__ void k_so3_fft_a(int bw_in, int bw_out, So3Batch bt, FftPlan plan) {
       if (e0 + u * blockDim.x < n * Wt) tile[e0 + u * blockDim.x] = v[u];
   }
   __syncthreads();
-  fft_any<NF, false, 4>(tile, Wt, 1, Wt, plan);
+  fft_any<NF, false, LOG2W>(tile, Wt, 1, Wt, plan);
   for (int e = threadIdx.x; e < n * Wt; e += blockDim.x) {
     const int a = e / Wt, t = e % Wt;
     if (t < wt) S[(size_t)a * astride + t] = tile[e];
@@ -304,7 +303,9 @@ __global__ void __launch_bounds__(256) k_so3_c2r_tail(int bw_in, So3Batch bt, Ff
 template <int NF>
 static cudaError_t so3_attrs() {
   const int m = 227 * 1024;
-  cudaError_t e = cudaFuncSetAttribute(k_so3_fft_a<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+  cudaError_t e = cudaFuncSetAttribute(k_so3_fft_a<NF, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_so3_fft_a<NF, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_so3_fft_a<NF, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_so3_c2r<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, m);
   if constexpr (Tail<NF>::ok) {
     if (e == cudaSuccess)
@@ -352,14 +353,27 @@ static void launch_so3_c2r(const So3Args& a, int n, cudaStream_t st) {
   }
 }
 
+template <int NF>
+static void launch_so3_fft_a(const So3Args& a, int n, int wt, cudaStream_t st) {
+  dim3 g((n + wt - 1) / wt, a.bw_in, a.batch.count);
+  const size_t sm = (size_t)n * wt * sizeof(float2);
+  if (wt == 8)
+    k_so3_fft_a<NF, 3><<<g, 256, sm, st>>>(a.bw_in, a.bw_out, a.batch, *a.plan);
+  else if (wt == 32)
+    k_so3_fft_a<NF, 5><<<g, 256, sm, st>>>(a.bw_in, a.bw_out, a.batch, *a.plan);
+  else
+    k_so3_fft_a<NF, 4><<<g, 256, sm, st>>>(a.bw_in, a.bw_out, a.batch, *a.plan);
+}
+
+bool so3_beta_tile_ok(int bw_out, int wt) {
+  return (wt == 8 || wt == 16 || wt == 32) && (size_t)2 * bw_out * wt * sizeof(float2) <= 227u * 1024u;
+}
+
 cudaError_t launch_so3_fft(const So3Args& a, cudaStream_t st) {
   if (a.batch.count < 1 || a.batch.count > kMaxWave) return cudaErrorInvalidValue;
   const int n = 2 * a.bw_out;
-  dim3 g2((n + kFftABetas - 1) / kFftABetas, a.bw_in, a.batch.count);
-  PHGPU_DISPATCH_N(n,
-      k_so3_fft_a<NF><<<g2, 256, (size_t)n * kFftABetas * sizeof(float2), st>>>(a.bw_in, a.bw_out, a.batch,
-                                                                                 *a.plan);
-      launch_so3_c2r<NF>(a, n, st));
+  const int wt = so3_beta_tile_ok(a.bw_out, a.beta_tile) ? a.beta_tile : 16;
+  PHGPU_DISPATCH_N(n, launch_so3_fft_a<NF>(a, n, wt, st); launch_so3_c2r<NF>(a, n, st));
   count_launches(2);
   return cudaGetLastError();
 }

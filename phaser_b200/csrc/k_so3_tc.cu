@@ -68,7 +68,7 @@ struct TcGeom {
   uint32_t tcols;  // tensor-memory columns allocated
 };
 
-static bool tc_geom(int bw_out, int count, int precision, TcGeom* g) {
+static bool tc_geom(int bw_out, int count, int precision, TcGeom* g, int chunk = 0) {
   if (precision != kSo3Tf32x3 && precision != kSo3Bf16x3) return false;
   if (count < 1 || count > kMaxWave || bw_out < 1 || bw_out > 256) return false;
   g->precision = precision;
@@ -79,6 +79,7 @@ static bool tc_geom(int bw_out, int count, int precision, TcGeom* g) {
   if (g->nmt * g->N > 512) return false;
   const uint32_t ctrl = 1024;
   for (int KC : {32, 16}) {
+    if (chunk && KC != chunk) continue;
     g->KC = KC;
     g->a32 = (uint32_t)KC * g->MP * 4;
     g->aconv = g->a32;
@@ -87,7 +88,7 @@ static bool tc_geom(int bw_out, int count, int precision, TcGeom* g) {
     g->smem = kTcStages * g->stage + ctrl;
     if (g->smem <= 227u * 1024u) break;
   }
-  if (g->smem > 227u * 1024u) return false;
+  if (g->smem > 227u * 1024u || (chunk && g->KC != chunk)) return false;
   // at most one CTA per SM, so the tensor-memory allocation never waits
   if (g->smem < 116u * 1024u) g->smem = 116u * 1024u;
   uint32_t c = 32;
@@ -96,9 +97,9 @@ static bool tc_geom(int bw_out, int count, int precision, TcGeom* g) {
   return true;
 }
 
-bool so3_tc_supported(int bw_out, int count, int precision) {
+bool so3_tc_supported(int bw_out, int count, int precision, int chunk) {
   TcGeom g;
-  return tc_geom(bw_out, count, precision, &g);
+  return tc_geom(bw_out, count, precision, &g, chunk);
 }
 
 size_t so3_table_layout(int bw_in, int bw_out, std::vector<size_t>* off) {
@@ -459,7 +460,9 @@ cudaError_t so3_tc_init_attributes() {
 
 cudaError_t launch_so3_synth_tc(const So3Args& a, const So3Table& t, unsigned long long* status, cudaStream_t st) {
   TcGeom geo;
-  if (!tc_geom(a.bw_out, a.batch.count, t.precision, &geo)) return cudaErrorInvalidValue;
+  if (!tc_geom(a.bw_out, a.batch.count, t.precision, &geo, a.tc_chunk) &&
+      !tc_geom(a.bw_out, a.batch.count, t.precision, &geo))
+    return cudaErrorInvalidValue;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

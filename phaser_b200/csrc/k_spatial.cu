@@ -675,6 +675,16 @@ bool spatial_slab_path(int N) { return N == 64 || N == 128 || N == 200; }
   }
 
 // Tile width of the z pass: as many ky columns as fit (<= 8) in shared memory.
+static size_t fuse_z_smem(int N, int A, int wt) {
+  const int chunks = (N + 255) / 256;
+  const size_t rows = (size_t)chunks * ((N + chunks - 1) / chunks);
+  return rows * A * wt * sizeof(float2) + 16 + sizeof(FusionBands) + (size_t)N * sizeof(int);
+}
+
+bool fuse_z_tile_ok(int N, int A, int wt) {
+  return (wt == 2 || wt == 4 || wt == 8 || wt == 16) && fuse_z_smem(N, A, wt) <= (size_t)kMaxSmem;
+}
+
 static int fuse_z_tile(int N, int A) {
   // >= 2: the loader moves two complex per 16-byte access, and a bulk copy's
   // innermost extent must be a multiple of 16 bytes
@@ -726,7 +736,7 @@ cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t 
 cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st) {
   const int N = a.N, H2 = N / 2 + 1;
   const int A = a.laplace ? 2 * a.n_data_ch : 2;
-  const int wt = fuse_z_tile(N, A);
+  const int wt = fuse_z_tile_ok(N, A, a.fuse_tile) ? a.fuse_tile : fuse_z_tile(N, A);
   // bulk tensor copies of the [z][array][ky] tile (element = one complex)
   CUtensorMap tmap;
   memset(&tmap, 0, sizeof(tmap));

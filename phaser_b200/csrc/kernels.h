@@ -93,7 +93,10 @@ struct So3Args {
   const double* wig_tab;  // so3_wigner_table(bw_in): recurrence square roots, per-degree factors
   const FftPlan* plan;    // length 2 bw_out
   So3Batch batch;
+  int beta_tile = 0;      // betas per alpha-FFT block (8, 16, 32; 0 = 16): tuned
+  int tc_chunk = 0;       // degrees per tensor-core chunk (16, 32; 0 = the largest that fits): tuned
 };
+bool so3_beta_tile_ok(int bw_out, int wt);
 cudaError_t launch_so3_synth(const So3Args& a, cudaStream_t st);  // coefficient product + FP32 Wigner synthesis
 cudaError_t launch_so3_fft(const So3Args& a, cudaStream_t st);    // alpha FFT + gamma C2R + argmax
 cudaError_t so3_init_attributes();  // once per device
@@ -116,7 +119,7 @@ cudaError_t launch_so3_table(int bw_in, int bw_out, const double* beta_tab, cons
                              const size_t* class_off, float* table, cudaStream_t st);
 // Whether a launch of `count` requests fits the tensor-core kernel's shared
 // and tensor memory (bw_out <= 256, count <= kMaxWave).
-bool so3_tc_supported(int bw_out, int count, int precision);
+bool so3_tc_supported(int bw_out, int count, int precision, int chunk = 0);
 cudaError_t launch_so3_synth_tc(const So3Args& a, const So3Table& t, unsigned long long* status, cudaStream_t st);
 cudaError_t so3_tc_init_attributes();
 
@@ -177,7 +180,10 @@ struct SpatialArgs {
   float* volume;          // optional N^3 correlation, [z][x][y]
   unsigned long long* status;  // bit 0: a bulk-copy wait gave up (result invalid)
   uint32_t argmax_limit = 0;   // argmax over indices < limit (0: all)
+  int fuse_tile = 0;           // ky columns per k_fuse_z block (2, 4, 8, 16; 0 = widest with two blocks per SM): tuned
 };
+// Whether a k_fuse_z tile of wt ky columns fits shared memory for N and A arrays.
+bool fuse_z_tile_ok(int N, int A, int wt);
 cudaError_t launch_spatial_forward(const SpatialArgs& a, int side, cudaStream_t st);
 cudaError_t launch_spatial_combine(const SpatialArgs& a, cudaStream_t st);
 cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st);   // z FFTs + fusion + cross power

@@ -134,6 +134,8 @@ struct phgpu_server {
   // destroyed: allocation, frees and synchronous set-up calls synchronise the
   // device, which would invalidate a capture running in another lane.
   std::mutex cuda_excl;
+  // tunings by (bandwidth, spherical zero padding, voxels, precision)
+  std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, phgpu_tuning> tunings;
   uint64_t next_ticket = 1;
   uint64_t used_bytes = 0;
   size_t in_flight = 0;
@@ -237,6 +239,12 @@ struct phgpu_server {
       }
       e->slots.push_back(c);
       e->bytes += c->device_bytes;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = tunings.find(std::make_tuple(p.spherical_bandwidth, p.spherical_zero_padding, p.spatial_n_voxels,
+                                               e->prm.precision));
+        if (it != tunings.end()) phgpu_tuning_set(c, &it->second);
+      }
       // point counts from device memory (any count up to the capacity replays
       // the same graph); grids zeroed once, the graph's clears keep them so
       c->dev_counts = true;
@@ -704,6 +712,14 @@ int phgpu_server_get_stats(phgpu_server* s, phgpu_server_stats* out) {
   *out = s->stats;
   out->executors = (uint64_t)s->execs.size();
   out->bytes_in_use = s->used_bytes;
+  return PHGPU_OK;
+}
+
+int phgpu_server_set_tuning(phgpu_server* s, const phgpu_params* shape, const phgpu_tuning* t) {
+  if (!s || !shape || !t) return PHGPU_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->tunings[std::make_tuple(shape->spherical_bandwidth, shape->spherical_zero_padding, shape->spatial_n_voxels,
+                             shape->precision)] = *t;
   return PHGPU_OK;
 }
 

@@ -101,6 +101,17 @@ class ServerParams(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("fuse_z_tile", "so3_beta_tile", "tc_chunk", "radix_order")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+    @classmethod
+    def from_dict(cls, d):
+        return cls(*[int(d.get(n, 0)) for n, _ in cls._fields_])
+
+
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("waves", "requests", "graph_captures", "direct_waves", "evictions", "pose_reruns",
                                           "executors", "bytes_in_use")]
@@ -124,7 +135,8 @@ EXPORTED = [
     "phgpu_ply_info", "phgpu_ply_read", "phgpu_ply_last_error", "phgpu_voxel_grid_create",
     "phgpu_voxel_grid_destroy", "phgpu_voxel_grid_filter", "phgpu_voxel_grid_last_error",
     "phgpu_spatial_correlation_size", "phgpu_pose_reruns", "phgpu_server_poll_volumes",
-    "phgpu_server_get_stats",
+    "phgpu_server_get_stats", "phgpu_tuning_get", "phgpu_tuning_set", "phgpu_autotune",
+    "phgpu_server_set_tuning",
 ]
 
 _LIB = None
@@ -172,6 +184,11 @@ def load(path: str = LIB_PATH):
     lib.phgpu_server_drain.argtypes = [vp]
     lib.phgpu_server_poll_volumes.argtypes = [vp, C.c_uint64, C.POINTER(Pose), C.POINTER(C.c_double), vp, vp]
     lib.phgpu_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
+    lib.phgpu_tuning_get.argtypes = [vp, C.POINTER(Tuning)]
+    lib.phgpu_tuning_set.argtypes = [vp, C.POINTER(Tuning)]
+    lib.phgpu_autotune.argtypes = [vp, C.POINTER(Cloud), C.POINTER(Cloud), C.c_uint32, C.POINTER(Tuning),
+                                   C.POINTER(C.c_double)]
+    lib.phgpu_server_set_tuning.argtypes = [vp, C.POINTER(Params), C.POINTER(Tuning)]
     lib.phgpu_server_last_error.restype = C.c_char_p
     lib.phgpu_server_last_error.argtypes = [vp]
     lib.phgpu_profile_enable.argtypes = [vp, C.c_int]
@@ -510,8 +527,10 @@ class Context:
         return self.lib.phgpu_stream(self.h)
 
     # ---- tracing
-    def profile(self, enable=True):
-        self.check(self.lib.phgpu_profile_enable(self.h, 1 if enable else 0))
+    def profile(self, enable=True, serial=False):
+        """Per-stage CUDA events; serial=True puts both halves of a
+        registration on one stream so the stage times do not overlap."""
+        self.check(self.lib.phgpu_profile_enable(self.h, (2 if serial else 1) if enable else 0))
 
     def profile_read(self):
         n = self.lib.phgpu_profile_stage_count()
@@ -585,6 +604,26 @@ class Context:
         return (v.value, pk.value, vol) if volume else (v.value, pk.value)
 
     # ---- full pipeline
+    # ---- tuning
+    def tuning(self) -> dict:
+        t = Tuning()
+        self.check(self.lib.phgpu_tuning_get(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, tuning: dict):
+        t = Tuning.from_dict(tuning)
+        self.check(self.lib.phgpu_tuning_set(self.h, C.byref(t)))
+
+    def autotune(self, target, source, reps=3):
+        """Coordinate search over the launch parameters on this pair; keeps and
+        returns the fastest (dict) and the registration's device ms under it."""
+        ct, k1 = make_cloud(*target)
+        cs, k2 = make_cloud(*source)
+        t = Tuning()
+        ms = C.c_double()
+        self.check(self.lib.phgpu_autotune(self.h, C.byref(ct), C.byref(cs), int(reps), C.byref(t), C.byref(ms)))
+        return t.as_dict(), ms.value
+
     def pose_reruns(self) -> int:
         """Translations register_pair redid with the host transform."""
         return int(self.lib.phgpu_pose_reruns(self.h))
@@ -652,6 +691,12 @@ class Server:
         if volumes:
             return pose, lat.value, rv, tv
         return pose, lat.value
+
+    def set_tuning(self, params: Params, tuning: dict):
+        t = Tuning.from_dict(tuning)
+        rc = self.lib.phgpu_server_set_tuning(self.h, C.byref(params), C.byref(t))
+        if rc != PHGPU_OK:
+            raise PhgpuError(f"set_tuning failed ({rc})")
 
     def stats(self) -> dict:
         st = ServerStats()

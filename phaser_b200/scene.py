@@ -189,6 +189,38 @@ CONFIG3_MIX = [
 ]
 
 
+# Batched workload: independent pairs of the room generator, pair k with its
+# own seed (1000 * 2 + k), a beam count from {32, 64, 128} x 1024 columns, B
+# from {32, 64, 100, 128} and N from {64, 128, 200} over [-10, 10]^3 m, all
+# drawn uniformly from a stream of its own per pair.
+CONFIG2_BEAMS = (32, 64, 128)
+CONFIG2_B = (32, 64, 100, 128)
+CONFIG2_N = (64, 128, 200)
+
+
+def config2_specs(n: int = 256) -> list[dict]:
+    out = []
+    for k in range(n):
+        rng = np.random.default_rng([2000 + k, 7])
+        out.append(dict(k=k, beams=int(rng.choice(CONFIG2_BEAMS)), bw=int(rng.choice(CONFIG2_B)),
+                        n_voxels=int(rng.choice(CONFIG2_N)), lo=-10, hi=10))
+    return out
+
+
+def _config2_pair(spec):
+    return make_pair(2, spec["k"], spec["beams"])
+
+
+def config2_pairs(specs, processes: int | None = None) -> list[Pair]:
+    """The pairs of config2_specs, generated in spawned processes (safe in a
+    process that already uses the GPU)."""
+    import multiprocessing as mp
+    import os
+    n = processes or min(len(specs), os.cpu_count() or 1)
+    with mp.get_context("spawn").Pool(n) as pool:
+        return pool.map(_config2_pair, specs)
+
+
 def workload_pair(workload: int, k: int = 0) -> Pair:
     w = WORKLOADS[workload]
     return make_pair(workload, k, w["beams"], w["cols"], w["reflectivity"])

@@ -101,3 +101,16 @@ def test_noalloc_wrapper_rejects_host_cloud(native):
     p = native.default_params(spherical_bandwidth=8)
     with pytest.raises(ValueError):
         native.sample_s2_noalloc(p, torch.zeros(10, 4), None, None, torch.zeros(4 * 256))
+
+
+def test_tuning_cache_round_trip(native, tmp_path):
+    from phaser_b200 import tuning
+    p = native.default_params(spherical_bandwidth=100, spatial_n_voxels=200, precision=1)
+    path = str(tmp_path / "t.json")
+    assert tuning.load(p, "B200", path) is None
+    tuning.save(p, "B200", {"fuse_z_tile": 4, "so3_beta_tile": 16, "tc_chunk": 32, "radix_order": 0}, 0.5, path)
+    hit = tuning.load(p, "B200", path)
+    assert hit["tuning"]["fuse_z_tile"] == 4 and hit["ms_per_pair"] == 0.5
+    assert tuning.load(p, "other", path) is None
+    p2 = native.default_params(spherical_bandwidth=100, spatial_n_voxels=200, precision=0)
+    assert tuning.load(p2, "B200", path) is None
