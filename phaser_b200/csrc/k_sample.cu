@@ -365,6 +365,7 @@ k_nn_rows(int n2b, const float4* __restrict__ grid, const float4* __restrict__ s
 // ---------------------------------------------------------------- launcher
 
 std::atomic<unsigned long long> g_launch_count{0};
+thread_local int g_capture_depth = 0;
 
 namespace {
 int grid_side(int max_queries) {

@@ -15,7 +15,12 @@ namespace phgpu {
 
 // Number of kernels this library has launched (all contexts).
 extern std::atomic<unsigned long long> g_launch_count;
-inline void count_launches(int n) { g_launch_count.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+// > 0 while this thread captures a CUDA graph (its kernels are counted when
+// the graph is launched)
+extern thread_local int g_capture_depth;
+inline void count_launches(int n) {
+  if (!g_capture_depth) g_launch_count.fetch_add((unsigned long long)n, std::memory_order_relaxed);
+}
 
 // ------------------------------------------------------------ S^2 sampling
 struct SampleArgs {

@@ -112,6 +112,7 @@ struct Executor {
   std::vector<cudaEvent_t> ev_join;
   std::vector<cudaGraphExec_t> exec;  // [k] wave of k requests
   std::vector<int> capture_failures;  // [k] captures of a k-request wave that were invalidated
+  std::vector<unsigned long long> graph_kernels;  // [k] kernels in the graph of a k-request wave
   std::shared_ptr<Table> table;
   uint64_t bytes = 0;
   bool busy = false;
@@ -139,6 +140,7 @@ struct phgpu_server {
   uint64_t next_ticket = 1;
   uint64_t used_bytes = 0;
   size_t in_flight = 0;
+  int running = 0;  // lanes running a wave
   bool stop = false;
   std::string err;
   phgpu_server_stats stats{};
@@ -283,6 +285,7 @@ struct phgpu_server {
       return PHGPU_ERR_CUDA;
     }
     e->capture_failures.assign(e->kmax + 1, 0);
+    e->graph_kernels.assign(e->kmax + 1, 0);
     return PHGPU_OK;
   }
 
@@ -398,8 +401,22 @@ struct phgpu_server {
       *why = "stream capture could not start";
       return PHGPU_ERR_CUDA;
     }
+    ++g_capture_depth;
     const int rc = enqueue_wave(e, k);
+    --g_capture_depth;
     const cudaError_t ce = cudaStreamEndCapture(e->st, &g);
+    // the graph's kernels run (and are counted) at each replay
+    unsigned long long kernels = 0;
+    size_t nn = 0;
+    if (g && cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn) {
+      std::vector<cudaGraphNode_t> nodes(nn);
+      cudaGraphGetNodes(g, nodes.data(), &nn);
+      for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType ty;
+        if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++kernels;
+      }
+    }
+    e->graph_kernels[k] = kernels;
     if (rc != PHGPU_OK || ce != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
       *why = rc != PHGPU_OK ? std::string("wave capture: ") + phgpu_last_error(e->slots[0])
@@ -466,6 +483,7 @@ struct phgpu_server {
         if (rc != PHGPU_OK) why = phgpu_last_error(e->slots[0]);
       } else {
         ce = cudaGraphLaunch(e->exec[k], e->st);
+        count_launches((int)e->graph_kernels[k]);
       }
       if (rc == PHGPU_OK && ce == cudaSuccess) ce = cudaEventRecord(e->ev_done, e->st);
       if (rc == PHGPU_OK && ce == cudaSuccess) ce = cudaEventSynchronize(e->ev_done);
@@ -517,10 +535,30 @@ struct phgpu_server {
         std::unique_lock<std::mutex> lk(mu);
         cv_work.wait(lk, [&] { return stop || !queue.empty(); });
         if (stop && queue.empty()) break;
+        const size_t kmax = std::max<uint32_t>(1u, std::min<uint32_t>(prm.max_wave, kMaxWave));
+        // Dynamic batching: while another lane's wave is on the GPU, a partial
+        // wave is held back so the queue can fill it -- until the oldest
+        // request's shape has max_wave requests queued, no wave runs, or the
+        // oldest request has waited max_delay_us.  An idle GPU starts at once.
+        for (;;) {
+          if (stop || queue.empty()) break;
+          const ShapeKey k0 = key_of(queue.front()->prm, queue.front()->t, queue.front()->s);
+          size_t same = 0;
+          for (Request* r : queue)
+            if (key_of(r->prm, r->t, r->s) == k0 && ++same >= kmax) break;
+          if (same >= kmax || running == 0) break;
+          const auto waited = Clock::now() - queue.front()->t_submit;
+          const auto limit = std::chrono::microseconds(prm.max_delay_us);
+          if (waited >= limit) break;
+          cv_work.wait_for(lk, limit - waited);
+        }
+        if (queue.empty()) {
+          if (stop) break;
+          continue;
+        }
         // the oldest request and every queued request of its key, up to max_wave
         Request* first = queue.front();
         key = key_of(first->prm, first->t, first->s);
-        const size_t kmax = std::max<uint32_t>(1u, std::min<uint32_t>(prm.max_wave, kMaxWave));
         for (auto it = queue.begin(); it != queue.end() && wave.size() < kmax;) {
           if (key_of((*it)->prm, (*it)->t, (*it)->s) == key) {
             wave.push_back(*it);
@@ -546,9 +584,12 @@ struct phgpu_server {
           wave.resize(e->kmax);
           cv_work.notify_one();
         }
+        ++running;
         lk.unlock();
         run_wave(e, wave);
         lk.lock();
+        --running;
+        cv_work.notify_all();
         release(e);
         for (Request* r : wave) finish(r);
       }
@@ -577,6 +618,7 @@ int phgpu_server_create(const phgpu_server_params* params, phgpu_server** out) {
   if (s->prm.max_points == 0) s->prm.max_points = 1u << 18;
   if (s->prm.hbm_budget_bytes == 0) s->prm.hbm_budget_bytes = 150ull << 30;
   if (s->prm.lanes == 0) s->prm.lanes = 2;
+  if (s->prm.max_delay_us == 0) s->prm.max_delay_us = 1000;
   for (uint32_t w = 0; w < s->prm.lanes; ++w) s->workers.emplace_back(&phgpu_server::worker_main, s);
   *out = s;
   return PHGPU_OK;

@@ -98,6 +98,7 @@ class ServerParams(C.Structure):
         ("device", C.c_int32),
         ("flags", C.c_uint32),
         ("lanes", C.c_uint32),
+        ("max_delay_us", C.c_uint32),
     ]
 
 
@@ -641,10 +642,12 @@ class Server:
     """Continuous-batching request server (C ABI phgpu_server_*): waves of up
     to max_wave same-shape pairs, `lanes` waves in flight."""
 
-    def __init__(self, max_wave=16, hbm_budget_bytes=150 << 30, max_points=1 << 18, device=0, flags=0, lanes=2):
+    def __init__(self, max_wave=16, hbm_budget_bytes=150 << 30, max_points=1 << 18, device=0, flags=0, lanes=2,
+                 max_delay_us=1000):
         lib = load()
         self.lib = lib
-        sp = ServerParams(int(hbm_budget_bytes), int(max_wave), int(max_points), int(device), int(flags), int(lanes))
+        sp = ServerParams(int(hbm_budget_bytes), int(max_wave), int(max_points), int(device), int(flags), int(lanes),
+                          int(max_delay_us))
         h = C.c_void_p()
         rc = lib.phgpu_server_create(C.byref(sp), C.byref(h))
         if rc != PHGPU_OK:

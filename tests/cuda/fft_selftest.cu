@@ -85,7 +85,7 @@ static cudaError_t run_selftest(int n, int ntrans, int inverse, int columns, con
 
 using namespace phgpu;
 
-int phgpu_selftest_fft(int n, int ntrans, int inverse, int columns, int engine, float* data) {
+extern "C" int phgpu_selftest_fft(int n, int ntrans, int inverse, int columns, int engine, float* data) {
   if (n < 1 || ntrans < 1 || !data || (size_t)ntrans * (n + 1) * sizeof(float2) > 227 * 1024) return PHGPU_ERR_INVALID;
   FftPlan p;
   float2* tw = nullptr;
