@@ -479,7 +479,9 @@ static int ensure_cloud_capacity(phgpu_ctx* ctx, uint32_t n) {
   return PHGPU_OK;
 }
 
-int phgpu_ctx_create(const phgpu_params* prm, phgpu_ctx** out) {
+int phgpu_ctx_create(const phgpu_params* prm, phgpu_ctx** out) { return phgpu_ctx_create_internal(prm, out, true); }
+
+int phgpu_ctx_create_internal(const phgpu_params* prm, phgpu_ctx** out, bool wigner_table) {
   if (!prm || !out) {
     g_create_error = "null argument";
     return PHGPU_ERR_INVALID;
@@ -499,6 +501,7 @@ int phgpu_ctx_create(const phgpu_params* prm, phgpu_ctx** out) {
   }
   phgpu_ctx* ctx = new phgpu_ctx();
   ctx->prm = *prm;
+  ctx->own_wigner_table = wigner_table;
   ctx->bw = bw;
   ctx->bw_out = bw_out;
   ctx->N = N;
@@ -592,6 +595,14 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
   CK(cudaMemcpy(ctx->d_weights, w.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
   CKV(dalloc(ctx, &ctx->d_legendre, sizeof(float) * legendre_table_entries(bw)));
   CK(launch_legendre_table(bw, ctx->d_weights, ctx->d_legendre, ctx->s0));
+  if (prm->precision != PHGPU_PRECISION_FP32) {
+    if (!sht_leg_tc_supported(bw, 1, (int)prm->precision)) {
+      ctx->err = "the tensor-core Legendre contraction supports bandwidths <= 256";
+      return PHGPU_ERR_INVALID;
+    }
+    CKV(dalloc(ctx, &ctx->d_legendre_tc, sizeof(float) * legendre_tc_floats(bw)));
+    CK(launch_legendre_tc_layout(bw, ctx->d_legendre, ctx->d_legendre_tc, ctx->s0));
+  }
   // histc edges (phase-aligner.cc:27-30): float LinSpaced of Eigen >= 3.3,
   // which counts down from the high end when |hi| < |lo|
   std::vector<float> e(N);
@@ -633,7 +644,7 @@ int phgpu_ctx_init(phgpu_ctx* ctx) {
     CKV(dalloc(ctx, &ctx->d_wig_tab, sizeof(double) * wt.size()));
     CK(cudaMemcpy(ctx->d_wig_tab, wt.data(), sizeof(double) * wt.size(), cudaMemcpyHostToDevice));
   }
-  if (prm->precision != PHGPU_PRECISION_FP32) {
+  if (prm->precision != PHGPU_PRECISION_FP32 && ctx->own_wigner_table) {
     // tensor-core synthesis: the Wigner-d table, generated once in FP64
     if (!so3_tc_supported(bw_out, 1, (int)prm->precision)) {
       ctx->err = "the tensor-core SO(3) synthesis supports bandwidth + spherical zero padding <= 256";
@@ -817,23 +828,28 @@ So3Table so3_table(phgpu_ctx* ctx) {
 // Spherical correlation of the sample grids currently in d_samples.
 // SHT of both sides' sample grids and their fusion (up to the fused spectra);
 // resets the rotation argmax.
-int phgpu_run_sph_front(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st, bool mix) {
-  const int bw = ctx->bw;
-  const size_t nq = (size_t)4 * bw * bw;
-  if (mix) CK(launch_mix_signal(ctx->d_samples, 4 * nq, (int)nq, ctx->d_mix, st));
-  {
-    ShtArgs s;
-    s.bw = bw;
-    s.n_data = mix ? 1 : n_data;
-    s.side_stride = mix ? nq : 4 * nq;
-    s.signal = mix ? ctx->d_mix : ctx->d_samples;
-    s.plan = &ctx->plan_s2;
-    s.table = ctx->d_legendre;
-    s.fphi = ctx->d_fphi;
-    s.coef = ctx->d_coef;
-    ProfScope ps(ctx, st, PS_SHT);
-    CK(launch_sht(s, st));
+static ShtArgs sht_args(phgpu_ctx* ctx, int n_data, bool mix) {
+  const size_t nq = (size_t)4 * ctx->bw * ctx->bw;
+  ShtArgs s;
+  s.bw = ctx->bw;
+  s.n_data = mix ? 1 : n_data;
+  s.side_stride = mix ? nq : 4 * nq;
+  s.signal = mix ? ctx->d_mix : ctx->d_samples;
+  s.plan = &ctx->plan_s2;
+  s.table = ctx->d_legendre;
+  s.fphi = ctx->d_fphi;
+  s.coef = ctx->d_coef;
+  if (ctx->prm.precision != PHGPU_PRECISION_FP32) {
+    s.table_tc = ctx->d_legendre_tc;
+    s.precision = (int)ctx->prm.precision;
+    s.tc_chunk = (int)ctx->tune.tc_chunk;
+    s.status = ctx->d_argmax + 2;
   }
+  return s;
+}
+
+static FuseS2Args fuse_args(phgpu_ctx* ctx, int n_data, int n_total, int laplace) {
+  const int bw = ctx->bw;
   FuseS2Args f;
   f.bw = bw;
   f.lowpass = (!laplace && ctx->prm.spherical_fusion == PHGPU_FUSION_LOW_PASS) ? 1 : 0;
@@ -845,9 +861,58 @@ int phgpu_run_sph_front(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cu
   f.bands = ctx->bands_s2;
   f.coef = ctx->d_coef;
   f.fused = ctx->d_fused;
+  return f;
+}
+
+// Sampled grids to the phi transform alone (the Legendre contraction and the
+// fusion then run batched across a wave, phgpu_run_sph_leg_fuse_batch).
+int phgpu_run_sph_phi(phgpu_ctx* ctx, int n_data, cudaStream_t st, bool mix) {
+  const size_t nq = (size_t)4 * ctx->bw * ctx->bw;
+  if (mix) CK(launch_mix_signal(ctx->d_samples, 4 * nq, (int)nq, ctx->d_mix, st));
+  ProfScope ps(ctx, st, PS_SHT);
+  CK(launch_sht_phi(sht_args(ctx, n_data, mix), st));
+  return PHGPU_OK;
+}
+
+int phgpu_run_sph_leg_fuse_batch(phgpu_ctx* const* ctx, int k, int n_data, int n_total, int laplace, bool mix,
+                                 cudaStream_t st) {
+  phgpu_ctx* c0 = ctx[0];
+  if (k < 1 || k > kMaxWave || c0->prm.precision == PHGPU_PRECISION_FP32) return PHGPU_ERR_INVALID;
+  const ShtArgs s = sht_args(c0, n_data, mix);
+  ShtBatch b;
+  b.count = k;
+  for (int i = 0; i < k; ++i) {
+    b.fphi[i] = ctx[i]->d_fphi;
+    b.coef[i] = ctx[i]->d_coef;
+  }
+  {
+    ProfScope ps(c0, st, PS_SHT);
+    CKC(c0, launch_sht_leg_tc(s.bw, s.n_data, b, s.table_tc, s.precision, s.tc_chunk, s.status, st));
+  }
+  FuseS2Args f = fuse_args(c0, mix ? 1 : n_data, n_total, laplace);
+  f.count = k;
+  for (int i = 0; i < k; ++i) {
+    f.coef_b[i] = ctx[i]->d_coef;
+    f.fused_b[i] = ctx[i]->d_fused;
+  }
+  {
+    ProfScope ps(c0, st, PS_FUSE_S2);
+    CKC(c0, launch_fuse_s2(f, st));
+  }
+  for (int i = 0; i < k; ++i) CKC(c0, cudaMemsetAsync(ctx[i]->d_argmax, 0, sizeof(unsigned long long), st));
+  return PHGPU_OK;
+}
+
+int phgpu_run_sph_front(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st, bool mix) {
+  const size_t nq = (size_t)4 * ctx->bw * ctx->bw;
+  if (mix) CK(launch_mix_signal(ctx->d_samples, 4 * nq, (int)nq, ctx->d_mix, st));
+  {
+    ProfScope ps(ctx, st, PS_SHT);
+    CK(launch_sht(sht_args(ctx, n_data, mix), st));
+  }
   {
     ProfScope ps(ctx, st, PS_FUSE_S2);
-    CK(launch_fuse_s2(f, st));
+    CK(launch_fuse_s2(fuse_args(ctx, n_data, n_total, laplace), st));
   }
   CK(cudaMemsetAsync(ctx->d_argmax, 0, sizeof(unsigned long long), st));
   return PHGPU_OK;
@@ -891,7 +956,7 @@ int phgpu_run_so3_batch(phgpu_ctx* const* ctx, int k, const So3Table* table, cud
 int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st, bool mix) {
   CKV(phgpu_run_sph_front(ctx, n_data, n_total, laplace, st, mix));
   So3Table t = so3_table(ctx);
-  CKV(phgpu_run_so3_batch(&ctx, 1, ctx->prm.precision != PHGPU_PRECISION_FP32 ? &t : nullptr, st));
+  CKV(phgpu_run_so3_batch(&ctx, 1, t.table ? &t : nullptr, st));
   CK(cudaMemcpyAsync(ctx->h_argmax, ctx->d_argmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(ctx->h_argmax + 2, ctx->d_argmax + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   return PHGPU_OK;
@@ -1230,7 +1295,7 @@ PairPlan pair_plan(const phgpu_ctx* ctx, bool t_refl, bool t_amb, bool s_refl, b
   return pp;
 }
 
-int phgpu_pair_front(phgpu_ctx* ctx, const PairPlan& pp) {
+int phgpu_pair_front(phgpu_ctx* ctx, const PairPlan& pp, bool until_phi) {
   // serialised profiling: the target's translation side on s0 as well, so the
   // per-stage events do not overlap
   cudaStream_t s0 = ctx->s0, s1 = ctx->prof_serial ? ctx->s0 : ctx->s1;
@@ -1248,8 +1313,12 @@ int phgpu_pair_front(phgpu_ctx* ctx, const PairPlan& pp) {
   // rotation up to the fused spectra
   CKV(run_sample(ctx, 0, s0));
   CKV(run_sample(ctx, 1, s0));
-  CKV(phgpu_run_sph_front(ctx, pp.laplace_s2 ? pp.nd_s2 : 1, (int)ctx->prm.n_channels, pp.laplace_s2, s0,
-                          ctx->prm.spherical_fusion == PHGPU_FUSION_MIX));
+  const bool mix = ctx->prm.spherical_fusion == PHGPU_FUSION_MIX;
+  if (until_phi) {
+    CKV(phgpu_run_sph_phi(ctx, pp.laplace_s2 ? pp.nd_s2 : 1, s0, mix));
+  } else {
+    CKV(phgpu_run_sph_front(ctx, pp.laplace_s2 ? pp.nd_s2 : 1, (int)ctx->prm.n_channels, pp.laplace_s2, s0, mix));
+  }
   return PHGPU_OK;
 }
 
@@ -1367,7 +1436,7 @@ int phgpu_register_pair(phgpu_ctx* ctx, const phgpu_cloud* target, const phgpu_c
   const PairPlan pp = pair_plan(ctx, target->reflectivity, target->ambient, source->reflectivity, source->ambient);
   CKV(phgpu_pair_front(ctx, pp));
   So3Table t = so3_table(ctx);
-  CKV(phgpu_run_so3_batch(&ctx, 1, ctx->prm.precision != PHGPU_PRECISION_FP32 ? &t : nullptr, s0));
+  CKV(phgpu_run_so3_batch(&ctx, 1, t.table ? &t : nullptr, s0));
   // The rotation pose and the source's transform are computed on the device
   // and the translation follows without a host round trip.  A peak
   // neighbourhood fit (host, FP64) or the padded correlation (whose Laplace

@@ -45,6 +45,7 @@ struct phgpu_ctx {
   float4* d_grid = nullptr;
   double* d_weights = nullptr;
   float* d_legendre = nullptr;
+  float* d_legendre_tc = nullptr;  // tensor-core layout of the Legendre table (precision != FP32)
   float* d_edges = nullptr;
   // clouds
   uint32_t cap_points = 0;
@@ -66,6 +67,7 @@ struct phgpu_ctx {
   double* d_beta_tab = nullptr;  // [3][2 bw_out] for the Wigner seeds
   double* d_wig_tab = nullptr;   // Wigner recurrence tables (so3_wigner_table)
   float* d_wtable = nullptr;     // Wigner-d values of the tensor-core synthesis (precision != FP32)
+  bool own_wigner_table = true;  // false: a server executor's slot (the executor holds the table)
   size_t* d_class_off = nullptr; // per-class offsets into d_wtable
   float* d_rotvol = nullptr;
   // translation
@@ -127,6 +129,9 @@ struct ProfScope {
 };
 
 int phgpu_ctx_init(phgpu_ctx* ctx);
+// phgpu_ctx_create; wigner_table false leaves the tensor-core Wigner-d table
+// to the caller (a server executor shares one among its slots)
+int phgpu_ctx_create_internal(const phgpu_params* prm, phgpu_ctx** out, bool wigner_table);
 int phgpu_upload_cloud(phgpu_ctx* ctx, const phgpu_cloud* c, int side, cudaStream_t st);
 int phgpu_run_sph(phgpu_ctx* ctx, int n_data, int n_total, int laplace, cudaStream_t st, bool mix = false);
 int phgpu_run_voxelize(phgpu_ctx* ctx, int side, const float* T12, int n_data, cudaStream_t st,
@@ -146,7 +151,10 @@ struct PairPlan {
   int nd_s2, nd_sp, laplace_s2, laplace_sp;
 };
 PairPlan pair_plan(const phgpu_ctx* ctx, bool t_refl, bool t_amb, bool s_refl, bool s_amb);
-int phgpu_pair_front(phgpu_ctx* ctx, const PairPlan& pp);
+int phgpu_pair_front(phgpu_ctx* ctx, const PairPlan& pp, bool until_phi = false);
+int phgpu_run_sph_phi(phgpu_ctx* ctx, int n_data, cudaStream_t st, bool mix);
+int phgpu_run_sph_leg_fuse_batch(phgpu_ctx* const* ctx, int k, int n_data, int n_total, int laplace, bool mix,
+                                 cudaStream_t st);
 int phgpu_pair_back(phgpu_ctx* ctx, const PairPlan& pp, const float* T, const float* T_dev);
 int phgpu_pair_finish(phgpu_ctx* ctx, const PairPlan& pp, bool device_pose, phgpu_pose* out);
 bool pair_device_pose(const phgpu_ctx* ctx);

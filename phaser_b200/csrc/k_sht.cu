@@ -20,6 +20,7 @@
 #include <algorithm>
 
 #include "kernels.h"
+#include "tc_gemm.cuh"
 
 namespace phgpu {
 
@@ -278,8 +279,29 @@ bool leg_chunking(int bw, int n_data, int* cr, int* nslot, size_t* smem) {
 
 size_t sht_scratch_entries(int bw) { return (size_t)2 * kMaxSig * bw * 2 * bw; }
 
+struct LegendreGemm;
+template <int PREC>
+__global__ void k_sht_leg_tc(TcGemmArgs g, LegendreGemm prob);
+
 cudaError_t sht_init_attributes() {
-  return cudaFuncSetAttribute(k_sht_leg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShtSmemLimit);
+  cudaError_t e = cudaFuncSetAttribute(k_sht_leg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kShtSmemLimit);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sht_leg_tc<kSo3Tf32x3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sht_leg_tc<kSo3Bf16x3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  return e;
+}
+
+cudaError_t launch_sht_phi(const ShtArgs& a, cudaStream_t st) {
+  if (a.n_data < 1 || a.n_data > kMaxSig) return cudaErrorInvalidValue;
+  const int n = 2 * a.bw;
+  if (a.plan->n != n) return cudaErrorInvalidValue;
+  dim3 g1((n + kPhiRows - 1) / kPhiRows, 2 * a.n_data);
+  const size_t sm1 = (size_t)(kPhiRows / 2) * n * sizeof(float2);
+  PHGPU_DISPATCH_N(n, k_sht_phi<NF><<<g1, kPhiThreads, sm1, st>>>(a.bw, a.n_data, a.side_stride, a.signal,
+                                                                   *a.plan, a.fphi));
+  count_launches(1);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st) {
@@ -287,15 +309,119 @@ cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st) {
   size_t sm = 0;
   if (a.n_data < 1 || a.n_data > kMaxSig || !leg_chunking(a.bw, a.n_data, &cr, &nslot, &sm))
     return cudaErrorInvalidValue;
-  const int n = 2 * a.bw;
-  if (a.plan->n != n) return cudaErrorInvalidValue;
-  dim3 g1((n + kPhiRows - 1) / kPhiRows, 2 * a.n_data);
-  const size_t sm1 = (size_t)(kPhiRows / 2) * n * sizeof(float2);
-  PHGPU_DISPATCH_N(n, k_sht_phi<NF><<<g1, kPhiThreads, sm1, st>>>(a.bw, a.n_data, a.side_stride, a.signal,
-                                                                   *a.plan, a.fphi));
+  cudaError_t e = launch_sht_phi(a, st);
+  if (e != cudaSuccess) return e;
+  if (a.table_tc) {
+    ShtBatch b;
+    b.count = 1;
+    b.fphi[0] = a.fphi;
+    b.coef[0] = a.coef;
+    return launch_sht_leg_tc(a.bw, a.n_data, b, a.table_tc, a.precision, a.tc_chunk, a.status, st);
+  }
   dim3 g2((a.bw + 1) / 2, 2);
   k_sht_leg<<<g2, kLegThreads, sm, st>>>(a.bw, a.n_data, cr, nslot, a.table, a.fphi, a.coef);
-  count_launches(2);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ tensor-core Legendre contraction
+//
+// fhat(l, m) = sum_k T[m][l][k] F_m(theta_k) for every signal as a tc_gemm
+// problem (tc_gemm.cuh): class = order m (largest first), rows = degrees
+// l = m .. B-1, k = the 2B rows theta_k, one group of 8 columns per (request,
+// side): the four channels' real and imaginary parts.  A wave of K requests
+// reads the table once.  Table layout per order: [k / 4][B - m][4] floats,
+// k padded to a multiple of 8 with zeros (legendre_tc_offset).
+
+__host__ __device__ inline int legendre_tc_kdim(int bw) { return (2 * bw + 7) & ~7; }
+
+__host__ __device__ inline size_t legendre_tc_offset(int m, int bw) {
+  return (size_t)legendre_tc_kdim(bw) * ((size_t)m * bw - (size_t)m * (m - 1) / 2);
+}
+
+size_t legendre_tc_floats(int bw) { return legendre_tc_offset(bw, bw); }
+
+// T_tc from the row-major table T[m][l][k] (k fastest): one thread per entry.
+__global__ void k_legendre_tc_layout(int bw, const float* __restrict__ T, float* __restrict__ Ttc) {
+  const int n = 2 * bw, kd = legendre_tc_kdim(bw);
+  const int m = blockIdx.y;
+  const int rows = bw - m;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < rows * kd; e += gridDim.x * blockDim.x) {
+    const int r = e / kd, k = e - r * kd;
+    const float v = k < n ? T[legendre_offset(m, bw) + (size_t)r * n + k] : 0.0f;
+    Ttc[legendre_tc_offset(m, bw) + ((size_t)(k >> 2) * rows + r) * 4 + (k & 3)] = v;
+  }
+}
+
+cudaError_t launch_legendre_tc_layout(int bw, const float* table, float* table_tc, cudaStream_t st) {
+  k_legendre_tc_layout<<<dim3(64, bw), 256, 0, st>>>(bw, table, table_tc);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+struct LegendreGemm {
+  int bw, n_data;
+  const float* table;
+  ShtBatch b;
+
+  __device__ int classes() const { return bw; }
+  __device__ TcClass cls(int m) const {
+    TcClass t;
+    t.rows = bw - m;
+    t.kdim = legendre_tc_kdim(bw);
+    t.a = table + legendre_tc_offset(m, bw);
+    t.u0 = m;
+    t.u1 = 0;
+    return t;
+  }
+  __device__ void bvals(const TcClass& c, int grp, int k, float v[8]) const {
+    const int r = grp >> 1, side = grp & 1, n = 2 * bw;
+#pragma unroll
+    for (int q = 0; q < kMaxSig; ++q) {
+      float2 f = make_float2(0.f, 0.f);
+      if (q < n_data && k < n) f = __ldg(&b.fphi[r][(((size_t)side * n_data + q) * bw + c.u0) * n + k]);
+      v[2 * q] = f.x;
+      v[2 * q + 1] = f.y;
+    }
+  }
+  __device__ void store(const TcClass& c, int grp, int row, const float v[8]) const {
+    const int r = grp >> 1, side = grp & 1, l = c.u0 + row;
+    for (int q = 0; q < n_data; ++q)
+      b.coef[r][(((size_t)side * n_data + q) * bw + l) * bw + c.u0] = make_float2(v[2 * q], v[2 * q + 1]);
+  }
+};
+
+template <int PREC>
+__global__ void __launch_bounds__(kTcThreads, 1) k_sht_leg_tc(TcGemmArgs g, LegendreGemm prob) {
+  tc_class_gemm<PREC>(g, prob);
+}
+
+bool sht_leg_tc_supported(int bw, int count, int precision) {
+  TcGemmArgs g;
+  return count >= 1 && count <= kMaxWave && tc_gemm_geom(bw, 2 * count, precision, 0, &g);
+}
+
+cudaError_t launch_sht_leg_tc(int bw, int n_data, const ShtBatch& b, const float* table_tc, int precision,
+                              int chunk, unsigned long long* status, cudaStream_t st) {
+  if (n_data < 1 || n_data > kMaxSig || b.count < 1 || b.count > kMaxWave) return cudaErrorInvalidValue;
+  TcGemmArgs g;
+  if (!tc_gemm_geom(bw, 2 * b.count, precision, chunk, &g) && !tc_gemm_geom(bw, 2 * b.count, precision, 0, &g))
+    return cudaErrorInvalidValue;
+  g.status = status;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  LegendreGemm prob;
+  prob.bw = bw;
+  prob.n_data = n_data;
+  prob.table = table_tc;
+  prob.b = b;
+  const int grid = bw < sms ? bw : sms;
+  if (precision == kSo3Tf32x3)
+    k_sht_leg_tc<kSo3Tf32x3><<<grid, kTcThreads, g.smem, st>>>(g, prob);
+  else
+    k_sht_leg_tc<kSo3Bf16x3><<<grid, kTcThreads, g.smem, st>>>(g, prob);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -312,9 +438,11 @@ __device__ __forceinline__ float2 coef_at(const float2* __restrict__ c, int bw, 
   return v;
 }
 
-// One thread per (l, m) with |m| <= l; both sides.
+// One thread per (l, m) with |m| <= l; both sides; request blockIdx.y.
 __global__ void k_fuse_s2(FuseS2Args a) {
   const int bw = a.bw;
+  const float2* __restrict__ coef = a.coef_b[blockIdx.y];
+  float2* __restrict__ fused = a.fused_b[blockIdx.y];
   const int w = 2 * bw - 1;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= bw * w) return;
@@ -327,7 +455,7 @@ __global__ void k_fuse_s2(FuseS2Args a) {
   if (a.laplace) op = fusion_op(p, a.bands);
   const bool dropped = a.lowpass && (p < a.lp_lo || p >= a.lp_hi);
   for (int side = 0; side < 2; ++side) {
-    const float2* base = a.coef + (size_t)side * a.n_data_ch * bw * bw;
+    const float2* base = coef + (size_t)side * a.n_data_ch * bw * bw;
     float2 r = make_float2(0.f, 0.f);
     if (!a.laplace) {
       r = coef_at(base, bw, l, m);
@@ -351,7 +479,7 @@ __global__ void k_fuse_s2(FuseS2Args a) {
       }
     }
     if (dropped) r = make_float2(0.f, 0.f);
-    a.fused[((size_t)side * bw + l) * w + mi] = r;
+    fused[((size_t)side * bw + l) * w + mi] = r;
   }
 }
 
@@ -373,9 +501,16 @@ cudaError_t launch_mix_signal(const float* samples, size_t side_stride, int n, f
   return cudaGetLastError();
 }
 
-cudaError_t launch_fuse_s2(const FuseS2Args& a, cudaStream_t st) {
+cudaError_t launch_fuse_s2(const FuseS2Args& a0, cudaStream_t st) {
+  FuseS2Args a = a0;
+  if (a.count < 1) {
+    a.count = 1;
+    a.coef_b[0] = a.coef;
+    a.fused_b[0] = a.fused;
+  }
+  if (a.count > kMaxWave) return cudaErrorInvalidValue;
   const int tot = a.bw * (2 * a.bw - 1);
-  k_fuse_s2<<<(tot + 255) / 256, 256, 0, st>>>(a);
+  k_fuse_s2<<<dim3((tot + 255) / 256, a.count), 256, 0, st>>>(a);
   count_launches(1);
   return cudaGetLastError();
 }

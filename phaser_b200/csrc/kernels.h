@@ -49,6 +49,7 @@ size_t legendre_table_entries(int bw);
 cudaError_t launch_legendre_table(int bw, const double* weights_dev, float* table, cudaStream_t st);
 
 // Both sides at once: signal (side, c) at signal + side * side_stride + c (2B)^2.
+constexpr int kMaxWaveSht = 32;  // requests per batched Legendre launch (kMaxWave)
 struct ShtArgs {
   int bw;
   int n_data;             // channels per side (1..4)
@@ -58,10 +59,28 @@ struct ShtArgs {
   const float* table;     // Legendre table
   float2* fphi;           // scratch [side][c][B (m)][2B (k)], sht_scratch_entries(B) complex
   float2* coef;           // [side][c][B (l)][B (m>=0)]
+  const float* table_tc = nullptr;  // tensor-core layout of the table (legendre_tc_floats): the
+                                    // contraction runs on the tensor cores when set
+  int precision = 0;                // kSo3Tf32x3 / kSo3Bf16x3 with table_tc
+  int tc_chunk = 0;
+  unsigned long long* status = nullptr;
+};
+// The Legendre contraction of several requests (one launch): fphi / coef per request.
+struct ShtBatch {
+  int count;
+  const float2* fphi[kMaxWaveSht];
+  float2* coef[kMaxWaveSht];
 };
 size_t sht_scratch_entries(int bw);
-cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st);
+cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st);      // phi pass + Legendre contraction
+cudaError_t launch_sht_phi(const ShtArgs& a, cudaStream_t st);  // phi pass alone
 cudaError_t sht_init_attributes();  // once per device
+// Tensor-core Legendre contraction (k_sht.cu): the table relaid [m][k / 4][l][4].
+size_t legendre_tc_floats(int bw);
+cudaError_t launch_legendre_tc_layout(int bw, const float* table, float* table_tc, cudaStream_t st);
+bool sht_leg_tc_supported(int bw, int count, int precision);
+cudaError_t launch_sht_leg_tc(int bw, int n_data, const ShtBatch& b, const float* table_tc, int precision, int chunk,
+                              unsigned long long* status, cudaStream_t st);
 
 struct FuseS2Args {
   int bw;
@@ -73,6 +92,9 @@ struct FuseS2Args {
   FusionBands bands;      // for n = B^2
   const float2* coef;     // [2][n_data_ch][B][B]   (side-major)
   float2* fused;          // [2][B (l)][2B-1 (m + B - 1)]
+  int count = 0;          // > 0: requests of one launch, coef_b / fused_b per request (else coef / fused)
+  const float2* coef_b[32];
+  float2* fused_b[32];
 };
 cudaError_t launch_fuse_s2(const FuseS2Args& a, cudaStream_t st);
 // out[side][k] = 0.6 * intensity + 0.4 * range of samples [side][c][n] (n = 4B^2)

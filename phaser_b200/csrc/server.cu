@@ -226,14 +226,17 @@ struct phgpu_server {
     phgpu_params p = e->prm;
     p.max_points = prm.max_points;
     p.device = prm.device;
-    p.precision = PHGPU_PRECISION_FP32;  // the executor owns the shape's table
+    // slots keep the request's precision (tensor-core Legendre tables of their
+    // own); the executor holds the shape's Wigner-d table
     const int bw_out = (int)(p.spherical_bandwidth + p.spherical_zero_padding);
     if (e->prm.precision != PHGPU_PRECISION_FP32)
-      while (e->kmax > 1 && !so3_tc_supported(bw_out, e->kmax, (int)e->prm.precision)) --e->kmax;
+      while (e->kmax > 1 && (!so3_tc_supported(bw_out, e->kmax, (int)e->prm.precision) ||
+                             !sht_leg_tc_supported((int)p.spherical_bandwidth, e->kmax, (int)e->prm.precision)))
+        --e->kmax;
     e->graphs = e->prm.rot_peak_neighbors == 0 && e->prm.spatial_zero_padding == 0;
     for (int i = 0; i < e->kmax; ++i) {
       phgpu_ctx* c = nullptr;
-      const int rc = phgpu_ctx_create(&p, &c);
+      const int rc = phgpu_ctx_create_internal(&p, &c, false);
       if (rc != PHGPU_OK) {
         *why = phgpu_last_error(nullptr);
         destroy_exec(e);
@@ -357,13 +360,22 @@ struct phgpu_server {
     std::vector<phgpu_ctx*> sl(e->slots.begin(), e->slots.begin() + k);
     phgpu_ctx* c0 = sl[0];
     if (cudaEventRecord(e->ev_fork, e->st) != cudaSuccess) return PHGPU_ERR_CUDA;
+    // tensor-core precisions: the fronts stop after the phi transform and the
+    // Legendre contraction and the fusion run once for the whole wave
+    const bool batch_leg = e->table != nullptr;
     for (int i = 0; i < k; ++i) {
       if (cudaStreamWaitEvent(sl[i]->s0, e->ev_fork, 0) != cudaSuccess) return PHGPU_ERR_CUDA;
-      const int rc = phgpu_pair_front(sl[i], e->pp);
+      const int rc = phgpu_pair_front(sl[i], e->pp, batch_leg);
       if (rc != PHGPU_OK) return rc;
       if (cudaEventRecord(e->ev_join[i], sl[i]->s0) != cudaSuccess ||
           cudaStreamWaitEvent(e->st, e->ev_join[i], 0) != cudaSuccess)
         return PHGPU_ERR_CUDA;
+    }
+    if (batch_leg) {
+      const int rc = phgpu_run_sph_leg_fuse_batch(sl.data(), k, e->pp.laplace_s2 ? e->pp.nd_s2 : 1,
+                                                  (int)c0->prm.n_channels, e->pp.laplace_s2,
+                                                  c0->prm.spherical_fusion == PHGPU_FUSION_MIX, e->st);
+      if (rc != PHGPU_OK) return rc;
     }
     So3Table tab;
     if (e->table) {
