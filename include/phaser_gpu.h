@@ -361,7 +361,7 @@ typedef struct {
   uint32_t flags;              /* PHGPU_SERVER_* */
   uint32_t lanes;              /* waves in flight at once (2 when 0) */
   uint32_t max_delay_us;       /* longest a request is held back to fill a wave while another wave
-                                  runs (1000 when 0); an idle GPU starts a wave at once */
+                                  runs (500 when 0); an idle GPU starts a wave at once */
 } phgpu_server_params;
 
 /* Host clouds are read in place by the worker (copied to the device inside the

@@ -1387,6 +1387,10 @@ int phgpu_pair_finish(phgpu_ctx* ctx, const PairPlan& pp, bool device_pose, phgp
     // transform that differs in some bit from the host restatement (the two
     // sides' double trig functions may round differently)
     if (device_pose) ++ctx->pose_reruns;
+    // the target's side finished with the registration; ev_b may last have
+    // been recorded inside a captured graph (a server wave), which a stream
+    // outside the graph cannot wait on: record it again on the idle stream
+    CK(cudaEventRecord(ctx->ev_b, ctx->s1));
     CKV(phgpu_pair_back(ctx, pp, T, nullptr));
     CK(cudaStreamSynchronize(s0));
   }

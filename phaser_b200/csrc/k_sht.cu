@@ -392,7 +392,7 @@ struct LegendreGemm {
 };
 
 template <int PREC>
-__global__ void __launch_bounds__(kTcThreads, 1) k_sht_leg_tc(TcGemmArgs g, LegendreGemm prob) {
+__global__ void __launch_bounds__(kTcThreads, kTcCtasPerSm) k_sht_leg_tc(TcGemmArgs g, LegendreGemm prob) {
   tc_class_gemm<PREC>(g, prob);
 }
 
@@ -416,7 +416,7 @@ cudaError_t launch_sht_leg_tc(int bw, int n_data, const ShtBatch& b, const float
   prob.n_data = n_data;
   prob.table = table_tc;
   prob.b = b;
-  const int grid = bw < sms ? bw : sms;
+  const int grid = bw < sms * g.ctas_per_sm ? bw : sms * g.ctas_per_sm;
   if (precision == kSo3Tf32x3)
     k_sht_leg_tc<kSo3Tf32x3><<<grid, kTcThreads, g.smem, st>>>(g, prob);
   else

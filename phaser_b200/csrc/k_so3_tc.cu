@@ -145,7 +145,7 @@ struct WignerGemm {
 };
 
 template <int PREC>
-__global__ void __launch_bounds__(kTcThreads, 1) k_so3_synth_tc(TcGemmArgs g, WignerGemm prob) {
+__global__ void __launch_bounds__(kTcThreads, kTcCtasPerSm) k_so3_synth_tc(TcGemmArgs g, WignerGemm prob) {
   tc_class_gemm<PREC>(g, prob);
 }
 
@@ -175,7 +175,7 @@ cudaError_t launch_so3_synth_tc(const So3Args& a, const So3Table& t, unsigned lo
   prob.wtab = a.wig_tab;
   prob.bt = a.batch;
   const int ncls = a.bw_in * (a.bw_in + 1) / 2;
-  const int grid = ncls < sms ? ncls : sms;
+  const int grid = ncls < sms * g.ctas_per_sm ? ncls : sms * g.ctas_per_sm;
   if (t.precision == kSo3Tf32x3)
     k_so3_synth_tc<kSo3Tf32x3><<<grid, kTcThreads, g.smem, st>>>(g, prob);
   else

@@ -116,6 +116,7 @@ struct Executor {
   std::shared_ptr<Table> table;
   uint64_t bytes = 0;
   bool busy = false;
+  bool captured_all = false;  // the graphs of every wave size were captured (first wave)
   Clock::time_point last_used;
 };
 
@@ -473,10 +474,21 @@ struct phgpu_server {
       if (rc == PHGPU_OK) rc = phgpu_upload_cloud(e->slots[i], &wave[i]->s, 1, e->st);
       if (rc != PHGPU_OK) why = phgpu_last_error(e->slots[i]);
     }
-    // capture the graph of a k-request wave on first use; CUDA work of other
-    // threads of the process that synchronises the device invalidates a
-    // capture, so after a failed capture the wave runs uncaptured (the same
-    // launches) and capturing is retried on later waves (twice at most)
+    // the first wave of an executor captures the graphs of every wave size, so
+    // no later wave waits for a capture; CUDA work of other threads of the
+    // process that synchronises the device invalidates a capture, so after a
+    // failed capture the wave runs uncaptured (the same launches) and capturing
+    // is retried on later waves (twice at most)
+    if (rc == PHGPU_OK && !e->captured_all) {
+      e->captured_all = true;
+      for (int kk = 1; kk <= e->kmax; ++kk) {
+        std::string ignore;
+        if (!e->exec[kk] && capture(e, kk, &ignore) != PHGPU_OK) {
+          ++e->capture_failures[kk];
+          cudaGetLastError();
+        }
+      }
+    }
     bool direct = false;
     if (rc == PHGPU_OK && !e->exec[k]) {
       if (e->capture_failures[k] < 2 && capture(e, k, &why) == PHGPU_OK) {
@@ -630,7 +642,7 @@ int phgpu_server_create(const phgpu_server_params* params, phgpu_server** out) {
   if (s->prm.max_points == 0) s->prm.max_points = 1u << 18;
   if (s->prm.hbm_budget_bytes == 0) s->prm.hbm_budget_bytes = 150ull << 30;
   if (s->prm.lanes == 0) s->prm.lanes = 2;
-  if (s->prm.max_delay_us == 0) s->prm.max_delay_us = 1000;
+  if (s->prm.max_delay_us == 0) s->prm.max_delay_us = 500;
   for (uint32_t w = 0; w < s->prm.lanes; ++w) s->workers.emplace_back(&phgpu_server::worker_main, s);
   *out = s;
   return PHGPU_OK;

@@ -40,6 +40,7 @@
 namespace phgpu {
 
 constexpr int kTcThreads = 256;
+constexpr int kTcCtasPerSm = 3;  // 3 x 256 threads x at most 85 registers fit 64K registers
 constexpr int kTcStages = 2;
 
 // Per-launch geometry (host-computed, tc_gemm_geom).
@@ -56,6 +57,7 @@ struct TcGemmArgs {
   uint32_t stage;
   uint32_t smem;
   uint32_t tcols;  // tensor-memory columns
+  int ctas_per_sm; // CTAs one SM runs at once (tensor and shared memory)
   unsigned long long* status;
 };
 
@@ -93,11 +95,19 @@ inline bool tc_gemm_geom(int max_rows, int groups, int precision, int chunk, TcG
     }
   }
   if (!ok) return false;
-  // at most one CTA per SM, so the tensor-memory allocation never waits
-  if (g->smem < 116u * 1024u) g->smem = 116u * 1024u;
   uint32_t c = 32;
   while (c < (uint32_t)(g->nmt * g->N)) c <<= 1;
   g->tcols = c;
+  // CTAs that may share an SM: as many as the 512 tensor-memory columns hold
+  // (so an allocation never waits) and the registers hold (kTcCtasPerSm, the
+  // kernels' launch bound), enforced through the shared memory each CTA takes
+  // (228 KB per SM, 1 KB of it reserved per CTA)
+  g->ctas_per_sm = (int)(512u / c);
+  if (g->ctas_per_sm > kTcCtasPerSm) g->ctas_per_sm = kTcCtasPerSm;
+  const uint32_t fit = 228u * 1024u / (g->smem + 1024u);
+  if ((uint32_t)g->ctas_per_sm > fit) g->ctas_per_sm = (int)(fit > 0 ? fit : 1);
+  const uint32_t floor_smem = 228u * 1024u / (uint32_t)(g->ctas_per_sm + 1) + 1u;
+  if (g->smem < floor_smem) g->smem = floor_smem;
   return true;
 }
 

@@ -643,7 +643,7 @@ class Server:
     to max_wave same-shape pairs, `lanes` waves in flight."""
 
     def __init__(self, max_wave=16, hbm_budget_bytes=150 << 30, max_points=1 << 18, device=0, flags=0, lanes=2,
-                 max_delay_us=1000):
+                 max_delay_us=500):
         lib = load()
         self.lib = lib
         sp = ServerParams(int(hbm_budget_bytes), int(max_wave), int(max_points), int(device), int(flags), int(lanes),

@@ -41,7 +41,7 @@ def _selftest_lib():
 class _Native:
     @staticmethod
     def selftest_fft(x, inverse=False, columns=False, engine=2):
-        a = np.ascontiguousarray(x, np.complex64)
+        a = np.ascontiguousarray(x, np.complex64).copy()  # transformed in place
         ntrans, n = a.shape
         rc = _selftest_lib().phgpu_selftest_fft(n, ntrans, 1 if inverse else 0, 1 if columns else 0, engine,
                                                 a.ctypes.data)
