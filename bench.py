@@ -23,6 +23,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -201,14 +202,51 @@ def pair_bytes(bw, N, C, P):
     return rot + trans
 
 
-# DRAM read + write per stage call (sum over the stage's kernels; per cloud for
-# the per-cloud stages), B = 100 / N = 200 workload, from one-kernel ncu
-# captures of the current kernels:
-#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
-#       --clock-control none -k regex:<kernel> -s <n> -c 1
-#       python bench.py --profile pair --workload 1 --pairs 2 --precision 1
-# None where no capture exists.
-NCU_TRAFFIC_B100_N200 = {}
+# Kernels of each profiled stage (one launch of each per stage call).
+STAGE_KERNELS = {
+    "s2_sample": ("k_project", "k_bin_scan", "k_bin_scatter", "k_nn_rows"),
+    "sht": ("k_sht_phi", "k_sht_leg", "k_sht_leg_tc"),
+    "fuse_s2": ("k_fuse_s2",),
+    "so3_synth": ("k_so3_synth", "k_so3_synth_tc"),
+    "so3_fft": ("k_so3_fft_a", "k_so3_c2r_tail"),
+    "voxelize": ("k_voxelize",),
+    "spatial_fwd": ("k_slab_fwd",),
+    "fuse_z": ("k_fuse_z",),
+    "spatial_inv": ("k_slab_inv",),
+}
+
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "traffic_register_pair_B100_N200.md")
+
+
+def ncu_traffic(path=TRAFFIC_PROFILE):
+    """DRAM read + write bytes per stage call at B = 100 / N = 200, summed over
+    the stage's kernels, from the committed table of one-kernel ncu captures
+    (`dram__bytes_read.sum + dram__bytes_write.sum` per launch of the current
+    kernels; the file gives the capture command).  A stage is left out when
+    one of the kernels it launched has no row (variant kernels of a stage,
+    e.g. the CUDA-core and tensor-core synthesis, count whichever has one)."""
+    per_kernel = {}
+    try:
+        lines = open(path).read().splitlines()
+    except OSError:
+        return {}
+    for ln in lines:
+        if not ln.startswith("| `"):
+            continue
+        cells = [c.strip() for c in ln.strip().strip("|").split("|")]
+        if len(cells) < 5:
+            continue
+        name = re.sub(r"<.*", "", cells[0].strip("`").replace("void ", "")).strip()
+        try:
+            per_kernel[name] = (float(cells[3]) + float(cells[4])) * 1e6
+        except ValueError:
+            continue
+    out = {}
+    for stage, kernels in STAGE_KERNELS.items():
+        have = [per_kernel[k] for k in kernels if k in per_kernel]
+        if have:
+            out[stage] = int(sum(have))
+    return out
 
 
 def measured_peak():
@@ -249,6 +287,7 @@ def roofline(nat, pool, params, tuning, served_value):
     peak, src = measured_peak()
     tot = {k: v for k, v in st.items() if v[1] > 0 and k != "upload"}
     workload_is_bench = (bw, N) == (100, 200)
+    traffic = ncu_traffic()
     stages = {}
     for k, (ms, calls) in tot.items():
         nb = stage_bytes(k, bw, N, C, P)
@@ -258,7 +297,7 @@ def roofline(nat, pool, params, tuning, served_value):
         if nb:
             gbs = nb / (per * 1e-3) / 1e9
             e.update({"algorithmic_bytes": nb, "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)})
-        tr = NCU_TRAFFIC_B100_N200.get(k) if workload_is_bench else None
+        tr = traffic.get(k) if workload_is_bench else None
         if tr:
             e.update({"traffic": tr, "traffic_gbs": round(tr / (per * 1e-3) / 1e9, 1),
                       "frac_actual": round(tr / (per * 1e-3) / 1e9 / peak, 4)})

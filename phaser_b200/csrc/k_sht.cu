@@ -331,7 +331,13 @@ cudaError_t launch_sht(const ShtArgs& a, cudaStream_t st) {
 // l = m .. B-1, k = the 2B rows theta_k, one group of 8 columns per (request,
 // side): the four channels' real and imaginary parts.  A wave of K requests
 // reads the table once.  Table layout per order: [k / 4][B - m][4] floats,
-// k padded to a multiple of 8 with zeros (legendre_tc_offset).
+// k padded to a multiple of 8 with zeros (legendre_tc_offset), followed by the
+// B row sums S_l = sum_k T[0][l][k] (FP64 sums of the FP32 table).
+//
+// Order 0 contracts F_0(theta_k) - D with D = F_0(theta_B) (the ring below the
+// equator) and adds D S_l afterwards: the same sum, but a range or intensity
+// channel's large constant part no longer enters the tensor-core accumulation,
+// whose truncation error scales with the magnitude of the partial sums.
 
 __host__ __device__ inline int legendre_tc_kdim(int bw) { return (2 * bw + 7) & ~7; }
 
@@ -339,7 +345,7 @@ __host__ __device__ inline size_t legendre_tc_offset(int m, int bw) {
   return (size_t)legendre_tc_kdim(bw) * ((size_t)m * bw - (size_t)m * (m - 1) / 2);
 }
 
-size_t legendre_tc_floats(int bw) { return legendre_tc_offset(bw, bw); }
+size_t legendre_tc_floats(int bw) { return legendre_tc_offset(bw, bw) + (size_t)bw; }
 
 // T_tc from the row-major table T[m][l][k] (k fastest): one thread per entry.
 __global__ void k_legendre_tc_layout(int bw, const float* __restrict__ T, float* __restrict__ Ttc) {
@@ -353,9 +359,21 @@ __global__ void k_legendre_tc_layout(int bw, const float* __restrict__ T, float*
   }
 }
 
+// S_l = sum_k T[0][l][k] in FP64, one thread per degree.
+__global__ void k_legendre_row_sums(int bw, const float* __restrict__ T, float* __restrict__ S) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= bw) return;
+  const int n = 2 * bw;
+  const float* row = T + legendre_offset(0, bw) + (size_t)l * n;
+  double s = 0.0;
+  for (int k = 0; k < n; ++k) s += (double)row[k];
+  S[l] = (float)s;
+}
+
 cudaError_t launch_legendre_tc_layout(int bw, const float* table, float* table_tc, cudaStream_t st) {
   k_legendre_tc_layout<<<dim3(64, bw), 256, 0, st>>>(bw, table, table_tc);
-  count_launches(1);
+  k_legendre_row_sums<<<(bw + 127) / 128, 128, 0, st>>>(bw, table, table_tc + legendre_tc_offset(bw, bw));
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -379,15 +397,29 @@ struct LegendreGemm {
 #pragma unroll
     for (int q = 0; q < kMaxSig; ++q) {
       float2 f = make_float2(0.f, 0.f);
-      if (q < n_data && k < n) f = __ldg(&b.fphi[r][(((size_t)side * n_data + q) * bw + c.u0) * n + k]);
+      if (q < n_data && k < n) {
+        const float2* F = b.fphi[r] + (((size_t)side * n_data + q) * bw + c.u0) * n;
+        f = __ldg(&F[k]);
+        if (c.u0 == 0) {
+          const float2 d = __ldg(&F[bw]);
+          f = make_float2(f.x - d.x, f.y - d.y);
+        }
+      }
       v[2 * q] = f.x;
       v[2 * q + 1] = f.y;
     }
   }
   __device__ void store(const TcClass& c, int grp, int row, const float v[8]) const {
-    const int r = grp >> 1, side = grp & 1, l = c.u0 + row;
-    for (int q = 0; q < n_data; ++q)
-      b.coef[r][(((size_t)side * n_data + q) * bw + l) * bw + c.u0] = make_float2(v[2 * q], v[2 * q + 1]);
+    const int r = grp >> 1, side = grp & 1, l = c.u0 + row, n = 2 * bw;
+    for (int q = 0; q < n_data; ++q) {
+      float2 o = make_float2(v[2 * q], v[2 * q + 1]);
+      if (c.u0 == 0) {
+        const float2 d = __ldg(&b.fphi[r][(((size_t)side * n_data + q) * bw) * n + bw]);
+        const float sl = __ldg(&table[legendre_tc_offset(bw, bw) + l]);
+        o = make_float2(fmaf(d.x, sl, o.x), fmaf(d.y, sl, o.y));
+      }
+      b.coef[r][(((size_t)side * n_data + q) * bw + l) * bw + c.u0] = o;
+    }
   }
 };
 

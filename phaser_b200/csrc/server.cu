@@ -8,8 +8,8 @@
 //     plans; point counts read from device memory) and, for the tensor-core
 //     precisions, shares the shape's Wigner-d table with the other executors of
 //     that bandwidth;
-//   * a wave of k requests is one CUDA graph launch, captured the first time an
-//     executor runs k requests: the k pairs' front halves (target translation
+//   * a wave of k requests is one CUDA graph launch; an executor's first wave
+//     captures the graphs of every k up to max_wave: the k pairs' front halves (target translation
 //     side, sampling, SHT, fusion) on their own streams, one batched launch of
 //     each SO(3) stage (synthesis on the tensor cores, angle transforms,
 //     argmax) and of the pose kernel, then the k source translations, each
@@ -19,6 +19,9 @@
 //
 // Lanes run waves concurrently, so requests that arrive while a wave is on the
 // GPU are admitted into the next wave on another executor and overlap with it.
+// While some wave runs, a lane holds back a wave smaller than max_wave until
+// it fills or its oldest request has waited max_delay_us; an idle GPU starts a
+// wave at once.
 // Executors are admitted against the HBM budget with their allocators' byte
 // counts; when a new one does not fit, idle executors of any shape are evicted
 // (least recently used first), and a lane waits only while some other lane's
@@ -481,6 +484,14 @@ struct phgpu_server {
     // is retried on later waves (twice at most)
     if (rc == PHGPU_OK && !e->captured_all) {
       e->captured_all = true;
+      // a captured launch keeps the optional-channel pointers its slot had at
+      // capture time: slots this wave leaves empty take the channel layout
+      // every request of the executor's key has
+      for (int i = k; i < e->kmax; ++i)
+        for (int sd = 0; sd < 2; ++sd) {
+          e->slots[i]->has_refl[sd] = e->slots[0]->has_refl[sd];
+          e->slots[i]->has_amb[sd] = e->slots[0]->has_amb[sd];
+        }
       for (int kk = 1; kk <= e->kmax; ++kk) {
         std::string ignore;
         if (!e->exec[kk] && capture(e, kk, &ignore) != PHGPU_OK) {

@@ -16,9 +16,19 @@ def test_config_is_identical_across_arms():
     assert a == b and "pairs_per_step" not in a
 
 
-def test_traffic_constants_name_known_stages():
-    for k in bench.NCU_TRAFFIC_B100_N200:
+def test_traffic_table_parsed_per_stage(tmp_path):
+    # the committed traffic table maps onto known stages
+    for k in bench.ncu_traffic():
         assert bench.stage_bytes(k, 100, 200, 3, 131072) is not None
+    # kernels of one stage are summed; template arguments are ignored
+    p = tmp_path / "t.md"
+    p.write_text("| kernel | launches | us / launch | DRAM read MB / launch | DRAM write MB / launch |\n"
+                 "|---|---|---|---|---|\n"
+                 "| `k_so3_fft_a<200, 4>` | 1 | 22.0 | 31.50 | 0.50 |\n"
+                 "| `void k_so3_c2r_tail<200>` | 1 | 33.0 | 32.00 | 0.00 |\n"
+                 "| `k_fuse_z<200>` | 1 | 130.0 | 200.00 | 24.00 |\n")
+    t = bench.ncu_traffic(str(p))
+    assert t == {"so3_fft": 64_000_000, "fuse_z": 224_000_000}
 
 
 def test_stage_bytes_per_call():

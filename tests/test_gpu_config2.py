@@ -55,8 +55,11 @@ def test_config2_waves_match_plain_and_oracle(batch, tmp_path):
             if (s["bw"], s["n_voxels"]) == sh:
                 plain[i] = c.register_pair(*clouds[i])
         c.close()
-    diff = [(i, specs[i]) for i in range(len(specs))
+    diff = [(i, specs[i]["bw"], specs[i]["n_voxels"], (served[i].rot_bin, served[i].voxel),
+             (plain[i].rot_bin, plain[i].voxel)) for i in range(len(specs))
             if (served[i].rot_bin, served[i].voxel) != (plain[i].rot_bin, plain[i].voxel)]
+    for d in diff:
+        print("served != plain:", d)
     assert diff == []
 
     def oracle(i):
