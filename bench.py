@@ -234,7 +234,7 @@ def ncu_traffic(path=TRAFFIC_PROFILE):
         if not ln.startswith("| `"):
             continue
         cells = [c.strip() for c in ln.strip().strip("|").split("|")]
-        if len(cells) < 5:
+        if len(cells) != 5:  # the first table: kernel, launches, us, read MB, write MB
             continue
         name = re.sub(r"<.*", "", cells[0].strip("`").replace("void ", "")).strip()
         try:

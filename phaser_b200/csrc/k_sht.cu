@@ -430,14 +430,15 @@ __global__ void __launch_bounds__(kTcThreads, kTcCtasPerSm) k_sht_leg_tc(TcGemmA
 
 bool sht_leg_tc_supported(int bw, int count, int precision) {
   TcGemmArgs g;
-  return count >= 1 && count <= kMaxWave && tc_gemm_geom(bw, 2 * count, precision, 0, &g);
+  return count >= 1 && count <= kMaxWave && tc_gemm_geom(bw, 2 * count, precision, 0, true, &g);
 }
 
 cudaError_t launch_sht_leg_tc(int bw, int n_data, const ShtBatch& b, const float* table_tc, int precision,
                               int chunk, unsigned long long* status, cudaStream_t st) {
   if (n_data < 1 || n_data > kMaxSig || b.count < 1 || b.count > kMaxWave) return cudaErrorInvalidValue;
   TcGemmArgs g;
-  if (!tc_gemm_geom(bw, 2 * b.count, precision, chunk, &g) && !tc_gemm_geom(bw, 2 * b.count, precision, 0, &g))
+  if (!tc_gemm_geom(bw, 2 * b.count, precision, chunk, true, &g) &&
+      !tc_gemm_geom(bw, 2 * b.count, precision, 0, true, &g))
     return cudaErrorInvalidValue;
   g.status = status;
   int dev = 0, sms = 148;

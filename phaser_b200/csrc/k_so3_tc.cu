@@ -35,7 +35,8 @@ namespace phgpu {
 
 bool so3_tc_supported(int bw_out, int count, int precision, int chunk) {
   TcGemmArgs g;
-  return bw_out <= 256 && count >= 1 && count <= kMaxWave && tc_gemm_geom(2 * bw_out, count, precision, chunk, &g);
+  return bw_out <= 256 && count >= 1 && count <= kMaxWave &&
+         tc_gemm_geom(2 * bw_out, count, precision, chunk, false, &g);
 }
 
 size_t so3_table_layout(int bw_in, int bw_out, std::vector<size_t>* off) {
@@ -160,8 +161,8 @@ cudaError_t so3_tc_init_attributes() {
 cudaError_t launch_so3_synth_tc(const So3Args& a, const So3Table& t, unsigned long long* status, cudaStream_t st) {
   TcGemmArgs g;
   if (a.bw_out > 256 || a.batch.count < 1 || a.batch.count > kMaxWave) return cudaErrorInvalidValue;
-  if (!tc_gemm_geom(2 * a.bw_out, a.batch.count, t.precision, a.tc_chunk, &g) &&
-      !tc_gemm_geom(2 * a.bw_out, a.batch.count, t.precision, 0, &g))
+  if (!tc_gemm_geom(2 * a.bw_out, a.batch.count, t.precision, a.tc_chunk, false, &g) &&
+      !tc_gemm_geom(2 * a.bw_out, a.batch.count, t.precision, 0, false, &g))
     return cudaErrorInvalidValue;
   g.status = status;
   int dev = 0, sms = 148;

@@ -14,12 +14,15 @@
 //   tf32x3: hi = tf32_rn(x), lo = tf32_rn(x - hi); kind::tf32
 //   bf16x3: hi = bf16(x), lo = bf16(x - hi); kind::f16 with BF16 inputs
 //   Out = (sum Ahi Bhi) + (sum Ahi Blo + Alo Bhi)
-// The two sums accumulate in separate tensor-memory columns and are added in
-// FP32 by the epilogue.  The tensor cores add each MMA's products to the
-// accumulator with truncation, an error that grows with the number of MMAs
-// and with the accumulator's magnitude: kept apart, the small cross terms
-// are not truncated against the large high-part sum, and rounding both splits
-// to nearest (rather than truncating the high part) removes their bias.
+// With `sep` (the Legendre contraction) the two sums accumulate in separate
+// tensor-memory columns and are added in FP32 by the epilogue; without it
+// (the Wigner-d synthesis, whose wave-wide accumulators would otherwise halve
+// the CTAs per SM) all three products share one accumulator.  The tensor
+// cores add each MMA's products to the accumulator with truncation, an error
+// that grows with the number of MMAs and with the accumulator's magnitude:
+// kept apart, the small cross terms are not truncated against the large
+// high-part sum, and rounding both splits to nearest (rather than truncating
+// the high part) removes their bias.
 // Measured on B200 against FP64 (128 rows, 8 columns, K = 200, positive
 // inputs): truncated split + one accumulator 4.5e-6, rounded split + two
 // accumulators 1.1e-6 (FP32 FMA chain 2.2e-7).
@@ -79,8 +82,9 @@ struct TcClass {
   int u0, u1;  // problem data (e.g. the orders of the class)
 };
 
-// Shared and tensor memory of a launch; false when it does not fit.
-inline bool tc_gemm_geom(int max_rows, int groups, int precision, int chunk, TcGemmArgs* g) {
+// Shared and tensor memory of a launch with KC k values per chunk; false
+// when it does not fit.
+inline bool tc_gemm_geom_kc(int max_rows, int groups, int precision, int KC, bool sep, TcGemmArgs* g) {
   if (precision != kSo3Tf32x3 && precision != kSo3Bf16x3) return false;
   if (groups < 1 || max_rows < 1) return false;
   g->precision = precision;
@@ -88,26 +92,18 @@ inline bool tc_gemm_geom(int max_rows, int groups, int precision, int chunk, TcG
   g->nmt = (max_rows + 127) / 128;
   g->MP = g->nmt * 128;
   g->N = ((8 * groups + 15) / 16) * 16;
-  if (g->N > 256 || 2 * g->nmt * g->N > 512) return false;
-  const uint32_t ctrl = 1024;
-  bool ok = false;
-  for (int KC : {32, 16}) {
-    if (chunk && KC != chunk) continue;
-    g->KC = KC;
-    g->a32 = (uint32_t)KC * g->MP * 4;
-    g->aconv = g->a32;
-    g->bop = (uint32_t)(precision == kSo3Tf32x3 ? 8 : 4) * KC * g->N;
-    g->stage = g->a32 + g->aconv + g->bop;
-    g->smem = kTcStages * g->stage + ctrl;
-    if (g->smem <= 227u * 1024u) {
-      ok = true;
-      break;
-    }
-  }
-  if (!ok) return false;
-  g->xoff = (uint32_t)(g->nmt * g->N);
+  const int nacc = sep ? 2 : 1;
+  if (g->N > 256 || nacc * g->nmt * g->N > 512) return false;
+  g->KC = KC;
+  g->a32 = (uint32_t)KC * g->MP * 4;
+  g->aconv = g->a32;
+  g->bop = (uint32_t)(precision == kSo3Tf32x3 ? 8 : 4) * KC * g->N;
+  g->stage = g->a32 + g->aconv + g->bop;
+  g->smem = kTcStages * g->stage + 1024u;
+  if (g->smem > 227u * 1024u) return false;
+  g->xoff = sep ? (uint32_t)(g->nmt * g->N) : 0u;
   uint32_t c = 32;
-  while (c < 2 * g->xoff) c <<= 1;
+  while (c < (uint32_t)(nacc * g->nmt * g->N)) c <<= 1;
   g->tcols = c;
   // CTAs that may share an SM: as many as the 512 tensor-memory columns hold
   // (so an allocation never waits) and the registers hold (kTcCtasPerSm, the
@@ -119,6 +115,19 @@ inline bool tc_gemm_geom(int max_rows, int groups, int precision, int chunk, TcG
   if ((uint32_t)g->ctas_per_sm > fit) g->ctas_per_sm = (int)(fit > 0 ? fit : 1);
   const uint32_t floor_smem = 228u * 1024u / (uint32_t)(g->ctas_per_sm + 1) + 1u;
   if (g->smem < floor_smem) g->smem = floor_smem;
+  return true;
+}
+
+// The launch geometry: chunk = 16 or 32 k values, or 0 for the one of the two
+// that lets more CTAs share an SM (32 on a tie).  sep: the cross terms
+// accumulate in tensor-memory columns of their own (see the file comment).
+inline bool tc_gemm_geom(int max_rows, int groups, int precision, int chunk, bool sep, TcGemmArgs* g) {
+  if (chunk) return tc_gemm_geom_kc(max_rows, groups, precision, chunk, sep, g);
+  TcGemmArgs a, b;
+  const bool ok32 = tc_gemm_geom_kc(max_rows, groups, precision, 32, sep, &a);
+  const bool ok16 = tc_gemm_geom_kc(max_rows, groups, precision, 16, sep, &b);
+  if (!ok32 && !ok16) return false;
+  *g = ok32 && (!ok16 || a.ctas_per_sm >= b.ctas_per_sm) ? a : b;
   return true;
 }
 
@@ -352,7 +361,8 @@ __device__ __forceinline__ void tc_class_gemm(const TcGemmArgs& g, const P& prob
             const uint32_t bo = (uint32_t)ks * 2u * lboB;
             const uint32_t first = (ch == 0 && ks == 0) ? 0u : 1u;
             umma<PREC>(dt, umma_desc(aH + ao, lboA, 128), umma_desc(bH + bo, lboB, 128), idesc, first);
-            umma<PREC>(dt + g.xoff, umma_desc(aH + ao, lboA, 128), umma_desc(bL + bo, lboB, 128), idesc, first);
+            umma<PREC>(dt + g.xoff, umma_desc(aH + ao, lboA, 128), umma_desc(bL + bo, lboB, 128), idesc,
+                       g.xoff ? first : 1u);
             umma<PREC>(dt + g.xoff, umma_desc(aL + ao, lboA, 128), umma_desc(bH + bo, lboB, 128), idesc, 1u);
           }
         }
@@ -369,14 +379,15 @@ __device__ __forceinline__ void tc_class_gemm(const TcGemmArgs& g, const P& prob
     for (int t = warp >> 2; t < ntile; t += 2) {
       const int row = t * 128 + qd * 32 + lane;
       for (int grp = 0; grp < g.groups; ++grp) {
-        uint32_t v[8], w[8];
+        uint32_t v[8], w[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
         const uint32_t ta = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(t * N + 8 * grp);
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                      : "r"(ta));
-        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                     : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
-                     : "r"(ta + g.xoff));
+        if (g.xoff)  // block-uniform
+          asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                       : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+                       : "r"(ta + g.xoff));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (row < rows && !*s_abort) {
           float f[8];
