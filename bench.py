@@ -11,6 +11,8 @@ larger than the 126 MB L2, so no flush is needed between iterations.
   e2e        served pipeline through the public API from pinned host memory
              (host->device copies and the pose read-back inside the timed region)
   plain_gpu  one pair at a time through phgpu_register_pair
+  mixed_arrivals  open-loop Poisson arrivals of a three-shape mix through one server
+  config2    256 pairs over twelve (B, N) shapes through one server (reg/s, waves/s)
   --impl reference  the reference's CPU path (SOFT sources + restated glue,
              oracle/_ref) on the host cores
 
@@ -60,6 +62,7 @@ def parse():
     ap.add_argument("--pairs", type=int, default=2)
     ap.add_argument("--calls", type=int, default=4)
     ap.add_argument("--precision", type=int, default=0, help="--profile pair: PHGPU_PRECISION_* of the context")
+    ap.add_argument("--no-config2", action="store_true", help="skip the 256-pair, 12-shape batched workload leg")
     ap.add_argument("--no-cpu-throughput", action="store_true",
                     help="reference arm: skip the nproc single-threaded processes leg")
     return ap.parse_args()
@@ -427,6 +430,50 @@ def config3(nat, local, rates=(50, 200, 500, 1000, 2000), seconds=1.0, cap=600):
             "rates": out}
 
 
+def config2(nat, local, n=256, max_wave=8):
+    """The batched workload: n independent pairs over twelve (B, N) shapes
+    (beams {32, 64, 128} x 1024, B {32, 64, 100, 128}, N {64, 128, 200},
+    seeded per pair) through one server in size-grouped waves, tf32x3, clouds
+    resident in HBM, default launch parameters.  The batch runs twice (the
+    first pass creates the executors and captures their graphs); the second
+    is reported: registrations/s and waves/s over the wall time from the first
+    submit to the drain, and the per-request latency."""
+    import torch
+    from phaser_b200 import scene
+    specs = scene.config2_specs(n)
+    pairs = scene.config2_pairs(specs)
+
+    def dev(a):
+        return None if a is None else torch.from_numpy(a).cuda()
+
+    clouds = [((dev(p.target.xyzi), dev(p.target.reflectivity)), (dev(p.source.xyzi), dev(p.source.reflectivity)))
+              for p in pairs]
+    prms = [nat.default_params(spherical_bandwidth=sp["bw"], spatial_n_voxels=sp["n_voxels"],
+                               spatial_discretize_lower=sp["lo"], spatial_discretize_upper=sp["hi"],
+                               precision=nat.PHGPU_PRECISION_TF32X3, device=local) for sp in specs]
+    srv = nat.Server(max_wave=max_wave, lanes=2, device=local)
+
+    def batch():
+        w0 = srv.stats()["waves"]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tickets = [srv.submit(prms[i], *clouds[i]) for i in range(n)]
+        srv.drain()
+        wall = time.perf_counter() - t0
+        lat = [srv.poll(t)[1] for t in tickets]
+        return wall, lat, srv.stats()["waves"] - w0
+
+    batch()
+    wall, lat, waves = batch()
+    st = srv.stats()
+    srv.close()
+    return {"workload": f"{n} pairs, 12 (B, N) shapes, beams 32/64/128 x 1024", "max_wave": max_wave,
+            "server_lanes": 2, "precision": "tf32x3", "registrations_per_s": round(n / wall, 1),
+            "waves_per_s": round(waves / wall, 1), "waves": waves, "wall_s": round(wall, 4),
+            "p50_ms": round(pct(lat, 50), 3), "p99_ms": round(pct(lat, 99), 3),
+            "executors": st["executors"], "graph_captures": st["graph_captures"]}
+
+
 def run_script_config(nat, pool, local, reps=10):
     """One pair at a time with the configuration of the reference's run script
     (phaser_share/run_phaser_core_driver: B = 150 with spherical zero padding
@@ -749,6 +796,14 @@ def main():
         except Exception as exc:  # the headline line is printed regardless
             mix = {"error": f"{type(exc).__name__}: {exc}"}
 
+    # ---------------- the batched 256-pair, 12-shape workload (rank 0)
+    c2 = None
+    if rank == 0 and not a.no_config2:
+        try:
+            c2 = config2(nat, local)
+        except Exception as exc:  # the headline line is printed regardless
+            c2 = {"error": f"{type(exc).__name__}: {exc}"}
+
     # ---------------- the reference run script's configuration (rank 0)
     rsc = None
     if rank == 0:
@@ -806,6 +861,7 @@ def main():
             "tuning": {"plain": tuned_plain, "served": tuned_served},
             "ingest": ing,
             "mixed_arrivals": mix,
+            "config2": c2,
             "run_script_config": rsc,
         }
         print(json.dumps(line), flush=True)
