@@ -157,7 +157,8 @@ int phgpu_get_samples(phgpu_ctx* ctx, int side, double* values, int32_t* nn_inde
  * array up (and may load the module there): make it before any stream
  * capture.  A call whose bandwidth differs from the previous call's on that
  * device also copies the grid directions into the array (host to device, on
- * `stream`).  After cudaDeviceReset of a device, do not call this again in
+ * `stream`, from pageable memory): make such a call outside stream capture
+ * too.  After cudaDeviceReset of a device, do not call this again in
  * the same process: the looked-up address belonged to the destroyed context. */
 #define PHGPU_NOALLOC_MAX_POINTS (1 << 18)
 #define PHGPU_NOALLOC_MAX_BANDWIDTH 128
