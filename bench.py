@@ -511,7 +511,7 @@ CPU_PATH = ("SOFT 2.0 sources of the reference (unmodified) + project FP64 FFTW-
 
 
 def config_desc(desc, world):
-    """The `config` both arms print (identical, so the driver can pair them)."""
+    """The `config` both arms print (identical, so the two arms' lines pair up)."""
     return {"workload": desc, "l2": "per-pair working set ~1 GB > 126 MB L2 (no flush needed)",
             "parallelism": f"replicas x{world}, pairs sharded per rank"}
 
