@@ -232,8 +232,10 @@ constexpr int c2r_pair_rows() {
 // (its imaginary part only ever reaches the imaginary output, which the real
 // transform discards) and the Nyquist term is zero, as the one-sequence-per-
 // transform kernel above fills it.  A pair of betas is one 16-byte load.
+// Four blocks per SM (64 registers) rather than the three that 74 registers
+// allowed: 0.0488 vs 0.0511 ms for the SO(3) angle transforms at B = 100.
 template <int NF>
-__global__ void __launch_bounds__(256) k_so3_c2r_tail(int bw_in, So3Batch bt, FftPlan plan) {
+__global__ void __launch_bounds__(256, 4) k_so3_c2r_tail(int bw_in, So3Batch bt, FftPlan plan) {
   constexpr int n = NF, Bo = NF / 2, RB = c2r_pair_rows<NF>(), ST = NF + 1;
   extern __shared__ float2 zrow[];  // [RB / 2][ST]: one beta pair per complex transform
   __shared__ int s_pos[NF];

@@ -30,17 +30,23 @@
 
 namespace phgpu {
 
-__device__ __forceinline__ int histc_bin(float x, const float* __restrict__ E, int N) {
-  if (x < E[0] || x > E[N - 1]) return -1;
-  int l = 0, h = N - 1, k = 0;
-  while ((h - l) > 1) {
-    k = (h + l) / 2;
-    if (x < E[k])
-      h = k;
-    else
-      l = k;
-  }
-  return (x == E[h]) ? h : l;
+// histc's bin (igl/histc.cpp:34-73): -1 outside [E[0], E[N-1]], else the
+// result of its binary search over the sorted edges -- the largest l <= N-2
+// with E[l] <= x, or N-1 when x == E[N-1] (NaN: N-2, where the search ends;
+// N = 1: 0).
+// The search is replaced by a start at the linear estimate (x - E[0]) * inv,
+// inv = (N-1) / (E[N-1] - E[0]), corrected by exact comparisons with the
+// edges, which gives the same bin in one or two loads instead of log2 N.
+__device__ __forceinline__ int histc_bin(float x, const float* __restrict__ E, int N, float e0, float e1,
+                                         float inv) {
+  if (x < e0 || x > e1) return -1;
+  if (N < 2) return 0;
+  if (x != x) return N - 2;
+  int l = (int)((x - e0) * inv);
+  l = min(max(l, 0), N - 2);
+  while (l > 0 && x < E[l]) --l;
+  while (l < N - 2 && x >= E[l + 1]) ++l;
+  return (x == E[l + 1]) ? l + 1 : l;
 }
 
 __global__ void k_voxelize(VoxelArgs a) {
@@ -68,9 +74,11 @@ __global__ void k_voxelize(VoxelArgs a) {
     z = nz;
   }
   const uint32_t N = (uint32_t)a.N;
-  const uint32_t bx = (uint32_t)histc_bin(x, a.edges, a.N);
-  const uint32_t by = (uint32_t)histc_bin(y, a.edges, a.N);
-  const uint32_t bz = (uint32_t)histc_bin(z, a.edges, a.N);
+  const float e0 = __ldg(&a.edges[0]), e1 = __ldg(&a.edges[a.N - 1]);
+  const float inv = a.N > 1 ? (float)(a.N - 1) / (e1 - e0) : 0.0f;
+  const uint32_t bx = (uint32_t)histc_bin(x, a.edges, a.N, e0, e1, inv);
+  const uint32_t by = (uint32_t)histc_bin(y, a.edges, a.N, e0, e1, inv);
+  const uint32_t bz = (uint32_t)histc_bin(z, a.edges, a.N, e0, e1, inv);
   const uint32_t lin = (bx * N + by) + (N * N * bz);
   const uint32_t nv = N * N * N;
   const bool ok = lin < nv;
