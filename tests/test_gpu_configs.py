@@ -107,6 +107,36 @@ def test_spatial_n512_sparse_vs_oracle():
     assert vox == O.argmax(ref)
 
 
+def test_large_translation_vs_oracle(large_pair):
+    """The N = 512 translation of the large pair itself against the FP64
+    oracle: the source rotated by the GPU's pose, both clouds voxelised by the
+    oracle, the Laplace-fused correlation in FP64 (~35 GB of host memory),
+    relative L2 and the voxel."""
+    import psutil
+    if psutil.virtual_memory().available < (96 << 30):
+        pytest.skip("the FP64 N = 512 correlation needs ~35 GB of free host memory")
+    from phaser_b200 import native as nat, scene
+    w = scene.WORKLOADS[4]
+    p = large_pair
+    N, lo, hi = w["n_voxels"], w["lo"], w["hi"]
+    c = nat.Context(spherical_bandwidth=w["bw"], spatial_n_voxels=N, spatial_discretize_lower=lo,
+                    spatial_discretize_upper=hi, flags=nat.PHGPU_FLAG_KEEP_VOLUMES,
+                    max_points=max(p.target.xyzi.shape[0], p.source.xyzi.shape[0]))
+    pose = c.register_pair((p.target.xyzi, p.target.reflectivity), (p.source.xyzi, p.source.reflectivity))
+    vox, _, vol = c.spatial_result(volume=True)
+    c.close()
+    src = O.transform(p.source.xyzi, O.rotation_xyz(*pose.xyz))
+    fv = O.discretize(p.target.xyzi, p.target.reflectivity, None, N, lo, hi)
+    gv = O.discretize(src, p.source.reflectivity, None, N, lo, hi)
+    ref = O.spatial_correlation(fv, gv, N, laplace=True)
+    del fv, gv
+    err = rel_l2(vol, ref)
+    print(f"N=512 pair translation: rel_l2 {err:.3e}, voxel {vox} (oracle {O.argmax(ref)})")
+    assert vox == pose.voxel
+    assert err <= REL_L2
+    assert vox == O.argmax(ref)
+
+
 def test_large_registration_equals_stage_composition(large_pair):
     from phaser_b200 import native as nat, scene
     w = scene.WORKLOADS[4]
