@@ -798,7 +798,7 @@ def main():
 
     # ---------------- the batched 256-pair, 12-shape workload (rank 0)
     c2 = None
-    if rank == 0 and not a.no_config2:
+    if rank == 0 and world == 1 and not a.no_config2:
         try:
             c2 = config2(nat, local)
         except Exception as exc:  # the headline line is printed regardless
