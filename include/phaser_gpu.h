@@ -251,6 +251,30 @@ int phgpu_bingham_peak(const double* values, uint32_t first_bin, uint32_t count,
                        double* mode4, double* omega4, double* xyz3);
 int phgpu_gaussian_peak(const double* values, uint32_t first_voxel, uint32_t count, uint32_t n_voxels,
                         int32_t lower, int32_t upper, double* mean3, double* cov9);
+/* Smoothed z-score peak extraction of a correlation vector
+ * (ZScorePeakExtraction::extractPeaks / calculateSmoothedZScore,
+ * phaser_core/src/backend/uncertainty/z-score-peak-extraction.cc:42-112), on
+ * the host in FP64: lag = min(lag_max, (uint32)(n * lag_percentile)); the
+ * mean and sample standard deviation of a window of `lag` values slide along
+ * the vector, and an index i > lag whose value exceeds filter_threshold and
+ * lies more than threshold deviations from the window mean is a peak when it
+ * lies above the mean; such a value is damped (influence * x + (1 - influence)
+ * * previous) before the window moves on.  Peaks are written in ascending
+ * order; *n_peaks receives their count (PHGPU_ERR_LIMIT when it exceeds
+ * capacity, the first `capacity` written).  Parameter checks as the
+ * reference's constructor: 0 < lag_percentile < 1, threshold > 0,
+ * 0 <= influence <= 1. */
+typedef struct phgpu_zscore_params {
+  double lag_percentile;    /* z_score_lag_percentile (0.05) */
+  uint32_t lag_max;         /* z_score_lag_max (20) */
+  double threshold;         /* z_score_threshold (4.33) */
+  double influence;         /* z_score_influence (0.05) */
+  double filter_threshold;  /* z_score_filter_threshold (0.405) */
+} phgpu_zscore_params;
+int phgpu_zscore_params_default(phgpu_zscore_params* params);
+int phgpu_zscore_peaks(const double* values, uint64_t n, const phgpu_zscore_params* params, uint32_t* peaks,
+                       uint64_t capacity, uint64_t* n_peaks);
+
 /* The linear-index window [first, first + count) the two evaluators take
  * around an argmax `index` of an n-element volume for k neighbours
  * (calculateStartEndNeighbor, gaussian-peak-based-eval.cc:31-41). */

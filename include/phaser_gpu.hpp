@@ -27,6 +27,7 @@
 #include <cstdint>
 #include <algorithm>
 #include <memory>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -366,6 +367,33 @@ class SphRegistration {
 // Driscoll-Healy directions, [theta][phi] order, each sampled by its nearest
 // point of the cloud's projection on the unit sphere.  The rejection radius
 // comes from the parameters as in a context.
+// ZScorePeakExtraction (phaser_core/include/phaser/backend/uncertainty/
+// z-score-peak-extraction.h): smoothed z-score peaks of a correlation vector,
+// the parameters defaulting to the reference's z_score_* flags.
+class ZScorePeakExtraction {
+ public:
+  ZScorePeakExtraction() { phgpu_zscore_params_default(&p_); }
+  void extractPeaks(const std::vector<double>& corr, std::set<uint32_t>* peaks) {
+    std::vector<uint32_t> out(corr.empty() ? 1 : corr.size());
+    uint64_t n = 0;
+    const int rc = phgpu_zscore_peaks(corr.data(), corr.size(), &p_, out.data(), out.size(), &n);
+    if (rc != PHGPU_OK) throw std::runtime_error("phgpu_zscore_peaks failed");
+    peaks->clear();
+    peaks->insert(out.begin(), out.begin() + n);
+  }
+  double getLagPercentile() const { return p_.lag_percentile; }
+  double& getLagPercentile() { return p_.lag_percentile; }
+  double getScoreThreshold() const { return p_.threshold; }
+  double& getScoreThreshold() { return p_.threshold; }
+  double getInfluence() const { return p_.influence; }
+  double& getInfluence() { return p_.influence; }
+  uint32_t getMaxLag() const { return p_.lag_max; }
+  uint32_t& getMaxLag() { return p_.lag_max; }
+
+ private:
+  phgpu_zscore_params p_;
+};
+
 class SphericalSampler {
  public:
   explicit SphericalSampler(int bandwith, const phgpu_params& base = default_params()) : base_(base) {

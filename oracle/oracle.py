@@ -117,6 +117,9 @@ def _declare(lib):
     lib.orc_voxel_grid.restype = C.c_int64
     lib.orc_voxel_grid.argtypes = [_f32p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_float, C.c_float, C.c_float,
                                    C.c_uint32, _f32p, C.c_void_p, C.c_void_p]
+    lib.orc_zscore_peaks.restype = C.c_uint64
+    lib.orc_zscore_peaks.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.c_uint32, C.c_double, C.c_double,
+                                     C.c_double, C.c_void_p, C.c_uint64]
     lib.orc_gaussian_peak.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
                                       C.c_void_p, C.c_void_p]
     lib.orc_num_threads.restype = C.c_int
@@ -429,6 +432,15 @@ def peak_window(index, n, k):
     f, c = C.c_uint32(), C.c_uint32()
     lib().orc_peak_window(int(index), int(n), int(k), C.byref(f), C.byref(c))
     return f.value, c.value
+
+
+def zscore_peaks(corr, lag_percentile=0.05, lag_max=20, threshold=4.33, influence=0.05, filter_threshold=0.405):
+    """ZScorePeakExtraction::extractPeaks (z-score-peak-extraction.cc:42-112): ascending signal indices."""
+    v = np.ascontiguousarray(corr, np.float64)
+    out = np.zeros(max(len(v), 1), np.uint32)
+    k = lib().orc_zscore_peaks(v.ctypes.data, len(v), float(lag_percentile), int(lag_max), float(threshold),
+                               float(influence), float(filter_threshold), out.ctypes.data, len(out))
+    return out[:k].copy()
 
 
 def bingham_peak(values, first, bw):

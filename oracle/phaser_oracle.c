@@ -1689,3 +1689,45 @@ uint32_t orc_spatial_correlation_padded(int N, int pad, int C, const double* f, 
   free(vg);
   return size;
 }
+
+/* ZScorePeakExtraction::extractPeaks + calculateSmoothedZScore             */
+/* (phaser_core/src/backend/uncertainty/z-score-peak-extraction.cc:42-112):  */
+/* a sliding window of `lag` values (mean, standard deviation with divisor  */
+/* lag - 1) over a copy of the input; an index above filter_thr that is     */
+/* more than thr deviations from the mean is a signal when above it and is  */
+/* damped by `influence` before the window moves.  Window sums in index     */
+/* order.  Returns the number of signals (indices written to out, at most   */
+/* cap of them).                                                            */
+uint64_t orc_zscore_peaks(const double* corr, uint64_t n, double lag_pct, uint32_t lag_max, double thr,
+                          double influence, double filter_thr, uint32_t* out, uint64_t cap) {
+  const uint32_t share = (uint32_t)((double)n * lag_pct);
+  const uint64_t lag = share < lag_max ? share : lag_max;
+  if (n <= lag + 2) return 0;
+  double* in = (double*)malloc(sizeof(double) * n);
+  memcpy(in, corr, sizeof(double) * n);
+  double avg = 0.0, dev = 0.0, s = 0.0, q = 0.0;
+  for (uint64_t k = 0; k < lag; ++k) s += in[k];
+  avg = s / (double)lag;
+  for (uint64_t k = 0; k < lag; ++k) q += (in[k] - avg) * (in[k] - avg);
+  dev = sqrt(q / ((double)lag - 1.0));
+  uint64_t count = 0;
+  for (uint64_t i = lag + 1; i < n; ++i) {
+    const double x = in[i];
+    if (x <= filter_thr) continue;
+    if (fabs(x - avg) > thr * dev) {
+      if (x >= avg) {
+        if (count < cap) out[count] = (uint32_t)i;
+        ++count;
+      }
+      in[i] = influence * x + (1.0 - influence) * in[i - 1];
+    }
+    s = 0.0;
+    for (uint64_t k = i - lag; k < i; ++k) s += in[k];
+    avg = s / (double)lag;
+    q = 0.0;
+    for (uint64_t k = i - lag; k < i; ++k) q += (in[k] - avg) * (in[k] - avg);
+    dev = sqrt(q / ((double)lag - 1.0));
+  }
+  free(in);
+  return count;
+}

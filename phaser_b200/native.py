@@ -137,7 +137,7 @@ EXPORTED = [
     "phgpu_voxel_grid_destroy", "phgpu_voxel_grid_filter", "phgpu_voxel_grid_last_error",
     "phgpu_spatial_correlation_size", "phgpu_pose_reruns", "phgpu_server_poll_volumes",
     "phgpu_server_get_stats", "phgpu_tuning_get", "phgpu_tuning_set", "phgpu_autotune",
-    "phgpu_server_set_tuning",
+    "phgpu_server_set_tuning", "phgpu_zscore_params_default", "phgpu_zscore_peaks",
 ]
 
 _LIB = None
@@ -207,6 +207,9 @@ def load(path: str = LIB_PATH):
     lib.phgpu_peak_window.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
                                       C.POINTER(C.c_uint32)]
     lib.phgpu_peak_window.restype = None
+    lib.phgpu_zscore_params_default.argtypes = [C.POINTER(ZScoreParams)]
+    lib.phgpu_zscore_peaks.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(ZScoreParams), C.c_void_p, C.c_uint64,
+                                       C.POINTER(C.c_uint64)]
     lib.phgpu_sample_s2_noalloc.argtypes = [C.POINTER(Params), C.POINTER(Cloud), C.c_void_p, C.c_void_p,
                                             C.c_void_p]
     lib.phgpu_ply_info.argtypes = [C.c_char_p, C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
@@ -321,6 +324,37 @@ def sample_s2_noalloc(params: Params, xyzi, reflectivity, ambient, values_dev, n
         _check_device_tensor("nn_index_dev", nn_index_dev, torch.int32, nq, xyzi.device)
     return load().phgpu_sample_s2_noalloc(C.byref(params), C.byref(c), _addr(values_dev), _addr(nn_index_dev),
                                           None if stream is None else stream.cuda_stream)
+
+
+class ZScoreParams(C.Structure):
+    """phgpu_zscore_params (the reference's z_score_* flags)."""
+    _fields_ = [
+        ("lag_percentile", C.c_double),
+        ("lag_max", C.c_uint32),
+        ("threshold", C.c_double),
+        ("influence", C.c_double),
+        ("filter_threshold", C.c_double),
+    ]
+
+
+def zscore_peaks(values, **overrides):
+    """Smoothed z-score peaks of a correlation vector (ZScorePeakExtraction::
+    extractPeaks): ascending indices (uint32).  Keyword overrides of the
+    defaults: lag_percentile, lag_max, threshold, influence, filter_threshold."""
+    lib = load()
+    p = ZScoreParams()
+    lib.phgpu_zscore_params_default(C.byref(p))
+    for k, v in overrides.items():
+        if k not in dict(ZScoreParams._fields_):
+            raise ValueError(f"unknown z-score parameter {k!r}")
+        setattr(p, k, v)
+    v = np.ascontiguousarray(values, np.float64).reshape(-1)
+    out = np.zeros(max(v.size, 1), np.uint32)
+    n = C.c_uint64()
+    rc = lib.phgpu_zscore_peaks(v.ctypes.data, v.size, C.byref(p), out.ctypes.data, out.size, C.byref(n))
+    if rc != PHGPU_OK:
+        raise PhgpuError(f"phgpu_zscore_peaks failed ({rc})")
+    return out[:n.value].copy()
 
 
 def peak_window(index, n, k):

@@ -145,6 +145,20 @@ int main() {
     for (int k = 0; k < 8; ++k)
       if (pc.xyzi[k] != want[k]) return 6;
   }
+  {
+    // ZScorePeakExtraction: spikes on a flat signal (the reference's flags)
+    std::vector<double> corr(2000);
+    for (size_t i = 0; i < corr.size(); ++i) corr[i] = 1.0 + 1e-3 * std::sin((double)i);
+    corr[300] = corr[777] = corr[1500] = 50.0;
+    phaser_gpu::ZScorePeakExtraction z;
+    std::set<uint32_t> peaks;
+    z.extractPeaks(corr, &peaks);
+    std::printf("zscore_peaks %zu\n", peaks.size());
+    if (peaks != std::set<uint32_t>{300u, 777u, 1500u}) return 7;
+    z.getScoreThreshold() = 1e9;  // nothing stands out any more
+    z.extractPeaks(corr, &peaks);
+    if (!peaks.empty()) return 8;
+  }
   std::printf("ok\n");
   return 0;
 }
