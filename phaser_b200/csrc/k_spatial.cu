@@ -315,8 +315,10 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
   // MEAN divides by the total channel count: a product with the reciprocal,
   // exact for the reference's 4 channels (within one rounding otherwise)
   const float inv_total = 1.0f / (float)a.n_total_ch;
+  // Wt is a power of two (fuse_z_tile_ok): shifts, not a runtime division per element
+  const int lwt = __ffs(Wt) - 1;
   for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
-    const int zp = e / Wt, t = e - zp * Wt;
+    const int zp = e >> lwt, t = e & (Wt - 1);
     float2* row = tile + (size_t)zp * rowlen;
     float2 F, G;
     if (!a.laplace) {
@@ -370,7 +372,7 @@ __global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int
   __syncthreads();
   fft_any_cols<NF, true>(tile, Wt, rowlen, plan);
   for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
-    const int z = e / Wt, t = e - z * Wt;
+    const int z = e >> lwt, t = e & (Wt - 1);
     if (t < wt) a.cspec[((size_t)z * N + xp) * H2p + ky0 + t] = tile[(size_t)z * rowlen + t];
   }
 }
