@@ -309,41 +309,44 @@ __device__ __forceinline__ void tc_class_gemm(const TcGemmArgs& g, const P& prob
       if constexpr (PREC == kSo3Tf32x3) {
         uint4* hi = reinterpret_cast<uint4*>(A32);
         float4* lo = reinterpret_cast<float4*>(AX);
-        for (int e = tid; e < kcc * rows; e += kTcThreads) {
-          const int cc = e / rows, row = e - cc * rows;
-          const size_t idx = (size_t)cc * MP + row;
-          const uint4 x = hi[idx];
-          const uint4 h = make_uint4(tf32_rn(x.x), tf32_rn(x.y), tf32_rn(x.z), tf32_rn(x.w));
-          hi[idx] = h;
-          lo[idx] = make_float4(tf32_lo(__uint_as_float(x.x), h.x), tf32_lo(__uint_as_float(x.y), h.y),
-                                tf32_lo(__uint_as_float(x.z), h.z), tf32_lo(__uint_as_float(x.w), h.w));
+        // (k group, row) walked without a per-element division
+        for (int cc = 0; cc < kcc; ++cc) {
+          for (int row = tid; row < rows; row += kTcThreads) {
+            const size_t idx = (size_t)cc * MP + row;
+            const uint4 x = hi[idx];
+            const uint4 h = make_uint4(tf32_rn(x.x), tf32_rn(x.y), tf32_rn(x.z), tf32_rn(x.w));
+            hi[idx] = h;
+            lo[idx] = make_float4(tf32_lo(__uint_as_float(x.x), h.x), tf32_lo(__uint_as_float(x.y), h.y),
+                                  tf32_lo(__uint_as_float(x.z), h.z), tf32_lo(__uint_as_float(x.w), h.w));
+          }
         }
       } else {
         uint4* hi16 = reinterpret_cast<uint4*>(AX);
         uint4* lo16 = reinterpret_cast<uint4*>(AX + g.aconv / 2);
         const float4* src = reinterpret_cast<const float4*>(A32);
-        for (int e = tid; e < (kread / 8) * rows; e += kTcThreads) {
-          const int c16 = e / rows, row = e - c16 * rows;
-          float x[8];
+        for (int c16 = 0; c16 < kread / 8; ++c16) {
+          for (int row = tid; row < rows; row += kTcThreads) {
+            float x[8];
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int cc = 2 * c16 + h;
-            const float4 v = cc < kcc ? src[(size_t)cc * MP + row] : make_float4(0.f, 0.f, 0.f, 0.f);
-            x[4 * h] = v.x;
-            x[4 * h + 1] = v.y;
-            x[4 * h + 2] = v.z;
-            x[4 * h + 3] = v.w;
-          }
-          __nv_bfloat162 h2[4], l2[4];
+            for (int h = 0; h < 2; ++h) {
+              const int cc = 2 * c16 + h;
+              const float4 v = cc < kcc ? src[(size_t)cc * MP + row] : make_float4(0.f, 0.f, 0.f, 0.f);
+              x[4 * h] = v.x;
+              x[4 * h + 1] = v.y;
+              x[4 * h + 2] = v.z;
+              x[4 * h + 3] = v.w;
+            }
+            __nv_bfloat162 h2[4], l2[4];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const __nv_bfloat16 a = __float2bfloat16_rn(x[2 * u]), b = __float2bfloat16_rn(x[2 * u + 1]);
-            h2[u] = __halves2bfloat162(a, b);
-            l2[u] = __halves2bfloat162(__float2bfloat16_rn(x[2 * u] - __bfloat162float(a)),
-                                       __float2bfloat16_rn(x[2 * u + 1] - __bfloat162float(b)));
+            for (int u = 0; u < 4; ++u) {
+              const __nv_bfloat16 a = __float2bfloat16_rn(x[2 * u]), b = __float2bfloat16_rn(x[2 * u + 1]);
+              h2[u] = __halves2bfloat162(a, b);
+              l2[u] = __halves2bfloat162(__float2bfloat16_rn(x[2 * u] - __bfloat162float(a)),
+                                         __float2bfloat16_rn(x[2 * u + 1] - __bfloat162float(b)));
+            }
+            hi16[(size_t)c16 * MP + row] = *reinterpret_cast<uint4*>(h2);
+            lo16[(size_t)c16 * MP + row] = *reinterpret_cast<uint4*>(l2);
           }
-          hi16[(size_t)c16 * MP + row] = *reinterpret_cast<uint4*>(h2);
-          lo16[(size_t)c16 * MP + row] = *reinterpret_cast<uint4*>(l2);
         }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
