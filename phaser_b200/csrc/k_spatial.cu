@@ -464,12 +464,13 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
     s_live[r] = 0;
     s_flag[r] = rowlive ? (rowlive[z * N + 2 * r] | rowlive[z * N + 2 * r + 1]) : 1;
     any_flag |= s_flag[r];
-    s_posH[r] = fixed_freq2pos<NH>(r);
   }
-  for (int k = threadIdx.x; k < N; k += blockDim.x) s_posN[k] = fixed_freq2pos<N>(k);
   // a slab without a flagged row transforms to zero: nothing to do where the
-  // array already holds zeros there
+  // array already holds zeros there (about half the slabs of a room scan, so
+  // they leave before any other set-up)
   if (!__syncthreads_or(any_flag) && !held_nonzero) return;
+  for (int r = threadIdx.x; r < NH; r += blockDim.x) s_posH[r] = fixed_freq2pos<NH>(r);
+  for (int k = threadIdx.x; k < N; k += blockDim.x) s_posN[k] = fixed_freq2pos<N>(k);
   for (int e = threadIdx.x; e < NH * Q; e += blockDim.x) {
     const int r = e / Q, y4 = (e - r * Q) * 4;
     if (!s_flag[r]) {  // no point in either row: skip the loads
