@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--pairs-per-step", type=int, default=128)
+    ap.add_argument("--pairs-per-step", type=int, default=512)
     ap.add_argument("--max-wave", type=int, default=16, help="pairs per wave of the server")
     ap.add_argument("--lanes", type=int, default=2, help="waves in flight at once")
     ap.add_argument("--pool", type=int, default=4, help="distinct synthetic pairs per rank")
