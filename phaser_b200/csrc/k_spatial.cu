@@ -246,8 +246,12 @@ struct FuseZTma {
   int chunks;   // copies (zbox * chunks >= N)
 };
 
+// Two blocks per SM for the compile-time lengths (the bound lets the
+// compiler schedule for it: 0.1294 against 0.1336 ms at N = 200; 640 or 672
+// threads, whose radix passes divide more evenly, ran the same); the runtime
+// plan's generic transform needs its 128 registers.
 template <int NF>
-__global__ void __launch_bounds__(512) k_fuse_z(SpatialArgs a, FftPlan plan, int Wt, int x_natural,
+__global__ void __launch_bounds__(512, NF > 0 ? 2 : 1) k_fuse_z(SpatialArgs a, FftPlan plan, int Wt, int x_natural,
                                                 const __grid_constant__ CUtensorMap tmap, FuseZTma tma) {
   extern __shared__ __align__(128) float2 tile[];  // [z][arr][t]
   const int N = NF > 0 ? NF : a.N;
