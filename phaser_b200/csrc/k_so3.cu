@@ -140,7 +140,7 @@ void so3_beta_table(int bw_out, double* tab) {
 // Forward DFT over a (alpha) for one b and a tile of Wt = 2^LOG2W betas
 // (8, 16 or 32: a tuned parameter, 16 by default).
 template <int NF, int LOG2W>
-__global__ void __launch_bounds__(256, NF > 0 ? 8 : 2) k_so3_fft_a(int bw_in, int bw_out, So3Batch bt, FftPlan plan) {
+__global__ void k_so3_fft_a(int bw_in, int bw_out, So3Batch bt, FftPlan plan) {
   extern __shared__ float2 tile[];  // [a][beta tile]
   constexpr int Wt = 1 << LOG2W;
   const int n = NF > 0 ? NF : 2 * bw_out;
