@@ -158,8 +158,9 @@ int phgpu_get_samples(phgpu_ctx* ctx, int side, double* values, int32_t* nn_inde
  * capture.  A call whose bandwidth differs from the previous call's on that
  * device also copies the grid directions into the array (host to device, on
  * `stream`, from pageable memory): make such a call outside stream capture
- * too.  After cudaDeviceReset of a device, do not call this again in
- * the same process: the looked-up address belonged to the destroyed context. */
+ * too (under capture it returns PHGPU_ERR_INVALID and enqueues nothing).
+ * After cudaDeviceReset of a device, do not call this again in the same
+ * process: the looked-up address belonged to the destroyed context. */
 #define PHGPU_NOALLOC_MAX_POINTS (1 << 18)
 #define PHGPU_NOALLOC_MAX_BANDWIDTH 128
 int phgpu_sample_s2_noalloc(const phgpu_params* params, const phgpu_cloud* cloud, float* values_dev,

@@ -89,6 +89,11 @@ int phgpu_sample_s2_noalloc(const phgpu_params* params, const phgpu_cloud* cloud
       slot.scratch = (char*)p;
     }
     if (slot.grid_bw != bw) {
+      // a pageable host-to-device copy cannot be captured: refuse instead of
+      // invalidating the caller's capture
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return PHGPU_ERR_CUDA;
+      if (cs != cudaStreamCaptureStatusNone) return PHGPU_ERR_INVALID;
       dh_grid(bw, g_host_grid);
       // pageable source: the call returns once the source has been staged
       if (cudaMemcpyAsync(slot.scratch, g_host_grid, sizeof(float4) * 4 * (size_t)bw * bw, cudaMemcpyHostToDevice,

@@ -87,3 +87,29 @@ def test_noalloc_rejections():
     assert lib.phgpu_sample_s2_noalloc(C.byref(p), C.byref(host_cloud), addr, None, None) == native.PHGPU_ERR_INVALID
     assert lib.phgpu_sample_s2_noalloc(C.byref(p), C.byref(dev_cloud), None, None, None) == native.PHGPU_ERR_INVALID
     assert lib.phgpu_sample_s2_noalloc(None, C.byref(dev_cloud), addr, None, None) == native.PHGPU_ERR_INVALID
+
+
+@pytest.mark.gpu
+def test_noalloc_new_bandwidth_refused_under_capture():
+    """A bandwidth change needs a pageable host-to-device copy, which cannot be
+    captured: under stream capture the call returns PHGPU_ERR_INVALID and
+    enqueues nothing; outside capture the same call then succeeds."""
+    import torch
+    from phaser_b200 import native
+    cl = _clouds()[0]
+    x = torch.from_numpy(np.ascontiguousarray(cl.xyzi, np.float32)).cuda()
+    bw_a, bw_b = 16, 20
+    vals = {bw: torch.empty(16 * bw * bw, dtype=torch.float32, device="cuda") for bw in (bw_a, bw_b)}
+    p_a = native.default_params(spherical_bandwidth=bw_a)
+    p_b = native.default_params(spherical_bandwidth=bw_b)
+    assert native.sample_s2_noalloc(p_a, x, None, None, vals[bw_a], None, torch.cuda.current_stream()) == native.PHGPU_OK
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        rc = native.sample_s2_noalloc(p_b, x, None, None, vals[bw_b], None, torch.cuda.current_stream())
+    assert rc == native.PHGPU_ERR_INVALID
+    del g
+    assert native.sample_s2_noalloc(p_b, x, None, None, vals[bw_b], None, torch.cuda.current_stream()) == native.PHGPU_OK
+    torch.cuda.synchronize()
+    ref_vals, _ = _run_context(native, p_b, x, None)
+    np.testing.assert_array_equal(vals[bw_b].cpu().numpy().astype(np.float64).reshape(4, -1), ref_vals)
