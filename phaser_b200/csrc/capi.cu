@@ -722,11 +722,6 @@ int phgpu_ctx_destroy(phgpu_ctx* ctx) {
 
 // ------------------------------------------------------------------ stages
 
-// S^2 channel count with data: {range, intensity} always, + reflectivity, + ambient.
-static int s2_channels(const phgpu_cloud* c) {
-  return c->ambient ? 4 : (c->reflectivity ? 3 : 2);
-}
-
 int phgpu_upload_cloud(phgpu_ctx* ctx, const phgpu_cloud* c, int side, cudaStream_t st) {
   CKV(ensure_cloud_capacity(ctx, c->n_points));
   const cudaMemcpyKind kind = c->on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;

@@ -53,72 +53,100 @@ __host__ __device__ inline int fft_pos2freq(int pos, const FftPlan& p) {
   return k;
 }
 
-template <int R, bool INV>
+// Packed FP32 pairs (sm_100 FADD2 / FFMA2 / FMUL2, PK = true): one
+// instruction for both components of a complex sum, or of a complex times a
+// real constant; PK = false gives the same arithmetic per component.  The
+// rotations by +-i swap the components, which a packed pair cannot do for
+// free, so the sums that take them stay per component.
+template <bool PK>
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+  if constexpr (PK) return __fadd2_rn(a, b);
+  else return make_float2(a.x + b.x, a.y + b.y);
+}
+template <bool PK>
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  if constexpr (PK) return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+  else return make_float2(a.x - b.x, a.y - b.y);
+}
+// c + s a
+template <bool PK>
+__device__ __forceinline__ float2 pfma(float s, float2 a, float2 c) {
+  if constexpr (PK) return __ffma2_rn(make_float2(s, s), a, c);
+  else return make_float2(__fmaf_rn(s, a.x, c.x), __fmaf_rn(s, a.y, c.y));
+}
+template <bool PK>
+__device__ __forceinline__ float2 pmul(float s, float2 a) {
+  if constexpr (PK) return __fmul2_rn(make_float2(s, s), a);
+  else return make_float2(s * a.x, s * a.y);
+}
+// a + i*sg*d and a - i*sg*d
+template <bool INV>
+__device__ __forceinline__ void rot_pm(float2 a, float2 d, float2& plus, float2& minus) {
+  if constexpr (INV) {  // sg = +1: i d = (-d.y, d.x)
+    plus = make_float2(a.x - d.y, a.y + d.x);
+    minus = make_float2(a.x + d.y, a.y - d.x);
+  } else {  // sg = -1: -i d = (d.y, -d.x)
+    plus = make_float2(a.x + d.y, a.y - d.x);
+    minus = make_float2(a.x - d.y, a.y + d.x);
+  }
+}
+
+template <int R, bool INV, bool PK = true>
 __device__ __forceinline__ void dft_small(float2 (&x)[R]) {
   constexpr float sg = INV ? 1.0f : -1.0f;  // exponent sign
   if constexpr (R == 2) {
     const float2 a = x[0], b = x[1];
-    x[0] = cadd(a, b);
-    x[1] = csub(a, b);
+    x[0] = padd<PK>(a, b);
+    x[1] = psub<PK>(a, b);
   } else if constexpr (R == 3) {
     const float s3 = 0.86602540378443864676f;
-    const float2 t1 = cadd(x[1], x[2]);
-    const float2 t2 = csub(x[1], x[2]);
-    const float2 y0 = cadd(x[0], t1);
-    const float2 m1 = make_float2(x[0].x - 0.5f * t1.x, x[0].y - 0.5f * t1.y);
-    // i * sg * s3 * t2
-    const float2 m2 = make_float2(-sg * s3 * t2.y, sg * s3 * t2.x);
+    const float2 t1 = padd<PK>(x[1], x[2]);
+    const float2 t2 = psub<PK>(x[1], x[2]);
+    const float2 y0 = padd<PK>(x[0], t1);
+    const float2 m1 = pfma<PK>(-0.5f, t1, x[0]);
+    // m1 +- i*sg*s3*t2
+    rot_pm<INV>(m1, pmul<PK>(s3, t2), x[1], x[2]);
     x[0] = y0;
-    x[1] = cadd(m1, m2);
-    x[2] = csub(m1, m2);
   } else if constexpr (R == 4) {
-    const float2 t0 = cadd(x[0], x[2]);
-    const float2 t1 = csub(x[0], x[2]);
-    const float2 t2 = cadd(x[1], x[3]);
-    const float2 d = csub(x[1], x[3]);
-    const float2 t3 = make_float2(-sg * d.y, sg * d.x);  // i*sg*d
-    x[0] = cadd(t0, t2);
-    x[2] = csub(t0, t2);
-    x[1] = cadd(t1, t3);
-    x[3] = csub(t1, t3);
+    const float2 t0 = padd<PK>(x[0], x[2]);
+    const float2 t1 = psub<PK>(x[0], x[2]);
+    const float2 t2 = padd<PK>(x[1], x[3]);
+    const float2 d = psub<PK>(x[1], x[3]);
+    x[0] = padd<PK>(t0, t2);
+    x[2] = psub<PK>(t0, t2);
+    rot_pm<INV>(t1, d, x[1], x[3]);
   } else if constexpr (R == 5) {
     const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;
     const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;
-    const float2 t1 = cadd(x[1], x[4]), t2 = cadd(x[2], x[3]);
-    const float2 t3 = csub(x[1], x[4]), t4 = csub(x[2], x[3]);
-    const float2 y0 = cadd(x[0], cadd(t1, t2));
-    const float2 a1 = make_float2(x[0].x + c1 * t1.x + c2 * t2.x, x[0].y + c1 * t1.y + c2 * t2.y);
-    const float2 a2 = make_float2(x[0].x + c2 * t1.x + c1 * t2.x, x[0].y + c2 * t1.y + c1 * t2.y);
-    const float2 b1 = make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
-    const float2 b2 = make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+    const float2 t1 = padd<PK>(x[1], x[4]), t2 = padd<PK>(x[2], x[3]);
+    const float2 t3 = psub<PK>(x[1], x[4]), t4 = psub<PK>(x[2], x[3]);
+    const float2 y0 = padd<PK>(x[0], padd<PK>(t1, t2));
+    const float2 a1 = pfma<PK>(c2, t2, pfma<PK>(c1, t1, x[0]));
+    const float2 a2 = pfma<PK>(c1, t2, pfma<PK>(c2, t1, x[0]));
+    const float2 b1 = pfma<PK>(s2, t4, pmul<PK>(s1, t3));
+    const float2 b2 = pfma<PK>(-s1, t4, pmul<PK>(s2, t3));
     // y1 = a1 + i*sg*b1, y4 = a1 - i*sg*b1, y2 = a2 + i*sg*b2, y3 = a2 - i*sg*b2
-    const float2 ib1 = make_float2(-sg * b1.y, sg * b1.x);
-    const float2 ib2 = make_float2(-sg * b2.y, sg * b2.x);
     x[0] = y0;
-    x[1] = cadd(a1, ib1);
-    x[4] = csub(a1, ib1);
-    x[2] = cadd(a2, ib2);
-    x[3] = csub(a2, ib2);
+    rot_pm<INV>(a1, b1, x[1], x[4]);
+    rot_pm<INV>(a2, b2, x[2], x[3]);
   } else if constexpr (R == 8) {
     float2 e[4] = {x[0], x[2], x[4], x[6]};
     float2 o[4] = {x[1], x[3], x[5], x[7]};
-    dft_small<4, INV>(e);
-    dft_small<4, INV>(o);
+    dft_small<4, INV, PK>(e);
+    dft_small<4, INV, PK>(o);
     const float h = 0.70710678118654752440f;
-    // w8^k = exp(sg * i * pi k / 4)
-    const float2 w1 = make_float2(h, sg * h);
-    const float2 w3 = make_float2(-h, sg * h);
-    const float2 o1 = cmul(o[1], w1);
-    const float2 o2 = make_float2(-sg * o[2].y, sg * o[2].x);
-    const float2 o3 = cmul(o[3], w3);
-    x[0] = cadd(e[0], o[0]);
-    x[4] = csub(e[0], o[0]);
-    x[1] = cadd(e[1], o1);
-    x[5] = csub(e[1], o1);
-    x[2] = cadd(e[2], o2);
-    x[6] = csub(e[2], o2);
-    x[3] = cadd(e[3], o3);
-    x[7] = csub(e[3], o3);
+    // w8^k = exp(sg * i * pi k / 4): o1 w8 = h (o.x - sg o.y, o.y + sg o.x),
+    // o3 w8^3 = (-h (o.x + sg o.y), h (sg o.x - o.y))
+    const float2 o1 = pmul<PK>(h, make_float2(o[1].x - sg * o[1].y, o[1].y + sg * o[1].x));
+    const float2 p3 = make_float2(o[3].x + sg * o[3].y, sg * o[3].x - o[3].y);
+    const float2 o3 = PK ? __fmul2_rn(make_float2(-h, h), p3) : make_float2(-h * p3.x, h * p3.y);
+    x[0] = padd<PK>(e[0], o[0]);
+    x[4] = psub<PK>(e[0], o[0]);
+    x[1] = padd<PK>(e[1], o1);
+    x[5] = psub<PK>(e[1], o1);
+    rot_pm<INV>(e[2], o[2], x[2], x[6]);
+    x[3] = padd<PK>(e[3], o3);
+    x[7] = psub<PK>(e[3], o3);
   } else {
     // generic small odd prime
     float2 y[R];
@@ -167,14 +195,19 @@ __device__ __forceinline__ void fft_stage(float2* buf, int ntrans, int tstride, 
     float2 x[R];
 #pragma unroll
     for (int j = 0; j < R; ++j) x[j] = base[j * es];
+    // m == 1: j2 == 0, every twiddle is 1 (a block-uniform branch)
     if (INV) {
+      if (m > 1) {
 #pragma unroll
-      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], cconj(__ldg(&tw[twstep * j2 * k])));
+        for (int k = 1; k < R; ++k) x[k] = cmul(x[k], cconj(__ldg(&tw[twstep * j2 * k])));
+      }
       dft_small<R, true>(x);
     } else {
       dft_small<R, false>(x);
+      if (m > 1) {
 #pragma unroll
-      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], __ldg(&tw[twstep * j2 * k]));
+        for (int k = 1; k < R; ++k) x[k] = cmul(x[k], __ldg(&tw[twstep * j2 * k]));
+      }
     }
 #pragma unroll
     for (int j = 0; j < R; ++j) base[j * es] = x[j];
@@ -443,9 +476,9 @@ __device__ __forceinline__ void fixed_stage(float2* buf, int ntrans, int tstride
     if constexpr (INV) {
 #pragma unroll
       for (int k = 1; k < R; ++k) x[k] = cmul(x[k], cconj(__ldg(&tw[twstep * j2 * k])));
-      dft_small<R, true>(x);
+      dft_small<R, true, false>(x);
     } else {
-      dft_small<R, false>(x);
+      dft_small<R, false, false>(x);
 #pragma unroll
       for (int k = 1; k < R; ++k) x[k] = cmul(x[k], __ldg(&tw[twstep * j2 * k]));
     }
@@ -493,9 +526,11 @@ __device__ __forceinline__ void fft_any(float2* buf, int ntrans, int tstride, in
 // is one division per call instead of one per butterfly, and a warp touches
 // neighbouring columns of one butterfly.  Needs ntrans <= nthr (callers fall
 // back to fft_fixed otherwise).
-template <int N, int R, int L, bool INV>
+// PODD: element i of a column sits `podd` further when i is odd (a row-parity
+// slot that spreads neighbouring rows over both halves of the banks).
+template <int N, int R, int L, bool INV, bool PODD = false>
 __device__ __forceinline__ void fixed_col_stage(float2* buf, int stride, const float2* __restrict__ tw, int t, int g,
-                                                int groups) {
+                                                int groups, int podd = 0) {
   constexpr int m = L / R;
   constexpr int nb = N / R;
   constexpr int twstep = N / L;
@@ -503,32 +538,40 @@ __device__ __forceinline__ void fixed_col_stage(float2* buf, int stride, const f
   const size_t es = (size_t)m * stride;
   for (int bf = g; bf < nb; bf += groups) {
     const int blk = bf / m, j2 = bf - blk * m;
-    float2* base = buf + t + (size_t)(blk * L + j2) * stride;
+    const int r0 = blk * L + j2;
+    float2* base = buf + t + (size_t)r0 * stride;
+    // element j is row r0 + j m: its parity is r0's when j m is even
+    const int po0 = PODD ? (r0 & 1) * podd : 0, po1 = PODD ? podd - po0 : 0;
     float2 x[R];
 #pragma unroll
-    for (int j = 0; j < R; ++j) x[j] = base[j * es];
+    for (int j = 0; j < R; ++j) x[j] = base[j * es + (((j * m) & 1) ? po1 : po0)];
+    // m == 1 (the last forward / first inverse stage): j2 == 0, every twiddle is 1
     if constexpr (INV) {
+      if constexpr (m > 1) {
 #pragma unroll
-      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], cconj(__ldg(&tw[twstep * j2 * k])));
+        for (int k = 1; k < R; ++k) x[k] = cmul(x[k], cconj(__ldg(&tw[twstep * j2 * k])));
+      }
       dft_small<R, true>(x);
     } else {
       dft_small<R, false>(x);
+      if constexpr (m > 1) {
 #pragma unroll
-      for (int k = 1; k < R; ++k) x[k] = cmul(x[k], __ldg(&tw[twstep * j2 * k]));
+        for (int k = 1; k < R; ++k) x[k] = cmul(x[k], __ldg(&tw[twstep * j2 * k]));
+      }
     }
 #pragma unroll
-    for (int j = 0; j < R; ++j) base[j * es] = x[j];
+    for (int j = 0; j < R; ++j) base[j * es + (((j * m) & 1) ? po1 : po0)] = x[j];
   }
 }
 
-template <int N, bool INV, int SI = 0>
+template <int N, bool INV, bool PODD = false, int SI = 0>
 __device__ __forceinline__ void fixed_col_stages(float2* buf, int stride, const float2* __restrict__ tw, int t, int g,
-                                                 int groups) {
+                                                 int groups, int podd = 0) {
   if constexpr (SI < FixedFft<N>::count) {
     constexpr int S = INV ? (FixedFft<N>::count - 1 - SI) : SI;
-    fixed_col_stage<N, FixedFft<N>::r[S], fixed_L<N, S>(), INV>(buf, stride, tw, t, g, groups);
+    fixed_col_stage<N, FixedFft<N>::r[S], fixed_L<N, S>(), INV, PODD>(buf, stride, tw, t, g, groups, podd);
     __syncthreads();
-    fixed_col_stages<N, INV, SI + 1>(buf, stride, tw, t, g, groups);
+    fixed_col_stages<N, INV, PODD, SI + 1>(buf, stride, tw, t, g, groups, podd);
   }
 }
 
@@ -545,6 +588,17 @@ __device__ __forceinline__ void fft_any_cols(float2* buf, int ntrans, int stride
     }
   }
   fft_any<NF, INV, -2>(buf, ntrans, 1, stride, p);
+}
+
+// The same with the row-parity slot: element i of column t at
+// buf[t + i * stride + (i odd ? podd : 0)].  Compile-time lengths only, and
+// ntrans <= blockDim.x.
+template <int NF, bool INV>
+__device__ __forceinline__ void fft_fixed_cols_podd(float2* buf, int ntrans, int stride, int podd,
+                                                    const float2* __restrict__ tw) {
+  static_assert(NF > 0, "row-parity slots need a compile-time plan");
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  fixed_col_stages<NF, INV, true>(buf, stride, tw, tid % ntrans, tid / ntrans, nthr / ntrans, podd);
 }
 
 

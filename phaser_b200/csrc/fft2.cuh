@@ -61,11 +61,11 @@ __device__ __forceinline__ float2 ctw(int e) {
 
 // In-register DIF transform of M points (M = RA * RB or a single radix);
 // output in the digit-reversed order of the (RA, RB) factorisation.
-template <int RA, int RB, bool INV>
+template <int RA, int RB, bool INV, bool PK = true>
 __device__ __forceinline__ void reg_block(float2 (&x)[RA * RB]) {
   constexpr int M = RA * RB;
   if constexpr (RB == 1) {
-    dft_small<RA, INV>(x);
+    dft_small<RA, INV, PK>(x);
   } else if constexpr (!INV) {
     // radix RA over stride RB, twiddle w_M^{j2 k1}
 #pragma unroll
@@ -73,7 +73,7 @@ __device__ __forceinline__ void reg_block(float2 (&x)[RA * RB]) {
       float2 v[RA];
 #pragma unroll
       for (int j1 = 0; j1 < RA; ++j1) v[j1] = x[j2 + RB * j1];
-      dft_small<RA, false>(v);
+      dft_small<RA, false, PK>(v);
 #pragma unroll
       for (int k1 = 0; k1 < RA; ++k1) x[j2 + RB * k1] = (j2 * k1 == 0) ? v[k1] : cmul(v[k1], ctw<M>((j2 * k1) % M));
     }
@@ -83,7 +83,7 @@ __device__ __forceinline__ void reg_block(float2 (&x)[RA * RB]) {
       float2 v[RB];
 #pragma unroll
       for (int j = 0; j < RB; ++j) v[j] = x[RB * k1 + j];
-      dft_small<RB, false>(v);
+      dft_small<RB, false, PK>(v);
 #pragma unroll
       for (int j = 0; j < RB; ++j) x[RB * k1 + j] = v[j];
     }
@@ -93,7 +93,7 @@ __device__ __forceinline__ void reg_block(float2 (&x)[RA * RB]) {
       float2 v[RB];
 #pragma unroll
       for (int j = 0; j < RB; ++j) v[j] = x[RB * k1 + j];
-      dft_small<RB, true>(v);
+      dft_small<RB, true, PK>(v);
 #pragma unroll
       for (int j = 0; j < RB; ++j) x[RB * k1 + j] = v[j];
     }
@@ -105,7 +105,7 @@ __device__ __forceinline__ void reg_block(float2 (&x)[RA * RB]) {
         const float2 a = x[j2 + RB * j1];
         v[j1] = (j2 * j1 == 0) ? a : cmul(a, cconj(ctw<M>((j2 * j1) % M)));
       }
-      dft_small<RA, true>(v);
+      dft_small<RA, true, PK>(v);
 #pragma unroll
       for (int k1 = 0; k1 < RA; ++k1) x[j2 + RB * k1] = v[k1];
     }
@@ -139,7 +139,7 @@ constexpr int tail_threads() {
 // transform t at offset t), neighbouring threads take neighbouring columns;
 // rows: transform t at t * stride, neighbouring threads take neighbouring
 // butterflies of the same row.
-template <int N, int R, int L, bool INV, bool COL>
+template <int N, int R, int L, bool INV, bool COL, bool PK = true>
 __device__ __forceinline__ void tail_smem_stage(float2* buf, int ntrans, int stride, const float2* __restrict__ tw,
                                                 int tid, int T, const int* rowmap = nullptr) {
   constexpr int m = L / R;
@@ -173,9 +173,9 @@ __device__ __forceinline__ void tail_smem_stage(float2* buf, int ntrans, int str
     if (INV) {
 #pragma unroll
       for (int k = 1; k < R; ++k) x[k] = cmul(x[k], w[k]);
-      dft_small<R, true>(x);
+      dft_small<R, true, PK>(x);
     } else {
-      dft_small<R, false>(x);
+      dft_small<R, false, PK>(x);
 #pragma unroll
       for (int k = 1; k < R; ++k) x[k] = cmul(x[k], w[k]);
     }
@@ -186,7 +186,7 @@ __device__ __forceinline__ void tail_smem_stage(float2* buf, int ntrans, int str
 
 // Register blocks: neighbouring threads take neighbouring transforms (rows
 // need an odd-ish row stride, e.g. N + 1, to stay conflict-free).
-template <int N, bool INV, bool COL>
+template <int N, bool INV, bool COL, bool PK = true>
 __device__ __forceinline__ void tail_reg_stage(float2* buf, int ntrans, int stride, int tid, int T,
                                                const int* rowmap = nullptr) {
   using P = Tail<N>;
@@ -202,7 +202,7 @@ __device__ __forceinline__ void tail_reg_stage(float2* buf, int ntrans, int stri
     float2 x[M];
 #pragma unroll
     for (int j = 0; j < M; ++j) x[j] = base[j * es];
-    reg_block<P::TA, P::TB, INV>(x);
+    reg_block<P::TA, P::TB, INV, PK>(x);
 #pragma unroll
     for (int j = 0; j < M; ++j) base[j * es] = x[j];
   }
@@ -213,29 +213,29 @@ __device__ __forceinline__ void tail_reg_stage(float2* buf, int ntrans, int stri
 // be a multiple of every stage's butterfly count (tail_threads<N>() is).
 // Rows only: with rowmap, transform t is row rowmap[t] (t < ntrans), which
 // lets a caller transform just the rows that are not all zero.
-template <int N, bool INV, bool COL>
+template <int N, bool INV, bool COL, bool PK = true>
 __device__ __forceinline__ void fft_tail(float2* buf, int ntrans, int stride, const float2* __restrict__ tw,
                                          const int* rowmap = nullptr) {
   using P = Tail<N>;
   static_assert(P::ok, "no register-tail plan for this length");
   const int tid = threadIdx.x, T = blockDim.x;
   if constexpr (!INV) {
-    tail_smem_stage<N, P::S0, N, false, COL>(buf, ntrans, stride, tw, tid, T, rowmap);
+    tail_smem_stage<N, P::S0, N, false, COL, PK>(buf, ntrans, stride, tw, tid, T, rowmap);
     __syncthreads();
     if constexpr (P::S1 > 1) {
-      tail_smem_stage<N, P::S1, N / P::S0, false, COL>(buf, ntrans, stride, tw, tid, T, rowmap);
+      tail_smem_stage<N, P::S1, N / P::S0, false, COL, PK>(buf, ntrans, stride, tw, tid, T, rowmap);
       __syncthreads();
     }
-    tail_reg_stage<N, false, COL>(buf, ntrans, stride, tid, T, rowmap);
+    tail_reg_stage<N, false, COL, PK>(buf, ntrans, stride, tid, T, rowmap);
     __syncthreads();
   } else {
-    tail_reg_stage<N, true, COL>(buf, ntrans, stride, tid, T, rowmap);
+    tail_reg_stage<N, true, COL, PK>(buf, ntrans, stride, tid, T, rowmap);
     __syncthreads();
     if constexpr (P::S1 > 1) {
-      tail_smem_stage<N, P::S1, N / P::S0, true, COL>(buf, ntrans, stride, tw, tid, T, rowmap);
+      tail_smem_stage<N, P::S1, N / P::S0, true, COL, PK>(buf, ntrans, stride, tw, tid, T, rowmap);
       __syncthreads();
     }
-    tail_smem_stage<N, P::S0, N, true, COL>(buf, ntrans, stride, tw, tid, T, rowmap);
+    tail_smem_stage<N, P::S0, N, true, COL, PK>(buf, ntrans, stride, tw, tid, T, rowmap);
     __syncthreads();
   }
 }

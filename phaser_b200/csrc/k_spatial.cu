@@ -321,13 +321,21 @@ __global__ void __launch_bounds__(512, NF > 0 ? 2 : 1) k_fuse_z(SpatialArgs a, F
   const float inv_total = 1.0f / (float)a.n_total_ch;
   // Wt is a power of two (fuse_z_tile_ok): shifts, not a runtime division per element
   const int lwt = __ffs(Wt) - 1;
+  // With Wt = 8 a half-warp covers two rows whose slots start on the same
+  // banks (a row is A * 64 bytes): odd rows load their two sides in the
+  // opposite order (conflict-free when the slots of a channel's sides are an
+  // odd number of slots apart) and keep the product in slot 1 instead of 0,
+  // which the inverse transform and the store follow.
+  const int podd = (NF > 0 && Wt == 8) ? Wt : 0;
   for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
     const int zp = e >> lwt, t = e & (Wt - 1);
+    const bool odd = podd && (zp & 1);
     float2* row = tile + (size_t)zp * rowlen;
     float2 F, G;
     if (!a.laplace) {
-      F = row[t];
-      G = row[Wt + t];
+      const float2 p0 = row[(odd ? Wt : 0) + t], p1 = row[(odd ? 0 : Wt) + t];
+      F = odd ? p1 : p0;
+      G = odd ? p0 : p1;
       if (a.lowpass) {
         // keep the products whose FFT-shifted index p = (i N + j) + N^2 k has
         // i, j, k in [lp_lo, lp_hi]
@@ -355,8 +363,10 @@ __global__ void __launch_bounds__(512, NF > 0 ? 2 : 1) k_fuse_z(SpatialArgs a, F
       float2 sf = make_float2(0.f, 0.f), sg = sf, mf = sf, mg = sf;
       float bf = -1.f, bg = -1.f;
       for (int c = 0; c < C; ++c) {
-        const float2 u = row[c * Wt + t];
-        const float2 v = row[(C + c) * Wt + t];
+        const float2 p0 = row[(odd ? C + c : c) * Wt + t];
+        const float2 p1 = row[(odd ? c : C + c) * Wt + t];
+        const float2 u = odd ? p1 : p0;
+        const float2 v = odd ? p0 : p1;
         sf = cadd(sf, u);
         sg = cadd(sg, v);
         const float eu = u.x * u.x + u.y * u.y;
@@ -371,13 +381,20 @@ __global__ void __launch_bounds__(512, NF > 0 ? 2 : 1) k_fuse_z(SpatialArgs a, F
       G = op == kFuseMax ? mg : (op == kFuseMean ? make_float2(sg.x * inv, sg.y * inv) : make_float2(0.f, 0.f));
     }
     // complexMulSeq: C = F * conj(G); only this thread touches position (zp, t)
-    row[t] = make_float2(F.x * G.x - F.y * (-G.y), F.x * (-G.y) + F.y * G.x);
+    row[(odd ? Wt : 0) + t] = make_float2(F.x * G.x - F.y * (-G.y), F.x * (-G.y) + F.y * G.x);
   }
   __syncthreads();
-  fft_any_cols<NF, true>(tile, Wt, rowlen, plan);
+  if constexpr (NF > 0) {
+    if (podd)
+      fft_fixed_cols_podd<NF, true>(tile, Wt, rowlen, podd, plan.tw);
+    else
+      fft_any_cols<NF, true>(tile, Wt, rowlen, plan);
+  } else {
+    fft_any_cols<NF, true>(tile, Wt, rowlen, plan);
+  }
   for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
     const int z = e >> lwt, t = e & (Wt - 1);
-    if (t < wt) a.cspec[((size_t)z * N + xp) * H2p + ky0 + t] = tile[(size_t)z * rowlen + t];
+    if (t < wt) a.cspec[((size_t)z * N + xp) * H2p + ky0 + t] = tile[(size_t)z * rowlen + ((z & 1) ? podd : 0) + t];
   }
 }
 
