@@ -240,6 +240,37 @@ __device__ __forceinline__ bool mbar_wait0(uint64_t* bar) {
   return done != 0;
 }
 
+// Channel sums (MEAN) and the first channel of largest energy (MAX) of both
+// sides at one position of a fuse_z tile row: channel c of side f in slot c,
+// of side g in slot C + c.  Odd rows (odd = true) load g before f, which
+// keeps the two loads on different banks (see k_fuse_z).  CC > 0: C == CC
+// known at compile time.
+template <int CC>
+__device__ __forceinline__ void fuse_sides(const float2* row, int C, int Wt, int t, bool odd, float2& sf, float2& sg,
+                                           float2& mf, float2& mg) {
+  if constexpr (CC > 0) C = CC;
+  sf = make_float2(0.f, 0.f);
+  sg = sf;
+  mf = sf;
+  mg = sf;
+  float bf = -1.f, bg = -1.f;
+#pragma unroll
+  for (int c = 0; c < (CC > 0 ? CC : C); ++c) {
+    const float2 p0 = row[(odd ? C + c : c) * Wt + t];
+    const float2 p1 = row[(odd ? c : C + c) * Wt + t];
+    const float2 u = odd ? p1 : p0;
+    const float2 v = odd ? p0 : p1;
+    sf = cadd(sf, u);
+    sg = cadd(sg, v);
+    const float eu = u.x * u.x + u.y * u.y;
+    const float ev = v.x * v.x + v.y * v.y;
+    mf = eu > bf ? u : mf;
+    bf = eu > bf ? eu : bf;
+    mg = ev > bg ? v : mg;
+    bg = ev > bg ? ev : bg;
+  }
+}
+
 struct FuseZTma {
   int enabled;  // tensor map valid
   int zbox;     // z rows per copy
@@ -360,22 +391,11 @@ __global__ void __launch_bounds__(512, NF > 0 ? 2 : 1) k_fuse_z(SpatialArgs a, F
       // one branch-free pass serves every rule (a divergent switch between
       // the rules cost more than the arithmetic): channel sums for MEAN, the
       // first channel of largest energy for MAX
-      float2 sf = make_float2(0.f, 0.f), sg = sf, mf = sf, mg = sf;
-      float bf = -1.f, bg = -1.f;
-      for (int c = 0; c < C; ++c) {
-        const float2 p0 = row[(odd ? C + c : c) * Wt + t];
-        const float2 p1 = row[(odd ? c : C + c) * Wt + t];
-        const float2 u = odd ? p1 : p0;
-        const float2 v = odd ? p0 : p1;
-        sf = cadd(sf, u);
-        sg = cadd(sg, v);
-        const float eu = u.x * u.x + u.y * u.y;
-        const float ev = v.x * v.x + v.y * v.y;
-        mf = eu > bf ? u : mf;
-        bf = eu > bf ? eu : bf;
-        mg = ev > bg ? v : mg;
-        bg = ev > bg ? ev : bg;
-      }
+      float2 sf, sg, mf, mg;
+      if (C == 3)  // range, intensity, reflectivity: the loop unrolled
+        fuse_sides<3>(row, 3, Wt, t, odd, sf, sg, mf, mg);
+      else
+        fuse_sides<0>(row, C, Wt, t, odd, sf, sg, mf, mg);
       const float inv = inv_total;
       F = op == kFuseMax ? mf : (op == kFuseMean ? make_float2(sf.x * inv, sf.y * inv) : make_float2(0.f, 0.f));
       G = op == kFuseMax ? mg : (op == kFuseMean ? make_float2(sg.x * inv, sg.y * inv) : make_float2(0.f, 0.f));
