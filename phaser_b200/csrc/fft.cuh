@@ -602,6 +602,17 @@ __device__ __forceinline__ void fft_fixed_cols_podd(float2* buf, int ntrans, int
 }
 
 
+// Column transforms with every count known at compile time: NTRANS columns
+// of a buffer with row stride STRIDE, NTHR threads (== blockDim.x), so the
+// shared-memory offsets and the thread-to-column split fold to constants.
+// PODD as in fixed_col_stage.
+template <int NF, bool INV, int NTRANS, int STRIDE, int NTHR, bool PODD>
+__device__ __forceinline__ void fixed_cols_ct(float2* buf, const float2* __restrict__ tw, int podd) {
+  static_assert(NF > 0 && NTRANS <= NTHR, "compile-time column plan");
+  const int tid = threadIdx.x;
+  fixed_col_stages<NF, INV, PODD>(buf, STRIDE, tw, tid % NTRANS, tid / NTRANS, NTHR / NTRANS, podd);
+}
+
 template <int NF>
 __device__ __forceinline__ int freq2pos(int k, const FftPlan& p) {
   if constexpr (NF > 0) {

@@ -281,15 +281,22 @@ struct FuseZTma {
 // compiler schedule for it: 0.1294 against 0.1336 ms at N = 200; 640 or 672
 // threads, whose radix passes divide more evenly, ran the same); the runtime
 // plan's generic transform needs its 128 registers.
-template <int NF>
-__global__ void __launch_bounds__(512, NF > 0 ? 2 : 1) k_fuse_z(SpatialArgs a, FftPlan plan, int Wt, int x_natural,
-                                                const __grid_constant__ CUtensorMap tmap, FuseZTma tma) {
+// CA, CW > 0: the Laplace fusion of C = CA / 2 channels with tile width CW,
+// known at compile time (every shared-memory offset of the transforms folds
+// to a constant); CA = CW = 0: any shape (the host picks).
+constexpr int kFuseZThreads = 512;
+template <int NF, int CA = 0, int CW = 0>
+__global__ void __launch_bounds__(kFuseZThreads, NF > 0 ? 2 : 1)
+    k_fuse_z(SpatialArgs a, FftPlan plan, int Wt_arg, int x_natural, const __grid_constant__ CUtensorMap tmap,
+             FuseZTma tma) {
   extern __shared__ __align__(128) float2 tile[];  // [z][arr][t]
+  static_assert(CA == 0 || (NF > 0 && CW == 8 && CA % 2 == 0), "compile-time shape: NF > 0, Wt = 8");
   const int N = NF > 0 ? NF : a.N;
   const int H2 = N / 2 + 1;
   const int H2p = spatial_h2p(N);
-  const int C = a.n_data_ch;
-  const int A = a.laplace ? 2 * C : 2;
+  const int C = CA > 0 ? CA / 2 : a.n_data_ch;
+  const int A = CA > 0 ? CA : (a.laplace ? 2 * C : 2);
+  const int Wt = CW > 0 ? CW : Wt_arg;
   const int ky0 = blockIdx.x * Wt;
   const int wt = min(Wt, H2 - ky0);
   const int xp = blockIdx.y;
@@ -344,7 +351,10 @@ __global__ void __launch_bounds__(512, NF > 0 ? 2 : 1) k_fuse_z(SpatialArgs a, F
     }
   }
   __syncthreads();
-  fft_any_cols<NF, false>(tile, rowlen, rowlen, plan);
+  if constexpr (CA > 0)
+    fixed_cols_ct<NF, false, CA * CW, CA * CW, kFuseZThreads, false>(tile, plan.tw, 0);
+  else
+    fft_any_cols<NF, false>(tile, rowlen, rowlen, plan);
   const int kx = x_natural ? xp : pos2freq<NF>(xp, plan);
   const uint32_t nv = (uint32_t)N * (uint32_t)N * (uint32_t)N;
   // MEAN divides by the total channel count: a product with the reciprocal,
@@ -363,7 +373,7 @@ __global__ void __launch_bounds__(512, NF > 0 ? 2 : 1) k_fuse_z(SpatialArgs a, F
     const bool odd = podd && (zp & 1);
     float2* row = tile + (size_t)zp * rowlen;
     float2 F, G;
-    if (!a.laplace) {
+    if (CA == 0 && !a.laplace) {
       const float2 p0 = row[(odd ? Wt : 0) + t], p1 = row[(odd ? 0 : Wt) + t];
       F = odd ? p1 : p0;
       G = odd ? p0 : p1;
@@ -392,7 +402,9 @@ __global__ void __launch_bounds__(512, NF > 0 ? 2 : 1) k_fuse_z(SpatialArgs a, F
       // the rules cost more than the arithmetic): channel sums for MEAN, the
       // first channel of largest energy for MAX
       float2 sf, sg, mf, mg;
-      if (C == 3)  // range, intensity, reflectivity: the loop unrolled
+      if constexpr (CA > 0)
+        fuse_sides<CA / 2>(row, C, Wt, t, odd, sf, sg, mf, mg);
+      else if (C == 3)  // range, intensity, reflectivity: the loop unrolled
         fuse_sides<3>(row, 3, Wt, t, odd, sf, sg, mf, mg);
       else
         fuse_sides<0>(row, C, Wt, t, odd, sf, sg, mf, mg);
@@ -404,7 +416,9 @@ __global__ void __launch_bounds__(512, NF > 0 ? 2 : 1) k_fuse_z(SpatialArgs a, F
     row[(odd ? Wt : 0) + t] = make_float2(F.x * G.x - F.y * (-G.y), F.x * (-G.y) + F.y * G.x);
   }
   __syncthreads();
-  if constexpr (NF > 0) {
+  if constexpr (CA > 0) {
+    fixed_cols_ct<NF, true, CW, CA * CW, kFuseZThreads, true>(tile, plan.tw, CW);
+  } else if constexpr (NF > 0) {
     if (podd)
       fft_fixed_cols_podd<NF, true>(tile, Wt, rowlen, podd, plan.tw);
     else
@@ -669,6 +683,8 @@ static cudaError_t allow_max_smem(const void* fn) {
 template <int NF>
 static cudaError_t set_attrs() {
   cudaError_t e = allow_max_smem((const void*)k_fuse_z<NF>);
+  if constexpr (NF > 0)
+    if (e == cudaSuccess) e = allow_max_smem((const void*)k_fuse_z<NF, 6, 8>);
   if (e == cudaSuccess) e = allow_max_smem((const void*)k_r2c_y<NF>);
   if (e == cudaSuccess) e = allow_max_smem((const void*)k_fft_x<NF, false>);
   if (e == cudaSuccess) e = allow_max_smem((const void*)k_fft_x<NF, true>);
@@ -814,7 +830,19 @@ cudaError_t launch_spatial_fuse_z(const SpatialArgs& a, cudaStream_t st) {
   if (smB > (size_t)kMaxSmem) return cudaErrorInvalidConfiguration;
   dim3 gB((H2 + wt - 1) / wt, N);
   const int xnat = (spatial_slab_path(N) && a.plan_half) ? 1 : 0;
-  PHGPU_DISPATCH_N(N, k_fuse_z<NF><<<gB, 512, smB, st>>>(a, *a.plan, wt, xnat, tmap, tma));
+  // the bench shape (Laplace fusion of three channels, tile width 8) has its
+  // own instantiation with the tile shape known at compile time
+  const bool shape68 = A == 6 && wt == 8;
+  PHGPU_DISPATCH_N(N, {
+    bool done = false;
+    if constexpr (NF > 0) {
+      if (shape68) {
+        k_fuse_z<NF, 6, 8><<<gB, kFuseZThreads, smB, st>>>(a, *a.plan, wt, xnat, tmap, tma);
+        done = true;
+      }
+    }
+    if (!done) k_fuse_z<NF><<<gB, kFuseZThreads, smB, st>>>(a, *a.plan, wt, xnat, tmap, tma);
+  });
   count_launches(1);
   return cudaGetLastError();
 }
