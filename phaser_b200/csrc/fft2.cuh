@@ -213,12 +213,14 @@ __device__ __forceinline__ void tail_reg_stage(float2* buf, int ntrans, int stri
 // be a multiple of every stage's butterfly count (tail_threads<N>() is).
 // Rows only: with rowmap, transform t is row rowmap[t] (t < ntrans), which
 // lets a caller transform just the rows that are not all zero.
-template <int N, bool INV, bool COL, bool PK = true>
+// NT > 0: the block has exactly NT threads (the per-thread split folds to
+// constants); NT = 0: blockDim.x.
+template <int N, bool INV, bool COL, bool PK = true, int NT = 0>
 __device__ __forceinline__ void fft_tail(float2* buf, int ntrans, int stride, const float2* __restrict__ tw,
                                          const int* rowmap = nullptr) {
   using P = Tail<N>;
   static_assert(P::ok, "no register-tail plan for this length");
-  const int tid = threadIdx.x, T = blockDim.x;
+  const int tid = threadIdx.x, T = NT > 0 ? NT : (int)blockDim.x;
   if constexpr (!INV) {
     tail_smem_stage<N, P::S0, N, false, COL, PK>(buf, ntrans, stride, tw, tid, T, rowmap);
     __syncthreads();

@@ -234,8 +234,9 @@ constexpr int c2r_pair_rows() {
 // transform kernel above fills it.  A pair of betas is one 16-byte load.
 // Four blocks per SM (64 registers) rather than the three that 74 registers
 // allowed: 0.0488 vs 0.0511 ms for the SO(3) angle transforms at B = 100.
+constexpr int kSo3TailThreads = 256;
 template <int NF>
-__global__ void __launch_bounds__(256, 4) k_so3_c2r_tail(int bw_in, So3Batch bt, FftPlan plan) {
+__global__ void __launch_bounds__(kSo3TailThreads, 4) k_so3_c2r_tail(int bw_in, So3Batch bt, FftPlan plan) {
   constexpr int n = NF, Bo = NF / 2, RB = c2r_pair_rows<NF>(), ST = NF + 1;
   extern __shared__ float2 zrow[];  // [RB / 2][ST]: one beta pair per complex transform
   __shared__ int s_pos[NF];
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(256, 4) k_so3_c2r_tail(int bw_in, So3Batch bt,
     }
   }
   __syncthreads();
-  fft_tail<NF, true, false>(zrow, np, ST, plan.tw);
+  fft_tail<NF, true, false, true, kSo3TailThreads>(zrow, np, ST, plan.tw);
   const float K = (float)((1.0 / (double)n) * ((double)Bo / M_PI));
   // per thread: the largest value, the lowest index among equal ones
   float bv = -1.0f;
@@ -347,7 +348,8 @@ static void launch_so3_c2r(const So3Args& a, int n, cudaStream_t st) {
   if constexpr (Tail<NF>::ok) {
     constexpr int RB = c2r_pair_rows<NF>();
     dim3 g((n + RB - 1) / RB, n, a.batch.count);
-    k_so3_c2r_tail<NF><<<g, 256, (size_t)(RB / 2) * (NF + 1) * sizeof(float2), st>>>(a.bw_in, a.batch, *a.plan);
+    k_so3_c2r_tail<NF><<<g, kSo3TailThreads, (size_t)(RB / 2) * (NF + 1) * sizeof(float2), st>>>(a.bw_in, a.batch,
+                                                                                               *a.plan);
   } else {
     dim3 g((n + 15) / 16, n, a.batch.count);
     k_so3_c2r<NF><<<g, 256, (size_t)16 * n * sizeof(float2) + (size_t)n * sizeof(int), st>>>(a.bw_in, a.bw_out,

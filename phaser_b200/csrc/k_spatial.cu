@@ -574,8 +574,8 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
   }
   if (nz && threadIdx.x == 0) *nz = 1;
   // rows that are all zero stay zero under the y transform
-  fft_tail<N, false, false>(W, nrows, S, pN.tw, s_rows);  // over y, live rows
-  fft_tail<NH, false, true>(W, N, S, pH.tw);               // over r, columns
+  fft_tail<N, false, false, true, tail_threads<NF>()>(W, nrows, S, pN.tw, s_rows);  // over y, live rows
+  fft_tail<NH, false, true, true, tail_threads<NF>()>(W, N, S, pH.tw);               // over r, columns
   for (int e = threadIdx.x; e < NH * H2; e += blockDim.x) {
     const int k = e / H2, ky = e - k * H2;
     const float2 w1 = W[s_posH[k] * S + s_posN[ky]];
@@ -640,8 +640,8 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
     }
   }
   __syncthreads();
-  fft_tail<NH, true, true>(W, N, S, pH.tw);    // over r, columns
-  fft_tail<N, true, false>(W, NH, S, pN.tw);   // over y, rows
+  fft_tail<NH, true, true, true, tail_threads<NF>()>(W, N, S, pH.tw);    // over r, columns
+  fft_tail<N, true, false, true, tail_threads<NF>()>(W, NH, S, pN.tw);   // over y, rows
   // per thread: the largest value, the lowest index among equal ones (the
   // reference's first occurrence, whatever order the thread visits them in)
   float bv = -INFINITY;
