@@ -139,6 +139,7 @@ void so3_beta_table(int bw_out, double* tab) {
 
 // Forward DFT over a (alpha) for one b and a tile of Wt = 2^LOG2W betas
 // (8, 16 or 32: a tuned parameter, 16 by default).
+constexpr int kSo3FftAThreads = 256;
 template <int NF, int LOG2W>
 __global__ void k_so3_fft_a(int bw_in, int bw_out, So3Batch bt, FftPlan plan) {
   extern __shared__ float2 tile[];  // [a][beta tile]
@@ -166,6 +167,10 @@ __global__ void k_so3_fft_a(int bw_in, int bw_out, So3Batch bt, FftPlan plan) {
       if (e0 + u * blockDim.x < n * Wt) tile[e0 + u * blockDim.x] = v[u];
   }
   __syncthreads();
+  // per-component butterflies (fixed_stage): the packed column-resident form
+  // ran about 1 % faster but rounds the SO(3) volume differently, and one
+  // near-tied pair of the 256-pair batched workload then picked another bin
+  // under the tf32x3 synthesis than under FP32 and the FP64 oracle
   fft_any<NF, false, LOG2W>(tile, Wt, 1, Wt, plan);
   for (int e = threadIdx.x; e < n * Wt; e += blockDim.x) {
     const int a = e / Wt, t = e % Wt;
@@ -362,11 +367,11 @@ static void launch_so3_fft_a(const So3Args& a, int n, int wt, cudaStream_t st) {
   dim3 g((n + wt - 1) / wt, a.bw_in, a.batch.count);
   const size_t sm = (size_t)n * wt * sizeof(float2);
   if (wt == 8)
-    k_so3_fft_a<NF, 3><<<g, 256, sm, st>>>(a.bw_in, a.bw_out, a.batch, *a.plan);
+    k_so3_fft_a<NF, 3><<<g, kSo3FftAThreads, sm, st>>>(a.bw_in, a.bw_out, a.batch, *a.plan);
   else if (wt == 32)
-    k_so3_fft_a<NF, 5><<<g, 256, sm, st>>>(a.bw_in, a.bw_out, a.batch, *a.plan);
+    k_so3_fft_a<NF, 5><<<g, kSo3FftAThreads, sm, st>>>(a.bw_in, a.bw_out, a.batch, *a.plan);
   else
-    k_so3_fft_a<NF, 4><<<g, 256, sm, st>>>(a.bw_in, a.bw_out, a.batch, *a.plan);
+    k_so3_fft_a<NF, 4><<<g, kSo3FftAThreads, sm, st>>>(a.bw_in, a.bw_out, a.batch, *a.plan);
 }
 
 bool so3_beta_tile_ok(int bw_out, int wt) {

@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(kFuseZThreads, NF > 0 ? 2 : 1)
   FusionBands* s_bands = reinterpret_cast<FusionBands*>(bar + 2);
   int* s_kz = reinterpret_cast<int*>(s_bands + 1);  // [N] z frequency of each position
   if (threadIdx.x == 0) *s_bands = a.bands;  // divergent band lookups are cheap in shared memory
-  for (int zp = threadIdx.x; zp < N; zp += blockDim.x) s_kz[zp] = pos2freq<NF>(zp, plan);
+  for (int zp = threadIdx.x; zp < N; zp += kFuseZThreads) s_kz[zp] = pos2freq<NF>(zp, plan);
   // the bulk copy needs a 128-byte aligned destination (block-uniform test)
   const bool use_tma = tma.enabled && (smem_addr(tile) & 127u) == 0;
   if (use_tma) {
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(kFuseZThreads, NF > 0 ? 2 : 1)
     // tiles start at ky0 (multiple of Wt) in rows padded to 8 complex: load two
     // complex per 16-byte access
     const int half = Wt >> 1;
-    for (int e = threadIdx.x; e < N * A * half; e += blockDim.x) {
+    for (int e = threadIdx.x; e < N * A * half; e += kFuseZThreads) {
       const int z = e / (A * half), rem = e - z * (A * half), ar = rem / half, t2 = rem - ar * half;
       // arrays: f channels 0..C-1 then g channels; plain mode uses channel 0 of
       // each side, the low-pass mode channel 1
@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(kFuseZThreads, NF > 0 ? 2 : 1)
   // odd number of slots apart) and keep the product in slot 1 instead of 0,
   // which the inverse transform and the store follow.
   const int podd = (NF > 0 && Wt == 8) ? Wt : 0;
-  for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
+  for (int e = threadIdx.x; e < N * Wt; e += kFuseZThreads) {
     const int zp = e >> lwt, t = e & (Wt - 1);
     const bool odd = podd && (zp & 1);
     float2* row = tile + (size_t)zp * rowlen;
@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(kFuseZThreads, NF > 0 ? 2 : 1)
   } else {
     fft_any_cols<NF, true>(tile, Wt, rowlen, plan);
   }
-  for (int e = threadIdx.x; e < N * Wt; e += blockDim.x) {
+  for (int e = threadIdx.x; e < N * Wt; e += kFuseZThreads) {
     const int z = e >> lwt, t = e & (Wt - 1);
     if (t < wt) a.cspec[((size_t)z * N + xp) * H2p + ky0 + t] = tile[(size_t)z * rowlen + ((z & 1) ? podd : 0) + t];
   }
@@ -501,6 +501,7 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
                                                    size_t spec_cstride, FftPlan pN, FftPlan pH,
                                                    uint8_t* __restrict__ slab_nz) {
   constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1, Q = NF / 4, S = NF + 1;
+  constexpr int T = tail_threads<NF>();  // the launch's block size
   const int H2p = spatial_h2p(N);
   extern __shared__ float2 W[];  // [NH][S]
   __shared__ int s_flag[NH];      // packed row r may hold a point (row flags), else all zero
@@ -515,7 +516,7 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
   uint8_t* nz = slab_nz ? slab_nz + (size_t)c * N + z : nullptr;
   const int held_nonzero = nz ? *nz : 1;
   int any_flag = 0;
-  for (int r = threadIdx.x; r < NH; r += blockDim.x) {
+  for (int r = threadIdx.x; r < NH; r += T) {
     s_live[r] = 0;
     s_flag[r] = rowlive ? (rowlive[z * N + 2 * r] | rowlive[z * N + 2 * r + 1]) : 1;
     any_flag |= s_flag[r];
@@ -524,9 +525,9 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
   // array already holds zeros there (about half the slabs of a room scan, so
   // they leave before any other set-up)
   if (!__syncthreads_or(any_flag) && !held_nonzero) return;
-  for (int r = threadIdx.x; r < NH; r += blockDim.x) s_posH[r] = fixed_freq2pos<NH>(r);
-  for (int k = threadIdx.x; k < N; k += blockDim.x) s_posN[k] = fixed_freq2pos<N>(k);
-  for (int e = threadIdx.x; e < NH * Q; e += blockDim.x) {
+  for (int r = threadIdx.x; r < NH; r += T) s_posH[r] = fixed_freq2pos<NH>(r);
+  for (int k = threadIdx.x; k < N; k += T) s_posN[k] = fixed_freq2pos<N>(k);
+  for (int e = threadIdx.x; e < NH * Q; e += T) {
     const int r = e / Q, y4 = (e - r * Q) * 4;
     if (!s_flag[r]) {  // no point in either row: skip the loads
       float2* d = W + r * S + y4;
@@ -565,7 +566,7 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
   const int nrows = s_nrows;
   float2* out = spec + (size_t)c * spec_cstride + (size_t)z * N * H2p;
   if (nrows == 0) {  // empty slab: its 2-D spectrum is zero
-    for (int e = threadIdx.x; e < N * H2; e += blockDim.x) {
+    for (int e = threadIdx.x; e < N * H2; e += T) {
       const int k = e / H2, ky = e - k * H2;
       out[(size_t)k * H2p + ky] = make_float2(0.f, 0.f);
     }
@@ -576,7 +577,7 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_fwd(const float* __
   // rows that are all zero stay zero under the y transform
   fft_tail<N, false, false, true, tail_threads<NF>()>(W, nrows, S, pN.tw, s_rows);  // over y, live rows
   fft_tail<NH, false, true, true, tail_threads<NF>()>(W, N, S, pH.tw);               // over r, columns
-  for (int e = threadIdx.x; e < NH * H2; e += blockDim.x) {
+  for (int e = threadIdx.x; e < NH * H2; e += T) {
     const int k = e / H2, ky = e - k * H2;
     const float2 w1 = W[s_posH[k] * S + s_posN[ky]];
     const float2 w2 = W[s_posH[k == 0 ? 0 : NH - k] * S + s_posN[ky == 0 ? 0 : N - ky]];
@@ -598,23 +599,24 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
                                                    FftPlan pH, unsigned long long* __restrict__ argmax,
                                                    float* __restrict__ volume, uint32_t limit) {
   constexpr int N = NF, NH = NF / 2, H2 = NF / 2 + 1, S = NF + 1;
+  constexpr int T = tail_threads<NF>();  // the launch's block size
   const int H2p = spatial_h2p(N);
   extern __shared__ float2 W[];  // [NH][S]
   __shared__ int s_posN[N], s_posH[NH];  // digit-reversed positions of frequencies
   const int z = blockIdx.x;
   const float2* X = cspec + (size_t)z * N * H2p;
-  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+  for (int k = threadIdx.x; k < N; k += T) {
     s_posN[k] = fixed_freq2pos<N>(k);
     if (k < NH) s_posH[k] = fixed_freq2pos<NH>(k);
   }
   __syncthreads();
   // four elements' loads in flight per thread
   constexpr int U = 4;
-  for (int e0 = threadIdx.x; e0 < NH * H2; e0 += U * blockDim.x) {
+  for (int e0 = threadIdx.x; e0 < NH * H2; e0 += U * T) {
     float2 x0u[U], x1u[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const int e = e0 + u * blockDim.x;
+      const int e = e0 + u * T;
       const int k = e / H2, ky = e - k * H2;
       const bool ok = e < NH * H2;
       x0u[u] = ok ? X[(size_t)k * H2p + ky] : make_float2(0.f, 0.f);
@@ -622,7 +624,7 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-    const int e = e0 + u * blockDim.x;
+    const int e = e0 + u * T;
     if (e >= NH * H2) break;
     const int k = e / H2, ky = e - k * H2;
     float2 x0 = x0u[u], x1 = x1u[u];
@@ -646,7 +648,7 @@ __global__ void __launch_bounds__(tail_threads<NF>()) k_slab_inv(const float2* _
   // reference's first occurrence, whatever order the thread visits them in)
   float bv = -INFINITY;
   uint32_t bi = 0xffffffffu;
-  for (int e = threadIdx.x; e < NH * N; e += blockDim.x) {
+  for (int e = threadIdx.x; e < NH * N; e += T) {
     const int r = e / N, y = e - r * N;
     const float2 v = W[r * S + y];
     const float a0 = 2.0f * v.x, a1 = 2.0f * v.y;
