@@ -61,8 +61,15 @@ __host__ __device__ inline uint32_t unpack_index(unsigned long long k) {
   return 0xffffffffu - (uint32_t)(k & 0xffffffffull);
 }
 
-// Warp-level reduction of a packed argmax key followed by one atomicMax per warp.
+// Warp-level reduction of a packed argmax key followed by one atomicMax per
+// warp (1-D blocks).  The last warp of a block whose size is not a multiple
+// of 32 (1000 threads at N = 200) has lanes that do not exist, and a shuffle
+// from such a lane returns an undefined value: its lanes commit one by one.
 __device__ __forceinline__ void warp_argmax_commit(unsigned long long key, unsigned long long* dst) {
+  if ((threadIdx.x | 31u) >= blockDim.x) {
+    if (key) atomicMax(dst, key);
+    return;
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
