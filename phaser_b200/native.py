@@ -141,16 +141,19 @@ EXPORTED = [
 ]
 
 _LIB = None
+_LIB_FILE = None
+_BUILD_ID = None
 
 
 def load(path: str = LIB_PATH):
     """Load the library (no GPU needed just to load it)."""
-    global _LIB
+    global _LIB, _LIB_FILE
     if _LIB is not None:
         return _LIB
     if not os.path.exists(path):
         raise PhgpuError(f"CUDA library not built: {path} (run python -m phaser_b200.build)")
     lib = C.CDLL(path)
+    _LIB_FILE = path
     vp = C.c_void_p
     lib.phgpu_params_default.argtypes = [C.POINTER(Params)]
     lib.phgpu_ctx_create.argtypes = [C.POINTER(Params), C.POINTER(vp)]
@@ -226,6 +229,22 @@ def load(path: str = LIB_PATH):
     _LIB = lib
     return lib
 
+
+
+def build_id() -> str:
+    """Identity of the loaded library build: the first 12 hex digits of the
+    SHA-1 of its file (autotuned parameters are kept per build, since a
+    kernel change can move the best launch parameters)."""
+    global _BUILD_ID
+    if _BUILD_ID is None:
+        import hashlib
+        load()
+        h = hashlib.sha1()
+        with open(_LIB_FILE, "rb") as f:
+            for chunk in iter(lambda: f.read(1 << 20), b""):
+                h.update(chunk)
+        _BUILD_ID = h.hexdigest()[:12]
+    return _BUILD_ID
 
 def default_params(**kw) -> Params:
     p = Params()

@@ -2,10 +2,12 @@
 and device model.
 
 The cache is a JSON file (PHGPU_TUNING_CACHE, or ~/.cache/phaser_b200/
-tuning.json) mapping a shape key -- device name, bandwidth, spherical zero
-padding, voxels, precision -- to the parameters and the registration time the
-search measured under them.  `tuned(params, clouds)` returns the cached entry
-or runs the search on the given pair and stores it.
+tuning.json) mapping a shape key -- device name, library build, bandwidth,
+spherical zero padding, voxels, precision -- to the parameters and the
+registration time the search measured under them.  The build is part of the
+key because a kernel change can move the best parameters.  `tuned(params,
+clouds)` returns the cached entry or runs the search on the given pair and
+stores it.
 """
 from __future__ import annotations
 
@@ -19,8 +21,8 @@ def cache_path() -> str:
                           os.path.join(os.path.expanduser("~"), ".cache", "phaser_b200", "tuning.json"))
 
 
-def shape_key(params, device_name: str) -> str:
-    return (f"{device_name}|B{params.spherical_bandwidth}+{params.spherical_zero_padding}|"
+def shape_key(params, device_name: str, build: str = "") -> str:
+    return (f"{device_name}|{build}|B{params.spherical_bandwidth}+{params.spherical_zero_padding}|"
             f"N{params.spatial_n_voxels}|P{params.precision}")
 
 
@@ -32,14 +34,14 @@ def _read(path):
         return {}
 
 
-def load(params, device_name: str, path: str | None = None):
-    return _read(path or cache_path()).get(shape_key(params, device_name))
+def load(params, device_name: str, path: str | None = None, build: str = ""):
+    return _read(path or cache_path()).get(shape_key(params, device_name, build))
 
 
-def save(params, device_name: str, tuning: dict, ms_per_pair: float, path: str | None = None):
+def save(params, device_name: str, tuning: dict, ms_per_pair: float, path: str | None = None, build: str = ""):
     path = path or cache_path()
     d = _read(path)
-    d[shape_key(params, device_name)] = {"tuning": tuning, "ms_per_pair": ms_per_pair}
+    d[shape_key(params, device_name, build)] = {"tuning": tuning, "ms_per_pair": ms_per_pair}
     os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
     fd, tmp = tempfile.mkstemp(dir=os.path.dirname(path) or ".", suffix=".json")
     with os.fdopen(fd, "w") as f:
@@ -53,8 +55,9 @@ def tuned(params, target, source, reps: int = 3, force: bool = False, path: str 
     import torch
     from . import native
     dev = torch.cuda.get_device_name(params.device)
+    build = native.build_id()
     if not force:
-        hit = load(params, dev, path)
+        hit = load(params, dev, path, build)
         if hit is not None:
             return dict(hit, cached=True)
     ctx = native.Context(params)
@@ -62,5 +65,5 @@ def tuned(params, target, source, reps: int = 3, force: bool = False, path: str 
         t, ms = ctx.autotune(target, source, reps=reps)
     finally:
         ctx.close()
-    save(params, dev, t, ms, path)
+    save(params, dev, t, ms, path, build)
     return {"tuning": t, "ms_per_pair": ms, "cached": False}

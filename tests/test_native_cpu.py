@@ -114,3 +114,16 @@ def test_tuning_cache_round_trip(native, tmp_path):
     assert tuning.load(p, "other", path) is None
     p2 = native.default_params(spherical_bandwidth=100, spatial_n_voxels=200, precision=0)
     assert tuning.load(p2, "B200", path) is None
+
+
+def test_tuning_cache_is_per_build(native, tmp_path):
+    """Parameters tuned under one library build are not reused by another."""
+    from phaser_b200 import tuning
+    p = native.default_params(spherical_bandwidth=100, spatial_n_voxels=200, precision=1)
+    path = str(tmp_path / "t.json")
+    b = native.build_id()
+    assert len(b) == 12 and int(b, 16) >= 0 and native.build_id() == b
+    tuning.save(p, "B200", {"fuse_z_tile": 8}, 0.4, path, build=b)
+    assert tuning.load(p, "B200", path, build=b)["tuning"]["fuse_z_tile"] == 8
+    assert tuning.load(p, "B200", path, build="0" * 12) is None
+    assert tuning.load(p, "B200", path) is None
