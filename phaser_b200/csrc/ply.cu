@@ -66,6 +66,21 @@ struct Header {
   std::vector<Element> elements;
 };
 
+// A header line quoted in an error message: printable ASCII only (a damaged
+// file can put any byte there), at most 80 characters.
+std::string quoted(const std::string& line) {
+  std::string q;
+  for (char ch : line) {
+    if (q.size() >= 80) {
+      q += "...";
+      break;
+    }
+    const unsigned char u = (unsigned char)ch;
+    q += (u >= 0x20 && u < 0x7f) ? ch : '?';
+  }
+  return q;
+}
+
 bool parse_header(std::istream& in, Header* h, std::string* err) {
   std::string line;
   if (!std::getline(in, line) || line.compare(0, 3, "ply") != 0) {
@@ -84,7 +99,7 @@ bool parse_header(std::istream& in, Header* h, std::string* err) {
     } else if (key == "element") {
       Element e;
       if (!(ls >> e.name >> e.count)) {
-        *err = "bad element line: " + line;
+        *err = "bad element line: " + quoted(line);
         return false;
       }
       h->elements.push_back(e);
@@ -107,7 +122,7 @@ bool parse_header(std::istream& in, Header* h, std::string* err) {
         ls >> p.name;
       }
       if (p.type == kBad || (p.is_list && p.count_type == kBad)) {
-        *err = "unknown property type in: " + line;
+        *err = "unknown property type in: " + quoted(line);
         return false;
       }
       h->elements.back().props.push_back(p);
@@ -215,7 +230,7 @@ int open_layout(const char* path, const char* const* names_in, std::ifstream* in
   }
   for (int f = 0; f < 4; ++f)
     if (L->col[f] < 0) {
-      g_ply_error = "vertex property missing: " + names[f];
+      g_ply_error = "vertex property missing: " + quoted(names[f]);
       return PHGPU_ERR_INVALID;
     }
   if (ve.count > 0xffffffffull) {

@@ -428,7 +428,7 @@ def ply_info(path, field_names=None):
     lib = load()
     rc = lib.phgpu_ply_info(os.fsencode(path), names, C.byref(n), C.byref(present))
     if rc != PHGPU_OK:
-        raise PhgpuError(f"phgpu_ply_info: {lib.phgpu_ply_last_error().decode()} ({rc})")
+        raise PhgpuError(f"phgpu_ply_info: {lib.phgpu_ply_last_error().decode(errors="replace")} ({rc})")
     return n.value, present.value
 
 
@@ -457,7 +457,7 @@ def ply_read(path, field_names=None, pinned=False):
                             _addr(opt["reflectivity"]), _addr(opt["ambient"]), _addr(opt["range"]), n,
                             C.byref(got))
     if rc != PHGPU_OK:
-        raise PhgpuError(f"phgpu_ply_read: {lib.phgpu_ply_last_error().decode()} ({rc})")
+        raise PhgpuError(f"phgpu_ply_read: {lib.phgpu_ply_last_error().decode(errors="replace")} ({rc})")
     return dict(xyzi=xyzi, **opt)
 
 
@@ -470,7 +470,7 @@ class VoxelGrid:
         h = C.c_void_p()
         rc = lib.phgpu_voxel_grid_create(int(max_points), int(device), C.byref(h))
         if rc != PHGPU_OK:
-            raise PhgpuError(f"phgpu_voxel_grid_create: {lib.phgpu_voxel_grid_last_error(None).decode()} ({rc})")
+            raise PhgpuError(f"phgpu_voxel_grid_create: {lib.phgpu_voxel_grid_last_error(None).decode(errors="replace")} ({rc})")
         self._h = h
         self.max_points = int(max_points)
         self.device = int(device)
@@ -499,7 +499,7 @@ class VoxelGrid:
         rc = lib.phgpu_voxel_grid_filter(self._h, C.byref(c), lf.ctypes.data, int(min_points_per_voxel), _addr(o),
                                          _addr(orf), _addr(oam), 1 if out_device else 0, C.byref(m))
         if rc != PHGPU_OK:
-            raise PhgpuError(f"phgpu_voxel_grid_filter: {lib.phgpu_voxel_grid_last_error(self._h).decode()} ({rc})")
+            raise PhgpuError(f"phgpu_voxel_grid_filter: {lib.phgpu_voxel_grid_last_error(self._h).decode(errors="replace")} ({rc})")
         k = m.value
         return o[:k], None if orf is None else orf[:k], None if oam is None else oam[:k]
 
@@ -545,7 +545,7 @@ class Context:
         h = C.c_void_p()
         rc = lib.phgpu_ctx_create(C.byref(self.params), C.byref(h))
         if rc != PHGPU_OK:
-            raise PhgpuError(f"phgpu_ctx_create failed ({rc}): {lib.phgpu_last_error(None).decode()}")
+            raise PhgpuError(f"phgpu_ctx_create failed ({rc}): {lib.phgpu_last_error(None).decode(errors="replace")}")
         self.h = h
         self.lib = lib
 
@@ -562,7 +562,7 @@ class Context:
 
     def check(self, rc):
         if rc != PHGPU_OK:
-            raise PhgpuError(f"phaser_gpu error {rc}: {self.lib.phgpu_last_error(self.h).decode()}")
+            raise PhgpuError(f"phaser_gpu error {rc}: {self.lib.phgpu_last_error(self.h).decode(errors="replace")}")
 
     @property
     def bw(self):
@@ -716,7 +716,7 @@ class Server:
         t = C.c_uint64()
         rc = self.lib.phgpu_server_submit(self.h, C.byref(params), C.byref(ct), C.byref(cs), C.byref(t))
         if rc != PHGPU_OK:
-            raise PhgpuError(f"submit failed ({rc}): {self.lib.phgpu_server_last_error(self.h).decode()}")
+            raise PhgpuError(f"submit failed ({rc}): {self.lib.phgpu_server_last_error(self.h).decode(errors="replace")}")
         if (ct.on_device and cs.on_device) or self._borrow:
             self._keep[t.value] = (k1, k2)  # read in place until the ticket completes
         if params.flags & PHGPU_FLAG_KEEP_VOLUMES:
@@ -739,7 +739,7 @@ class Server:
                                                 rv.ctypes.data if volumes else None,
                                                 tv.ctypes.data if volumes else None)
         if rc < 0:
-            raise PhgpuError(f"request {ticket} failed ({rc}): {self.lib.phgpu_server_last_error(self.h).decode()}")
+            raise PhgpuError(f"request {ticket} failed ({rc}): {self.lib.phgpu_server_last_error(self.h).decode(errors="replace")}")
         if rc == 0:
             return None
         self._keep.pop(ticket, None)

@@ -193,3 +193,50 @@ def test_errors(nat, tmp_path):
     write_ply(w, "binary_little_endian", [("vertex", OUSTER, ouster_rows(10, 2))])
     rc = nat.load().phgpu_ply_read(str(w).encode(), None, buf.ctypes.data, None, None, None, 4, C.byref(got))
     assert rc == -5
+
+
+def test_error_messages_are_printable(nat, tmp_path):
+    """A damaged header line is quoted in the error as printable ASCII, so the
+    message decodes and the call raises PhgpuError (not a decode error)."""
+    p = tmp_path / "bin.ply"
+    p.write_bytes(b"ply\nformat ascii 1.0\nelement vert\xfa\xff\x01x\nend_header\n")
+    with pytest.raises(nat.PhgpuError) as e:
+        nat.ply_info(p)
+    msg = str(e.value)
+    assert "bad element line" in msg and all(32 <= ord(ch) < 127 for ch in msg)
+
+
+def test_damaged_files_fail_cleanly(nat, tmp_path):
+    """Seeded byte flips, truncations and header edits of valid files: every
+    call either reads the file or raises PhgpuError."""
+    import random
+    src = []
+    for fmt in ("binary_little_endian", "ascii", "binary_big_endian"):
+        q = tmp_path / f"src_{fmt}.ply"
+        write_ply(q, fmt, [("vertex", OUSTER, ouster_rows(12, 7)), ("face", [("vi", ("list", "uchar", "int"))],
+                                                                     [([1, 2, 3],)])])
+        src.append(q.read_bytes())
+    rng = random.Random(1)
+    read = failed = 0
+    for k in range(150):
+        b = bytearray(rng.choice(src))
+        hdr_end = bytes(b).find(b"end_header")
+        mode = k % 3
+        if mode == 0:
+            for _ in range(rng.randrange(1, 12)):
+                b[rng.randrange(len(b))] = rng.randrange(256)
+        elif mode == 1:
+            b = b[:rng.randrange(len(b))]
+        else:
+            for _ in range(rng.randrange(1, 4)):
+                b[rng.randrange(max(1, hdr_end))] = rng.choice(b"0123456789 \n\x00abcxyz-\xfa")
+        f = tmp_path / f"d{k}.ply"
+        f.write_bytes(bytes(b))
+        try:
+            n, _ = nat.ply_info(f)
+            if n <= 1000:
+                nat.ply_read(f)
+            read += 1
+        except nat.PhgpuError:
+            failed += 1
+    assert read + failed == 150 and failed > 0
